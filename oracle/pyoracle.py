@@ -1,0 +1,248 @@
+"""ctypes front end of the C oracle (oracle/sbe_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as the
+checker, and by bench.py's CPU-baseline leg.  The product package never
+imports it.
+
+A *case* is the dict form of an ``inputParam.cfg`` (see
+``antelope_b200.cfgtext``): top-level ``target``/``gauge``, a ``laser`` group,
+a ``calc`` group and one material group.  ``to_problem`` turns it into the
+oracle's ``orc_problem`` struct with the reference's defaults
+(SBEs.h:432-509, antelope.cpp:111-129).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_sbe.so")
+REF_EXE = os.path.join(HERE, "_ref", "exec_hhg_ref")
+
+ENV = {"gauss": 0, "gauss_clipped": 1, "cos4": 2, "cos4_clipped": 3, "sin2": 4}
+GAUGE = {"Wannier": 0, "LengthWannier": 0, "Hamiltonian": 1, "LengthHamiltonian": 1,
+         "Velocity": 2, "VelocityHamiltonian": 2}
+MAX_PULSES = 8
+
+
+class OrcPulse(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "E0", "w0", "ellip", "ncycles", "cep_deg", "t0", "phix_deg", "ncycles_clipped",
+        "thetaz_deg", "phiz_deg")] + [("env", C.c_int)]
+
+
+class OrcProblem(C.Structure):
+    _fields_ = [
+        ("npulses", C.c_int), ("pulses", OrcPulse * MAX_PULSES),
+        ("offset_before", C.c_double), ("offset_after", C.c_double),
+        ("dt", C.c_double), ("T1", C.c_double), ("T2", C.c_double),
+        ("rk", C.c_int), ("rk_tol", C.c_double), ("inter_intra", C.c_int), ("gauge", C.c_int),
+        ("Nk", C.c_int * 3), ("ksfactor", C.c_double * 3),
+        ("n_bzaxes", C.c_int), ("bzaxes", C.c_double * 9),
+        ("n_bzorigin", C.c_int), ("bzorigin", C.c_double * 3),
+        ("model", C.c_int),
+        ("hal_a0_ang", C.c_double), ("hal_t1", C.c_double), ("hal_t2", C.c_double),
+        ("hal_M0", C.c_double), ("hal_phi0", C.c_double),
+        ("use_fermi", C.c_int), ("Ef", C.c_double),
+        ("w_nband", C.c_int), ("w_nval", C.c_int), ("w_nR", C.c_int),
+        ("w_R", C.POINTER(C.c_int)), ("w_lat", C.c_double * 4),
+        ("w_h", C.POINTER(C.c_double)), ("w_d", C.POINTER(C.c_double)),
+        ("nthreads", C.c_int),
+    ]
+
+
+class OrcDims(C.Structure):
+    _fields_ = [("Nt", C.c_int), ("nband", C.c_int), ("nval", C.c_int), ("ntotal", C.c_int),
+                ("atmin", C.c_double), ("dV", C.c_double), ("total_weight", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.check_call(["make", "-s", "-C", HERE, "port"])
+        _lib = C.CDLL(LIB_PATH)
+        _lib.orc_get_dims.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcDims)]
+        _lib.orc_run.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.POINTER(C.c_long)]
+        _lib.orc_laser_eval.argtypes = [C.POINTER(OrcProblem), C.c_double, C.c_void_p, C.c_void_p]
+        _lib.orc_kgrid.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p]
+        _lib.orc_model_hj.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_eigh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def to_problem(case: dict, nthreads: int = 1):
+    """Build an ``orc_problem`` (and the arrays it points to) from a case dict."""
+    p = OrcProblem()
+    keep = []
+    laser = case["laser"]
+    pulses = laser["pulses"]
+    if not 1 <= len(pulses) <= MAX_PULSES:
+        raise ValueError("1..8 pulses supported")
+    p.npulses = len(pulses)
+    for i, q in enumerate(pulses):
+        o = p.pulses[i]
+        o.E0, o.w0, o.ellip, o.ncycles = q["E0"], q["w0"], q["ellip"], q["ncycles"]
+        o.cep_deg, o.t0, o.phix_deg = q["cep"], q["t0"], q["phix"]
+        o.ncycles_clipped = q.get("ncycles_clipped", 0.0)
+        o.thetaz_deg, o.phiz_deg = q.get("thetaz", 0.0), q.get("phiz", 0.0)
+        o.env = ENV[q["env_name"]]
+    off = laser.get("offset", [0.0, 0.0])
+    p.offset_before, p.offset_after = off[0], off[1]
+    calc = case["calc"]
+    p.dt = calc.get("dt", 0.1)
+    p.T1 = calc.get("T1", -1.0)
+    p.T2 = calc.get("T2", -1.0)
+    rk = calc.get("rk", None)
+    p.rk = 45 if rk == "cashkarp45" else int(calc.get("RKorder", 5))
+    p.rk_tol = calc.get("tol", 1e-8)
+    p.inter_intra = 1 if calc.get("InterIntra", False) else 0
+    p.gauge = GAUGE.get(case.get("gauge", ""), 0)
+    npts = list(calc["Npoints"]) + [1] * (3 - len(calc["Npoints"]))
+    for i in range(3):
+        p.Nk[i] = npts[i]
+    ks = list(calc["ksfactor"]) + [1.0] * (3 - len(calc["ksfactor"]))
+    for i in range(3):
+        p.ksfactor[i] = ks[i]
+    if "BZaxes" in calc:
+        p.n_bzaxes = len(calc["BZaxes"])
+        for i, v in enumerate(calc["BZaxes"]):
+            p.bzaxes[i] = v
+    if "BZorigin" in calc:
+        p.n_bzorigin = len(calc["BZorigin"])
+        for i, v in enumerate(calc["BZorigin"]):
+            p.bzorigin[i] = v
+    target = case["target"]
+    mat = case.get(target, {})
+    if "Ef" in mat:
+        p.use_fermi, p.Ef = 1, mat["Ef"]
+    if target == "Haldane":
+        p.model = 0
+        p.hal_a0_ang, p.hal_t1, p.hal_t2, p.hal_phi0 = mat["a0"], mat["t1"], mat["t2"], mat["phi0"]
+        p.hal_M0 = mat["M0"] if "M0" in mat else mat["Mt2"] * mat["t2"]
+    elif target == "SyntheticWannier":
+        from antelope_b200 import wannier  # pure-numpy model generator, shared definition
+
+        model = wannier.synthetic_model(mat)
+        p.model = 1
+        p.w_nband, p.w_nval, p.w_nR = model["nband"], model["nval"], len(model["R"])
+        R = np.ascontiguousarray(model["R"], dtype=np.int32)
+        h = np.ascontiguousarray(model["h"], dtype=np.complex128)
+        keep += [R, h]
+        p.w_R = R.ctypes.data_as(C.POINTER(C.c_int))
+        p.w_h = h.ctypes.data_as(C.POINTER(C.c_double))
+        if model.get("d") is not None:
+            d = np.ascontiguousarray(model["d"], dtype=np.complex128)
+            keep.append(d)
+            p.w_d = d.ctypes.data_as(C.POINTER(C.c_double))
+        for i, v in enumerate(model["lattice"]):
+            p.w_lat[i] = v
+    else:
+        raise ValueError(f"oracle has no model '{target}'")
+    p.nthreads = nthreads
+    p._keep = keep
+    return p
+
+
+def dims(case: dict) -> dict:
+    p = to_problem(case)
+    d = OrcDims()
+    if lib().orc_get_dims(C.byref(p), C.byref(d)) != 0:
+        raise ValueError("oracle rejected the case")
+    return {f: getattr(d, f) for f, _ in OrcDims._fields_}
+
+
+def run(case: dict, nthreads: int = 1) -> dict:
+    """Propagate a case on the CPU.  Returns the arrays the reference writes:
+    ``inter``/``intra`` [Nt,3] (already times dV), ``occ`` [Nt,N] and the raw
+    weighted density-matrix integral ``dmi`` [Nt,N,N] (complex)."""
+    p = to_problem(case, nthreads)
+    d = dims(case)
+    Nt, N = d["Nt"], d["nband"]
+    inter = np.zeros((Nt, 3))
+    intra = np.zeros((Nt, 3))
+    dmi = np.zeros((Nt, N, N), dtype=np.complex128)
+    steps = C.c_long(0)
+    rc = lib().orc_run(C.byref(p), _ptr(inter), _ptr(intra), _ptr(dmi), C.byref(steps))
+    if rc != 0:
+        raise RuntimeError(f"oracle run failed ({rc})")
+    occ = np.real(np.einsum("tii->ti", dmi)) / d["ntotal"]
+    return {"inter": inter, "intra": intra, "dmi": dmi, "occ": occ, "dims": d,
+            "steps": steps.value}
+
+
+def laser_eval(case: dict, t: float):
+    p = to_problem(case)
+    A = np.zeros(3)
+    E = np.zeros(3)
+    lib().orc_laser_eval(C.byref(p), float(t), _ptr(A), _ptr(E))
+    return A, E
+
+
+def kgrid(case: dict):
+    p = to_problem(case)
+    n = dims(case)["ntotal"]
+    k = np.zeros((n, 3))
+    w = np.zeros(n)
+    lib().orc_kgrid(C.byref(p), _ptr(k), _ptr(w))
+    return k, w
+
+
+def model_hj(case: dict, k3):
+    p = to_problem(case)
+    N = dims(case)["nband"]
+    H = np.zeros((N, N), dtype=np.complex128)
+    J = np.zeros((3, N, N), dtype=np.complex128)
+    k = np.ascontiguousarray(k3, dtype=np.float64)
+    lib().orc_model_hj(C.byref(p), _ptr(k), _ptr(H), _ptr(J))
+    return H, J
+
+
+def eigh(a):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    n = a.shape[0]
+    w = np.zeros(n)
+    v = np.zeros((n, n), dtype=np.complex128)
+    if lib().orc_eigh(n, _ptr(a), _ptr(w), _ptr(v)) != 0:
+        raise ValueError("bad size")
+    return w, v
+
+
+def run_reference(case: dict, workdir: str, env: dict | None = None, timeout: float = 3600):
+    """Run the unmodified reference build (oracle/_ref) on a case in
+    ``workdir``; returns the parsed output files."""
+    from antelope_b200 import cfgtext
+
+    if not os.path.exists(REF_EXE):
+        raise FileNotFoundError("oracle/_ref/exec_hhg_ref not built (needs the reference sources)")
+    os.makedirs(workdir, exist_ok=True)
+    with open(os.path.join(workdir, "inputParam.cfg"), "w") as f:
+        f.write(cfgtext.dumps(case))
+    e = dict(os.environ)
+    if env:
+        e.update(env)
+    subprocess.run([REF_EXE], cwd=workdir, env=e, check=True, timeout=timeout,
+                   stdout=subprocess.DEVNULL)
+    return read_outputs(workdir)
+
+
+def read_outputs(workdir: str) -> dict:
+    def load(name):
+        return np.loadtxt(os.path.join(workdir, name), ndmin=2)
+
+    return {"inter": load("interband_dipole_full_evol.dat"),
+            "intra": load("intraband_current_full_evol.dat"),
+            "occ_file": load("occupation__full__evol.dat"),
+            "coh_file": load("coherence__full__evol.dat"),
+            "laser": load("outlaserdata.dat")}

@@ -1,0 +1,80 @@
+"""The CPU oracle (oracle/sbe_oracle.c) against outputs of the reference
+itself (golden fixtures made by tests/golden/make_golden.py from the
+unmodified reference sources).  This pins the oracle before the GPU kernels are
+compared with it."""
+import os
+
+import numpy as np
+import pytest
+
+from cases import GOLDEN_CASES
+from oracle import pyoracle
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _rel(a, b):
+    m = np.abs(b).max()
+    return np.abs(a - b).max() / (m if m > 0 else 1.0)
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_oracle_matches_reference_outputs(name):
+    case = GOLDEN_CASES[name]
+    ref = np.load(os.path.join(GOLDEN, f"golden_{name}.npz"))
+    out = pyoracle.run(case)
+    N = out["dims"]["nband"]
+    # the files hold 17 significant digits; the oracle repeats the
+    # reference's arithmetic, so the match is to the last printed digit
+    assert _rel(out["inter"], ref["inter"]) < 1e-15
+    assert _rel(out["intra"], ref["intra"]) < 1e-15
+    occ = ref["occ_file"]
+    assert np.abs(out["occ"] - occ[:, :N]).max() < 1e-15
+    assert np.abs(out["occ"].sum(1) - occ[:, N]).max() < 1e-14
+    # laser file: time axis and the A/E columns
+    t = out["dims"]["atmin"] + case["calc"].get("dt", 0.1) * np.arange(out["dims"]["Nt"])
+    assert np.allclose(ref["laser"][:, 0], t, rtol=1e-6, atol=1e-6)
+
+
+def test_oracle_threads_match_sequential():
+    """The ParaRange k-split (utility.h:104-115) changes only summation order."""
+    case = GOLDEN_CASES["vg_rk4"]
+    a = pyoracle.run(case, nthreads=1)
+    b = pyoracle.run(case, nthreads=3)
+    assert _rel(b["inter"], a["inter"]) < 1e-13
+    assert _rel(b["intra"], a["intra"]) < 1e-13
+
+
+def test_oracle_eigh_against_numpy():
+    rng = np.random.default_rng(7)
+    for n in (2, 3, 6, 8):
+        a = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+        a = a + a.conj().T
+        w, v = pyoracle.eigh(a)
+        assert np.allclose(w, np.linalg.eigvalsh(a), atol=1e-12)
+        assert np.allclose(a @ v, v * w, atol=1e-11)
+        assert np.allclose(v.conj().T @ v, np.eye(n), atol=1e-12)
+
+
+def test_oracle_haldane_j_is_minus_dh_dk():
+    case = GOLDEN_CASES["vg_rk4"]
+    k = np.array([0.31, -0.17, 0.0])
+    _, J = pyoracle.model_hj(case, k)
+    h = 1e-6
+    for a in range(2):
+        dk = np.zeros(3)
+        dk[a] = h
+        Hp, _ = pyoracle.model_hj(case, k + dk)
+        Hm, _ = pyoracle.model_hj(case, k - dk)
+        assert np.allclose(J[a], -(Hp - Hm) / (2 * h), atol=1e-8)
+    assert np.all(J[2] == 0)
+
+
+@pytest.mark.skipif(not os.path.exists(pyoracle.REF_EXE), reason="reference build absent")
+def test_oracle_matches_live_reference_build(tmp_path):
+    """Re-run one case through the reference build when it is present."""
+    case = GOLDEN_CASES["lw_t1_elliptic"]
+    ref = pyoracle.run_reference(case, str(tmp_path))
+    out = pyoracle.run(case)
+    assert _rel(out["inter"], ref["inter"]) < 1e-15
+    assert _rel(out["intra"], ref["intra"]) < 1e-15
