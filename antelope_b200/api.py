@@ -1,0 +1,229 @@
+"""Python front end of the native library (include/sbe.h).
+
+``Problem`` wraps an inputParam.cfg; ``solve`` runs one problem through the
+GPU solver; ``Batch`` runs many at once; ``Server`` is the continuous-
+batching request loop.  Output arrays have the reference's file layout.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import cfgtext
+from .capi import COutputs, Dims, Opts, P, ServerOpts, STATUS, lib
+
+
+class SbeError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+
+
+def _check(st: int):
+    if st != 0:
+        raise SbeError(st, lib.sbe_last_error_message().decode(errors="replace"))
+
+
+def _opts(precision=None, tile_k=0, k_per_thread=0, steps_per_launch=0, use_graph=False, device=0):
+    o = Opts()
+    lib.sbe_opts_default(C.byref(o))
+    o.device = device
+    o.precision = -1 if precision is None else {"fp64": 0, "mixed": 1, 0: 0, 1: 1}[precision]
+    o.tile_k, o.k_per_thread, o.steps_per_launch = tile_k, k_per_thread, steps_per_launch
+    o.use_graph = 1 if use_graph else 0
+    return o
+
+
+@dataclass
+class Outputs:
+    inter: np.ndarray   # [Nt, 3]
+    intra: np.ndarray   # [Nt, 3]
+    occ: np.ndarray     # [Nt, N+1]
+    coh: np.ndarray     # [Nt, 2]
+    laser: np.ndarray   # [Nt, 7]
+
+    @classmethod
+    def empty(cls, dims: Dims):
+        Nt, N = dims.Nt, dims.nband
+        return cls(np.zeros((Nt, 3)), np.zeros((Nt, 3)), np.zeros((Nt, N + 1)), np.zeros((Nt, 2)),
+                   np.zeros((Nt, 7)))
+
+    def c(self) -> COutputs:
+        return COutputs(*(a.ctypes.data for a in (self.inter, self.intra, self.occ, self.coh, self.laser)))
+
+
+class Problem:
+    """An inputParam.cfg, parsed by the native library."""
+
+    def __init__(self, handle):
+        self._h = handle
+        d = Dims()
+        _check(lib.sbe_problem_dims(self._h, C.byref(d)))
+        self.dims = d
+
+    @classmethod
+    def from_cfg(cls, path: str) -> "Problem":
+        h = P()
+        _check(lib.sbe_problem_from_cfg(os.fsencode(path), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_text(cls, text: str) -> "Problem":
+        h = P()
+        _check(lib.sbe_problem_from_string(text.encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_dict(cls, case: dict) -> "Problem":
+        return cls.from_text(cfgtext.dumps(case))
+
+    @property
+    def Nt(self):
+        return self.dims.Nt
+
+    @property
+    def ntotal(self):
+        return self.dims.ntotal
+
+    def laser(self) -> np.ndarray:
+        out = np.zeros((self.dims.Nt, 7))
+        _check(lib.sbe_problem_laser(self._h, out.ctypes.data))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.sbe_problem_destroy(self._h)
+            self._h = None
+
+
+class Solver:
+    """One solve on the GPU (``sbe_solver_*``)."""
+
+    def __init__(self, problem: Problem, **opts):
+        self.problem = problem
+        self._h = P()
+        _check(lib.sbe_solver_create(problem._h, C.byref(_opts(**opts)), C.byref(self._h)))
+
+    def run(self, stream: int = 0):
+        _check(lib.sbe_solver_run(self._h, C.c_void_p(stream)))
+
+    def get(self, out: Outputs | None = None) -> Outputs:
+        out = out or Outputs.empty(self.problem.dims)
+        _check(lib.sbe_solver_get(self._h, C.byref(out.c())))
+        return out
+
+    @property
+    def launches(self) -> int:
+        return lib.sbe_solver_launches(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.sbe_solver_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+
+def solve(problem, **opts) -> Outputs:
+    """Run one problem (a Problem, a cfg path or a case dict) to completion."""
+    if isinstance(problem, dict):
+        problem = Problem.from_dict(problem)
+    elif isinstance(problem, (str, os.PathLike)):
+        problem = Problem.from_cfg(problem)
+    s = Solver(problem, **opts)
+    try:
+        s.run()
+        return s.get()
+    finally:
+        s.close()
+
+
+def run_cfg(cfg_path: str, out_dir: str = ".", **opts):
+    """The drop-in: read an inputParam.cfg, solve, write the reference's files."""
+    _check(lib.sbe_run_cfg(os.fsencode(cfg_path), os.fsencode(out_dir), C.byref(_opts(**opts))))
+
+
+def write_outputs(problem: Problem, out: Outputs, out_dir: str):
+    _check(lib.sbe_write_outputs(problem._h, C.byref(out.c()), os.fsencode(out_dir)))
+
+
+class Batch:
+    """Many solves advanced together (``sbe_batch_*``)."""
+
+    def __init__(self, problems: list[Problem], **opts):
+        self.problems = list(problems)
+        arr = (P * len(self.problems))(*[p._h for p in self.problems])
+        self._h = P()
+        _check(lib.sbe_batch_create(arr, len(self.problems), C.byref(_opts(**opts)), C.byref(self._h)))
+
+    def run(self, stream: int = 0):
+        _check(lib.sbe_batch_run(self._h, C.c_void_p(stream)))
+
+    def get(self, i: int) -> Outputs:
+        out = Outputs.empty(self.problems[i].dims)
+        _check(lib.sbe_batch_get(self._h, i, C.byref(out.c())))
+        return out
+
+    @property
+    def launches(self) -> int:
+        return lib.sbe_batch_launches(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.sbe_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+
+class Server:
+    """Continuous-batching request loop (``sbe_server_*``)."""
+
+    def __init__(self, precision=None, steps_per_launch=0, max_resident=0, mem_budget_bytes=0.0,
+                 tile_k=0, k_per_thread=0, device=0):
+        o = ServerOpts()
+        o.device = device
+        o.precision = -1 if precision is None else {"fp64": 0, "mixed": 1}[precision]
+        o.steps_per_launch, o.max_resident, o.mem_budget_bytes = steps_per_launch, max_resident, mem_budget_bytes
+        o.tile_k, o.k_per_thread = tile_k, k_per_thread
+        self._h = P()
+        self._problems = {}
+        _check(lib.sbe_server_create(C.byref(o), C.byref(self._h)))
+
+    def submit(self, problem: Problem) -> int:
+        rid = C.c_longlong(0)
+        _check(lib.sbe_server_submit(self._h, problem._h, C.byref(rid)))
+        self._problems[rid.value] = problem
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0):
+        prob = self._problems[rid]
+        out = Outputs.empty(prob.dims)
+        lat = C.c_double(0.0)
+        _check(lib.sbe_server_wait(self._h, rid, float(timeout), C.byref(out.c()), C.byref(lat)))
+        return out, lat.value
+
+    def cancel(self, rid: int):
+        _check(lib.sbe_server_cancel(self._h, rid))
+
+    def stats(self) -> dict:
+        c = (C.c_longlong * 5)()
+        _check(lib.sbe_server_stats(self._h, c))
+        return dict(zip(("submitted", "completed", "failed", "resident", "launches"), list(c)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.sbe_server_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+
+def measure_fma_peaks(device: int = 0):
+    a, b = C.c_double(0), C.c_double(0)
+    _check(lib.sbe_measure_fma_peaks(device, C.byref(a), C.byref(b)))
+    return a.value, b.value

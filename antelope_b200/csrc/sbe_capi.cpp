@@ -1,0 +1,704 @@
+// extern "C" layer (include/sbe.h): problems, single solves, batches, the
+// continuous-batching server, and the drop-in run of an inputParam.cfg.
+#include "../../include/sbe.h"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <thread>
+#include <unordered_map>
+
+#include "sbe_engine.h"
+#include "sbe_kernels.h"
+
+using namespace sbe;
+
+struct sbe_problem {
+    Problem p;
+    std::string unsupported;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+sbe_status fail(sbe_status st, const std::string &msg)
+{
+    g_err = msg;
+    return st;
+}
+
+template <class F>
+sbe_status guard(F &&f)
+{
+    try {
+        g_err.clear();
+        return f();
+    } catch (const OomError &e) {
+        return fail(SBE_OOM, e.what());
+    } catch (const CudaError &e) {
+        return fail(SBE_CUDA_ERROR, e.what());
+    } catch (const CfgError &e) {
+        return fail(SBE_BAD_CONFIG, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(SBE_OOM, "host out of memory");
+    } catch (const std::exception &e) {
+        return fail(SBE_INVALID_ARGUMENT, e.what());
+    }
+}
+
+EngineOptions to_engine_opts(const sbe_opts *o)
+{
+    EngineOptions e;
+    if (o) {
+        e.precision = o->precision;
+        e.tile_k = o->tile_k;
+        e.kpt = o->k_per_thread;
+        e.steps_per_launch = o->steps_per_launch;
+    }
+    return e;
+}
+
+int default_steps(const sbe_opts *o) { return (o && o->steps_per_launch > 0) ? o->steps_per_launch : 1024; }
+
+sbe_status check_problem(const sbe_problem *p)
+{
+    if (!p) return fail(SBE_INVALID_ARGUMENT, "null problem");
+    if (!p->unsupported.empty()) return fail(SBE_UNSUPPORTED, p->unsupported);
+    return SBE_OK;
+}
+
+void copy_out(const SolveOutputs &o, const sbe_outputs *out)
+{
+    if (!out) return;
+    if (out->inter) std::memcpy(out->inter, o.inter.data(), o.inter.size() * 8);
+    if (out->intra) std::memcpy(out->intra, o.intra.data(), o.intra.size() * 8);
+    if (out->occ) std::memcpy(out->occ, o.occ.data(), o.occ.size() * 8);
+    if (out->coh) std::memcpy(out->coh, o.coh.data(), o.coh.size() * 8);
+    if (out->laser) std::memcpy(out->laser, o.laser.data(), o.laser.size() * 8);
+}
+
+// Runs every tick of an engine on `stream`, optionally as one CUDA graph.
+void run_engine(Engine &eng, bool use_graph, int *launches)
+{
+    const int ticks = eng.max_remaining_ticks();
+    int n = 0;
+    if (use_graph && ticks > 0) {
+        eng.step();  // first tick outside the capture: builds the launch lists
+        n += eng.last_launches();
+        if (ticks > 1) {
+            cudaGraph_t g;
+            cudaGraphExec_t ge;
+            cuda_check(cudaStreamBeginCapture(eng.stream(), cudaStreamCaptureModeThreadLocal), "begin capture");
+            for (int t = 1; t < ticks; ++t) {
+                eng.step_frozen();
+                n += eng.last_launches();
+            }
+            cuda_check(cudaStreamEndCapture(eng.stream(), &g), "end capture");
+            cuda_check(cudaGraphInstantiate(&ge, g, 0), "graph instantiate");
+            cuda_check(cudaGraphLaunch(ge, eng.stream()), "graph launch");
+            cudaGraphExecDestroy(ge);
+            cudaGraphDestroy(g);
+        }
+    } else {
+        for (int t = 0; t < ticks; ++t) {
+            eng.step();
+            n += eng.last_launches();
+        }
+    }
+    if (launches) *launches = n;
+}
+
+}  // namespace
+
+// ================================================================= misc
+extern "C" int sbe_abi_version(void) { return SBE_ABI_VERSION; }
+extern "C" const char *sbe_last_error_message(void) { return g_err.c_str(); }
+extern "C" void sbe_opts_default(sbe_opts *o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = -1;
+}
+
+// ================================================================= problem
+static sbe_status problem_from_text(const std::string &text, sbe_problem **out)
+{
+    return guard([&]() -> sbe_status {
+        if (!out) return fail(SBE_INVALID_ARGUMENT, "null output pointer");
+        *out = nullptr;
+        std::unique_ptr<CfgValue> root;
+        try {
+            root = parse_cfg(text);
+        } catch (const CfgError &e) {
+            return fail(SBE_BAD_CONFIG, std::string("Parse error at ") + e.what());
+        }
+        auto p = std::make_unique<sbe_problem>();
+        p->p = problem_from_cfg(*root, &p->unsupported);
+        *out = p.release();
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_problem_from_cfg(const char *path, sbe_problem **out)
+{
+    if (!path) return fail(SBE_INVALID_ARGUMENT, "null path");
+    std::ifstream f(path);
+    if (!f) return fail(SBE_BAD_CONFIG, "I/O error while reading file.");  // antelope.cpp:95-99
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return problem_from_text(ss.str(), out);
+}
+
+extern "C" sbe_status sbe_problem_from_string(const char *text, sbe_problem **out)
+{
+    if (!text) return fail(SBE_INVALID_ARGUMENT, "null text");
+    return problem_from_text(text, out);
+}
+
+extern "C" sbe_status sbe_problem_dims(const sbe_problem *p, sbe_dims *d)
+{
+    if (!p || !d) return fail(SBE_INVALID_ARGUMENT, "null argument");
+    const Problem &q = p->p;
+    std::memset(d, 0, sizeof(*d));
+    d->Nt = q.laser.Nt;
+    d->nband = q.nband;
+    d->nval = q.nval;
+    d->ntotal = q.ntotal();
+    for (int i = 0; i < 3; ++i) d->Nk[i] = q.Nk[i];
+    d->gauge = q.gauge;
+    d->rk = q.rk;
+    d->precision = q.precision;
+    d->model = q.model;
+    d->inter_intra = q.inter_intra ? 1 : 0;
+    d->atmin = q.laser.atmin;
+    d->dt = q.dt;
+    d->dV = q.dV;
+    d->total_weight = q.total_weight;
+    return SBE_OK;
+}
+
+extern "C" sbe_status sbe_problem_laser(const sbe_problem *p, double *laser)
+{
+    if (!p || !laser) return fail(SBE_INVALID_ARGUMENT, "null argument");
+    const Laser &L = p->p.laser;
+    for (int n = 0; n < L.Nt; ++n) {
+        const double t = L.atmin + L.dt * n;  // antelope.cpp:215
+        double *row = laser + (size_t)n * 7;
+        row[0] = t;
+        L.eval(t, row + 4, row + 1);
+    }
+    return SBE_OK;
+}
+
+extern "C" void sbe_problem_destroy(sbe_problem *p) { delete p; }
+
+// ================================================================= solver
+struct sbe_solver {
+    std::unique_ptr<Engine> eng;
+    cudaStream_t own = nullptr;
+    cudaEvent_t ready = nullptr;
+    int id = -1;
+    bool use_graph = false;
+    bool ran = false;
+    int launches = 0;
+    int device = 0;
+};
+
+extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *opts, sbe_solver **out)
+{
+    if (sbe_status st = check_problem(p)) return st;
+    if (!out) return fail(SBE_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    return guard([&]() -> sbe_status {
+        auto s = std::make_unique<sbe_solver>();
+        s->device = opts ? opts->device : 0;
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cuda_check(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking), "stream create");
+        cuda_check(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming), "event create");
+        s->eng = std::make_unique<Engine>(s->device, s->own, default_steps(opts));
+        s->id = s->eng->add(p->p, to_engine_opts(opts));
+        cuda_check(cudaEventRecord(s->ready, s->own), "event record");
+        s->use_graph = opts && opts->use_graph;
+        *out = s.release();
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_solver_run(sbe_solver *s, void *stream)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null solver");
+    if (s->ran) return fail(SBE_INVALID_ARGUMENT, "a solver runs once; create a new one");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        cuda_check(cudaStreamWaitEvent(st, s->ready, 0), "stream wait");
+        s->eng->set_stream(st);
+        run_engine(*s->eng, s->use_graph, &s->launches);
+        s->eng->fetch_async(s->id);
+        s->ran = true;
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null solver");
+    if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        SolveOutputs o = s->eng->outputs(s->id);
+        copy_out(o, out);
+        return SBE_OK;
+    });
+}
+
+extern "C" int sbe_solver_launches(const sbe_solver *s) { return s ? s->launches : 0; }
+
+extern "C" void sbe_solver_destroy(sbe_solver *s)
+{
+    if (!s) return;
+    cudaSetDevice(s->device);
+    s->eng.reset();
+    if (s->ready) cudaEventDestroy(s->ready);
+    if (s->own) {
+        cudaStreamSynchronize(s->own);
+        cudaStreamDestroy(s->own);
+    }
+    delete s;
+}
+
+// ================================================================= files
+extern "C" sbe_status sbe_write_outputs(const sbe_problem *p, const sbe_outputs *o, const char *dir)
+{
+    if (!p || !o || !o->inter || !o->intra || !o->occ || !o->coh || !o->laser)
+        return fail(SBE_INVALID_ARGUMENT, "all five output arrays are needed to write the files");
+    return guard([&]() -> sbe_status {
+        const Problem &q = p->p;
+        SolveOutputs so;
+        so.Nt = q.laser.Nt;
+        so.nband = q.nband;
+        const size_t Nt = (size_t)so.Nt, N = (size_t)so.nband;
+        so.inter.assign(o->inter, o->inter + Nt * 3);
+        so.intra.assign(o->intra, o->intra + Nt * 3);
+        so.occ.assign(o->occ, o->occ + Nt * (N + 1));
+        so.coh.assign(o->coh, o->coh + Nt * 2);
+        so.laser.assign(o->laser, o->laser + Nt * 7);
+        write_outputs(q, so, dir ? dir : "");
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_run_cfg(const char *cfg_path, const char *out_dir, const sbe_opts *opts)
+{
+    sbe_problem *p = nullptr;
+    if (sbe_status st = sbe_problem_from_cfg(cfg_path, &p)) return st;
+    std::unique_ptr<sbe_problem> hold(p);
+    sbe_solver *s = nullptr;
+    if (sbe_status st = sbe_solver_create(p, opts, &s)) return st;
+    std::unique_ptr<sbe_solver, void (*)(sbe_solver *)> sh(s, sbe_solver_destroy);
+    if (sbe_status st = sbe_solver_run(s, s->own)) return st;
+    const Problem &q = p->p;
+    const size_t Nt = q.laser.Nt, N = q.nband;
+    std::vector<double> inter(Nt * 3), intra(Nt * 3), occ(Nt * (N + 1)), coh(Nt * 2), laser(Nt * 7);
+    sbe_outputs o{inter.data(), intra.data(), occ.data(), coh.data(), laser.data()};
+    if (sbe_status st = sbe_solver_get(s, &o)) return st;
+    return sbe_write_outputs(p, &o, out_dir);
+}
+
+// ================================================================= batch
+struct sbe_batch {
+    std::unique_ptr<Engine> eng;
+    cudaStream_t own = nullptr;
+    cudaEvent_t ready = nullptr;
+    std::vector<int> ids;
+    bool use_graph = false, ran = false;
+    int launches = 0, device = 0;
+};
+
+extern "C" sbe_status sbe_batch_create(const sbe_problem *const *problems, int n, const sbe_opts *opts,
+                                       sbe_batch **out)
+{
+    if (!problems || n <= 0 || !out) return fail(SBE_INVALID_ARGUMENT, "need at least one problem");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i)
+        if (sbe_status st = check_problem(problems[i])) return st;
+    return guard([&]() -> sbe_status {
+        auto b = std::make_unique<sbe_batch>();
+        b->device = opts ? opts->device : 0;
+        cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+        cuda_check(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking), "stream create");
+        cuda_check(cudaEventCreateWithFlags(&b->ready, cudaEventDisableTiming), "event create");
+        b->eng = std::make_unique<Engine>(b->device, b->own, default_steps(opts));
+        // longest solves first: their tiles lead every launch's tile list
+        std::vector<int> order(n);
+        for (int i = 0; i < n; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+            return (double)problems[a]->p.laser.Nt * problems[a]->p.ntotal() >
+                   (double)problems[c]->p.laser.Nt * problems[c]->p.ntotal();
+        });
+        b->ids.assign(n, -1);
+        EngineOptions eo = to_engine_opts(opts);
+        for (int i : order) b->ids[i] = b->eng->add(problems[i]->p, eo);
+        cuda_check(cudaEventRecord(b->ready, b->own), "event record");
+        b->use_graph = opts && opts->use_graph;
+        *out = b.release();
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_batch_run(sbe_batch *b, void *stream)
+{
+    if (!b) return fail(SBE_INVALID_ARGUMENT, "null batch");
+    if (b->ran) return fail(SBE_INVALID_ARGUMENT, "a batch runs once; create a new one");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        cuda_check(cudaStreamWaitEvent(st, b->ready, 0), "stream wait");
+        b->eng->set_stream(st);
+        run_engine(*b->eng, b->use_graph, &b->launches);
+        for (int id : b->ids) b->eng->fetch_async(id);
+        b->ran = true;
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *out)
+{
+    if (!b || index < 0 || index >= (int)b->ids.size()) return fail(SBE_INVALID_ARGUMENT, "bad batch index");
+    if (!b->ran) return fail(SBE_NOT_READY, "sbe_batch_run has not been called");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+        copy_out(b->eng->outputs(b->ids[index]), out);
+        return SBE_OK;
+    });
+}
+
+extern "C" int sbe_batch_launches(const sbe_batch *b) { return b ? b->launches : 0; }
+
+extern "C" void sbe_batch_destroy(sbe_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    b->eng.reset();
+    if (b->ready) cudaEventDestroy(b->ready);
+    if (b->own) {
+        cudaStreamSynchronize(b->own);
+        cudaStreamDestroy(b->own);
+    }
+    delete b;
+}
+
+// ================================================================= server
+namespace {
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    long long id = 0;
+    Problem prob;
+    Clock::time_point t_submit, t_done;
+    enum State { QUEUED, RESIDENT, DONE, FAILED, CANCELLED } state = QUEUED;
+    int solve = -1;
+    bool fetching = false;
+    SolveOutputs out;
+    std::string err;
+};
+}  // namespace
+
+struct sbe_server {
+    sbe_server_opts opts{};
+    std::unique_ptr<Engine> eng;
+    cudaStream_t stream = nullptr;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    long long next_id = 1;
+    std::deque<long long> queue;
+    std::unordered_map<long long, std::unique_ptr<Request>> reqs;
+    long long n_submitted = 0, n_completed = 0, n_failed = 0, n_launches = 0;
+    double budget = 0;
+    std::string fatal;
+    std::deque<cudaEvent_t> inflight;  // one event per issued tick (bounded run-ahead)
+
+    void loop();
+};
+
+void sbe_server::loop()
+{
+    cudaSetDevice(opts.device);
+    EngineOptions eo;
+    eo.precision = opts.precision;
+    eo.tile_k = opts.tile_k;
+    eo.kpt = opts.k_per_thread;
+    std::vector<cudaEvent_t> pool;
+    for (;;) {
+        std::unique_lock<std::mutex> lk(mu);
+        // admission: FIFO while memory and slots allow
+        while (!queue.empty()) {
+            Request &r = *reqs[queue.front()];
+            if (r.state != Request::QUEUED) { queue.pop_front(); continue; }
+            size_t need = 0;
+            try {
+                need = eng->bytes_needed(r.prob, eo);
+            } catch (const std::exception &e) {
+                r.state = Request::FAILED;
+                r.err = e.what();
+                ++n_failed;
+                queue.pop_front();
+                cv_done.notify_all();
+                continue;
+            }
+            const bool slots_ok = opts.max_resident <= 0 || eng->nresident() < opts.max_resident;
+            if (!slots_ok || (double)(eng->bytes_in_use() + need) > budget) {
+                if (eng->nresident() == 0) {  // can never fit
+                    r.state = Request::FAILED;
+                    r.err = "admission refused: request needs more device memory than the budget";
+                    ++n_failed;
+                    queue.pop_front();
+                    cv_done.notify_all();
+                    continue;
+                }
+                break;
+            }
+            try {
+                r.solve = eng->add(r.prob, eo);
+                r.state = Request::RESIDENT;
+            } catch (const std::exception &e) {
+                r.state = Request::FAILED;
+                r.err = e.what();
+                ++n_failed;
+                cv_done.notify_all();
+            }
+            queue.pop_front();
+        }
+        bool active = false;
+        for (auto &kv : reqs)
+            if (kv.second->state == Request::RESIDENT) { active = true; break; }
+        if (!active) {
+            if (stop) break;
+            cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            continue;
+        }
+        lk.unlock();
+        try {
+            // bounded run-ahead: at most two ticks queued on the GPU, so new
+            // arrivals join after a short wait
+            while (inflight.size() >= 2) {
+                cuda_check(cudaEventSynchronize(inflight.front()), "tick wait");
+                pool.push_back(inflight.front());
+                inflight.pop_front();
+            }
+            if (eng->max_remaining_ticks() > 0) {
+                eng->step();
+                cudaEvent_t ev;
+                if (pool.empty()) cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+                else { ev = pool.back(); pool.pop_back(); }
+                cuda_check(cudaEventRecord(ev, stream), "event record");
+                inflight.push_back(ev);
+            }
+        } catch (const std::exception &e) {
+            std::lock_guard<std::mutex> g(mu);
+            fatal = e.what();
+            for (auto &kv : reqs)
+                if (kv.second->state == Request::RESIDENT || kv.second->state == Request::QUEUED) {
+                    kv.second->state = Request::FAILED;
+                    kv.second->err = fatal;
+                }
+            cv_done.notify_all();
+            break;
+        }
+        lk.lock();
+        n_launches += eng->last_launches();
+        // retire finished and cancelled solves
+        for (auto &kv : reqs) {
+            Request &r = *kv.second;
+            if (r.state == Request::CANCELLED && r.solve >= 0) {
+                try {
+                    eng->remove(r.solve);
+                } catch (...) {
+                }
+                r.solve = -1;
+                continue;
+            }
+            if (r.state != Request::RESIDENT) continue;
+            if (!eng->finished(r.solve)) continue;
+            try {
+                if (!r.fetching) { eng->fetch_async(r.solve); r.fetching = true; }
+                if (eng->ready(r.solve)) {
+                    r.out = eng->outputs(r.solve);
+                    eng->remove(r.solve);
+                    r.t_done = Clock::now();
+                    r.state = Request::DONE;
+                    ++n_completed;
+                    cv_done.notify_all();
+                }
+            } catch (const std::exception &e) {
+                r.state = Request::FAILED;
+                r.err = e.what();
+                ++n_failed;
+                cv_done.notify_all();
+            }
+        }
+    }
+    for (auto ev : inflight) cudaEventDestroy(ev);
+    for (auto ev : pool) cudaEventDestroy(ev);
+}
+
+extern "C" sbe_status sbe_server_create(const sbe_server_opts *opts, sbe_server **out)
+{
+    if (!out) return fail(SBE_INVALID_ARGUMENT, "null output pointer");
+    *out = nullptr;
+    return guard([&]() -> sbe_status {
+        auto s = std::make_unique<sbe_server>();
+        if (opts) s->opts = *opts;
+        else s->opts.precision = -1;
+        cuda_check(cudaSetDevice(s->opts.device), "cudaSetDevice");
+        cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream create");
+        const int S = s->opts.steps_per_launch > 0 ? s->opts.steps_per_launch : 256;
+        s->eng = std::make_unique<Engine>(s->opts.device, s->stream, S);
+        size_t fr = 0, tot = 0;
+        cuda_check(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+        s->budget = s->opts.mem_budget_bytes > 0 ? s->opts.mem_budget_bytes
+                                                 : std::max(0.0, (double)fr - 4.0 * (1ull << 30));
+        sbe_server *raw = s.get();
+        s->worker = std::thread([raw]() { raw->loop(); });
+        *out = s.release();
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, long long *request_id)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null server");
+    if (sbe_status st = check_problem(p)) return st;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->fatal.empty()) return fail(SBE_CUDA_ERROR, s->fatal);
+    auto r = std::make_unique<Request>();
+    r->id = s->next_id++;
+    r->prob = p->p;
+    r->t_submit = Clock::now();
+    if (request_id) *request_id = r->id;
+    s->queue.push_back(r->id);
+    s->reqs[r->id] = std::move(r);
+    ++s->n_submitted;
+    s->cv_work.notify_all();
+    return SBE_OK;
+}
+
+extern "C" sbe_status sbe_server_wait(sbe_server *s, long long id, double timeout_s, const sbe_outputs *out,
+                                      double *latency_s)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(SBE_INVALID_ARGUMENT, "unknown request id");
+    Request &r = *it->second;
+    auto pending = [&]() { return r.state == Request::QUEUED || r.state == Request::RESIDENT; };
+    if (timeout_s < 0) s->cv_done.wait(lk, [&]() { return !pending(); });
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&]() { return !pending(); }))
+        return fail(SBE_TIMEOUT, "request not finished within the timeout");
+    if (r.state == Request::CANCELLED) return fail(SBE_CANCELLED, "request was cancelled");
+    if (r.state == Request::FAILED) {
+        const bool oom = r.err.find("memory") != std::string::npos;
+        return fail(oom ? SBE_OOM : SBE_CUDA_ERROR, r.err);
+    }
+    copy_out(r.out, out);
+    if (latency_s) *latency_s = std::chrono::duration<double>(r.t_done - r.t_submit).count();
+    return SBE_OK;
+}
+
+extern "C" sbe_status sbe_server_cancel(sbe_server *s, long long id)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(SBE_INVALID_ARGUMENT, "unknown request id");
+    Request &r = *it->second;
+    if (r.state == Request::QUEUED) {
+        r.state = Request::CANCELLED;
+    } else if (r.state == Request::RESIDENT) {
+        r.state = Request::CANCELLED;  // the worker, which owns the engine, drops the solve
+        s->cv_work.notify_all();
+    }
+    s->cv_done.notify_all();
+    return SBE_OK;
+}
+
+extern "C" sbe_status sbe_server_stats(sbe_server *s, long long c[5])
+{
+    if (!s || !c) return fail(SBE_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    long long resident = 0;
+    for (auto &kv : s->reqs) resident += kv.second->state == Request::RESIDENT;
+    c[0] = s->n_submitted;
+    c[1] = s->n_completed;
+    c[2] = s->n_failed;
+    c[3] = resident;
+    c[4] = s->n_launches;
+    return SBE_OK;
+}
+
+extern "C" void sbe_server_destroy(sbe_server *s)
+{
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        for (auto &kv : s->reqs)
+            if (kv.second->state == Request::QUEUED) kv.second->state = Request::CANCELLED;
+        s->queue.clear();
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->opts.device);
+    s->eng.reset();
+    if (s->stream) {
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
+    }
+    delete s;
+}
+
+// ================================================================= peaks
+extern "C" sbe_status sbe_measure_fma_peaks(int device, double *fp64, double *fp32)
+{
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        int sms = 0;
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attr");
+        void *buf = nullptr;
+        cuda_check(cudaMalloc(&buf, 4096), "cudaMalloc");
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        const int blocks = sms * 8, iters = 1 << 16;
+        double res[2] = {0, 0};
+        for (int which = 0; which < 2; ++which) {
+            cuda_check(launch_fma_peak(which, blocks, 256, buf, 0), "warm-up");
+            float best = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaEventRecord(a, 0);
+                cuda_check(launch_fma_peak(which, blocks, iters, buf, 0), "fma peak");
+                cudaEventRecord(b, 0);
+                cuda_check(cudaEventSynchronize(b), "sync");
+                float ms = 0;
+                cudaEventElapsedTime(&ms, a, b);
+                best = std::min(best, ms);
+            }
+            const double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+            res[which] = flops / (best * 1e-3) / 1e12;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaFree(buf);
+        if (fp64) *fp64 = res[0];
+        if (fp32) *fp32 = res[1];
+        return SBE_OK;
+    });
+}

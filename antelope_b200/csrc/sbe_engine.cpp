@@ -1,0 +1,507 @@
+// Host engine: device buffers of resident solves, launch lists, per-launch
+// stepping, output assembly and the reference's file writers.
+#include "sbe_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "sbe_kernels.h"
+
+namespace sbe {
+
+void cuda_check(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        throw OomError(std::string(what) + ": out of device memory");
+    }
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+}  // namespace
+
+struct Engine::Solve {
+    Problem prob;
+    int id = 0, slot = 0, variant = 0, precision = 0, nts = 0;
+    Shape shape{};
+    int nk = 0, nk_pad = 0, ntiles = 0, Nt = 0, admit_tick = 0, nticks = 0;
+    bool g1 = false;
+    void *kc = nullptr, *st = nullptr, *tab = nullptr;
+    double *partial = nullptr, *jout = nullptr, *constpart = nullptr;
+    double *h_jout = nullptr, *h_const = nullptr;  // pinned
+    cudaEvent_t ev = nullptr;
+    bool fetched = false;
+    size_t bytes = 0;
+};
+
+struct Engine::Group {
+    int variant, precision, rk, kpt, threads;
+    bool g1;
+    std::vector<TileDev> tiles;
+    TileDev *d_tiles = nullptr;
+    int cap = 0;
+};
+
+Engine::Engine(int device, cudaStream_t stream, int steps_per_launch)
+    : device_(device), stream_(stream), S_(steps_per_launch > 0 ? steps_per_launch : 512)
+{
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    capacity_ = 64;
+    cuda_check(cudaMalloc(&d_solves_, sizeof(SolveDev) * capacity_), "cudaMalloc(solves)");
+    cuda_check(cudaMallocHost(&h_solves_, sizeof(SolveDev) * capacity_), "cudaMallocHost(solves)");
+    cuda_check(cudaMalloc(&d_ids_, sizeof(int) * capacity_), "cudaMalloc(ids)");
+    cuda_check(cudaMallocHost(&h_ids_, sizeof(int) * capacity_), "cudaMallocHost(ids)");
+    for (int i = capacity_ - 1; i >= 0; --i) free_slots_.push_back(i);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+}
+
+Engine::~Engine()
+{
+    cudaStreamSynchronize(stream_);
+    for (auto &kv : live_) {
+        Solve &s = *kv.second;
+        cudaFreeAsync(s.kc, stream_);
+        cudaFreeAsync(s.st, stream_);
+        cudaFreeAsync(s.tab, stream_);
+        cudaFreeAsync(s.partial, stream_);
+        cudaFreeAsync(s.jout, stream_);
+        cudaFreeAsync(s.constpart, stream_);
+        cudaFreeHost(s.h_jout);
+        cudaFreeHost(s.h_const);
+        if (s.ev) cudaEventDestroy(s.ev);
+    }
+    for (auto &kv : groups_) cudaFree(kv.second->d_tiles);
+    cudaStreamSynchronize(stream_);
+    cudaFree(d_solves_);
+    cudaFreeHost(h_solves_);
+    cudaFree(d_ids_);
+    cudaFreeHost(h_ids_);
+}
+
+Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
+{
+    const int prec = o.precision >= 0 ? o.precision : p.precision;
+    Shape s{};
+    s.kpt = o.kpt > 0 ? o.kpt : 1;
+    if (p.gauge != GAUGE_VELOCITY) s.kpt = 1;
+    s.tile_k = o.tile_k > 0 ? o.tile_k : 128 * s.kpt;
+    (void)prec;
+    s.threads = s.tile_k / s.kpt;
+    if (s.threads < 32 || s.threads > 256 || s.threads % 32 || s.tile_k % s.kpt)
+        throw CfgError("tile_k / kpt must be a multiple of 32 between 32 and 256");
+    return s;
+}
+
+size_t Engine::bytes_needed(const Problem &p, const EngineOptions &o) const
+{
+    const Shape sh = shape_for(p, o);
+    const int prec = o.precision >= 0 ? o.precision : p.precision;
+    const size_t real = prec == PREC_FP64 ? 8 : 4;
+    const int ntiles = ceil_div(p.ntotal(), sh.tile_k);
+    const size_t nk_pad = (size_t)ntiles * sh.tile_k;
+    const int nts = (int)stage_fractions(p.rk).size();
+    const bool vg = p.gauge == GAUGE_VELOCITY;
+    const size_t nc = vg ? (size_t)VG_NCONST : (size_t)LW_NCONST, ns = 4;
+    const size_t tab = (size_t)p.laser.Nt * nts * (vg ? 2 : LW_NPHASE) * real;
+    return (nc + ns) * nk_pad * real + tab + (size_t)S_ * ntiles * NSLOT * 8 + (size_t)p.laser.Nt * NSLOT * 8 +
+           (size_t)ntiles * NSLOT * 8;
+}
+
+int Engine::add(const Problem &p, const EngineOptions &o)
+{
+    if (p.model != MODEL_HALDANE) throw CfgError("only the Haldane model is built on this path");
+    if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) throw CfgError("gauge LengthHamiltonian is not implemented");
+    if (p.rk != 4 && p.rk != 5) throw CfgError("Haldane solves use RKorder 4 or 5");
+    auto s = std::make_unique<Solve>();
+    s->prob = p;
+    s->id = next_id_++;
+    s->precision = o.precision >= 0 ? o.precision : p.precision;
+    s->variant = p.gauge == GAUGE_VELOCITY ? VAR_HALDANE_VG : VAR_HALDANE_LW;
+    s->shape = shape_for(p, o);
+    s->nk = p.ntotal();
+    s->ntiles = ceil_div(s->nk, s->shape.tile_k);
+    s->nk_pad = s->ntiles * s->shape.tile_k;
+    s->Nt = p.laser.Nt;
+    const auto cfr = stage_fractions(p.rk);
+    s->nts = (int)cfr.size();
+    s->g1 = p.T1 > 1.0e-16;
+    if (free_slots_.empty()) throw OomError("too many resident solves (descriptor slots exhausted)");
+    const size_t real = s->precision == PREC_FP64 ? 8 : 4;
+    const bool vg = s->variant == VAR_HALDANE_VG;
+    const size_t nc = vg ? (size_t)VG_NCONST : (size_t)LW_NCONST;
+    const size_t kc_b = nc * s->nk_pad * real, st_b = 4 * (size_t)s->nk_pad * real;
+    const size_t tab_n = (size_t)s->Nt * s->nts * (vg ? 2 : LW_NPHASE);
+    const size_t part_b = (size_t)S_ * s->ntiles * NSLOT * 8, jout_b = (size_t)s->Nt * NSLOT * 8;
+    const size_t cp_b = (size_t)s->ntiles * NSLOT * 8;
+
+    auto alloc = [&](void **ptr, size_t b, const char *what) {
+        cudaError_t e = cudaMallocAsync(ptr, b, stream_);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(s->kc, stream_);
+            cudaFreeAsync(s->st, stream_);
+            cudaFreeAsync(s->tab, stream_);
+            cudaFreeAsync(s->partial, stream_);
+            cudaFreeAsync(s->jout, stream_);
+            cuda_check(e, what);
+        }
+    };
+    alloc(&s->kc, kc_b, "alloc constants");
+    alloc(&s->st, st_b, "alloc state");
+    alloc(&s->tab, tab_n * real, "alloc field table");
+    alloc((void **)&s->partial, part_b, "alloc partials");
+    alloc((void **)&s->jout, jout_b, "alloc outputs");
+    alloc((void **)&s->constpart, cp_b, "alloc constant parts");
+    s->bytes = kc_b + st_b + tab_n * real + part_b + jout_b + cp_b;
+    cuda_check(cudaMallocHost(&s->h_jout, jout_b), "cudaMallocHost(jout)");
+    cuda_check(cudaMallocHost(&s->h_const, cp_b), "cudaMallocHost(constpart)");
+    cuda_check(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate");
+
+    // field tables (host FP64, rounded once to the kernel's Real)
+    std::vector<double> atab = a_table(p);
+    std::vector<double> tabd = vg ? atab : phase_table(p, atab);
+    if (s->precision == PREC_FP64) {
+        cuda_check(cudaMemcpyAsync(s->tab, tabd.data(), tab_n * 8, cudaMemcpyHostToDevice, stream_), "copy table");
+    } else {
+        std::vector<float> tf(tabd.begin(), tabd.end());
+        cuda_check(cudaMemcpyAsync(s->tab, tf.data(), tab_n * 4, cudaMemcpyHostToDevice, stream_), "copy table");
+    }
+    InitArgs ia{};
+    ia.nk = s->nk;
+    ia.nk_pad = s->nk_pad;
+    ia.tile_k = s->shape.tile_k;
+    ia.variant = s->variant;
+    ia.nval = p.nval;
+    ia.use_fermi = p.use_fermi ? 1 : 0;
+    for (int i = 0; i < 3; ++i) ia.N[i] = p.Nk[i];
+    for (int i = 0; i < 9; ++i) ia.axes[i] = p.bzaxes[i];
+    for (int i = 0; i < 3; ++i) ia.origin[i] = p.bzorigin[i];
+    ia.t1 = p.hal_t1;
+    ia.t2 = p.hal_t2;
+    ia.M0 = p.hal_M0;
+    ia.phi0 = p.hal_phi0;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 2; ++j) { ia.va[i][j] = p.hal_va[i][j]; ia.vb[i][j] = p.hal_vb[i][j]; }
+    ia.Ef = p.Ef;
+    ia.dt = p.dt;
+    cuda_check(cudaMemsetAsync(s->kc, 0, kc_b, stream_), "memset constants");
+    cuda_check(cudaMemsetAsync(s->st, 0, st_b, stream_), "memset state");
+    cuda_check(launch_init_haldane(ia, s->precision, s->kc, s->st, s->constpart, stream_), "init kernel");
+
+    s->slot = free_slots_.back();
+    free_slots_.pop_back();
+    SolveDev &d = h_solves_[s->slot];
+    std::memset(&d, 0, sizeof(d));
+    d.nk = s->nk;
+    d.ntiles = s->ntiles;
+    d.Nt = s->Nt;
+    d.admit_tick = tick_;
+    d.nk_pad = s->nk_pad;
+    d.nts = s->nts;
+    d.variant = s->variant;
+    d.precision = s->precision;
+    d.kc = s->kc;
+    d.st = s->st;
+    d.tab = s->tab;
+    d.partial = s->partial;
+    d.jout = s->jout;
+    d.g1 = p.T1 > 1.0e-16 ? p.dt / p.T1 : 0.0;   // SBEs.h:484-493
+    d.g2 = p.T2 > 1.0e-16 ? p.dt / p.T2 : 0.0;
+    const double t2c = 2.0 * p.hal_t2 * std::cos(p.hal_phi0), t2s = 2.0 * p.hal_t2 * std::sin(p.hal_phi0);
+    d.t1dt = p.dt * p.hal_t1;
+    d.t2sdt = p.dt * t2s;
+    d.Mdt = p.dt * p.hal_M0;
+    d.t1 = p.hal_t1;
+    d.t2c = t2c;
+    d.t2s = t2s;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 2; ++j) { d.va[i][j] = p.hal_va[i][j]; d.vb[i][j] = p.hal_vb[i][j]; }
+    cuda_check(cudaMemcpyAsync(d_solves_ + s->slot, &d, sizeof(SolveDev), cudaMemcpyHostToDevice, stream_),
+               "copy descriptor");
+    s->admit_tick = tick_;
+    s->nticks = ceil_div(s->Nt, S_);
+    bytes_in_use_ += s->bytes;
+    const int id = s->id;
+    live_[id] = std::move(s);
+    dirty_ = true;
+    return id;
+}
+
+Engine::Solve &Engine::get(int id)
+{
+    auto it = live_.find(id);
+    if (it == live_.end()) throw CfgError("unknown solve id");
+    return *it->second;
+}
+const Engine::Solve &Engine::get(int id) const
+{
+    auto it = live_.find(id);
+    if (it == live_.end()) throw CfgError("unknown solve id");
+    return *it->second;
+}
+
+int Engine::remaining_ticks(int id) const
+{
+    const Solve &s = get(id);
+    return std::max(0, s.admit_tick + s.nticks - tick_);
+}
+
+int Engine::max_remaining_ticks() const
+{
+    int m = 0;
+    for (const auto &kv : live_) m = std::max(m, kv.second->admit_tick + kv.second->nticks - tick_);
+    return m;
+}
+
+void Engine::rebuild_lists()
+{
+    // the pinned id list may still feed an in-flight copy
+    cuda_check(cudaStreamSynchronize(stream_), "sync before list rebuild");
+    for (auto &kv : groups_) kv.second->tiles.clear();
+    nids_ = 0;
+    for (auto &kv : live_) {
+        Solve &s = *kv.second;
+        if (s.admit_tick + s.nticks - tick_ <= 0) continue;
+        auto key = std::make_tuple(s.variant, s.precision, s.prob.rk, s.shape.kpt, s.shape.threads, s.g1 ? 1 : 0);
+        auto &g = groups_[key];
+        if (!g) {
+            g = std::make_unique<Group>();
+            g->variant = s.variant;
+            g->precision = s.precision;
+            g->rk = s.prob.rk;
+            g->kpt = s.shape.kpt;
+            g->threads = s.shape.threads;
+            g->g1 = s.g1;
+        }
+        for (int t = 0; t < s.ntiles; ++t) {
+            TileDev td;
+            td.solve = s.slot;
+            td.k0 = t * s.shape.tile_k;
+            td.kcount = std::min(s.shape.tile_k, s.nk - td.k0);
+            td.tile = t;
+            g->tiles.push_back(td);
+        }
+        h_ids_[nids_++] = s.slot;
+    }
+    for (auto &kv : groups_) {
+        Group &g = *kv.second;
+        if ((int)g.tiles.size() > g.cap) {
+            cudaFree(g.d_tiles);
+            g.cap = std::max<int>((int)g.tiles.size(), 2 * g.cap);
+            cuda_check(cudaMalloc(&g.d_tiles, sizeof(TileDev) * g.cap), "cudaMalloc(tiles)");
+        }
+        if (!g.tiles.empty())
+            cuda_check(cudaMemcpyAsync(g.d_tiles, g.tiles.data(), sizeof(TileDev) * g.tiles.size(),
+                                       cudaMemcpyHostToDevice, stream_),
+                       "copy tiles");
+    }
+    if (nids_ > 0)
+        cuda_check(cudaMemcpyAsync(d_ids_, h_ids_, sizeof(int) * nids_, cudaMemcpyHostToDevice, stream_), "copy ids");
+    dirty_ = false;
+}
+
+void Engine::step()
+{
+    // a solve that finished at the previous tick leaves the launch lists
+    for (auto &kv : live_)
+        if (kv.second->admit_tick + kv.second->nticks == tick_) dirty_ = true;
+    if (dirty_) rebuild_lists();
+    step_frozen();
+}
+
+void Engine::step_frozen()
+{
+    last_launches_ = 0;
+    for (auto &kv : groups_) {
+        Group &g = *kv.second;
+        if (g.tiles.empty()) continue;
+        LaunchArgs la{};
+        la.tiles = g.d_tiles;
+        la.solves = d_solves_;
+        la.ntiles = (int)g.tiles.size();
+        la.threads = g.threads;
+        la.tick = tick_;
+        la.S = S_;
+        la.variant = g.variant;
+        la.precision = g.precision;
+        la.rk = g.rk;
+        la.kpt = g.kpt;
+        la.has_g1 = g.g1;
+        la.stream = stream_;
+        cuda_check(launch_propagate(la), "propagate launch");
+        ++last_launches_;
+    }
+    if (nids_ > 0) cuda_check(launch_reduce(d_solves_, d_ids_, nids_, tick_, S_, stream_), "reduce launch");
+    ++tick_;
+}
+
+void Engine::fetch_async(int id)
+{
+    Solve &s = get(id);
+    cuda_check(cudaMemcpyAsync(s.h_jout, s.jout, (size_t)s.Nt * NSLOT * 8, cudaMemcpyDeviceToHost, stream_),
+               "copy outputs");
+    cuda_check(cudaMemcpyAsync(s.h_const, s.constpart, (size_t)s.ntiles * NSLOT * 8, cudaMemcpyDeviceToHost, stream_),
+               "copy constant parts");
+    cuda_check(cudaEventRecord(s.ev, stream_), "event record");
+    s.fetched = true;
+}
+
+bool Engine::ready(int id)
+{
+    Solve &s = get(id);
+    if (!s.fetched) return false;
+    cudaError_t e = cudaEventQuery(s.ev);
+    if (e == cudaErrorNotReady) return false;
+    cuda_check(e, "event query");
+    return true;
+}
+
+SolveOutputs Engine::outputs(int id)
+{
+    Solve &s = get(id);
+    if (!s.fetched) fetch_async(id);
+    cuda_check(cudaEventSynchronize(s.ev), "event sync");
+    double cp[NSLOT] = {0};
+    for (int t = 0; t < s.ntiles; ++t)
+        for (int q = 0; q < NSLOT; ++q) cp[q] += s.h_const[(size_t)t * NSLOT + q];
+    std::vector<double> j(s.h_jout, s.h_jout + (size_t)s.Nt * NSLOT);
+    SolveOutputs o;
+    assemble_outputs(s.prob, j, cp, o);
+    return o;
+}
+
+void Engine::remove(int id)
+{
+    auto it = live_.find(id);
+    if (it == live_.end()) return;
+    Solve &s = *it->second;
+    cudaFreeAsync(s.kc, stream_);
+    cudaFreeAsync(s.st, stream_);
+    cudaFreeAsync(s.tab, stream_);
+    cudaFreeAsync(s.partial, stream_);
+    cudaFreeAsync(s.jout, stream_);
+    cudaFreeAsync(s.constpart, stream_);
+    if (s.fetched) cudaEventSynchronize(s.ev);
+    cudaFreeHost(s.h_jout);
+    cudaFreeHost(s.h_const);
+    cudaEventDestroy(s.ev);
+    bytes_in_use_ -= s.bytes;
+    free_slots_.push_back(s.slot);
+    live_.erase(it);
+    dirty_ = true;
+}
+
+// ================================================================ outputs
+void assemble_outputs(const Problem &p, const std::vector<double> &jout, const double cp[NSLOT], SolveOutputs &o)
+{
+    const int Nt = p.laser.Nt, N = p.nband;
+    o.Nt = Nt;
+    o.nband = N;
+    o.inter.assign((size_t)Nt * 3, 0.0);
+    o.intra.assign((size_t)Nt * 3, 0.0);
+    o.occ.assign((size_t)Nt * (N + 1), 0.0);
+    o.coh.assign((size_t)Nt * 2, 0.0);
+    o.laser.assign((size_t)Nt * 7, 0.0);
+    const bool vg = p.gauge == GAUGE_VELOCITY;
+    const double W = p.total_weight, dV = p.dV, Ntot = (double)p.ntotal();
+    std::vector<double> occ00((size_t)Nt), occ01r((size_t)Nt), occ01i((size_t)Nt);
+    for (int n = 0; n < Nt; ++n) {
+        const double *j = &jout[(size_t)n * NSLOT];
+        const double t = p.laser.atmin + p.laser.dt * n;
+        double A[3], E[3];
+        p.laser.eval(t, A, E);
+        double *L = &o.laser[(size_t)n * 7];
+        L[0] = t;
+        for (int d = 0; d < 3; ++d) { L[1 + d] = E[d]; L[4 + d] = A[d]; }
+        double inter[3] = {j[0], j[1], 0.0};
+        double intra[3] = {j[2], j[3], 0.0};
+        if (vg) {
+            intra[0] += cp[2];
+            intra[1] += cp[3];
+            for (int d = 0; d < 3; ++d) intra[d] += p.nval * A[d] * W;  // SBEs.h:750-757
+        }
+        for (int d = 0; d < 3; ++d) {
+            if (p.inter_intra) {
+                o.inter[(size_t)n * 3 + d] = inter[d] * dV;
+                o.intra[(size_t)n * 3 + d] = intra[d] * dV;
+            } else {  // GenCurrent: the total current goes to the inter column (antelope.cpp:316-324)
+                o.inter[(size_t)n * 3 + d] = (inter[d] + intra[d]) * dV;
+            }
+        }
+        const double r00 = j[4] + cp[4], r11 = j[5] + cp[5];
+        o.occ[(size_t)n * (N + 1) + 0] = r00 / Ntot;
+        o.occ[(size_t)n * (N + 1) + 1] = r11 / Ntot;
+        o.occ[(size_t)n * (N + 1) + 2] = (r00 + r11) / Ntot;
+        occ00[n] = r00;
+        occ01r[n] = j[6] + cp[6];
+        occ01i[n] = j[7] + cp[7];
+    }
+    // coherence__full__evol.dat reads flat element Nval*N + Nval + 1 of the
+    // per-step N x N array (antelope.cpp:539-542); for N = 2 that is element 0
+    // of the NEXT step, and past the end for the last step (written as 0 here).
+    const int e = p.nval * N + p.nval + 1;
+    for (int n = 0; n < Nt; ++n) {
+        const int row = n + e / (N * N), el = e % (N * N);
+        double re = 0.0, im = 0.0;
+        if (row < Nt) {
+            if (el == 0) re = occ00[row];
+            else if (el == 1) { re = occ01r[row]; im = occ01i[row]; }
+            else if (el == 2) { re = occ01r[row]; im = -occ01i[row]; }
+            else re = o.occ[(size_t)row * (N + 1) + 1] * Ntot;
+        }
+        o.coh[(size_t)n * 2] = re / Ntot;
+        o.coh[(size_t)n * 2 + 1] = im / Ntot;
+    }
+}
+
+void write_outputs(const Problem &p, const SolveOutputs &o, const std::string &dir)
+{
+    auto path = [&](const char *f) { return dir.empty() ? std::string(f) : dir + "/" + f; };
+    auto open = [&](const char *f) {
+        FILE *fp = std::fopen(path(f).c_str(), "w");
+        if (!fp) throw CfgError(std::string("cannot open ") + path(f) + " for writing");
+        return fp;
+    };
+    FILE *lf = open("outlaserdata.dat");
+    for (int n = 0; n < o.Nt; ++n) {
+        const double *L = &o.laser[(size_t)n * 7];
+        std::fprintf(lf, "%e    ", L[0]);
+        for (int d = 0; d < 3; ++d) std::fprintf(lf, "%e      ", L[1 + d]);
+        for (int d = 0; d < 3; ++d) std::fprintf(lf, "%e      ", L[4 + d]);
+        std::fprintf(lf, "\n");
+    }
+    std::fclose(lf);
+    std::fclose(open("laserParameters.dat"));  // opened but never written by the reference
+    FILE *fi = open("interband_dipole_full_evol.dat");
+    FILE *fa = open("intraband_current_full_evol.dat");
+    FILE *fo = open("occupation__full__evol.dat");
+    FILE *fc = open("coherence__full__evol.dat");
+    const int N = o.nband;
+    for (int n = 0; n < o.Nt; ++n) {
+        for (int d = 0; d < 3; ++d) {
+            std::fprintf(fi, "%.16e    ", o.inter[(size_t)n * 3 + d]);
+            std::fprintf(fa, "%.16e    ", o.intra[(size_t)n * 3 + d]);
+        }
+        std::fprintf(fi, "\n");
+        std::fprintf(fa, "\n");
+        for (int m = 0; m < N; ++m) std::fprintf(fo, "%.16e    ", o.occ[(size_t)n * (N + 1) + m]);
+        std::fprintf(fo, "%.16e\n", o.occ[(size_t)n * (N + 1) + N]);
+        std::fprintf(fc, "%.16e    ", o.coh[(size_t)n * 2]);
+        std::fprintf(fc, "%.16e\n", o.coh[(size_t)n * 2 + 1]);
+    }
+    std::fclose(fi);
+    std::fclose(fa);
+    std::fclose(fo);
+    std::fclose(fc);
+    (void)p;
+}
+
+}  // namespace sbe

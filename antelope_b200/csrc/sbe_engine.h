@@ -1,0 +1,122 @@
+// The tile engine: owns device-resident solves and advances them launch by
+// launch.  A single solve, a batched scan and the serving loop are all built
+// on it (sbe_capi.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "sbe_dev.h"
+#include "sbe_problem.h"
+
+namespace sbe {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct OomError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+void cuda_check(cudaError_t e, const char *what);
+
+struct EngineOptions {
+    int precision = -1;      // -1: take calc.precision from the problem
+    int tile_k = 0;          // k-points per tile (0: tuned default)
+    int kpt = 0;             // k-points per thread (0: tuned default)
+    int steps_per_launch = 0;  // S (0: default)
+};
+
+// One launch shape for a class of solves.
+struct Shape {
+    int tile_k, kpt, threads;
+};
+
+// Outputs of a finished solve in the reference's file quantities.
+struct SolveOutputs {
+    int Nt = 0, nband = 0;
+    std::vector<double> inter, intra;  // [Nt][3], times dV (antelope.cpp:522-527)
+    std::vector<double> occ;           // [Nt][N+1], divided by Ntotal, last column the sum (530-536)
+    std::vector<double> coh;           // [Nt][2] (539-542)
+    std::vector<double> laser;         // [Nt][7]: t, E[3], A[3] (208-235)
+};
+
+class Engine {
+public:
+    Engine(int device, cudaStream_t stream, int steps_per_launch);
+    ~Engine();
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+
+    // Device bytes a solve of this problem needs (admission control).
+    size_t bytes_needed(const Problem &p, const EngineOptions &o) const;
+    // Set up a solve on the stream; it starts advancing at the next step().
+    int add(const Problem &p, const EngineOptions &o);
+    // Advance every resident solve by up to S steps (one propagate launch per
+    // launch class, then the tile reduction).
+    void step();
+    // Same as step() but never rebuilds the launch lists (for CUDA graph
+    // capture, where the lists built by the first step() stay valid: tiles of
+    // solves that finished return at once).
+    void step_frozen();
+    void set_stream(cudaStream_t s) { stream_ = s; }
+    // Ticks still needed by a solve (0 when finished).
+    int remaining_ticks(int id) const;
+    bool finished(int id) const { return remaining_ticks(id) == 0; }
+    int max_remaining_ticks() const;
+    // Queue the D2H copy of a finished solve's per-step sums into pinned
+    // memory and record an event; ready() polls it, outputs() assembles.
+    void fetch_async(int id);
+    bool ready(int id);
+    SolveOutputs outputs(int id);
+    void remove(int id);
+    int nresident() const { return (int)live_.size(); }
+    int tick() const { return tick_; }
+    int steps_per_launch() const { return S_; }
+    cudaStream_t stream() const { return stream_; }
+    size_t bytes_in_use() const { return bytes_in_use_; }
+    // Number of propagate launches issued by the last step() (telemetry).
+    int last_launches() const { return last_launches_; }
+    // Launch shape the engine would use for a solve.
+    Shape shape_for(const Problem &p, const EngineOptions &o) const;
+
+private:
+    struct Solve;
+    struct Group;
+    void rebuild_lists();
+    Solve &get(int id);
+    const Solve &get(int id) const;
+
+    int device_;
+    cudaStream_t stream_;
+    int S_;
+    int tick_ = 0;
+    int next_id_ = 0;
+    int capacity_ = 0;
+    bool dirty_ = true;
+    int last_launches_ = 0;
+    size_t bytes_in_use_ = 0;
+    std::map<int, std::unique_ptr<Solve>> live_;
+    std::vector<int> free_slots_;
+    SolveDev *d_solves_ = nullptr;
+    SolveDev *h_solves_ = nullptr;   // pinned mirror
+    int *d_ids_ = nullptr, *h_ids_ = nullptr;
+    int nids_ = 0;
+    int status_dummy_ = 0;
+    std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<Group>> groups_;
+};
+
+// Assemble the reference's output quantities from the per-step slot sums.
+void assemble_outputs(const Problem &p, const std::vector<double> &jout, const double constpart[NSLOT],
+                      SolveOutputs &out);
+
+// Write the reference's output files into `dir` (antelope.cpp:176-184,
+// 208-235, 514-548), byte-for-byte in its formats.
+void write_outputs(const Problem &p, const SolveOutputs &o, const std::string &dir);
+
+}  // namespace sbe

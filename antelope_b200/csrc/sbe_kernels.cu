@@ -1,0 +1,666 @@
+// sm_100a kernels of the SBE propagator.
+//
+//   init_haldane      per-k set-up: k-grid point and trapezoid weight
+//                     (momaxis.h:147-186, 349-383), H0(k) and J(k)
+//                     (Haldane.h:86-127), closed-form 2x2 eigensystem standing
+//                     in for zheevr, rho0 (SBEs.h:319-356) and P = U^dag J U
+//                     (SBEs.h:366-372).
+//   propagate_vg      velocity gauge, 2 bands: one thread per k-point (or
+//                     KPT of them), rho in registers for every step of the
+//                     launch, RK4 or fixed-step Fehlberg-5 (SBEs.h:395-416,
+//                     596-624) of dRho/dt = -i[H,rho] - G o (rho - rho0)
+//                     (SBEs.h:787-805, 862-871), fused with the per-step
+//                     weighted k-sum of the currents and occupations
+//                     (SBEs.h:694-760, antelope.cpp:302-334).
+//   propagate_lw      length gauge, 2 bands (Haldane): H0(k+A) in place,
+//                     dephasing in the instantaneous eigenbasis (SBEs.h:762-
+//                     786, 831-861), written for the Bloch vector of rho.
+//   reduce_tiles      deterministic second pass: tile partials -> per-step sums.
+//
+// Precision: every kernel is a template on Real.  Real = double is the plain
+// FP64 method.  Real = float is the mixed method: RK stages in FP32, the A(t)
+// table computed in FP64 on the host then rounded per stage, and the k-sum of
+// the currents accumulated in FP64 from the warp level up.  In the velocity
+// gauge the state is the deviation rho - rho0 (small), so FP32 rounding acts
+// on the deviation only; the time-independent rho0 parts of the currents are
+// summed once, in FP64.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sbe_dev.h"
+#include "sbe_kernels.h"
+
+namespace sbe {
+
+// ------------------------------------------------------------ RK tableaux
+// Butcher tableaux of SBEs.h:395-416.  The stage slopes carry the factor dt
+// (all per-k constants are dt-scaled), so only the pure coefficients appear.
+template <int RK> struct Tableau;
+template <> struct Tableau<4> {
+    static constexpr int S = 4, NT = 3;
+    __device__ static constexpr double a(int i, int j)
+    {
+        return (i == 1 && j == 0) ? 0.5 : (i == 2 && j == 1) ? 0.5 : (i == 3 && j == 2) ? 1.0 : 0.0;
+    }
+    __device__ static constexpr double b(int i)
+    {
+        return (i == 0 || i == 3) ? 1.0 / 6.0 : 2.0 / 6.0;
+    }
+    __device__ static constexpr int ti(int i) { return i == 0 ? 0 : (i == 3 ? 2 : 1); }
+};
+template <> struct Tableau<5> {  // Fehlberg tableau with its 5th-order weights
+    static constexpr int S = 6, NT = 6;
+    __device__ static constexpr double a(int i, int j)
+    {
+        return i == 1 ? (j == 0 ? 1.0 / 4.0 : 0.0)
+             : i == 2 ? (j == 0 ? 3. / 32. : j == 1 ? 9. / 32. : 0.0)
+             : i == 3 ? (j == 0 ? 1932. / 2197. : j == 1 ? -7200. / 2197. : j == 2 ? 7296. / 2197. : 0.0)
+             : i == 4 ? (j == 0 ? 439. / 216. : j == 1 ? -8. : j == 2 ? 3680. / 513. : j == 3 ? -845. / 4104. : 0.0)
+             : i == 5 ? (j == 0 ? -8. / 27. : j == 1 ? 2. : j == 2 ? -3544. / 2565 : j == 3 ? 1859. / 4104
+                        : j == 4 ? -11. / 40. : 0.0)
+             : 0.0;
+    }
+    __device__ static constexpr double b(int i)
+    {
+        return i == 0 ? 16. / 135. : i == 1 ? 0.0 : i == 2 ? 6656. / 12825. : i == 3 ? 28561. / 56430.
+             : i == 4 ? -9. / 50. : 2. / 55.;
+    }
+    __device__ static constexpr int ti(int i) { return i; }
+};
+
+template <class Real> struct V2;
+template <> struct V2<double> { using T = double2; };
+template <> struct V2<float> { using T = float2; };
+
+// ---------------------------------------------------- warp reduce-scatter
+// Sums 8 doubles over the 32 lanes of a warp.  Three halving exchanges leave
+// each lane with one partially summed value (index lane>>2 for lanes that are
+// multiples of 4), two more exchanges finish it: 9 shuffles instead of 40.
+// The pattern is fixed, so the result is deterministic.
+__device__ __forceinline__ double warp_sum8(const double (&v)[8], int lane)
+{
+    const bool h4 = lane & 16, h2 = lane & 8, h1 = lane & 4;
+    double u[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        double send = h4 ? v[i] : v[i + 4];
+        double keep = h4 ? v[i + 4] : v[i];
+        u[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    double x[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        double send = h2 ? u[i] : u[i + 2];
+        double keep = h2 ? u[i + 2] : u[i];
+        x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    double send = h1 ? x[0] : x[1];
+    double y = (h1 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    y += __shfl_xor_sync(0xffffffffu, y, 2);
+    y += __shfl_xor_sync(0xffffffffu, y, 1);
+    return y;  // lanes 4*i hold the sum of v[i]
+}
+
+constexpr int MAX_WARPS = 8;
+
+// Per-step tile reduction staged through shared memory: each warp deposits
+// its 8 sums per step; every SUB steps (and at the end of the launch) the
+// block sums over warps and writes one row of the partial buffer per step.
+struct TileReducer {
+    double (*red)[MAX_WARPS][NSLOT];
+    __device__ __forceinline__ void push(const double (&v)[8], int r)
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        double y = warp_sum8(v, lane);
+        if ((lane & 3) == 0) red[r][warp][lane >> 2] = y;
+    }
+    __device__ __forceinline__ void flush(int nrows, int row0, int ntiles, int tile, double *partial)
+    {
+        __syncthreads();
+        const int nwarp = blockDim.x >> 5;
+        for (int idx = threadIdx.x; idx < nrows * NSLOT; idx += blockDim.x) {
+            const int row = idx / NSLOT, slot = idx % NSLOT;
+            double acc = 0.0;
+            for (int w = 0; w < nwarp; ++w) acc += red[row][w][slot];
+            partial[((size_t)(row0 + row) * ntiles + tile) * NSLOT + slot] = acc;
+        }
+        __syncthreads();
+    }
+};
+
+// ------------------------------------------------------ velocity gauge
+template <class Real, bool G1>
+__device__ __forceinline__ void vg_rhs(const Real (&c)[VG_NCONST], typename V2<Real>::T A, const Real (&y)[4],
+                                       Real g1, Real g2, Real (&k)[4])
+{
+    const Real delta = fma(A.y, c[VG_DPY], fma(A.x, c[VG_DPX], c[VG_DE]));
+    const Real wr = fma(A.y, c[VG_PYR], A.x * c[VG_PXR]);
+    const Real wi = fma(A.y, c[VG_PYI], A.x * c[VG_PXI]);
+    const Real im2 = Real(2) * fma(wi, y[VG_ZR], -(wr * y[VG_ZI]));  // 2 Im(w z*)
+    if (G1) {
+        k[VG_DA] = fma(-g1, y[VG_DA], im2);
+        k[VG_DB] = fma(-g1, y[VG_DB], -im2);
+    } else {
+        k[VG_DA] = im2;
+        k[VG_DB] = -im2;
+    }
+    const Real bma = c[VG_C0] + (y[VG_DB] - y[VG_DA]);               // rho_11 - rho_00
+    const Real xr = fma(bma, wr, delta * y[VG_ZR]);
+    const Real xi = fma(bma, wi, delta * y[VG_ZI]);
+    k[VG_ZR] = fma(-g2, y[VG_ZR], xi);                                // -i X - g2 z
+    k[VG_ZI] = fma(-g2, y[VG_ZI], -xr);
+}
+
+template <class Real, int RK, int KPT, bool G1>
+__global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ tiles,
+                                                    const SolveDev *__restrict__ solves, int tick, int S)
+{
+    using T2 = typename V2<Real>::T;
+    using TB = Tableau<RK>;
+    __shared__ double red_s[SUB][MAX_WARPS][NSLOT];
+    const TileDev tl = tiles[blockIdx.x];
+    const SolveDev &sd = solves[tl.solve];
+    const int s0 = (tick - sd.admit_tick) * S;
+    const int Nt = sd.Nt;
+    if (s0 < 0 || s0 >= Nt) return;
+    const int s1 = min(s0 + S, Nt);
+    const int nkp = sd.nk_pad, ntiles = sd.ntiles;
+    const Real *__restrict__ kc = static_cast<const Real *>(sd.kc);
+    Real *__restrict__ st = static_cast<Real *>(sd.st);
+    const T2 *__restrict__ tab = static_cast<const T2 *>(sd.tab);
+    const Real g1 = Real(sd.g1), g2 = Real(sd.g2);
+    double *partial = sd.partial;
+
+    Real c[KPT][VG_NCONST], y0[KPT][4];
+    int kidx[KPT];
+    bool ok[KPT];
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        const int local = threadIdx.x + j * blockDim.x;
+        ok[j] = local < tl.kcount;
+        kidx[j] = tl.k0 + local;
+#pragma unroll
+        for (int q = 0; q < VG_NCONST; ++q) c[j][q] = ok[j] ? kc[(size_t)q * nkp + kidx[j]] : Real(0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) y0[j][q] = ok[j] ? st[(size_t)q * nkp + kidx[j]] : Real(0);
+    }
+    TileReducer red{red_s};
+
+    for (int s = s0; s < s1; ++s) {
+        // currents and occupations at t_s, before rho advances (antelope.cpp:309-334)
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = 0.0;
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            const Real *cc = c[j];
+            const Real *yy = y0[j];
+            v[0] += double(fma(yy[VG_ZR], cc[VG_WQXR], yy[VG_ZI] * cc[VG_WQXI]));
+            v[1] += double(fma(yy[VG_ZR], cc[VG_WQYR], yy[VG_ZI] * cc[VG_WQYI]));
+            v[2] += double(fma(yy[VG_DA], cc[VG_WPX0], yy[VG_DB] * cc[VG_WPX1]));
+            v[3] += double(fma(yy[VG_DA], cc[VG_WPY0], yy[VG_DB] * cc[VG_WPY1]));
+            v[4] += double(cc[VG_W] * yy[VG_DA]);
+            v[5] += double(cc[VG_W] * yy[VG_DB]);
+            v[6] += double(cc[VG_W] * yy[VG_ZR]);
+            v[7] += double(cc[VG_W] * yy[VG_ZI]);
+        }
+        const int r = (s - s0) % SUB;
+        red.push(v, r);
+        if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
+
+        // one RK step
+        T2 A[TB::NT];
+#pragma unroll
+        for (int i = 0; i < TB::NT; ++i) A[i] = __ldg(tab + (size_t)s * TB::NT + i);
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) {
+            Real kk[TB::S][4], y[4], acc[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = y0[j][q];
+#pragma unroll
+            for (int i = 0; i < TB::S; ++i) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    Real t = y0[j][q];
+#pragma unroll
+                    for (int m = 0; m < i; ++m)
+                        if (TB::a(i, m) != 0.0) t = fma(Real(TB::a(i, m)), kk[m][q], t);
+                    y[q] = t;
+                }
+                vg_rhs<Real, G1>(c[j], A[TB::ti(i)], y, g1, g2, kk[i]);
+                if (TB::b(i) != 0.0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] = fma(Real(TB::b(i)), kk[i][q], acc[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) y0[j][q] = acc[q];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < KPT; ++j)
+        if (ok[j])
+#pragma unroll
+            for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx[j]] = y0[j][q];
+}
+
+// -------------------------------------------------------- length gauge
+// rho = al*I + s.sigma, H0(k+A) = B0*I + B.sigma.  -i[H, rho] = 2 (B x s).sigma
+// and the eigenbasis dephasing U[G o (U^dag rho U)]U^dag of SBEs.h:831-861 is
+// g1*al*I + g1*(s.n)n.sigma + g2*(s - (s.n)n).sigma with n = B/|B|.
+template <class Real>
+__device__ __forceinline__ void lw_field(const Real (&c)[LW_NCONST], const Real *ph, Real (&ca)[3], Real (&sa)[3],
+                                         Real (&cb)[3], Real (&sb)[3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        // cos/sin(k.v + A.v) from the per-k and per-stage-time factors
+        ca[i] = fma(c[LW_CA0 + i], ph[i], -(c[LW_SA0 + i] * ph[3 + i]));
+        sa[i] = fma(c[LW_SA0 + i], ph[i], c[LW_CA0 + i] * ph[3 + i]);
+        cb[i] = fma(c[LW_CB0 + i], ph[6 + i], -(c[LW_SB0 + i] * ph[9 + i]));
+        sb[i] = fma(c[LW_SB0 + i], ph[6 + i], c[LW_CB0 + i] * ph[9 + i]);
+    }
+}
+
+template <class Real, bool G1>
+__device__ __forceinline__ void lw_rhs(const Real (&c)[LW_NCONST], const Real *ph, const Real (&y)[4], Real t1dt,
+                                       Real t2sdt, Real Mdt, Real g1, Real g2, Real (&k)[4])
+{
+    Real ca[3], sa[3], cb[3], sb[3];
+    lw_field<Real>(c, ph, ca, sa, cb, sb);
+    const Real B1 = t1dt * (ca[0] + ca[1] + ca[2]);
+    const Real B2 = t1dt * (sa[0] + sa[1] + sa[2]);
+    const Real B3 = fma(-t2sdt, sb[0] + sb[1] + sb[2], Mdt);
+    const Real sx = y[LW_SX], sy = y[LW_SY], sz = y[LW_SZ];
+    const Real bb = fma(B1, B1, fma(B2, B2, B3 * B3));
+    const Real sB = fma(sx, B1, fma(sy, B2, sz * B3));
+    const Real f = bb > Real(0) ? (g2 - g1) * sB / bb : Real(0);  // (g2-g1) (s.n)/|B|
+    k[LW_AL] = G1 ? -g1 * y[LW_AL] : Real(0);
+    k[LW_SX] = fma(Real(2), fma(B2, sz, -(B3 * sy)), fma(f, B1, -g2 * sx));
+    k[LW_SY] = fma(Real(2), fma(B3, sx, -(B1 * sz)), fma(f, B2, -g2 * sy));
+    k[LW_SZ] = fma(Real(2), fma(B1, sy, -(B2 * sx)), fma(f, B3, -g2 * sz));
+}
+
+template <class Real, int RK, bool G1>
+__global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ tiles,
+                                                    const SolveDev *__restrict__ solves, int tick, int S)
+{
+    using TB = Tableau<RK>;
+    __shared__ double red_s[SUB][MAX_WARPS][NSLOT];
+    const TileDev tl = tiles[blockIdx.x];
+    const SolveDev &sd = solves[tl.solve];
+    const int s0 = (tick - sd.admit_tick) * S;
+    const int Nt = sd.Nt;
+    if (s0 < 0 || s0 >= Nt) return;
+    const int s1 = min(s0 + S, Nt);
+    const int nkp = sd.nk_pad, ntiles = sd.ntiles;
+    const Real *__restrict__ kc = static_cast<const Real *>(sd.kc);
+    Real *__restrict__ st = static_cast<Real *>(sd.st);
+    const Real *__restrict__ tab = static_cast<const Real *>(sd.tab);
+    const Real g1 = Real(sd.g1), g2 = Real(sd.g2);
+    const Real t1dt = Real(sd.t1dt), t2sdt = Real(sd.t2sdt), Mdt = Real(sd.Mdt);
+    const double t1 = sd.t1, t2c = sd.t2c, t2s = sd.t2s;
+    double va[3][2], vb[3][2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int a = 0; a < 2; ++a) { va[i][a] = sd.va[i][a]; vb[i][a] = sd.vb[i][a]; }
+
+    const int local = threadIdx.x;
+    const bool ok = local < tl.kcount;
+    const int kidx = tl.k0 + local;
+    Real c[LW_NCONST], y0[4];
+#pragma unroll
+    for (int q = 0; q < LW_NCONST; ++q) c[q] = ok ? kc[(size_t)q * nkp + kidx] : Real(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) y0[q] = ok ? st[(size_t)q * nkp + kidx] : Real(0);
+    if (!ok) c[LW_CA0] = c[LW_CB0] = Real(1);  // padding lanes: a harmless k = 0 point, weight 0
+    TileReducer red{red_s};
+
+    for (int s = s0; s < s1; ++s) {
+        const Real *row = tab + (size_t)s * TB::NT * LW_NPHASE;
+        // currents at k + A(t_s) (SBEs.h:694-760), computed in FP64
+        {
+            Real ca[3], sa[3], cb[3], sb[3];
+            lw_field<Real>(c, row, ca, sa, cb, sb);
+            double j0[2], j1[2], j2[2], j3[2];
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                j0[a] = t2c * (vb[0][a] * double(sb[0]) + vb[1][a] * double(sb[1]) + vb[2][a] * double(sb[2]));
+                j1[a] = t1 * (va[0][a] * double(sa[0]) + va[1][a] * double(sa[1]) + va[2][a] * double(sa[2]));
+                j2[a] = -t1 * (va[0][a] * double(ca[0]) + va[1][a] * double(ca[1]) + va[2][a] * double(ca[2]));
+                j3[a] = t2s * (vb[0][a] * double(cb[0]) + vb[1][a] * double(cb[1]) + vb[2][a] * double(cb[2]));
+            }
+            const double B1 = double(t1dt) * (double(ca[0]) + double(ca[1]) + double(ca[2]));
+            const double B2 = double(t1dt) * (double(sa[0]) + double(sa[1]) + double(sa[2]));
+            const double B3 = double(Mdt) - double(t2sdt) * (double(sb[0]) + double(sb[1]) + double(sb[2]));
+            const double al = y0[LW_AL], sx = y0[LW_SX], sy = y0[LW_SY], sz = y0[LW_SZ];
+            const double bb = B1 * B1 + B2 * B2 + B3 * B3;
+            const double sB = sx * B1 + sy * B2 + sz * B3;
+            const double w = c[LW_W];
+            double v[8];
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const double sj = sx * j1[a] + sy * j2[a] + sz * j3[a];
+                const double par = bb > 0.0 ? sB * (j1[a] * B1 + j2[a] * B2 + j3[a] * B3) / bb : 0.0;
+                v[a] = 2.0 * w * (sj - par);               // interband
+                v[2 + a] = 2.0 * w * (al * j0[a] + par);   // intraband
+            }
+            v[4] = w * (al + sz);
+            v[5] = w * (al - sz);
+            v[6] = w * sx;
+            v[7] = -w * sy;
+            const int r = (s - s0) % SUB;
+            red.push(v, r);
+            if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, sd.partial);
+        }
+        Real kk[TB::S][4], y[4], acc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] = y0[q];
+#pragma unroll
+        for (int i = 0; i < TB::S; ++i) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                Real t = y0[q];
+#pragma unroll
+                for (int m = 0; m < i; ++m)
+                    if (TB::a(i, m) != 0.0) t = fma(Real(TB::a(i, m)), kk[m][q], t);
+                y[q] = t;
+            }
+            lw_rhs<Real, G1>(c, row + TB::ti(i) * LW_NPHASE, y, t1dt, t2sdt, Mdt, g1, g2, kk[i]);
+            if (TB::b(i) != 0.0) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = fma(Real(TB::b(i)), kk[i][q], acc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) y0[q] = acc[q];
+    }
+    if (ok)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx] = y0[q];
+}
+
+// ------------------------------------------------------- second pass
+// One warp per (solve, step): lanes 8g..8g+7 sum slots 0..7 over tiles
+// g, g+4, g+8, ... ; two fixed shuffles combine the four groups.
+__global__ void __launch_bounds__(256) reduce_tiles(const SolveDev *__restrict__ solves,
+                                                    const int *__restrict__ solve_ids, int tick, int S)
+{
+    const SolveDev &sd = solves[solve_ids[blockIdx.y]];
+    const int s0 = (tick - sd.admit_tick) * S;
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (s0 < 0 || j >= S || s0 + j >= sd.Nt) return;
+    const int slot = lane & 7, g = lane >> 3, nt = sd.ntiles;
+    const double *p = sd.partial + (size_t)j * nt * NSLOT;
+    double acc = 0.0;
+    for (int t = g; t < nt; t += 4) acc += p[(size_t)t * NSLOT + slot];
+    acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+    if (lane < 8) sd.jout[(size_t)(s0 + j) * NSLOT + slot] = acc;
+}
+
+// ------------------------------------------------------------ set-up
+// Closed-form eigenvectors of n.sigma for unit n: |+> (eigenvalue +1) and
+// |-> (eigenvalue -1), choosing the chart that avoids 1 +/- nz -> 0.
+__device__ __forceinline__ void spinors(double nx, double ny, double nz, double2 (&up)[2], double2 (&dn)[2])
+{
+    if (nz >= 0.0) {
+        const double r = 1.0 / sqrt(2.0 * (1.0 + nz));
+        up[0] = make_double2((1.0 + nz) * r, 0.0);
+        up[1] = make_double2(nx * r, ny * r);
+        dn[0] = make_double2(-nx * r, ny * r);
+        dn[1] = make_double2((1.0 + nz) * r, 0.0);
+    } else {
+        const double r = 1.0 / sqrt(2.0 * (1.0 - nz));
+        up[0] = make_double2(nx * r, -ny * r);
+        up[1] = make_double2((1.0 - nz) * r, 0.0);
+        dn[0] = make_double2((1.0 - nz) * r, 0.0);
+        dn[1] = make_double2(-nx * r, -ny * r);
+    }
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconjmul(double2 a, double2 b)  // conj(a) * b
+{
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
+template <class Real>
+__global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restrict__ kc, Real *__restrict__ st,
+                                                    double *__restrict__ constpart)
+{
+    // one block per tile; threads loop over the tile's k-points
+    const int tile = blockIdx.x;
+    const int k0 = tile * ia.tile_k;
+    const int k1 = min(k0 + ia.tile_k, ia.nk);
+    double cp[4] = {0, 0, 0, 0};  // sum w rho0 P00/P11 (x, y), sum w rho0_00, sum w rho0_11
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        // momaxis grid point and weight
+        const int N0 = ia.N[0], N1 = ia.N[1], N2 = ia.N[2];
+        const int ii[3] = {k / (N1 * N2), (k / N2) % N1, k % N2};
+        const int NN[3] = {N0, N1, N2};
+        double f[3], w = 1.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            f[d] = (NN[d] == 1) ? 0.0 : double(ii[d]) / (NN[d] - 1) - 0.5;
+            if (NN[d] != 1 && (ii[d] == 0 || ii[d] == NN[d] - 1)) w /= 2;
+        }
+        double kv[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            kv[d] = ia.origin[d] + f[0] * ia.axes[0 * 3 + d] + f[1] * ia.axes[1 * 3 + d] + f[2] * ia.axes[2 * 3 + d];
+        // Haldane B(k) and J(k) = -dH/dk
+        double ca[3], sa[3], cb[3], sb[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double aa = kv[0] * ia.va[i][0] + kv[1] * ia.va[i][1];
+            const double ab = kv[0] * ia.vb[i][0] + kv[1] * ia.vb[i][1];
+            sincos(aa, &sa[i], &ca[i]);
+            sincos(ab, &sb[i], &cb[i]);
+        }
+        const double t2c = 2.0 * ia.t2 * cos(ia.phi0), t2s = 2.0 * ia.t2 * sin(ia.phi0);
+        const double B0 = t2c * (cb[0] + cb[1] + cb[2]);
+        const double B1 = ia.t1 * (ca[0] + ca[1] + ca[2]);
+        const double B2 = ia.t1 * (sa[0] + sa[1] + sa[2]);
+        const double B3 = ia.M0 - t2s * (sb[0] + sb[1] + sb[2]);
+        const double bn = sqrt(B1 * B1 + B2 * B2 + B3 * B3);
+        double nx = 0.0, ny = 0.0, nz = 1.0;
+        if (bn > 0.0) { nx = B1 / bn; ny = B2 / bn; nz = B3 / bn; }
+        const double e0 = B0 - bn, e1 = B0 + bn;   // ascending, as zheevr
+        double f0, f1;                             // rho0 in the band basis
+        if (ia.use_fermi) {
+            const double kT = 300. / 3.15775024804e5;
+            const double o0 = 1.0 / (exp((e0 - ia.Ef) / kT) + 1.0), o1 = 1.0 / (exp((e1 - ia.Ef) / kT) + 1.0);
+            f0 = o0 / (o0 + o1);
+            f1 = o1 / (o0 + o1);
+        } else {
+            f0 = ia.nval >= 1 ? 1.0 : 0.0;
+            f1 = ia.nval >= 2 ? 1.0 : 0.0;
+        }
+        const size_t P = ia.nk_pad;
+        if (ia.variant == VAR_HALDANE_VG) {
+            double j0[2], jv[2][3];
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                j0[a] = t2c * (ia.vb[0][a] * sb[0] + ia.vb[1][a] * sb[1] + ia.vb[2][a] * sb[2]);
+                jv[a][0] = ia.t1 * (ia.va[0][a] * sa[0] + ia.va[1][a] * sa[1] + ia.va[2][a] * sa[2]);
+                jv[a][1] = -ia.t1 * (ia.va[0][a] * ca[0] + ia.va[1][a] * ca[1] + ia.va[2][a] * ca[2]);
+                jv[a][2] = t2s * (ia.vb[0][a] * cb[0] + ia.vb[1][a] * cb[1] + ia.vb[2][a] * cb[2]);
+            }
+            double2 up[2], dn[2];
+            spinors(nx, ny, nz, up, dn);
+            double P00[2], P11[2];
+            double2 P01[2];
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const double jn = jv[a][0] * nx + jv[a][1] * ny + jv[a][2] * nz;
+                P00[a] = j0[a] - jn;
+                P11[a] = j0[a] + jn;
+                // <-| j.sigma |+>
+                const double2 m00 = make_double2(jv[a][2], 0.0), m11 = make_double2(-jv[a][2], 0.0);
+                const double2 m01 = make_double2(jv[a][0], -jv[a][1]), m10 = make_double2(jv[a][0], jv[a][1]);
+                const double2 v0 = make_double2(cmul(m00, up[0]).x + cmul(m01, up[1]).x,
+                                                cmul(m00, up[0]).y + cmul(m01, up[1]).y);
+                const double2 v1 = make_double2(cmul(m10, up[0]).x + cmul(m11, up[1]).x,
+                                                cmul(m10, up[0]).y + cmul(m11, up[1]).y);
+                const double2 q0 = cconjmul(dn[0], v0), q1 = cconjmul(dn[1], v1);
+                P01[a] = make_double2(q0.x + q1.x, q0.y + q1.y);
+            }
+            const double dt = ia.dt;
+            const double cv[VG_NCONST] = {
+                dt * (e0 - e1),
+                dt * (P00[0] - P11[0]), dt * (P00[1] - P11[1]),
+                dt * P01[0].x, dt * P01[0].y, dt * P01[1].x, dt * P01[1].y,
+                f1 - f0,
+                w * P00[0], w * P11[0], w * P00[1], w * P11[1],
+                2.0 * w * P01[0].x, 2.0 * w * P01[0].y, 2.0 * w * P01[1].x, 2.0 * w * P01[1].y,
+                w};
+#pragma unroll
+            for (int q = 0; q < VG_NCONST; ++q) kc[q * P + k] = Real(cv[q]);
+#pragma unroll
+            for (int q = 0; q < VG_NSTATE; ++q) st[q * P + k] = Real(0);
+            cp[0] += w * (f0 * P00[0] + f1 * P11[0]);
+            cp[1] += w * (f0 * P00[1] + f1 * P11[1]);
+            cp[2] += w * f0;
+            cp[3] += w * f1;
+        } else {
+            const double cv[LW_NCONST] = {ca[0], ca[1], ca[2], sa[0], sa[1], sa[2],
+                                          cb[0], cb[1], cb[2], sb[0], sb[1], sb[2], w};
+#pragma unroll
+            for (int q = 0; q < LW_NCONST; ++q) kc[q * P + k] = Real(cv[q]);
+            // rho0 = f0 |-><-| + f1 |+><+| = (f0+f1)/2 I + (f1-f0)/2 n.sigma (SBEs.h:352-356)
+            st[LW_AL * P + k] = Real(0.5 * (f0 + f1));
+            st[LW_SX * P + k] = Real(0.5 * (f1 - f0) * nx);
+            st[LW_SY * P + k] = Real(0.5 * (f1 - f0) * ny);
+            st[LW_SZ * P + k] = Real(0.5 * (f1 - f0) * nz);
+        }
+    }
+    // deterministic block sum of the constant parts -> constpart[tile][8]
+    __shared__ double sh[256][4];
+    for (int q = 0; q < 4; ++q) sh[threadIdx.x][q] = cp[q];
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off)
+            for (int q = 0; q < 4; ++q) sh[threadIdx.x][q] += sh[threadIdx.x + off][q];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double *o = constpart + (size_t)tile * NSLOT;
+        o[0] = 0.0; o[1] = 0.0;
+        o[2] = sh[0][0]; o[3] = sh[0][1];
+        o[4] = sh[0][2]; o[5] = sh[0][3];
+        o[6] = 0.0; o[7] = 0.0;
+    }
+}
+
+// ------------------------------------------------- FMA peak microbench
+// Independent FMA chains (8 per thread) to measure the FP64 / FP32 vector
+// pipe peaks that the roofline fractions are quoted against.
+template <class Real>
+__global__ void __launch_bounds__(256) fma_peak(Real *out, int iters, Real a, Real b)
+{
+    Real x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = Real(threadIdx.x + i) * Real(1e-3);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = fma(x[i], a, b);
+    }
+    Real s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += x[i];
+    if (s == Real(-12345.678)) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+// ------------------------------------------------------------- launchers
+#define SBE_CHECK_LAUNCH() return cudaGetLastError()
+
+template <class Real, int RK, int KPT>
+static cudaError_t launch_vg_t(const LaunchArgs &la, bool g1)
+{
+    if (g1)
+        propagate_vg<Real, RK, KPT, true><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+    else
+        propagate_vg<Real, RK, KPT, false><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+    SBE_CHECK_LAUNCH();
+}
+
+template <class Real, int RK>
+static cudaError_t launch_lw_t(const LaunchArgs &la, bool g1)
+{
+    if (g1)
+        propagate_lw<Real, RK, true><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+    else
+        propagate_lw<Real, RK, false><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+    SBE_CHECK_LAUNCH();
+}
+
+cudaError_t launch_propagate(const LaunchArgs &la)
+{
+    if (la.ntiles <= 0) return cudaSuccess;
+    if (la.threads <= 0 || la.threads > 256 || (la.threads & 31)) return cudaErrorInvalidValue;
+    const bool g1 = la.has_g1;
+    if (la.variant == VAR_HALDANE_VG) {
+#define SBE_VG(R, RK)                                                       \
+    switch (la.kpt) {                                                       \
+        case 1: return launch_vg_t<R, RK, 1>(la, g1);                       \
+        case 2: return launch_vg_t<R, RK, 2>(la, g1);                       \
+        default: return cudaErrorInvalidValue;                              \
+    }
+        if (la.precision == PREC_FP64) {
+            if (la.rk == 4) { SBE_VG(double, 4) } else if (la.rk == 5) { SBE_VG(double, 5) }
+        } else {
+            if (la.rk == 4) { SBE_VG(float, 4) } else if (la.rk == 5) { SBE_VG(float, 5) }
+        }
+#undef SBE_VG
+        return cudaErrorInvalidValue;
+    }
+    if (la.variant == VAR_HALDANE_LW) {
+        if (la.kpt != 1) return cudaErrorInvalidValue;
+        if (la.precision == PREC_FP64) {
+            if (la.rk == 4) return launch_lw_t<double, 4>(la, g1);
+            if (la.rk == 5) return launch_lw_t<double, 5>(la, g1);
+        } else {
+            if (la.rk == 4) return launch_lw_t<float, 4>(la, g1);
+            if (la.rk == 5) return launch_lw_t<float, 5>(la, g1);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_reduce(const SolveDev *solves, const int *solve_ids, int nsolves, int tick, int S,
+                          cudaStream_t stream)
+{
+    if (nsolves <= 0) return cudaSuccess;
+    const int warps = 8;
+    dim3 grid((S + warps - 1) / warps, nsolves);
+    reduce_tiles<<<grid, warps * 32, 0, stream>>>(solves, solve_ids, tick, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_haldane(const InitArgs &ia, int precision, void *kc, void *st, double *constpart,
+                                cudaStream_t stream)
+{
+    const int ntiles = (ia.nk + ia.tile_k - 1) / ia.tile_k;
+    if (precision == PREC_FP64)
+        init_haldane<double><<<ntiles, 256, 0, stream>>>(ia, static_cast<double *>(kc), static_cast<double *>(st),
+                                                         constpart);
+    else
+        init_haldane<float><<<ntiles, 256, 0, stream>>>(ia, static_cast<float *>(kc), static_cast<float *>(st),
+                                                        constpart);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fma_peak(int which, int blocks, int iters, void *out, cudaStream_t stream)
+{
+    if (which == 0) fma_peak<double><<<blocks, 256, 0, stream>>>(static_cast<double *>(out), iters, 0.999999, 1e-7);
+    else fma_peak<float><<<blocks, 256, 0, stream>>>(static_cast<float *>(out), iters, 0.999999f, 1e-7f);
+    return cudaGetLastError();
+}
+
+}  // namespace sbe

@@ -1,0 +1,36 @@
+// Launch interface between the host engine (sbe_engine.cpp) and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sbe_dev.h"
+
+namespace sbe {
+
+struct LaunchArgs {
+    const TileDev *tiles;    // device array of the tiles to advance
+    const SolveDev *solves;  // device array of solve descriptors
+    int ntiles;              // grid size (one CTA per tile)
+    int threads;             // CTA size: tile_k / kpt, multiple of 32, <= 256
+    int tick, S;             // launch index and steps per launch
+    int variant, precision, rk, kpt;
+    bool has_g1;             // T1 dephasing active
+    cudaStream_t stream;
+};
+
+struct InitArgs {
+    int nk, nk_pad, tile_k, variant, nval, use_fermi;
+    int N[3];
+    double axes[9], origin[3];
+    double t1, t2, M0, phi0, va[3][2], vb[3][2];
+    double Ef, dt;
+};
+
+cudaError_t launch_propagate(const LaunchArgs &la);
+cudaError_t launch_reduce(const SolveDev *solves, const int *solve_ids, int nsolves, int tick, int S,
+                          cudaStream_t stream);
+cudaError_t launch_init_haldane(const InitArgs &ia, int precision, void *kc, void *st, double *constpart,
+                                cudaStream_t stream);
+cudaError_t launch_fma_peak(int which, int blocks, int iters, void *out, cudaStream_t stream);
+
+}  // namespace sbe

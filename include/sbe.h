@@ -1,0 +1,158 @@
+/*
+ * sbe.h -- C ABI of the B200 SBE propagator (antelope_b200/libsbe_b200.so).
+ *
+ * Drop-in for the time propagation of ftachacon/antelope (src/GeneralModel).
+ * The reference drives its solver per (time step, k-point) from main():
+ *
+ *   SBEs(const libconfig::Setting*, GaugeType, int idx_start, int idx_end)  SBEs.h:102,125-430
+ *   void RunSBEs(int kindex, double t)                                      SBEs.h:105,596-624
+ *   std::tuple<...> GenInterIntraCurrent(int kindex, double t)              SBEs.h:108,694-760
+ *   std::array<double,3> GenCurrent(int kindex, double t)                   SBEs.h:107,626-693
+ *   time/k loop, k-sum, MPI reduce and file output                          antelope.cpp:297-548
+ *
+ * A per-(k, t) call cannot cross a device boundary efficiently, so this ABI
+ * replaces that whole loop with whole-solve calls: a problem is built from
+ * the same inputParam.cfg, a solver runs every time step on the GPU with the
+ * k-sum fused into the kernels, and the caller receives the same arrays the
+ * reference writes to its .dat files.  Plain C types only; no pointer passed
+ * in is retained after a call returns (except the problems of a batch, see
+ * below).  Errors never exit the process: every call returns an sbe_status
+ * and sets a thread-local message (sbe_last_error_message()).
+ */
+#ifndef SBE_B200_H
+#define SBE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SBE_ABI_VERSION 1
+
+typedef enum sbe_status {
+    SBE_OK = 0,
+    SBE_BAD_CONFIG = 1,       /* the reference would exit(EXIT_FAILURE) on this input */
+    SBE_UNSUPPORTED = 2,      /* valid input that this library does not build */
+    SBE_OOM = 3,              /* device memory exhausted or admission refused */
+    SBE_CUDA_ERROR = 4,
+    SBE_TIMEOUT = 5,
+    SBE_CANCELLED = 6,
+    SBE_INVALID_ARGUMENT = 7,
+    SBE_NOT_READY = 8
+} sbe_status;
+
+typedef struct sbe_problem sbe_problem;
+typedef struct sbe_solver sbe_solver;
+typedef struct sbe_batch sbe_batch;
+typedef struct sbe_server sbe_server;
+
+/* Sizes of a problem: output arrays are Nt rows.  gauge: 0 LengthWannier,
+ * 1 LengthHamiltonian, 2 Velocity (constant.h:41-46); rk: 4, 5 or 45. */
+typedef struct sbe_dims {
+    int Nt, nband, nval, ntotal;
+    int Nk[3];
+    int gauge, rk, precision, model, inter_intra;
+    double atmin, dt, dV, total_weight;
+} sbe_dims;
+
+/* Run options.  precision: -1 = calc.precision of the cfg (default fp64),
+ * 0 = plain FP64, 1 = mixed FP32 stages / FP64 sums.  tile_k, k_per_thread,
+ * steps_per_launch: 0 = tuned defaults.  use_graph: capture the launches of
+ * a run into one CUDA graph. */
+typedef struct sbe_opts {
+    int device;
+    int precision;
+    int tile_k;
+    int k_per_thread;
+    int steps_per_launch;
+    int use_graph;
+} sbe_opts;
+
+/* Caller-owned host arrays (any may be NULL):
+ *   inter[Nt*3]  columns of interband_dipole_full_evol.dat  (antelope.cpp:522-527)
+ *   intra[Nt*3]  columns of intraband_current_full_evol.dat (antelope.cpp:522-527)
+ *   occ[Nt*(N+1)] columns of occupation__full__evol.dat      (antelope.cpp:530-536)
+ *   coh[Nt*2]    columns of coherence__full__evol.dat       (antelope.cpp:538-542)
+ *   laser[Nt*7]  t, E[3], A[3] of outlaserdata.dat           (antelope.cpp:208-235) */
+typedef struct sbe_outputs {
+    double *inter;
+    double *intra;
+    double *occ;
+    double *coh;
+    double *laser;
+} sbe_outputs;
+
+int sbe_abi_version(void);
+const char *sbe_last_error_message(void);
+void sbe_opts_default(sbe_opts *opts);
+
+/* Parse an inputParam.cfg (libconfig text; antelope.cpp:90-129 and the
+ * SBEs constructor's reads, SBEs.h:125-241, 432-561).  Same keys, defaults
+ * and diagnostics as the reference, plus additive keys: env_name "sin2",
+ * calc.precision "fp64"|"mixed", calc.rk "rk4"|"rk5"|"cashkarp45", calc.tol. */
+sbe_status sbe_problem_from_cfg(const char *path, sbe_problem **out);
+sbe_status sbe_problem_from_string(const char *text, sbe_problem **out);
+sbe_status sbe_problem_dims(const sbe_problem *p, sbe_dims *out);
+/* Host-only: the columns of outlaserdata.dat (t, E[3], A[3]) into laser[Nt*7]
+ * (antelope.cpp:208-235; laser.h:278-322).  Needs no GPU. */
+sbe_status sbe_problem_laser(const sbe_problem *p, double *laser);
+void sbe_problem_destroy(sbe_problem *p);
+
+/* One solve (replaces SBEs + the driver loop of antelope.cpp:297-548). */
+sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *opts, sbe_solver **out);
+/* Enqueue the whole propagation on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream).  Returns without waiting for the GPU. */
+sbe_status sbe_solver_run(sbe_solver *s, void *stream);
+/* Wait for the run and fill the caller's host arrays. */
+sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out);
+/* Number of propagate kernel launches the last run issued. */
+int sbe_solver_launches(const sbe_solver *s);
+void sbe_solver_destroy(sbe_solver *s);
+
+/* Write the reference's six output files into `dir` (antelope.cpp:176-184,
+ * 208-235, 514-548) from arrays filled by a get call. */
+sbe_status sbe_write_outputs(const sbe_problem *p, const sbe_outputs *o, const char *dir);
+/* The whole drop-in: read `cfg_path`, solve on the GPU, write the files in
+ * `out_dir` (the reference reads ./inputParam.cfg and writes to ./). */
+sbe_status sbe_run_cfg(const char *cfg_path, const char *out_dir, const sbe_opts *opts);
+
+/* Many solves with their own grids, pulses and model parameters advanced
+ * together (one launch per launch class per step chunk).  The problems must
+ * stay alive until sbe_batch_destroy. */
+sbe_status sbe_batch_create(const sbe_problem *const *problems, int n, const sbe_opts *opts, sbe_batch **out);
+sbe_status sbe_batch_run(sbe_batch *b, void *stream);
+sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *out);
+int sbe_batch_launches(const sbe_batch *b);
+void sbe_batch_destroy(sbe_batch *b);
+
+/* Continuous-batching server: a worker thread admits submitted solves while
+ * device memory allows, advances all resident solves together, and retires
+ * them as they finish.  Thread-safe. */
+typedef struct sbe_server_opts {
+    int device;
+    int precision;
+    int steps_per_launch;
+    int max_resident;          /* 0 = no limit besides memory */
+    double mem_budget_bytes;   /* 0 = free device memory minus 4 GiB */
+    int tile_k;
+    int k_per_thread;
+} sbe_server_opts;
+
+sbe_status sbe_server_create(const sbe_server_opts *opts, sbe_server **out);
+sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, long long *request_id);
+/* Wait up to timeout_s (< 0: forever) for a request; fill its outputs and
+ * its latency (submit -> result available, seconds). */
+sbe_status sbe_server_wait(sbe_server *s, long long request_id, double timeout_s, const sbe_outputs *out,
+                           double *latency_s);
+sbe_status sbe_server_cancel(sbe_server *s, long long request_id);
+/* Counters: submitted, completed, failed, resident now, launches issued. */
+sbe_status sbe_server_stats(sbe_server *s, long long counters[5]);
+void sbe_server_destroy(sbe_server *s);
+
+/* Measured FP64 / FP32 FMA pipe peaks of the device (TFLOP/s), the
+ * denominators of the roofline fractions.  No reference counterpart. */
+sbe_status sbe_measure_fma_peaks(int device, double *fp64_tflops, double *fp32_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
