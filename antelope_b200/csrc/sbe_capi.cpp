@@ -236,7 +236,7 @@ extern "C" sbe_status sbe_solver_run(sbe_solver *s, void *stream)
     if (s->ran) return fail(SBE_INVALID_ARGUMENT, "a solver runs once; create a new one");
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
-        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->own;
         cuda_check(cudaStreamWaitEvent(st, s->ready, 0), "stream wait");
         s->eng->set_stream(st);
         run_engine(*s->eng, s->use_graph, &s->launches);
@@ -358,7 +358,7 @@ extern "C" sbe_status sbe_batch_run(sbe_batch *b, void *stream)
     if (b->ran) return fail(SBE_INVALID_ARGUMENT, "a batch runs once; create a new one");
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
-        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->own;
         cuda_check(cudaStreamWaitEvent(st, b->ready, 0), "stream wait");
         b->eng->set_stream(st);
         run_engine(*b->eng, b->use_graph, &b->launches);

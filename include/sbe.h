@@ -100,7 +100,7 @@ void sbe_problem_destroy(sbe_problem *p);
 /* One solve (replaces SBEs + the driver loop of antelope.cpp:297-548). */
 sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *opts, sbe_solver **out);
 /* Enqueue the whole propagation on `stream` (a cudaStream_t; NULL = the
- * legacy default stream).  Returns without waiting for the GPU. */
+ * solver's own stream).  Returns without waiting for the GPU. */
 sbe_status sbe_solver_run(sbe_solver *s, void *stream);
 /* Wait for the run and fill the caller's host arrays. */
 sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out);
