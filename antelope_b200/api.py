@@ -28,14 +28,24 @@ def _check(st: int):
         raise SbeError(st, lib.sbe_last_error_message().decode(errors="replace"))
 
 
-def _opts(precision=None, tile_k=0, k_per_thread=0, steps_per_launch=0, use_graph=False, device=0):
+def _opts(precision=None, tile_k=0, k_per_thread=0, steps_per_launch=0, use_graph=False, device=0,
+          profile=False):
     o = Opts()
     lib.sbe_opts_default(C.byref(o))
     o.device = device
     o.precision = -1 if precision is None else {"fp64": 0, "mixed": 1, 0: 0, 1: 1}[precision]
     o.tile_k, o.k_per_thread, o.steps_per_launch = tile_k, k_per_thread, steps_per_launch
     o.use_graph = 1 if use_graph else 0
+    o.profile = 1 if profile else 0
     return o
+
+
+def _kernel_times(fn, h):
+    pm, rm = C.c_double(0), C.c_double(0)
+    pn, rn = C.c_int(0), C.c_int(0)
+    _check(fn(h, C.byref(pm), C.byref(pn), C.byref(rm), C.byref(rn)))
+    return {"propagate_ms": pm.value, "propagate_launches": pn.value, "reduce_ms": rm.value,
+            "reduce_launches": rn.value}
 
 
 @dataclass
@@ -120,6 +130,9 @@ class Solver:
     def launches(self) -> int:
         return lib.sbe_solver_launches(self._h)
 
+    def kernel_times(self) -> dict:
+        return _kernel_times(lib.sbe_solver_kernel_times, self._h)
+
     def close(self):
         if getattr(self, "_h", None):
             lib.sbe_solver_destroy(self._h)
@@ -171,6 +184,9 @@ class Batch:
     @property
     def launches(self) -> int:
         return lib.sbe_batch_launches(self._h)
+
+    def kernel_times(self) -> dict:
+        return _kernel_times(lib.sbe_batch_kernel_times, self._h)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -25,7 +25,8 @@ class Dims(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int), ("tile_k", C.c_int),
-                ("k_per_thread", C.c_int), ("steps_per_launch", C.c_int), ("use_graph", C.c_int)]
+                ("k_per_thread", C.c_int), ("steps_per_launch", C.c_int), ("use_graph", C.c_int),
+                ("profile", C.c_int)]
 
 
 class COutputs(C.Structure):
@@ -60,6 +61,10 @@ def _load():
         "sbe_solver_get": (C.c_int, [P, C.POINTER(COutputs)]),
         "sbe_solver_launches": (C.c_int, [P]),
         "sbe_solver_destroy": (None, [P]),
+        "sbe_solver_kernel_times": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                              C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+        "sbe_batch_kernel_times": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_double), C.POINTER(C.c_int)]),
         "sbe_write_outputs": (C.c_int, [P, C.POINTER(COutputs), C.c_char_p]),
         "sbe_run_cfg": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Opts)]),
         "sbe_batch_create": (C.c_int, [C.POINTER(P), C.c_int, C.POINTER(Opts), C.POINTER(P)]),

@@ -224,7 +224,8 @@ extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *op
         s->eng = std::make_unique<Engine>(s->device, s->own, default_steps(opts));
         s->id = s->eng->add(p->p, to_engine_opts(opts));
         cuda_check(cudaEventRecord(s->ready, s->own), "event record");
-        s->use_graph = opts && opts->use_graph;
+        s->use_graph = opts && opts->use_graph && !opts->profile;
+        s->eng->set_profile(opts && opts->profile);
         *out = s.release();
         return SBE_OK;
     });
@@ -259,6 +260,15 @@ extern "C" sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out)
 }
 
 extern "C" int sbe_solver_launches(const sbe_solver *s) { return s ? s->launches : 0; }
+
+extern "C" sbe_status sbe_solver_kernel_times(sbe_solver *s, double *pms, int *pn, double *rms, int *rn)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null solver");
+    return guard([&]() -> sbe_status {
+        s->eng->kernel_times(pms, pn, rms, rn);
+        return SBE_OK;
+    });
+}
 
 extern "C" void sbe_solver_destroy(sbe_solver *s)
 {
@@ -346,7 +356,8 @@ extern "C" sbe_status sbe_batch_create(const sbe_problem *const *problems, int n
         EngineOptions eo = to_engine_opts(opts);
         for (int i : order) b->ids[i] = b->eng->add(problems[i]->p, eo);
         cuda_check(cudaEventRecord(b->ready, b->own), "event record");
-        b->use_graph = opts && opts->use_graph;
+        b->use_graph = opts && opts->use_graph && !opts->profile;
+        b->eng->set_profile(opts && opts->profile);
         *out = b.release();
         return SBE_OK;
     });
@@ -380,6 +391,15 @@ extern "C" sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *
 }
 
 extern "C" int sbe_batch_launches(const sbe_batch *b) { return b ? b->launches : 0; }
+
+extern "C" sbe_status sbe_batch_kernel_times(sbe_batch *b, double *pms, int *pn, double *rms, int *rn)
+{
+    if (!b) return fail(SBE_INVALID_ARGUMENT, "null batch");
+    return guard([&]() -> sbe_status {
+        b->eng->kernel_times(pms, pn, rms, rn);
+        return SBE_OK;
+    });
+}
 
 extern "C" void sbe_batch_destroy(sbe_batch *b)
 {

@@ -80,6 +80,8 @@ Engine::~Engine()
         if (s.ev) cudaEventDestroy(s.ev);
     }
     for (auto &kv : groups_) cudaFree(kv.second->d_tiles);
+    for (auto &e : prop_ev_) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    for (auto &e : red_ev_) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     cudaStreamSynchronize(stream_);
     cudaFree(d_solves_);
     cudaFreeHost(h_solves_);
@@ -112,7 +114,7 @@ size_t Engine::bytes_needed(const Problem &p, const EngineOptions &o) const
     const bool vg = p.gauge == GAUGE_VELOCITY;
     const size_t nc = vg ? (size_t)VG_NCONST : (size_t)LW_NCONST, ns = 4;
     const size_t tab = (size_t)p.laser.Nt * nts * (vg ? 2 : LW_NPHASE) * real;
-    return (nc + ns) * nk_pad * real + tab + (size_t)S_ * ntiles * NSLOT * 8 + (size_t)p.laser.Nt * NSLOT * 8 +
+    return nc * nk_pad * real + ns * nk_pad * 8 + tab + (size_t)S_ * ntiles * NSLOT * 8 + (size_t)p.laser.Nt * NSLOT * 8 +
            (size_t)ntiles * NSLOT * 8;
 }
 
@@ -138,7 +140,7 @@ int Engine::add(const Problem &p, const EngineOptions &o)
     const size_t real = s->precision == PREC_FP64 ? 8 : 4;
     const bool vg = s->variant == VAR_HALDANE_VG;
     const size_t nc = vg ? (size_t)VG_NCONST : (size_t)LW_NCONST;
-    const size_t kc_b = nc * s->nk_pad * real, st_b = 4 * (size_t)s->nk_pad * real;
+    const size_t kc_b = nc * s->nk_pad * real, st_b = 4 * (size_t)s->nk_pad * 8;  // state is FP64 in both methods
     const size_t tab_n = (size_t)s->Nt * s->nts * (vg ? 2 : LW_NPHASE);
     const size_t part_b = (size_t)S_ * s->ntiles * NSLOT * 8, jout_b = (size_t)s->Nt * NSLOT * 8;
     const size_t cp_b = (size_t)s->ntiles * NSLOT * 8;
@@ -336,11 +338,59 @@ void Engine::step_frozen()
         la.kpt = g.kpt;
         la.has_g1 = g.g1;
         la.stream = stream_;
+        std::pair<cudaEvent_t, cudaEvent_t> ev{};
+        if (profile_) {
+            ev = new_pair();
+            cuda_check(cudaEventRecord(ev.first, stream_), "event record");
+        }
         cuda_check(launch_propagate(la), "propagate launch");
+        if (profile_) {
+            cuda_check(cudaEventRecord(ev.second, stream_), "event record");
+            prop_ev_.push_back(ev);
+        }
         ++last_launches_;
     }
-    if (nids_ > 0) cuda_check(launch_reduce(d_solves_, d_ids_, nids_, tick_, S_, stream_), "reduce launch");
+    if (nids_ > 0) {
+        std::pair<cudaEvent_t, cudaEvent_t> ev{};
+        if (profile_) {
+            ev = new_pair();
+            cuda_check(cudaEventRecord(ev.first, stream_), "event record");
+        }
+        cuda_check(launch_reduce(d_solves_, d_ids_, nids_, tick_, S_, stream_), "reduce launch");
+        if (profile_) {
+            cuda_check(cudaEventRecord(ev.second, stream_), "event record");
+            red_ev_.push_back(ev);
+        }
+    }
     ++tick_;
+}
+
+std::pair<cudaEvent_t, cudaEvent_t> Engine::new_pair()
+{
+    std::pair<cudaEvent_t, cudaEvent_t> p;
+    cuda_check(cudaEventCreate(&p.first), "event create");
+    cuda_check(cudaEventCreate(&p.second), "event create");
+    return p;
+}
+
+void Engine::kernel_times(double *prop_ms, int *prop_n, double *red_ms, int *red_n)
+{
+    auto total = [&](std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &v, double *ms, int *n) {
+        double t = 0.0;
+        for (auto &e : v) {
+            cuda_check(cudaEventSynchronize(e.second), "event sync");
+            float x = 0.f;
+            cuda_check(cudaEventElapsedTime(&x, e.first, e.second), "event elapsed");
+            t += x;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        if (ms) *ms = t;
+        if (n) *n = (int)v.size();
+        v.clear();
+    };
+    total(prop_ev_, prop_ms, prop_n);
+    total(red_ev_, red_ms, red_n);
 }
 
 void Engine::fetch_async(int id)

@@ -82,6 +82,10 @@ public:
     size_t bytes_in_use() const { return bytes_in_use_; }
     // Number of propagate launches issued by the last step() (telemetry).
     int last_launches() const { return last_launches_; }
+    // CUDA-event timing of every propagate / reduce launch (telemetry for the
+    // roofline; off by default, not usable under graph capture).
+    void set_profile(bool on) { profile_ = on; }
+    void kernel_times(double *prop_ms, int *prop_n, double *red_ms, int *red_n);
     // Launch shape the engine would use for a solve.
     Shape shape_for(const Problem &p, const EngineOptions &o) const;
 
@@ -100,6 +104,9 @@ private:
     int capacity_ = 0;
     bool dirty_ = true;
     int last_launches_ = 0;
+    bool profile_ = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prop_ev_, red_ev_;
+    std::pair<cudaEvent_t, cudaEvent_t> new_pair();
     size_t bytes_in_use_ = 0;
     std::map<int, std::unique_ptr<Solve>> live_;
     std::vector<int> free_slots_;

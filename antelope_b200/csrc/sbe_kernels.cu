@@ -18,14 +18,18 @@
 //   reduce_tiles      deterministic second pass: tile partials -> per-step sums.
 //
 // Precision: every kernel is a template on Real.  Real = double is the plain
-// FP64 method.  Real = float is the mixed method: RK stages in FP32, the A(t)
-// table computed in FP64 on the host then rounded per stage, and the k-sum of
-// the currents accumulated in FP64 from the warp level up.  In the velocity
-// gauge the state is the deviation rho - rho0 (small), so FP32 rounding acts
-// on the deviation only; the time-independent rho0 parts of the currents are
-// summed once, in FP64.
+// FP64 method.  Real = float is the mixed method: the RK stages and the step
+// increment in FP32, the per-k state kept in FP64 (the increment is added in
+// FP64 once per step -- rounding the state itself to FP32 every step is what
+// limits an all-FP32 propagation), the A(t) table computed in FP64 on the
+// host and rounded per stage, and the k-sum of the currents accumulated in
+// FP64 from the warp level up.  In the velocity gauge the state is the
+// deviation rho - rho0, and the time-independent rho0 parts of the currents
+// are summed once, in FP64.
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include "sbe_dev.h"
 #include "sbe_kernels.h"
@@ -157,6 +161,7 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 {
     using T2 = typename V2<Real>::T;
     using TB = Tableau<RK>;
+    constexpr bool F64 = std::is_same<Real, double>::value;
     __shared__ double red_s[SUB][MAX_WARPS][NSLOT];
     const TileDev tl = tiles[blockIdx.x];
     const SolveDev &sd = solves[tl.solve];
@@ -166,12 +171,16 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
     const int s1 = min(s0 + S, Nt);
     const int nkp = sd.nk_pad, ntiles = sd.ntiles;
     const Real *__restrict__ kc = static_cast<const Real *>(sd.kc);
-    Real *__restrict__ st = static_cast<Real *>(sd.st);
+    double *__restrict__ st = static_cast<double *>(sd.st);
     const T2 *__restrict__ tab = static_cast<const T2 *>(sd.tab);
     const Real g1 = Real(sd.g1), g2 = Real(sd.g2);
     double *partial = sd.partial;
 
-    Real c[KPT][VG_NCONST], y0[KPT][4];
+    // the state (rho - rho0) is kept in FP64 in both methods; the mixed
+    // method rounds it to FP32 once per step for the stage arithmetic and
+    // adds the FP32 step increment back in FP64
+    Real c[KPT][VG_NCONST];
+    double y64[KPT][4];
     int kidx[KPT];
     bool ok[KPT];
 #pragma unroll
@@ -182,11 +191,16 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 #pragma unroll
         for (int q = 0; q < VG_NCONST; ++q) c[j][q] = ok[j] ? kc[(size_t)q * nkp + kidx[j]] : Real(0);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) y0[j][q] = ok[j] ? st[(size_t)q * nkp + kidx[j]] : Real(0);
+        for (int q = 0; q < 4; ++q) y64[j][q] = ok[j] ? st[(size_t)q * nkp + kidx[j]] : 0.0;
     }
     TileReducer red{red_s};
 
     for (int s = s0; s < s1; ++s) {
+        Real y0[KPT][4];
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) y0[j][q] = Real(y64[j][q]);
         // currents and occupations at t_s, before rho advances (antelope.cpp:309-334)
         double v[8];
 #pragma unroll
@@ -214,9 +228,11 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
         for (int i = 0; i < TB::NT; ++i) A[i] = __ldg(tab + (size_t)s * TB::NT + i);
 #pragma unroll
         for (int j = 0; j < KPT; ++j) {
+            // FP64: acc = rho + sum_i dt b_i k_i in the reference's order
+            // (SBEs.h:614-623); mixed: the sum is formed in FP32 first
             Real kk[TB::S][4], y[4], acc[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = y0[j][q];
+            for (int q = 0; q < 4; ++q) acc[q] = F64 ? y0[j][q] : Real(0);
 #pragma unroll
             for (int i = 0; i < TB::S; ++i) {
 #pragma unroll
@@ -234,14 +250,14 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) y0[j][q] = acc[q];
+            for (int q = 0; q < 4; ++q) y64[j][q] = F64 ? double(acc[q]) : y64[j][q] + double(acc[q]);
         }
     }
 #pragma unroll
     for (int j = 0; j < KPT; ++j)
         if (ok[j])
 #pragma unroll
-            for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx[j]] = y0[j][q];
+            for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx[j]] = y64[j][q];
 }
 
 // -------------------------------------------------------- length gauge
@@ -294,8 +310,9 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
     if (s0 < 0 || s0 >= Nt) return;
     const int s1 = min(s0 + S, Nt);
     const int nkp = sd.nk_pad, ntiles = sd.ntiles;
+    constexpr bool F64 = std::is_same<Real, double>::value;
     const Real *__restrict__ kc = static_cast<const Real *>(sd.kc);
-    Real *__restrict__ st = static_cast<Real *>(sd.st);
+    double *__restrict__ st = static_cast<double *>(sd.st);
     const Real *__restrict__ tab = static_cast<const Real *>(sd.tab);
     const Real g1 = Real(sd.g1), g2 = Real(sd.g2);
     const Real t1dt = Real(sd.t1dt), t2sdt = Real(sd.t2sdt), Mdt = Real(sd.Mdt);
@@ -309,16 +326,20 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
     const int local = threadIdx.x;
     const bool ok = local < tl.kcount;
     const int kidx = tl.k0 + local;
-    Real c[LW_NCONST], y0[4];
+    Real c[LW_NCONST];
+    double y64[4];
 #pragma unroll
     for (int q = 0; q < LW_NCONST; ++q) c[q] = ok ? kc[(size_t)q * nkp + kidx] : Real(0);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) y0[q] = ok ? st[(size_t)q * nkp + kidx] : Real(0);
+    for (int q = 0; q < 4; ++q) y64[q] = ok ? st[(size_t)q * nkp + kidx] : 0.0;
     if (!ok) c[LW_CA0] = c[LW_CB0] = Real(1);  // padding lanes: a harmless k = 0 point, weight 0
     TileReducer red{red_s};
 
     for (int s = s0; s < s1; ++s) {
         const Real *row = tab + (size_t)s * TB::NT * LW_NPHASE;
+        Real y0[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) y0[q] = Real(y64[q]);
         // currents at k + A(t_s) (SBEs.h:694-760), computed in FP64
         {
             Real ca[3], sa[3], cb[3], sb[3];
@@ -334,7 +355,7 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
             const double B1 = double(t1dt) * (double(ca[0]) + double(ca[1]) + double(ca[2]));
             const double B2 = double(t1dt) * (double(sa[0]) + double(sa[1]) + double(sa[2]));
             const double B3 = double(Mdt) - double(t2sdt) * (double(sb[0]) + double(sb[1]) + double(sb[2]));
-            const double al = y0[LW_AL], sx = y0[LW_SX], sy = y0[LW_SY], sz = y0[LW_SZ];
+            const double al = y64[LW_AL], sx = y64[LW_SX], sy = y64[LW_SY], sz = y64[LW_SZ];
             const double bb = B1 * B1 + B2 * B2 + B3 * B3;
             const double sB = sx * B1 + sy * B2 + sz * B3;
             const double w = c[LW_W];
@@ -356,7 +377,7 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
         }
         Real kk[TB::S][4], y[4], acc[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = y0[q];
+        for (int q = 0; q < 4; ++q) acc[q] = F64 ? y0[q] : Real(0);
 #pragma unroll
         for (int i = 0; i < TB::S; ++i) {
 #pragma unroll
@@ -374,11 +395,11 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
             }
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) y0[q] = acc[q];
+        for (int q = 0; q < 4; ++q) y64[q] = F64 ? double(acc[q]) : y64[q] + double(acc[q]);
     }
     if (ok)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx] = y0[q];
+        for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx] = y64[q];
 }
 
 // ------------------------------------------------------- second pass
@@ -431,7 +452,7 @@ __device__ __forceinline__ double2 cconjmul(double2 a, double2 b)  // conj(a) * 
 }
 
 template <class Real>
-__global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restrict__ kc, Real *__restrict__ st,
+__global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restrict__ kc, double *__restrict__ st,
                                                     double *__restrict__ constpart)
 {
     // one block per tile; threads loop over the tile's k-points
@@ -523,7 +544,7 @@ __global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restric
 #pragma unroll
             for (int q = 0; q < VG_NCONST; ++q) kc[q * P + k] = Real(cv[q]);
 #pragma unroll
-            for (int q = 0; q < VG_NSTATE; ++q) st[q * P + k] = Real(0);
+            for (int q = 0; q < VG_NSTATE; ++q) st[q * P + k] = 0.0;
             cp[0] += w * (f0 * P00[0] + f1 * P11[0]);
             cp[1] += w * (f0 * P00[1] + f1 * P11[1]);
             cp[2] += w * f0;
@@ -534,10 +555,10 @@ __global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restric
 #pragma unroll
             for (int q = 0; q < LW_NCONST; ++q) kc[q * P + k] = Real(cv[q]);
             // rho0 = f0 |-><-| + f1 |+><+| = (f0+f1)/2 I + (f1-f0)/2 n.sigma (SBEs.h:352-356)
-            st[LW_AL * P + k] = Real(0.5 * (f0 + f1));
-            st[LW_SX * P + k] = Real(0.5 * (f1 - f0) * nx);
-            st[LW_SY * P + k] = Real(0.5 * (f1 - f0) * ny);
-            st[LW_SZ * P + k] = Real(0.5 * (f1 - f0) * nz);
+            st[LW_AL * P + k] = 0.5 * (f0 + f1);
+            st[LW_SX * P + k] = 0.5 * (f1 - f0) * nx;
+            st[LW_SY * P + k] = 0.5 * (f1 - f0) * ny;
+            st[LW_SZ * P + k] = 0.5 * (f1 - f0) * nz;
         }
     }
     // deterministic block sum of the constant parts -> constpart[tile][8]
@@ -651,7 +672,7 @@ cudaError_t launch_init_haldane(const InitArgs &ia, int precision, void *kc, voi
         init_haldane<double><<<ntiles, 256, 0, stream>>>(ia, static_cast<double *>(kc), static_cast<double *>(st),
                                                          constpart);
     else
-        init_haldane<float><<<ntiles, 256, 0, stream>>>(ia, static_cast<float *>(kc), static_cast<float *>(st),
+        init_haldane<float><<<ntiles, 256, 0, stream>>>(ia, static_cast<float *>(kc), static_cast<double *>(st),
                                                         constpart);
     return cudaGetLastError();
 }

@@ -1,0 +1,350 @@
+"""Benchmark of the SBE propagation (one JSON line on stdout).
+
+Workload (default): the 600x600 Haldane problem -- a0 = 1.44 A, t1 = 0.075,
+t2 = t1/3, phi0 = 1.16, M = 2.54 t2, 3.2 um 8-cycle sin^2 pulse at
+E0 = 0.0045 a.u., velocity gauge, dt = 0.1 a.u. (35 302 steps), RK4,
+T2 = 220 a.u. -- run two ways: the mixed method (FP32 RK stages, FP64 sums;
+the headline `value`) and the plain FP64 method.  A step is one complete
+propagation of that problem.  Inputs are synthetic (no dataset exists for
+this path).  Metric: k-point time steps per second (k.steps/s) and HHG
+solves/hour.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU implementation (the
+unmodified reference sources built in oracle/_ref; the C oracle if that build
+is absent) over all host cores on a bounded k-slice of the same workload.
+Under torchrun (N > 1) each rank runs its own solves (independent solves:
+weak scaling, no collective on the data path); rank 0 prints.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "HHG solves/hour & k·steps/s, batched FP32 vs plain FP64 at ≤1e-3 err; p99 lat"
+UNIT = "k·steps/s"
+FLOPS_PER_KSTEP = {4: 198.0, 5: 370.0}   # algorithmic flops per k-point step, 2-band velocity gauge
+L2_FLUSH_BYTES = 512 << 20
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.proc, self.path = gpu, None, None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        busy = [s for s, _, _ in rows if s > 500] or [s for s, _, _ in rows]
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": rows[0][1], "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+
+    import antelope_b200 as ab
+    from antelope_b200 import cfgtext, workloads
+    from antelope_b200.api import Outputs, Solver
+    from antelope_b200.spectrum import per_harmonic_error
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    n = args.grid
+    case = {p: workloads.haldane_case(n=n, precision=p, ncycles=args.ncycles) for p in ("mixed", "fp64")}
+    probs = {p: ab.Problem.from_dict(c) for p, c in case.items()}
+    dims = probs["mixed"].dims
+    kst = float(dims.ntotal) * dims.Nt
+
+    def timed(prec, k, w, profile):
+        # solvers are created (tables uploaded, per-k set-up done) before timing
+        solvers = [Solver(probs[prec], precision=prec, profile=profile, tile_k=args.tile_k,
+                          k_per_thread=args.kpt, steps_per_launch=args.steps_per_launch) for _ in range(k + w)]
+        for s in solvers[:w]:
+            s.run(stream.cuda_stream)
+        torch.cuda.synchronize()
+        if profile:
+            for s in solvers[:w]:
+                s.kernel_times()
+        times, launches, ktimes = [], 0, []
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for s in solvers[w:]:
+            with torch.cuda.stream(stream):
+                flush.zero_()                          # L2 flush between steps, outside the events
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s.run(stream.cuda_stream)
+                e1.record(stream)
+            launches += s.launches
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ms = [a.elapsed_time(b) for a, b in times]
+        if profile:
+            ktimes = [s.kernel_times() for s in solvers[w:]]
+        out = solvers[-1].get()
+        for s in solvers:
+            s.close()
+        return ms, launches, ktimes, out
+
+    with ClockSampler(local) as clk:
+        ms_mixed, launches, kt_mixed, out_mixed = timed("mixed", args.steps, args.warmup, True)
+        ms_fp64, launches64, kt_fp64, out_fp64 = timed("fp64", max(2, args.steps // 3), 1, True)
+    clocks = clk.summary()
+
+    total_ms = sum(ms_mixed)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps * kst / (total_ms * 1e-3)
+    fp64_value = kst / (statistics.mean(ms_fp64) * 1e-3)
+
+    # per-harmonic spectral error of the mixed run against the FP64 run
+    orders, err, _ = per_harmonic_error({"inter": out_mixed.inter, "intra": out_mixed.intra},
+                                        {"inter": out_fp64.inter, "intra": out_fp64.intra}, dims.dt, 0.014238)
+
+    # e2e through the C ABI from host inputs to host outputs
+    e2e_s = []
+    text = cfgtext.dumps(case["mixed"])
+    h2d = d2h = 0
+    for i in range(max(2, args.steps // 3)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p = ab.Problem.from_text(text)
+        s = Solver(p, precision="mixed")
+        s.run(0)
+        o = s.get()
+        s.close()
+        e2e_s.append(time.perf_counter() - t0)
+    nts = 3
+    tile_k = args.tile_k or 128
+    ntiles = -(-dims.ntotal // tile_k)
+    h2d = dims.Nt * nts * 2 * 4 + 512            # FP32 A(t) table + solve descriptor
+    d2h = dims.Nt * 8 * 8 + ntiles * 8 * 8       # per-step sums + per-tile constants
+    e2e_value = kst / statistics.mean(e2e_s)
+
+    # roofline of the propagate kernel from its own launch events
+    prop_ms = sum(k["propagate_ms"] for k in kt_mixed)
+    prop_n = sum(k["propagate_launches"] for k in kt_mixed)
+    red_ms = sum(k["reduce_ms"] for k in kt_mixed)
+    fp64_tf, fp32_tf = ab.measure_fma_peaks(local)
+    flops = FLOPS_PER_KSTEP[4] * kst * args.steps
+    achieved = flops / (prop_ms * 1e-3) / 1e12
+    prop64 = sum(k["propagate_ms"] for k in kt_fp64)
+    ach64 = FLOPS_PER_KSTEP[4] * kst * len(kt_fp64) / (prop64 * 1e-3) / 1e12
+    traffic = read_traffic()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 stages / f64 sums", "data": "synthetic",
+        "config": {"workload": f"Haldane {n}x{n} velocity gauge, 3.2um 8-cycle sin2, dt=0.1 "
+                               f"({dims.Nt} steps), RK4, T2=220; mixed precision",
+                   "k_points": dims.ntotal, "time_steps": dims.Nt, "precision": "mixed",
+                   "l2": "flushed (512 MiB write) between timed steps",
+                   "parallelism": f"independent solves per GPU x{world}"},
+        "solves_per_hour": value / kst * 3600.0,
+        "fp64": {"value": fp64_value, "unit": UNIT, "solves_per_hour": fp64_value / kst * 3600.0,
+                 "ms_per_solve": statistics.mean(ms_fp64), "roofline_frac": ach64 / fp64_tf,
+                 "achieved_tflops": ach64},
+        "mixed_over_fp64": value / world / fp64_value,
+        "spectral_error": {"max_per_harmonic": float(err.max()), "harmonics": int(len(orders)),
+                           "floor": "band power >= 1e-8 of the strongest", "vs": "fp64 run"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "seconds_per_solve": statistics.mean(e2e_s),
+                "path": "sbe_problem_from_string -> sbe_solver_create -> run -> sbe_solver_get"},
+        "roofline": {"bound": "fp32 FMA pipe", "achieved": achieved, "peak": fp32_tf, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_tf, "traffic": traffic,
+                     "peak_source": "measured FMA-chain microbenchmark (MEASURED_PEAKS.json has no FP32/FP64)",
+                     "flops_per_kstep": FLOPS_PER_KSTEP[4], "kernel": "propagate_vg<float,4>",
+                     "kernel_share": prop_ms / (prop_ms + red_ms)},
+        "gpu_launches": int(launches) * 2,   # propagate + reduce per launch tick, timed steps only
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, dims.Nt, budget_s=args.cpu_seconds)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def read_traffic():
+    """DRAM bytes per propagate launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "propagate_vg_dram_bytes.txt")
+    try:
+        for line in open(path):
+            if line.startswith("bytes_per_launch_bench_workload"):
+                return float(line.split()[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------- CPU arms
+def cpu_baseline(n: int, Nt: int, budget_s: float = 15.0, samples: int = 1):
+    """Time the reference on the host cores on a bounded k-slice of the
+    n x n workload (each process = one emulated MPI rank of a large rank
+    count; ParaRange, utility.h:104-115, gives it ~budget_s of work)."""
+    from antelope_b200 import cfgtext, workloads
+    from oracle import pyoracle
+
+    cores = os.cpu_count() or 1
+    per_kstep = 2.4e-6   # single-core seconds per k.step measured for this path
+    kper = max(4, int(budget_s / (Nt * per_kstep)))
+    ntot = n * n
+    size = max(cores, ntot // kper)
+    # the unmodified reference has no sin2 envelope: cos4 has the same duration N*T
+    case = workloads.haldane_case(n=n, env="cos4")
+    del case["calc"]["precision"]
+    if os.path.exists(pyoracle.REF_EXE):
+        kind, vals = "reference", []
+        for _ in range(samples):
+            with tempfile.TemporaryDirectory() as d:
+                with open(os.path.join(d, "inputParam.cfg"), "w") as f:
+                    f.write(cfgtext.dumps(case))
+                t0 = time.perf_counter()
+                procs = [subprocess.Popen([pyoracle.REF_EXE], cwd=d, stdout=subprocess.DEVNULL,
+                                          env=dict(os.environ, REF_RANK=str(r), REF_SIZE=str(size)))
+                         for r in range(cores)]
+                rc = [p.wait() for p in procs]
+                wall = time.perf_counter() - t0
+            if any(rc):
+                raise RuntimeError(f"reference run failed: {rc}")
+            kdone = sum(ntot // size + (1 if ntot % size > r else 0) for r in range(cores))
+            vals.append(kdone * Nt / wall)
+        sample = (f"{cores} processes x 1 emulated rank of {size} (ParaRange slices of the {n}x{n} grid, "
+                  f"{kdone} k-points) x {Nt} steps, cos4 twin of the sin2 pulse")
+    else:
+        kind = "port"
+        g = max(2, int(np.sqrt(cores * kper)))
+        c2 = workloads.haldane_case(n=g, env="cos4")
+        vals = []
+        for _ in range(samples):
+            t0 = time.perf_counter()
+            pyoracle.run(c2, nthreads=cores)
+            wall = time.perf_counter() - t0
+            vals.append(g * g * Nt / wall)
+        sample = f"C oracle on a {g}x{g} grid x {Nt} steps, {cores} threads"
+    return {"value": float(statistics.median(vals)), "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": sample, "solves_per_hour": float(statistics.median(vals)) / (ntot * Nt) * 3600.0}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from antelope_b200 import workloads
+
+    Nt = 35302
+    try:
+        import antelope_b200 as ab
+        Nt = ab.Problem.from_dict(workloads.haldane_case(n=args.grid, ncycles=args.ncycles)).dims.Nt
+    except Exception:
+        pass
+    for _ in range(args.warmup):
+        cpu_baseline(args.grid, Nt, budget_s=args.ref_seconds)
+    vals = [cpu_baseline(args.grid, Nt, budget_s=args.ref_seconds) for _ in range(args.steps)]
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    ntot = args.grid * args.grid
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"Haldane {args.grid}x{args.grid} velocity gauge, 3.2um 8-cycle "
+                                   f"(cos4 twin), dt=0.1 ({Nt} steps), RK4, T2=220",
+                       "k_points": ntot, "time_steps": Nt},
+            "solves_per_hour": v / (ntot * Nt) * 3600.0,
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=600)
+    ap.add_argument("--ncycles", type=float, default=8.0)
+    ap.add_argument("--tile-k", dest="tile_k", type=int, default=0)
+    ap.add_argument("--kpt", type=int, default=0)
+    ap.add_argument("--steps-per-launch", dest="steps_per_launch", type=int, default=0)
+    ap.add_argument("--cpu-seconds", dest="cpu_seconds", type=float, default=12.0)
+    ap.add_argument("--ref-seconds", dest="ref_seconds", type=float, default=6.0)
+    ap.add_argument("--no-cpu-baseline", dest="no_cpu_baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,7 +57,7 @@ typedef struct sbe_dims {
 /* Run options.  precision: -1 = calc.precision of the cfg (default fp64),
  * 0 = plain FP64, 1 = mixed FP32 stages / FP64 sums.  tile_k, k_per_thread,
  * steps_per_launch: 0 = tuned defaults.  use_graph: capture the launches of
- * a run into one CUDA graph. */
+ * a run into one CUDA graph.  profile: see sbe_solver_kernel_times. */
 typedef struct sbe_opts {
     int device;
     int precision;
@@ -65,6 +65,7 @@ typedef struct sbe_opts {
     int k_per_thread;
     int steps_per_launch;
     int use_graph;
+    int profile;   /* 1: time every kernel launch with CUDA events (no graph) */
 } sbe_opts;
 
 /* Caller-owned host arrays (any may be NULL):
@@ -106,6 +107,10 @@ sbe_status sbe_solver_run(sbe_solver *s, void *stream);
 sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out);
 /* Number of propagate kernel launches the last run issued. */
 int sbe_solver_launches(const sbe_solver *s);
+/* With opts.profile = 1: total device time (ms) and count of the propagate
+ * and reduce launches of the run (CUDA events on the launching stream). */
+sbe_status sbe_solver_kernel_times(sbe_solver *s, double *propagate_ms, int *propagate_launches,
+                                   double *reduce_ms, int *reduce_launches);
 void sbe_solver_destroy(sbe_solver *s);
 
 /* Write the reference's six output files into `dir` (antelope.cpp:176-184,
@@ -122,6 +127,8 @@ sbe_status sbe_batch_create(const sbe_problem *const *problems, int n, const sbe
 sbe_status sbe_batch_run(sbe_batch *b, void *stream);
 sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *out);
 int sbe_batch_launches(const sbe_batch *b);
+sbe_status sbe_batch_kernel_times(sbe_batch *b, double *propagate_ms, int *propagate_launches,
+                                  double *reduce_ms, int *reduce_launches);
 void sbe_batch_destroy(sbe_batch *b);
 
 /* Continuous-batching server: a worker thread admits submitted solves while

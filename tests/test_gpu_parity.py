@@ -25,6 +25,15 @@ def rel(a, b):
     return np.abs(a - b).max() / (m if m > 0 else 1.0)
 
 
+def rel_series(a, b, scale):
+    """max_t |a - b| / max_t |b| for one current series; a series that is
+    zero up to rounding noise (e.g. the transverse intraband current of a
+    linearly polarised pulse, ~1e-18) is measured against 1e-5 of the
+    largest current of the run instead of against its own noise."""
+    m = max(np.abs(b).max(), 1e-5 * scale)
+    return np.abs(a - b).max() / m
+
+
 _oracle_cache = {}
 
 
@@ -40,10 +49,11 @@ def test_fp64_matches_oracle_and_reference(name):
     out = ab.solve(case, precision="fp64")
     ref = oracle(name, case)
     gold = np.load(os.path.join(GOLDEN, f"golden_{name}.npz"))
+    scale = max(np.abs(ref["inter"]).max(), np.abs(ref["intra"]).max())
     for key in ("inter", "intra"):
         for a in range(3):
-            assert rel(getattr(out, key)[:, a], ref[key][:, a]) < FP64_TOL, (key, a)
-        assert rel(getattr(out, key), gold[key]) < FP64_TOL
+            assert rel_series(getattr(out, key)[:, a], ref[key][:, a], scale) < FP64_TOL, (key, a)
+            assert rel_series(getattr(out, key)[:, a], gold[key][:, a], scale) < FP64_TOL, (key, a)
     N = ref["dims"]["nband"]
     assert np.abs(out.occ[:, :N] - ref["occ"]).max() < 1e-12
     assert np.abs(out.occ - gold["occ_file"]).max() < 1e-12
@@ -95,16 +105,34 @@ def test_batch_equals_single_solves_bitwise():
         b.close()
 
 
-def test_mixed_precision_close_to_fp64():
-    case = variant(calc__Npoints=[31, 31], pulse__w0=0.0285, pulse__ncycles=4.0)
-    a = ab.solve(case, precision="fp64")
-    b = ab.solve(case, precision="mixed")
+MIXED_TOL = 1e-3   # relative error per harmonic band, bands >= 1e-8 of the strongest
+
+
+@pytest.mark.parametrize("gauge", ["Velocity", "Wannier"])
+def test_mixed_precision_small_grid(gauge):
+    """A small grid is the hard case: rounding noise averages over fewer k."""
     from antelope_b200.spectrum import per_harmonic_error
 
+    case = variant(top__gauge=gauge, calc__Npoints=[31, 31], pulse__w0=0.0285, pulse__ncycles=4.0)
+    a = ab.solve(case, precision="fp64")
+    b = ab.solve(case, precision="mixed")
     orders, err, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra},
                                         {"inter": a.inter, "intra": a.intra}, 0.1, 0.0285)
     assert len(orders) > 5
-    assert err.max() < 1e-3, (orders, err)
+    assert err.max() < MIXED_TOL, (orders, err)
+
+
+def test_mixed_precision_plain_method_config():
+    """150x150 Haldane, 3.2 um 8-cycle sin^2 pulse, velocity gauge, RK4."""
+    from antelope_b200 import workloads
+    from antelope_b200.spectrum import per_harmonic_error
+
+    a = ab.solve(workloads.haldane_case(150), precision="fp64")
+    b = ab.solve(workloads.haldane_case(150), precision="mixed")
+    orders, err, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra},
+                                        {"inter": a.inter, "intra": a.intra}, 0.1, 0.014238)
+    assert len(orders) > 10
+    assert err.max() < MIXED_TOL, (orders, err)
 
 
 def test_server_alone_equals_in_mix():
