@@ -155,6 +155,14 @@ def solve(problem, **opts) -> Outputs:
         s.close()
 
 
+def solve_noalloc(problem: Problem, stream: int = 0, **opts) -> Outputs:
+    """Allocation-free solve (``sbe_solve_noalloc``): the library allocates no
+    device memory for it; working memory is a fixed array inside the library."""
+    out = Outputs.empty(problem.dims)
+    _check(lib.sbe_solve_noalloc(problem._h, C.byref(_opts(**opts)), C.c_void_p(stream), C.byref(out.c())))
+    return out
+
+
 def run_cfg(cfg_path: str, out_dir: str = ".", **opts):
     """The drop-in: read an inputParam.cfg, solve, write the reference's files."""
     _check(lib.sbe_run_cfg(os.fsencode(cfg_path), os.fsencode(out_dir), C.byref(_opts(**opts))))

@@ -14,14 +14,10 @@
 #include <unordered_map>
 
 #include "sbe_engine.h"
+#include "sbe_handles.h"
 #include "sbe_kernels.h"
 
 using namespace sbe;
-
-struct sbe_problem {
-    Problem p;
-    std::string unsupported;
-};
 
 namespace {
 
@@ -115,6 +111,8 @@ void run_engine(Engine &eng, bool use_graph, int *launches)
 }
 
 }  // namespace
+
+sbe_status sbe::set_error(sbe_status st, const char *msg) { return fail(st, msg); }
 
 // ================================================================= misc
 extern "C" int sbe_abi_version(void) { return SBE_ABI_VERSION; }

@@ -155,6 +155,20 @@ sbe_status sbe_server_cancel(sbe_server *s, long long request_id);
 sbe_status sbe_server_stats(sbe_server *s, long long counters[5]);
 void sbe_server_destroy(sbe_server *s);
 
+/* Allocation-free solve, for callers that must not allocate device memory
+ * themselves (code inside an application whose device memory belongs to that
+ * application's pool allocator, or latency-critical loops where cudaMalloc /
+ * cudaFree could synchronise the device).  No counterpart in the reference.
+ * Same result as sbe_solver_create + sbe_solver_run + sbe_solver_get (the
+ * same kernels), but all device working memory lives in one fixed 64 MiB
+ * array inside the library, held on every GPU that loads the library until
+ * exit; problems that do not fit are rejected with SBE_OOM.  The first call
+ * on a device looks up that array's address (make it before any stream
+ * capture on that device).  Calls share the array: they must not overlap on
+ * the GPU -- this function serialises its own calls and returns after its
+ * GPU work is done.  `stream` may be NULL (the legacy default stream). */
+sbe_status sbe_solve_noalloc(const sbe_problem *p, const sbe_opts *opts, void *stream, const sbe_outputs *out);
+
 /* Measured FP64 / FP32 FMA pipe peaks of the device (TFLOP/s), the
  * denominators of the roofline fractions.  No reference counterpart. */
 sbe_status sbe_measure_fma_peaks(int device, double *fp64_tflops, double *fp32_tflops);
