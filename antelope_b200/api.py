@@ -248,6 +248,7 @@ class Server:
 
 
 def measure_fma_peaks(device: int = 0):
-    a, b = C.c_double(0), C.c_double(0)
-    _check(lib.sbe_measure_fma_peaks(device, C.byref(a), C.byref(b)))
-    return a.value, b.value
+    """(fp64, fp32, packed f32x2) FMA-chain peaks in TFLOP/s."""
+    a, b, c = C.c_double(0), C.c_double(0), C.c_double(0)
+    _check(lib.sbe_measure_fma_peaks(device, C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value

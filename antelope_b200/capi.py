@@ -80,7 +80,8 @@ def _load():
         "sbe_server_stats": (C.c_int, [P, C.POINTER(C.c_longlong)]),
         "sbe_server_destroy": (None, [P]),
         "sbe_solve_noalloc": (C.c_int, [P, C.POINTER(Opts), C.c_void_p, C.POINTER(COutputs)]),
-        "sbe_measure_fma_peaks": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "sbe_measure_fma_peaks": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -684,7 +684,7 @@ extern "C" void sbe_server_destroy(sbe_server *s)
 }
 
 // ================================================================= peaks
-extern "C" sbe_status sbe_measure_fma_peaks(int device, double *fp64, double *fp32)
+extern "C" sbe_status sbe_measure_fma_peaks(int device, double *fp64, double *fp32, double *fp32x2)
 {
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(device), "cudaSetDevice");
@@ -696,8 +696,8 @@ extern "C" sbe_status sbe_measure_fma_peaks(int device, double *fp64, double *fp
         cudaEventCreate(&a);
         cudaEventCreate(&b);
         const int blocks = sms * 8, iters = 1 << 16;
-        double res[2] = {0, 0};
-        for (int which = 0; which < 2; ++which) {
+        double res[3] = {0, 0, 0};
+        for (int which = 0; which < 3; ++which) {
             cuda_check(launch_fma_peak(which, blocks, 256, buf, 0), "warm-up");
             float best = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
@@ -709,7 +709,7 @@ extern "C" sbe_status sbe_measure_fma_peaks(int device, double *fp64, double *fp
                 cudaEventElapsedTime(&ms, a, b);
                 best = std::min(best, ms);
             }
-            const double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+            const double flops = (which == 2 ? 4.0 : 2.0) * 8.0 * iters * 256.0 * blocks;
             res[which] = flops / (best * 1e-3) / 1e12;
         }
         cudaEventDestroy(a);
@@ -717,6 +717,7 @@ extern "C" sbe_status sbe_measure_fma_peaks(int device, double *fp64, double *fp
         cudaFree(buf);
         if (fp64) *fp64 = res[0];
         if (fp32) *fp32 = res[1];
+        if (fp32x2) *fp32x2 = res[2];
         return SBE_OK;
     });
 }

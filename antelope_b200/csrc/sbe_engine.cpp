@@ -92,11 +92,21 @@ Engine::~Engine()
 Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
 {
     const int prec = o.precision >= 0 ? o.precision : p.precision;
+    const bool vg = p.gauge == GAUGE_VELOCITY;
     Shape s{};
-    s.kpt = o.kpt > 0 ? o.kpt : 1;
-    if (p.gauge != GAUGE_VELOCITY) s.kpt = 1;
-    s.tile_k = o.tile_k > 0 ? o.tile_k : 128 * s.kpt;
-    (void)prec;
+    // mixed velocity gauge: two k-points per thread in packed f32x2 registers
+    s.kpt = o.kpt > 0 ? o.kpt : ((vg && prec == PREC_MIXED) ? 2 : 1);
+    if (!vg) s.kpt = 1;
+    if (o.tile_k > 0) {
+        s.tile_k = o.tile_k;
+    } else {
+        // largest CTA (<= 128 threads) that still gives >= 2 CTAs per SM
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
+        int threads = 128;
+        while (threads > 32 && (long long)p.ntotal() < 2LL * sms * threads * s.kpt) threads /= 2;
+        s.tile_k = threads * s.kpt;
+    }
     s.threads = s.tile_k / s.kpt;
     if (s.threads < 32 || s.threads > 256 || s.threads % 32 || s.tile_k % s.kpt)
         throw CfgError("tile_k / kpt must be a multiple of 32 between 32 and 256");

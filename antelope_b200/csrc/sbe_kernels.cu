@@ -72,6 +72,48 @@ template <> struct Tableau<5> {  // Fehlberg tableau with its 5th-order weights
     __device__ static constexpr int ti(int i) { return i; }
 };
 
+// ---------------------------------------------- packed FP32 (f32x2) math
+// Two k-points per thread share every instruction: .x belongs to the first,
+// .y to the second (PTX f32x2 arithmetic, sm_100+).
+__device__ __forceinline__ unsigned long long pk(float2 a)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 upk(unsigned long long r)
+{
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(pk(a)), "l"(pk(b)), "l"(pk(c)));
+    return upk(d);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b)
+{
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk(a)), "l"(pk(b)));
+    return upk(d);
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk(a)), "l"(pk(b)));
+    return upk(d);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk(a)), "l"(pk(b)));
+    return upk(d);
+}
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
 template <class Real> struct V2;
 template <> struct V2<double> { using T = double2; };
 template <> struct V2<float> { using T = float2; };
@@ -258,6 +300,162 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
         if (ok[j])
 #pragma unroll
             for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx[j]] = y64[j][q];
+}
+
+// Mixed method, velocity gauge, two k-points per thread packed into f32x2
+// registers: every RK instruction advances both.  The per-step current sums
+// are added across the pair and over the warp in FP32 (one conversion to
+// FP64 per lane per step instead of eight), then staged and summed over
+// warps in FP64 as in propagate_vg.  The state stays FP64.
+__device__ __forceinline__ float warp_sum8f(const float (&v)[8], int lane)
+{
+    const bool h4 = lane & 16, h2 = lane & 8, h1 = lane & 4;
+    float u[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float send = h4 ? v[i] : v[i + 4];
+        float keep = h4 ? v[i + 4] : v[i];
+        u[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    float x[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        float send = h2 ? u[i] : u[i + 2];
+        float keep = h2 ? u[i + 2] : u[i];
+        x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    float send = h1 ? x[0] : x[1];
+    float y = (h1 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    y += __shfl_xor_sync(0xffffffffu, y, 2);
+    y += __shfl_xor_sync(0xffffffffu, y, 1);
+    return y;  // lanes 4*i hold the sum of v[i]
+}
+
+template <bool G1>
+__device__ __forceinline__ void vg_rhs2(const float2 (&c)[VG_NCONST], float2 A, const float2 (&y)[4], float2 ng1,
+                                        float2 ng2, float2 (&k)[4])
+{
+    const float2 ax = bc2(A.x), ay = bc2(A.y);
+    const float2 delta = fma2(ay, c[VG_DPY], fma2(ax, c[VG_DPX], c[VG_DE]));
+    const float2 wr = fma2(ay, c[VG_PYR], mul2(ax, c[VG_PXR]));
+    const float2 wi = fma2(ay, c[VG_PYI], mul2(ax, c[VG_PXI]));
+    const float2 im = fma2(wi, y[VG_ZR], neg2(mul2(wr, y[VG_ZI])));   // Im(w z*)
+    const float2 im2 = add2(im, im);
+    if (G1) {
+        k[VG_DA] = fma2(ng1, y[VG_DA], im2);
+        k[VG_DB] = fma2(ng1, y[VG_DB], neg2(im2));
+    } else {
+        k[VG_DA] = im2;
+        k[VG_DB] = neg2(im2);
+    }
+    const float2 bma = add2(c[VG_C0], sub2(y[VG_DB], y[VG_DA]));
+    const float2 xr = fma2(bma, wr, mul2(delta, y[VG_ZR]));
+    const float2 xi = fma2(bma, wi, mul2(delta, y[VG_ZI]));
+    k[VG_ZR] = fma2(ng2, y[VG_ZR], xi);
+    k[VG_ZI] = fma2(ng2, y[VG_ZI], neg2(xr));
+}
+
+template <int RK, bool G1>
+__global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict__ tiles,
+                                                       const SolveDev *__restrict__ solves, int tick, int S)
+{
+    using TB = Tableau<RK>;
+    __shared__ double red_s[SUB][MAX_WARPS][NSLOT];
+    const TileDev tl = tiles[blockIdx.x];
+    const SolveDev &sd = solves[tl.solve];
+    const int s0 = (tick - sd.admit_tick) * S;
+    const int Nt = sd.Nt;
+    if (s0 < 0 || s0 >= Nt) return;
+    const int s1 = min(s0 + S, Nt);
+    const int nkp = sd.nk_pad, ntiles = sd.ntiles;
+    const float *__restrict__ kc = static_cast<const float *>(sd.kc);
+    double *__restrict__ st = static_cast<double *>(sd.st);
+    const float2 *__restrict__ tab = static_cast<const float2 *>(sd.tab);
+    const float2 ng1 = bc2(-float(sd.g1)), ng2 = bc2(-float(sd.g2));
+    double *partial = sd.partial;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    const int l0 = threadIdx.x, l1 = threadIdx.x + blockDim.x;
+    const bool ok0 = l0 < tl.kcount, ok1 = l1 < tl.kcount;
+    const int k0 = tl.k0 + l0, k1 = tl.k0 + l1;
+    float2 c[VG_NCONST];
+    double y64[2][4];
+#pragma unroll
+    for (int q = 0; q < VG_NCONST; ++q)
+        c[q] = make_float2(ok0 ? kc[(size_t)q * nkp + k0] : 0.f, ok1 ? kc[(size_t)q * nkp + k1] : 0.f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        y64[0][q] = ok0 ? st[(size_t)q * nkp + k0] : 0.0;
+        y64[1][q] = ok1 ? st[(size_t)q * nkp + k1] : 0.0;
+    }
+    float2 An[TB::NT];
+#pragma unroll
+    for (int i = 0; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)s0 * TB::NT + i);
+
+    for (int s = s0; s < s1; ++s) {
+        float2 A[TB::NT];
+#pragma unroll
+        for (int i = 0; i < TB::NT; ++i) A[i] = An[i];
+        if (s + 1 < s1) {
+#pragma unroll
+            for (int i = 0; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)(s + 1) * TB::NT + i);
+        }
+        float2 y0[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) y0[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+        // currents and occupations at t_s (antelope.cpp:309-334)
+        {
+            float2 t[8];
+            t[0] = fma2(y0[VG_ZR], c[VG_WQXR], mul2(y0[VG_ZI], c[VG_WQXI]));
+            t[1] = fma2(y0[VG_ZR], c[VG_WQYR], mul2(y0[VG_ZI], c[VG_WQYI]));
+            t[2] = fma2(y0[VG_DA], c[VG_WPX0], mul2(y0[VG_DB], c[VG_WPX1]));
+            t[3] = fma2(y0[VG_DA], c[VG_WPY0], mul2(y0[VG_DB], c[VG_WPY1]));
+            t[4] = mul2(c[VG_W], y0[VG_DA]);
+            t[5] = mul2(c[VG_W], y0[VG_DB]);
+            t[6] = mul2(c[VG_W], y0[VG_ZR]);
+            t[7] = mul2(c[VG_W], y0[VG_ZI]);
+            float v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = t[q].x + t[q].y;
+            const float y = warp_sum8f(v, lane);
+            const int r = (s - s0) % SUB;
+            if ((lane & 3) == 0) red_s[r][warp][lane >> 2] = double(y);
+            if (r == SUB - 1 || s == s1 - 1) {
+                TileReducer red{red_s};
+                red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
+            }
+        }
+        // one RK step of both k-points
+        float2 kk[TB::S][4], yy[4], inc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) inc[q] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < TB::S; ++i) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float2 t = y0[q];
+#pragma unroll
+                for (int m = 0; m < i; ++m)
+                    if (TB::a(i, m) != 0.0) t = fma2(bc2(float(TB::a(i, m))), kk[m][q], t);
+                yy[q] = t;
+            }
+            vg_rhs2<G1>(c, A[TB::ti(i)], yy, ng1, ng2, kk[i]);
+            if (TB::b(i) != 0.0) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) inc[q] = fma2(bc2(float(TB::b(i))), kk[i][q], inc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            y64[0][q] += double(inc[q].x);
+            y64[1][q] += double(inc[q].y);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (ok0) st[(size_t)q * nkp + k0] = y64[0][q];
+        if (ok1) st[(size_t)q * nkp + k1] = y64[1][q];
+    }
 }
 
 // -------------------------------------------------------- length gauge
@@ -598,6 +796,23 @@ __global__ void __launch_bounds__(256) fma_peak(Real *out, int iters, Real a, Re
     if (s == Real(-12345.678)) out[threadIdx.x] = s;  // keeps the chains live
 }
 
+// FFMA2 variant of the microbenchmark: 8 independent packed chains.
+__global__ void __launch_bounds__(256) fma_peak_x2(float *out, int iters, float a, float b)
+{
+    float2 x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = make_float2(float(threadIdx.x + i) * 1e-3f, float(i) * 1e-3f);
+    const float2 aa = bc2(a), bb = bc2(b);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = fma2(x[i], aa, bb);
+    }
+    float s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += x[i].x + x[i].y;
+    if (s == -12345.678f) out[threadIdx.x] = s;
+}
+
 // ------------------------------------------------------------- launchers
 #define SBE_CHECK_LAUNCH() return cudaGetLastError()
 
@@ -608,6 +823,14 @@ static cudaError_t launch_vg_t(const LaunchArgs &la, bool g1)
         propagate_vg<Real, RK, KPT, true><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
     else
         propagate_vg<Real, RK, KPT, false><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+    SBE_CHECK_LAUNCH();
+}
+
+template <int RK>
+static cudaError_t launch_vg_x2(const LaunchArgs &la, bool g1)
+{
+    if (g1) propagate_vg_x2<RK, true><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+    else propagate_vg_x2<RK, false><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
     SBE_CHECK_LAUNCH();
 }
 
@@ -635,6 +858,9 @@ cudaError_t launch_propagate(const LaunchArgs &la)
     }
         if (la.precision == PREC_FP64) {
             if (la.rk == 4) { SBE_VG(double, 4) } else if (la.rk == 5) { SBE_VG(double, 5) }
+        } else if (la.kpt == 2) {
+            if (la.rk == 4) return launch_vg_x2<4>(la, g1);
+            if (la.rk == 5) return launch_vg_x2<5>(la, g1);
         } else {
             if (la.rk == 4) { SBE_VG(float, 4) } else if (la.rk == 5) { SBE_VG(float, 5) }
         }
@@ -680,7 +906,8 @@ cudaError_t launch_init_haldane(const InitArgs &ia, int precision, void *kc, voi
 cudaError_t launch_fma_peak(int which, int blocks, int iters, void *out, cudaStream_t stream)
 {
     if (which == 0) fma_peak<double><<<blocks, 256, 0, stream>>>(static_cast<double *>(out), iters, 0.999999, 1e-7);
-    else fma_peak<float><<<blocks, 256, 0, stream>>>(static_cast<float *>(out), iters, 0.999999f, 1e-7f);
+    else if (which == 1) fma_peak<float><<<blocks, 256, 0, stream>>>(static_cast<float *>(out), iters, 0.999999f, 1e-7f);
+    else fma_peak_x2<<<blocks, 256, 0, stream>>>(static_cast<float *>(out), iters, 0.999999f, 1e-7f);
     return cudaGetLastError();
 }
 

@@ -27,7 +27,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -155,11 +154,9 @@ def run_ours(args):
         ms_fp64, launches64, kt_fp64, out_fp64 = timed("fp64", max(2, args.steps // 3), 1, True)
     clocks = clk.summary()
 
-    total_ms = sum(ms_mixed)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    from antelope_b200.dist import max_over_ranks
+
+    total_ms = max_over_ranks(sum(ms_mixed), dev)   # whole-job device time: max over ranks
     value = world * args.steps * kst / (total_ms * 1e-3)
     fp64_value = kst / (statistics.mean(ms_fp64) * 1e-3)
 
@@ -191,7 +188,7 @@ def run_ours(args):
     prop_ms = sum(k["propagate_ms"] for k in kt_mixed)
     prop_n = sum(k["propagate_launches"] for k in kt_mixed)
     red_ms = sum(k["reduce_ms"] for k in kt_mixed)
-    fp64_tf, fp32_tf = ab.measure_fma_peaks(local)
+    fp64_tf, fp32_tf, fp32x2_tf = ab.measure_fma_peaks(local)
     flops = FLOPS_PER_KSTEP[4] * kst * args.steps
     achieved = flops / (prop_ms * 1e-3) / 1e12
     prop64 = sum(k["propagate_ms"] for k in kt_fp64)

@@ -170,8 +170,9 @@ void sbe_server_destroy(sbe_server *s);
 sbe_status sbe_solve_noalloc(const sbe_problem *p, const sbe_opts *opts, void *stream, const sbe_outputs *out);
 
 /* Measured FP64 / FP32 FMA pipe peaks of the device (TFLOP/s), the
- * denominators of the roofline fractions.  No reference counterpart. */
-sbe_status sbe_measure_fma_peaks(int device, double *fp64_tflops, double *fp32_tflops);
+ * denominators of the roofline fractions; fp32x2: packed f32x2 FMAs.  No
+ * reference counterpart. */
+sbe_status sbe_measure_fma_peaks(int device, double *fp64_tflops, double *fp32_tflops, double *fp32x2_tflops);
 
 #ifdef __cplusplus
 }
