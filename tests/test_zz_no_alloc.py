@@ -49,11 +49,13 @@ def test_noalloc_matches_regular_entry_point_twice(case, opts):
     _check(second, ref)
 
 
-def test_noalloc_mixed_precision_twice():
+@pytest.mark.parametrize("kpt", [1, 2])
+def test_noalloc_mixed_precision_twice(kpt):
     p = ab.Problem.from_dict(variant(calc__Npoints=[24, 24]))
-    ref = ab.solve(p, precision="mixed")
+    opts = dict(precision="mixed", tile_k=64 * kpt, k_per_thread=kpt)   # same launch shape on both paths
+    ref = ab.solve(p, **opts)
     for _ in range(2):
-        out = solve_noalloc(p, precision="mixed")
+        out = solve_noalloc(p, **opts)
         # same kernels and tiling: the mixed results agree to FP64 rounding of the k-sum
         _check(out, ref)
 
