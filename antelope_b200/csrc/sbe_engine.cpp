@@ -99,6 +99,8 @@ Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
     if (!vg) s.kpt = 1;
     if (o.tile_k > 0) {
         s.tile_k = o.tile_k;
+    } else if (o.kpt <= 0 && autotune_enabled()) {
+        return autotune_shape(device_, p, prec);
     } else {
         // largest CTA (<= 128 threads) that still gives >= 2 CTAs per SM
         int sms = 148;

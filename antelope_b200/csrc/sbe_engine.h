@@ -118,6 +118,10 @@ private:
     std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<Group>> groups_;
 };
 
+// Autotuner (sbe_tune.cpp): the fastest launch shape for this class of solve.
+bool autotune_enabled();
+Shape autotune_shape(int device, const Problem &p, int precision);
+
 // Assemble the reference's output quantities from the per-step slot sums.
 void assemble_outputs(const Problem &p, const std::vector<double> &jout, const double constpart[NSLOT],
                       SolveOutputs &out);
