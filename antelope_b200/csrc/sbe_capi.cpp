@@ -419,6 +419,9 @@ using Clock = std::chrono::steady_clock;
 struct Request {
     long long id = 0;
     Problem prob;
+    std::vector<double> atab;     // built by the submitting thread
+    std::vector<double> jout;     // raw per-step sums, assembled by the waiting thread
+    double cp[NSLOT] = {0};
     Clock::time_point t_submit, t_done;
     enum State { QUEUED, RESIDENT, DONE, FAILED, CANCELLED } state = QUEUED;
     int solve = -1;
@@ -485,8 +488,9 @@ void sbe_server::loop()
                 break;
             }
             try {
-                r.solve = eng->add(r.prob, eo);
+                r.solve = eng->add(r.prob, eo, &r.atab);
                 r.state = Request::RESIDENT;
+                std::vector<double>().swap(r.atab);
             } catch (const std::exception &e) {
                 r.state = Request::FAILED;
                 r.err = e.what();
@@ -549,7 +553,7 @@ void sbe_server::loop()
             try {
                 if (!r.fetching) { eng->fetch_async(r.solve); r.fetching = true; }
                 if (eng->ready(r.solve)) {
-                    r.out = eng->outputs(r.solve);
+                    eng->raw_outputs(r.solve, r.jout, r.cp);
                     eng->remove(r.solve);
                     r.t_done = Clock::now();
                     r.state = Request::DONE;
@@ -595,12 +599,17 @@ extern "C" sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, lon
 {
     if (!s) return fail(SBE_INVALID_ARGUMENT, "null server");
     if (sbe_status st = check_problem(p)) return st;
+    auto r = std::make_unique<Request>();
+    r->t_submit = Clock::now();
+    r->prob = p->p;
+    try {
+        r->atab = a_table(r->prob);  // host FP64 field table, built on the caller's thread
+    } catch (const std::exception &e) {
+        return fail(SBE_INVALID_ARGUMENT, e.what());
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     if (!s->fatal.empty()) return fail(SBE_CUDA_ERROR, s->fatal);
-    auto r = std::make_unique<Request>();
     r->id = s->next_id++;
-    r->prob = p->p;
-    r->t_submit = Clock::now();
     if (request_id) *request_id = r->id;
     s->queue.push_back(r->id);
     s->reqs[r->id] = std::move(r);
@@ -626,8 +635,21 @@ extern "C" sbe_status sbe_server_wait(sbe_server *s, long long id, double timeou
         const bool oom = r.err.find("memory") != std::string::npos;
         return fail(oom ? SBE_OOM : SBE_CUDA_ERROR, r.err);
     }
-    copy_out(r.out, out);
     if (latency_s) *latency_s = std::chrono::duration<double>(r.t_done - r.t_submit).count();
+    if (out) {
+        // assemble on the waiting thread, outside the lock
+        std::vector<double> j = r.jout;
+        double cp[NSLOT];
+        for (int q = 0; q < NSLOT; ++q) cp[q] = r.cp[q];
+        Problem prob = r.prob;
+        lk.unlock();
+        return guard([&]() -> sbe_status {
+            SolveOutputs o;
+            assemble_outputs(prob, j, cp, o);
+            copy_out(o, out);
+            return SBE_OK;
+        });
+    }
     return SBE_OK;
 }
 

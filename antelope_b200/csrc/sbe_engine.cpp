@@ -51,7 +51,7 @@ Engine::Engine(int device, cudaStream_t stream, int steps_per_launch)
     : device_(device), stream_(stream), S_(steps_per_launch > 0 ? steps_per_launch : 512)
 {
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
-    capacity_ = 64;
+    capacity_ = 4096;
     cuda_check(cudaMalloc(&d_solves_, sizeof(SolveDev) * capacity_), "cudaMalloc(solves)");
     cuda_check(cudaMallocHost(&h_solves_, sizeof(SolveDev) * capacity_), "cudaMallocHost(solves)");
     cuda_check(cudaMalloc(&d_ids_, sizeof(int) * capacity_), "cudaMalloc(ids)");
@@ -130,7 +130,7 @@ size_t Engine::bytes_needed(const Problem &p, const EngineOptions &o) const
            (size_t)ntiles * NSLOT * 8;
 }
 
-int Engine::add(const Problem &p, const EngineOptions &o)
+int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<double> *atab_in)
 {
     if (p.model != MODEL_HALDANE) throw CfgError("only the Haldane model is built on this path");
     if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) throw CfgError("gauge LengthHamiltonian is not implemented");
@@ -180,8 +180,12 @@ int Engine::add(const Problem &p, const EngineOptions &o)
     cuda_check(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate");
 
     // field tables (host FP64, rounded once to the kernel's Real)
-    std::vector<double> atab = a_table(p);
-    std::vector<double> tabd = vg ? atab : phase_table(p, atab);
+    std::vector<double> atab_own;
+    if (!atab_in) atab_own = a_table(p);
+    const std::vector<double> &atab = atab_in ? *atab_in : atab_own;
+    std::vector<double> tabd_own;
+    if (!vg) tabd_own = phase_table(p, atab);
+    const std::vector<double> &tabd = vg ? atab : tabd_own;
     if (s->precision == PREC_FP64) {
         cuda_check(cudaMemcpyAsync(s->tab, tabd.data(), tab_n * 8, cudaMemcpyHostToDevice, stream_), "copy table");
     } else {
@@ -426,17 +430,24 @@ bool Engine::ready(int id)
     return true;
 }
 
-SolveOutputs Engine::outputs(int id)
+void Engine::raw_outputs(int id, std::vector<double> &jout, double cp[NSLOT])
 {
     Solve &s = get(id);
     if (!s.fetched) fetch_async(id);
     cuda_check(cudaEventSynchronize(s.ev), "event sync");
-    double cp[NSLOT] = {0};
+    for (int q = 0; q < NSLOT; ++q) cp[q] = 0.0;
     for (int t = 0; t < s.ntiles; ++t)
         for (int q = 0; q < NSLOT; ++q) cp[q] += s.h_const[(size_t)t * NSLOT + q];
-    std::vector<double> j(s.h_jout, s.h_jout + (size_t)s.Nt * NSLOT);
+    jout.assign(s.h_jout, s.h_jout + (size_t)s.Nt * NSLOT);
+}
+
+SolveOutputs Engine::outputs(int id)
+{
+    std::vector<double> j;
+    double cp[NSLOT];
+    raw_outputs(id, j, cp);
     SolveOutputs o;
-    assemble_outputs(s.prob, j, cp, o);
+    assemble_outputs(get(id).prob, j, cp, o);
     return o;
 }
 

@@ -56,7 +56,8 @@ public:
     // Device bytes a solve of this problem needs (admission control).
     size_t bytes_needed(const Problem &p, const EngineOptions &o) const;
     // Set up a solve on the stream; it starts advancing at the next step().
-    int add(const Problem &p, const EngineOptions &o);
+    // `atab` may hold the problem's a_table() already built by the caller.
+    int add(const Problem &p, const EngineOptions &o, const std::vector<double> *atab = nullptr);
     // Advance every resident solve by up to S steps (one propagate launch per
     // launch class, then the tile reduction).
     void step();
@@ -74,6 +75,10 @@ public:
     void fetch_async(int id);
     bool ready(int id);
     SolveOutputs outputs(int id);
+    // The raw per-step sums [Nt][NSLOT] and the summed constant parts of a
+    // fetched solve (waits for the copy); assemble_outputs() turns them into
+    // the output arrays.
+    void raw_outputs(int id, std::vector<double> &jout, double cp[NSLOT]);
     void remove(int id);
     int nresident() const { return (int)live_.size(); }
     int tick() const { return tick_; }

@@ -222,12 +222,133 @@ def run_ours(args):
         "gpu_launches": int(launches) * 2,   # propagate + reduce per launch tick, timed steps only
         "clocks": clocks,
     }
+    if args.scan_solves > 0:
+        line["scan"] = run_scan(args, stream, rank, world)
+    if args.serve_requests > 0 and world == 1:
+        line["serving"] = run_serve(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(n, dims.Nt, budget_s=args.cpu_seconds)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _fp64_sequential(problems, stream):
+    """Plain FP64 solves one after another (device time per solve)."""
+    import torch
+
+    from antelope_b200.api import Solver
+
+    total_ms, outs = 0.0, []
+    for p in problems:
+        s = Solver(p, precision="fp64")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.run(stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        outs.append(s.get())
+        s.close()
+    return total_ms, outs
+
+
+def run_scan(args, stream, rank, world):
+    """The seeded 256-solve parameter scan: uneven grids 100^2..400^2, 4..12
+    cycles, M/t2, phi0, ellipticity/helicity and CEP drawn per solve; mixed
+    precision in one batch (all launches of the run in one CUDA graph),
+    against the same solves run one by one in plain FP64 (every 4th solve)."""
+    import torch
+
+    import antelope_b200 as ab
+    from antelope_b200 import workloads
+    from antelope_b200.dist import max_over_ranks, para_range, sum_over_ranks
+    from antelope_b200.spectrum import per_harmonic_error
+
+    cases = workloads.scan_cases(n=args.scan_solves, precision="mixed")
+    a, b = para_range(len(cases), world, rank)
+    probs = [ab.Problem.from_dict(c) for c in cases[a:b]]
+    kst = sum(float(p.dims.ntotal) * p.dims.Nt for p in probs)
+    torch.cuda.synchronize()
+    t_create = time.perf_counter()
+    batch = ab.Batch(probs, precision="mixed", use_graph=True, steps_per_launch=256)
+    torch.cuda.synchronize()
+    t_create = time.perf_counter() - t_create
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    sub = list(range(0, len(probs), 4))
+    fp64_ms, fp64_out = _fp64_sequential([probs[i] for i in sub], stream)
+    errs = []
+    for j, i in enumerate(sub[:8]):
+        o = batch.get(i)
+        w0 = cases[a + i]["laser"]["pulses"][0]["w0"]
+        _, e, _ = per_harmonic_error({"inter": o.inter, "intra": o.intra},
+                                     {"inter": fp64_out[j].inter, "intra": fp64_out[j].intra}, 0.1, w0)
+        errs.append(float(e.max()))
+    launches = batch.launches
+    batch.close()
+    nsolves = sum_over_ranks(len(probs))
+    kst_all = sum_over_ranks(kst)
+    sph = nsolves / (ms * 1e-3) * 3600.0
+    sph64 = len(sub) / (fp64_ms * 1e-3) * 3600.0 * world
+    return {"solves": int(nsolves), "k_steps": kst_all, "ms": ms, "k_steps_per_s": kst_all / (ms * 1e-3),
+            "solves_per_hour": sph, "fp64_sequential_solves_per_hour": sph64,
+            "batched_mixed_over_sequential_fp64": sph / sph64,
+            "fp64_sequential_sample": f"{len(sub)} of {len(probs)} solves (every 4th)",
+            "max_per_harmonic_error_vs_fp64": max(errs), "error_sample": f"{len(errs)} solves",
+            "setup_s": t_create, "launches": launches, "graph": True, "steps_per_launch": 256}
+
+
+def run_serve(args):
+    """Poisson stream of Haldane and two-colour requests (64^2..512^2, 4..16
+    cycles, 1.6..3.2 um, E0 in [0.002, 0.006]) into the continuous-batching
+    server; p50/p99 latency from submit to result, and solves/hour against
+    plain FP64 solves one after another on the same request distribution."""
+    import concurrent.futures as cf
+
+    import torch
+
+    import antelope_b200 as ab
+    from antelope_b200 import workloads
+
+    arrivals, cases = workloads.serving_cases(n=args.serve_requests, rate_hz=args.serve_rate, precision="mixed")
+    probs = [ab.Problem.from_dict(c) for c in cases]
+    srv = ab.Server(precision="mixed", steps_per_launch=256)
+    lat = [None] * len(probs)
+    t0 = time.perf_counter()
+
+    def submit(i):
+        dt = t0 + arrivals[i] - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        return srv.submit(probs[i])
+
+    with cf.ThreadPoolExecutor(max_workers=16) as pool:
+        rids = list(pool.map(submit, range(len(probs))))
+    for i, rid in enumerate(rids):
+        _, lat[i] = srv.wait(rid, timeout=600)
+    wall = time.perf_counter() - t0
+    stats = srv.stats()
+    srv.close()
+    kst = sum(float(p.dims.ntotal) * p.dims.Nt for p in probs)
+    stream = torch.cuda.Stream()
+    sub = list(range(0, len(probs), 20))
+    fp64_ms, _ = _fp64_sequential([probs[i] for i in sub], stream)
+    sph = len(probs) / wall * 3600.0
+    sph64 = len(sub) / (fp64_ms * 1e-3) * 3600.0
+    lat = np.array(lat)
+    return {"requests": len(probs), "rate_hz": args.serve_rate, "wall_s": wall,
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "mean_latency_s": float(lat.mean()), "solves_per_hour": sph, "k_steps_per_s": kst / wall,
+            "fp64_sequential_solves_per_hour": sph64, "served_mixed_over_sequential_fp64": sph / sph64,
+            "fp64_sequential_sample": f"{len(sub)} of {len(probs)} requests (every 20th)",
+            "failed": stats["failed"], "launches": stats["launches"],
+            "note": "offered load = arrival rate; solves/hour over the wall time of the whole stream"}
 
 
 def read_traffic():
@@ -336,6 +457,9 @@ def main():
     ap.add_argument("--cpu-seconds", dest="cpu_seconds", type=float, default=12.0)
     ap.add_argument("--ref-seconds", dest="ref_seconds", type=float, default=6.0)
     ap.add_argument("--no-cpu-baseline", dest="no_cpu_baseline", action="store_true")
+    ap.add_argument("--scan-solves", dest="scan_solves", type=int, default=256)
+    ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=600)
+    ap.add_argument("--serve-rate", dest="serve_rate", type=float, default=40.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
