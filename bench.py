@@ -93,6 +93,10 @@ class ClockSampler:
 def run_ours(args):
     import torch
 
+    # record the launch shapes the autotuner picks (reported in the JSON line)
+    tune_file = tempfile.NamedTemporaryFile(prefix="sbe_tune_", suffix=".txt", delete=False).name
+    os.environ.setdefault("SBE_TUNE_CACHE", tune_file)
+
     import antelope_b200 as ab
     from antelope_b200 import cfgtext, workloads
     from antelope_b200.api import Outputs, Solver
@@ -219,6 +223,7 @@ def run_ours(args):
                      "peak_source": "measured FMA-chain microbenchmark (MEASURED_PEAKS.json has no FP32/FP64)",
                      "flops_per_kstep": FLOPS_PER_KSTEP[4], "kernel": "propagate_vg<float,4>",
                      "kernel_share": prop_ms / (prop_ms + red_ms)},
+        "launch_shapes": read_tune_cache(),
         "gpu_launches": int(launches) * 2,   # propagate + reduce per launch tick, timed steps only
         "clocks": clocks,
     }
@@ -349,6 +354,18 @@ def run_serve(args):
             "fp64_sequential_sample": f"{len(sub)} of {len(probs)} requests (every 20th)",
             "failed": stats["failed"], "launches": stats["launches"],
             "note": "offered load = arrival rate; solves/hour over the wall time of the whole stream"}
+
+
+def read_tune_cache():
+    path = os.environ.get("SBE_TUNE_CACHE")
+    out = {}
+    try:
+        for line in open(path):
+            k, tile, kpt = line.split()
+            out[k] = {"tile_k": int(tile), "k_per_thread": int(kpt)}
+    except (OSError, TypeError, ValueError):
+        pass
+    return out
 
 
 def read_traffic():
