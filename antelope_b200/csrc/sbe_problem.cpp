@@ -498,10 +498,72 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
         for (int i = 0; i < 3; ++i) p.bzorigin[i] = 0.0;
         if (custom)
             throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
+    } else if (p.target == "SyntheticWannier") {
+        // explicit tight-binding tables (model form of Materials/Wannier90.h:297-387)
+        p.model = MODEL_SYNTHETIC_WANNIER;
+        if (!mat || !get_int(mat, "Nband", p.nband) || !get_int(mat, "Nval", p.nval))
+            throw CfgError("SyntheticWannier needs Nband and Nval");
+        if (p.nband < 2 || p.nband > 8 || p.nval < 0 || p.nval > p.nband)
+            throw CfgError("SyntheticWannier: 2 <= Nband <= 8 and 0 <= Nval <= Nband");
+        const int N = p.nband;
+        auto arr = [&](const char *key) -> const CfgValue & {
+            const CfgValue *x = mat->get(key);
+            if (!x || (x->type != CfgValue::Array && x->type != CfgValue::List))
+                throw CfgError(std::string("SyntheticWannier.") + key + " missing");
+            return *x;
+        };
+        const CfgValue &lat = arr("lattice"), &R = arr("R"), &hre = arr("h_re"), &him = arr("h_im");
+        if (lat.items.size() != 4) throw CfgError("SyntheticWannier.lattice needs 4 floats");
+        for (int i = 0; i < 4; ++i) p.w_lat[i] = elem_double(lat, i, "SyntheticWannier.lattice: floats");
+        if (R.items.empty() || R.items.size() % 2) throw CfgError("SyntheticWannier.R needs pairs of integers");
+        p.w_nR = (int)R.items.size() / 2;
+        p.w_R.resize(R.items.size());
+        for (size_t i = 0; i < R.items.size(); ++i) p.w_R[i] = elem_int(R, i, "SyntheticWannier.R: integers");
+        const size_t nh = (size_t)p.w_nR * N * N;
+        if (hre.items.size() != nh || him.items.size() != nh)
+            throw CfgError("SyntheticWannier.h_re/h_im need nR*Nband*Nband floats");
+        p.w_h.resize(2 * nh);
+        for (size_t i = 0; i < nh; ++i) {
+            p.w_h[2 * i] = elem_double(hre, i, "SyntheticWannier.h_re: floats");
+            p.w_h[2 * i + 1] = elem_double(him, i, "SyntheticWannier.h_im: floats");
+        }
+        if (mat->get("d_re")) {
+            const CfgValue &dre = arr("d_re"), &dim = arr("d_im");
+            if (dre.items.size() != 2 * nh || dim.items.size() != 2 * nh)
+                throw CfgError("SyntheticWannier.d_re/d_im need nR*2*Nband*Nband floats");
+            p.w_d.resize(4 * nh);
+            for (size_t i = 0; i < 2 * nh; ++i) {
+                p.w_d[2 * i] = elem_double(dre, i, "SyntheticWannier.d_re: floats");
+                p.w_d[2 * i + 1] = elem_double(dim, i, "SyntheticWannier.d_im: floats");
+            }
+        }
+        // Hermiticity: h_{-R} = h_R^dagger (and the same for d)
+        for (int r = 0; r < p.w_nR; ++r) {
+            int m = -1;
+            for (int q = 0; q < p.w_nR; ++q)
+                if (p.w_R[2 * q] == -p.w_R[2 * r] && p.w_R[2 * q + 1] == -p.w_R[2 * r + 1]) m = q;
+            if (m < 0) throw CfgError("SyntheticWannier.R must contain -R for every R");
+            for (int i = 0; i < N; ++i)
+                for (int j = 0; j < N; ++j) {
+                    const size_t a = ((size_t)r * N + i) * N + j, b = ((size_t)m * N + j) * N + i;
+                    if (std::fabs(p.w_h[2 * a] - p.w_h[2 * b]) > 1e-12 ||
+                        std::fabs(p.w_h[2 * a + 1] + p.w_h[2 * b + 1]) > 1e-12)
+                        throw CfgError("SyntheticWannier: h_{-R} must equal h_R^dagger");
+                }
+        }
+        // reciprocal basis b_i . a_j = 2 pi delta_ij (Wannier90.h:489-502)
+        const double det = p.w_lat[0] * p.w_lat[3] - p.w_lat[1] * p.w_lat[2];
+        if (det == 0.0) throw CfgError("SyntheticWannier.lattice is singular");
+        const double axes[9] = {2 * PI * p.w_lat[3] / det, -2 * PI * p.w_lat[2] / det, 0,
+                                -2 * PI * p.w_lat[1] / det, 2 * PI * p.w_lat[0] / det, 0, 0, 0, 0};
+        for (int i = 0; i < 9; ++i) p.bzaxes[i] = axes[i];
+        for (int i = 0; i < 3; ++i) p.bzorigin[i] = 0.0;
+        if (custom)
+            throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
+        unsup("SyntheticWannier models are not built on the GPU path yet");
     } else if (p.target == "Haldane2L" || p.target == "KaneMele" || p.target == "WilsonMass" ||
                p.target == "Bi2Se3surf" || p.target == "TMDCs" || p.target == "XYHlattice" ||
-               p.target == "SquareSBand" || p.target == "WDSM_TaAs" || p.target == "MultiWSM" ||
-               p.target == "SyntheticWannier") {
+               p.target == "SquareSBand" || p.target == "WDSM_TaAs" || p.target == "MultiWSM") {
         unsup("material '" + p.target + "' is not built on the GPU path");
         return p;
     } else {
@@ -520,7 +582,8 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
 
     if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) unsup("gauge LengthHamiltonian is not implemented in the reference either");
     if (p.shot_number > 0) unsup("density snapshots (calc.shotNumber > 0) are not built");
-    if (p.rk == 45) unsup("adaptive Cash-Karp steps are built for Wannier models only");
+    if (p.rk == 45 && p.model != MODEL_SYNTHETIC_WANNIER)
+        unsup("adaptive Cash-Karp steps are built for Wannier models only");
     return p;
 }
 

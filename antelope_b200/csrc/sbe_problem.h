@@ -84,6 +84,13 @@ struct Problem {
     // Haldane (Materials/Haldane.h:46-84): a0 in bohr
     double hal_t1 = 0, hal_t2 = 0, hal_M0 = 0, hal_phi0 = 0, hal_a0 = 0;
     double hal_va[3][2] = {{0}}, hal_vb[3][2] = {{0}};
+    // Synthetic Wannier model (N <= 8 bands): H(k) = sum_R h_R e^{ik.R},
+    // D_a(k) = sum_R d_{a,R} e^{ik.R}, R = n1 a1 + n2 a2
+    int w_nR = 0;
+    double w_lat[4] = {0, 0, 0, 0};   // a1 = (w_lat[0], w_lat[1]), a2 = (w_lat[2], w_lat[3])
+    std::vector<int> w_R;             // [nR][2] lattice coordinates
+    std::vector<double> w_h;          // [nR][N][N] complex, interleaved
+    std::vector<double> w_d;          // [nR][2][N][N] complex, interleaved (empty: no dipoles)
 
     // derived grid quantities (momaxis.h:192-240)
     int ntotal() const { return Nk[0] * Nk[1] * Nk[2]; }

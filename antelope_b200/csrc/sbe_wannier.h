@@ -1,0 +1,67 @@
+// Device structures of the N-band (N <= 8) Wannier tight-binding solves,
+// length gauge (SBEs.h:762-872 with a Wannier model, Materials/Wannier90.h:
+// 297-387 model form).  One warp advances one k-point; a launch performs one
+// attempted step of every k-point of the solve; a one-block controller kernel
+// accepts or rejects it (Cash-Karp, one step size per solve) or always
+// accepts (fixed-step RK4 / Fehlberg-5).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace sbe {
+
+constexpr int WAN_MAXN = 8;
+constexpr int WAN_MAXR = 64;       // lattice vectors
+constexpr int WAN_NSLOT = 16;      // inter x,y; intra x,y; occupations (N); coherence re, im
+constexpr int WAN_WARPS = 4;       // warps (k-points) per CTA
+
+struct PulseDev {
+    double E0x, E0y, A0x, A0y, w0, cep, t0, twidth, twidth_clipped, envfactor;
+    double xdir[3], ydir[3];
+    int env;
+};
+
+struct LaserDev {
+    int npulses;
+    PulseDev p[8];
+    double init_A[3], init_E[3];
+};
+
+struct WanCtl {
+    double tc;          // time of the committed state
+    double h;           // proposed step size
+    double hs;          // step size of the next attempt
+    double emax;        // error of the last attempt
+    int n;              // output interval: the committed state is at t_n <= tc < t_{n+1}
+    int buf;            // committed state buffer (0/1)
+    int last;           // the next attempt ends the interval
+    int need_current;   // the next attempt records the currents at tc = t_n first
+    int done;
+    int error;          // 1: step-size underflow / too many rejections
+    long long steps, attempts, rejects;
+};
+
+struct WanDev {
+    int N, nval, nR, nk, Nt, ntiles, rk, inter_intra, use_fermi, has_dip;
+    double Ef, dt, atmin, tol, g1, g2;  // g1 = 1/T1, g2 = 1/T2 (0 when disabled)
+    int Ngrid[3];
+    double axes[9], origin[3];
+    double lat[4];
+    LaserDev laser;
+    const int *R;           // [nR][2]
+    const void *h;          // [nR][N*N] complex Real
+    const void *d;          // [nR][2][N*N] complex Real (or null)
+    double2 *rho[2];        // [nk][N*N] committed / trial state (Wannier basis, full matrix), FP64
+    void *U[2];             // [nk][N*N] tracked eigenbasis of H0(k+A), Real complex
+    double *weight;         // [nk]
+    double *tile_err;       // [ntiles]
+    double *cur_part;       // [ntiles][WAN_NSLOT]
+    double *jout;           // [Nt][WAN_NSLOT]
+    WanCtl *ctl;
+};
+
+cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st);
+cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st);
+cudaError_t launch_wan_control(const WanDev *dw, cudaStream_t st);
+
+}  // namespace sbe
