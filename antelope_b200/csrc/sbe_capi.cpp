@@ -457,6 +457,7 @@ void sbe_server::loop()
     eo.precision = opts.precision;
     eo.tile_k = opts.tile_k;
     eo.kpt = opts.k_per_thread;
+    eo.allow_tuning = false;  // never stall the serving loop on a tuning run
     std::vector<cudaEvent_t> pool;
     for (;;) {
         std::unique_lock<std::mutex> lk(mu);

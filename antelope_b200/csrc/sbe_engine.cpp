@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 
 #include "sbe_kernels.h"
 
@@ -24,6 +25,88 @@ void cuda_check(cudaError_t e, const char *what)
 namespace {
 int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 }  // namespace
+
+UploadRing::UploadRing(size_t bytes) : cap_(bytes)
+{
+    cuda_check(cudaMallocHost(&base_, cap_), "cudaMallocHost(upload ring)");
+}
+
+UploadRing::~UploadRing()
+{
+    for (auto &sp : inflight_) {
+        cudaEventSynchronize(sp.ev);
+        cudaEventDestroy(sp.ev);
+    }
+    for (auto ev : spare_) cudaEventDestroy(ev);
+    cudaFreeHost(base_);
+}
+
+void UploadRing::upload(void *dst, const void *src, size_t bytes, cudaStream_t st)
+{
+    if (bytes == 0) return;
+    if (bytes > cap_) {  // larger than the ring: stage it in pieces
+        const char *s = static_cast<const char *>(src);
+        char *d = static_cast<char *>(dst);
+        for (size_t off = 0; off < bytes; off += cap_ / 2) upload(d + off, s + off, std::min(cap_ / 2, bytes - off), st);
+        return;
+    }
+    const size_t need = (bytes + 255) & ~size_t(255);
+    if (head_ + need > cap_) head_ = 0;
+    const size_t lo = head_, hi = head_ + need;
+    // wait for copies still reading this region
+    for (size_t i = 0; i < inflight_.size();) {
+        Span &sp = inflight_[i];
+        const bool overlap = sp.lo < hi && lo < sp.hi;
+        if (overlap || cudaEventQuery(sp.ev) == cudaSuccess) {
+            if (overlap) cuda_check(cudaEventSynchronize(sp.ev), "upload ring wait");
+            spare_.push_back(sp.ev);
+            inflight_[i] = inflight_.back();
+            inflight_.pop_back();
+        } else {
+            ++i;
+        }
+    }
+    std::memcpy(base_ + lo, src, bytes);
+    cuda_check(cudaMemcpyAsync(dst, base_ + lo, bytes, cudaMemcpyHostToDevice, st), "upload");
+    cudaEvent_t ev;
+    if (spare_.empty()) cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event create");
+    else { ev = spare_.back(); spare_.pop_back(); }
+    cuda_check(cudaEventRecord(ev, st), "event record");
+    inflight_.push_back(Span{lo, hi, ev});
+    head_ = hi;
+}
+
+size_t PinnedPool::size_class(size_t b)
+{
+    size_t c = 4096;
+    while (c < b) c <<= 1;
+    return c;
+}
+
+void *PinnedPool::get(size_t bytes)
+{
+    const size_t c = size_class(bytes);
+    auto &v = free_[c];
+    if (!v.empty()) {
+        void *p = v.back();
+        v.pop_back();
+        return p;
+    }
+    void *p = nullptr;
+    cuda_check(cudaMallocHost(&p, c), "cudaMallocHost(results)");
+    return p;
+}
+
+void PinnedPool::put(void *p, size_t bytes)
+{
+    if (p) free_[size_class(bytes)].push_back(p);
+}
+
+PinnedPool::~PinnedPool()
+{
+    for (auto &kv : free_)
+        for (void *p : kv.second) cudaFreeHost(p);
+}
 
 struct Engine::Solve {
     Problem prob;
@@ -53,9 +136,9 @@ Engine::Engine(int device, cudaStream_t stream, int steps_per_launch)
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
     capacity_ = 4096;
     cuda_check(cudaMalloc(&d_solves_, sizeof(SolveDev) * capacity_), "cudaMalloc(solves)");
-    cuda_check(cudaMallocHost(&h_solves_, sizeof(SolveDev) * capacity_), "cudaMallocHost(solves)");
+    h_solves_ = new SolveDev[capacity_];
     cuda_check(cudaMalloc(&d_ids_, sizeof(int) * capacity_), "cudaMalloc(ids)");
-    cuda_check(cudaMallocHost(&h_ids_, sizeof(int) * capacity_), "cudaMallocHost(ids)");
+    h_ids_.assign(capacity_, 0);
     for (int i = capacity_ - 1; i >= 0; --i) free_slots_.push_back(i);
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess) {
@@ -75,18 +158,20 @@ Engine::~Engine()
         cudaFreeAsync(s.partial, stream_);
         cudaFreeAsync(s.jout, stream_);
         cudaFreeAsync(s.constpart, stream_);
-        cudaFreeHost(s.h_jout);
-        cudaFreeHost(s.h_const);
-        if (s.ev) cudaEventDestroy(s.ev);
+        if (s.ev) {
+            cudaEventSynchronize(s.ev);
+            cudaEventDestroy(s.ev);
+        }
+        pinned_.put(s.h_jout, (size_t)s.Nt * NSLOT * 8);
+        pinned_.put(s.h_const, (size_t)s.ntiles * NSLOT * 8);
     }
-    for (auto &kv : groups_) cudaFree(kv.second->d_tiles);
+    for (auto &kv : groups_) cudaFreeAsync(kv.second->d_tiles, stream_);
     for (auto &e : prop_ev_) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     for (auto &e : red_ev_) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     cudaStreamSynchronize(stream_);
     cudaFree(d_solves_);
-    cudaFreeHost(h_solves_);
+    delete[] h_solves_;
     cudaFree(d_ids_);
-    cudaFreeHost(h_ids_);
 }
 
 Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
@@ -99,8 +184,9 @@ Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
     if (!vg) s.kpt = 1;
     if (o.tile_k > 0) {
         s.tile_k = o.tile_k;
-    } else if (o.kpt <= 0 && autotune_enabled()) {
-        return autotune_shape(device_, p, prec);
+    } else if (o.kpt <= 0 && autotune_enabled() &&
+               (o.allow_tuning || autotune_lookup(device_, p, prec, &s))) {
+        return o.allow_tuning ? autotune_shape(device_, p, prec) : s;
     } else {
         // largest CTA (<= 128 threads) that still gives >= 2 CTAs per SM
         int sms = 148;
@@ -175,8 +261,8 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     alloc((void **)&s->jout, jout_b, "alloc outputs");
     alloc((void **)&s->constpart, cp_b, "alloc constant parts");
     s->bytes = kc_b + st_b + tab_n * real + part_b + jout_b + cp_b;
-    cuda_check(cudaMallocHost(&s->h_jout, jout_b), "cudaMallocHost(jout)");
-    cuda_check(cudaMallocHost(&s->h_const, cp_b), "cudaMallocHost(constpart)");
+    s->h_jout = static_cast<double *>(pinned_.get(jout_b));
+    s->h_const = static_cast<double *>(pinned_.get(cp_b));
     cuda_check(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate");
 
     // field tables (host FP64, rounded once to the kernel's Real)
@@ -187,10 +273,10 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     if (!vg) tabd_own = phase_table(p, atab);
     const std::vector<double> &tabd = vg ? atab : tabd_own;
     if (s->precision == PREC_FP64) {
-        cuda_check(cudaMemcpyAsync(s->tab, tabd.data(), tab_n * 8, cudaMemcpyHostToDevice, stream_), "copy table");
+        ring_.upload(s->tab, tabd.data(), tab_n * 8, stream_);
     } else {
         std::vector<float> tf(tabd.begin(), tabd.end());
-        cuda_check(cudaMemcpyAsync(s->tab, tf.data(), tab_n * 4, cudaMemcpyHostToDevice, stream_), "copy table");
+        ring_.upload(s->tab, tf.data(), tab_n * 4, stream_);
     }
     InitArgs ia{};
     ia.nk = s->nk;
@@ -242,8 +328,7 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     d.t2s = t2s;
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 2; ++j) { d.va[i][j] = p.hal_va[i][j]; d.vb[i][j] = p.hal_vb[i][j]; }
-    cuda_check(cudaMemcpyAsync(d_solves_ + s->slot, &d, sizeof(SolveDev), cudaMemcpyHostToDevice, stream_),
-               "copy descriptor");
+    ring_.upload(d_solves_ + s->slot, &d, sizeof(SolveDev), stream_);
     s->admit_tick = tick_;
     s->nticks = ceil_div(s->Nt, S_);
     bytes_in_use_ += s->bytes;
@@ -281,8 +366,6 @@ int Engine::max_remaining_ticks() const
 
 void Engine::rebuild_lists()
 {
-    // the pinned id list may still feed an in-flight copy
-    cuda_check(cudaStreamSynchronize(stream_), "sync before list rebuild");
     for (auto &kv : groups_) kv.second->tiles.clear();
     nids_ = 0;
     for (auto &kv : live_) {
@@ -312,17 +395,13 @@ void Engine::rebuild_lists()
     for (auto &kv : groups_) {
         Group &g = *kv.second;
         if ((int)g.tiles.size() > g.cap) {
-            cudaFree(g.d_tiles);
+            if (g.d_tiles) cudaFreeAsync(g.d_tiles, stream_);
             g.cap = std::max<int>((int)g.tiles.size(), 2 * g.cap);
-            cuda_check(cudaMalloc(&g.d_tiles, sizeof(TileDev) * g.cap), "cudaMalloc(tiles)");
+            cuda_check(cudaMallocAsync((void **)&g.d_tiles, sizeof(TileDev) * g.cap, stream_), "alloc tiles");
         }
-        if (!g.tiles.empty())
-            cuda_check(cudaMemcpyAsync(g.d_tiles, g.tiles.data(), sizeof(TileDev) * g.tiles.size(),
-                                       cudaMemcpyHostToDevice, stream_),
-                       "copy tiles");
+        if (!g.tiles.empty()) ring_.upload(g.d_tiles, g.tiles.data(), sizeof(TileDev) * g.tiles.size(), stream_);
     }
-    if (nids_ > 0)
-        cuda_check(cudaMemcpyAsync(d_ids_, h_ids_, sizeof(int) * nids_, cudaMemcpyHostToDevice, stream_), "copy ids");
+    if (nids_ > 0) ring_.upload(d_ids_, h_ids_.data(), sizeof(int) * nids_, stream_);
     dirty_ = false;
 }
 
@@ -463,8 +542,8 @@ void Engine::remove(int id)
     cudaFreeAsync(s.jout, stream_);
     cudaFreeAsync(s.constpart, stream_);
     if (s.fetched) cudaEventSynchronize(s.ev);
-    cudaFreeHost(s.h_jout);
-    cudaFreeHost(s.h_const);
+    pinned_.put(s.h_jout, (size_t)s.Nt * NSLOT * 8);
+    pinned_.put(s.h_const, (size_t)s.ntiles * NSLOT * 8);
     cudaEventDestroy(s.ev);
     bytes_in_use_ -= s.bytes;
     free_slots_.push_back(s.slot);

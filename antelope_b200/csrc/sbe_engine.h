@@ -30,6 +30,40 @@ struct EngineOptions {
     int tile_k = 0;          // k-points per tile (0: tuned default)
     int kpt = 0;             // k-points per thread (0: tuned default)
     int steps_per_launch = 0;  // S (0: default)
+    bool allow_tuning = true;  // false: a cached tuned shape or the heuristic, never a tuning run
+};
+
+// Pinned staging for host->device uploads: copies are issued from a pinned
+// ring (a pageable source would make cudaMemcpyAsync wait for the stream), and
+// a region is reused only after the event recorded behind its copy.
+class UploadRing {
+public:
+    explicit UploadRing(size_t bytes);
+    ~UploadRing();
+    void upload(void *dst, const void *src, size_t bytes, cudaStream_t st);
+
+private:
+    struct Span {
+        size_t lo, hi;
+        cudaEvent_t ev;
+    };
+    char *base_ = nullptr;
+    size_t cap_ = 0, head_ = 0;
+    std::vector<Span> inflight_;
+    std::vector<cudaEvent_t> spare_;
+};
+
+// Reusable pinned host buffers for device->host results (cudaMallocHost and
+// cudaFreeHost are expensive and can synchronise the device).
+class PinnedPool {
+public:
+    ~PinnedPool();
+    void *get(size_t bytes);
+    void put(void *p, size_t bytes);
+
+private:
+    static size_t size_class(size_t b);
+    std::map<size_t, std::vector<void *>> free_;
 };
 
 // One launch shape for a class of solves.
@@ -116,8 +150,11 @@ private:
     std::map<int, std::unique_ptr<Solve>> live_;
     std::vector<int> free_slots_;
     SolveDev *d_solves_ = nullptr;
-    SolveDev *h_solves_ = nullptr;   // pinned mirror
-    int *d_ids_ = nullptr, *h_ids_ = nullptr;
+    SolveDev *h_solves_ = nullptr;   // host mirror of the descriptors
+    int *d_ids_ = nullptr;
+    std::vector<int> h_ids_;
+    UploadRing ring_{32u << 20};
+    PinnedPool pinned_;
     int nids_ = 0;
     int status_dummy_ = 0;
     std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<Group>> groups_;
@@ -126,6 +163,8 @@ private:
 // Autotuner (sbe_tune.cpp): the fastest launch shape for this class of solve.
 bool autotune_enabled();
 Shape autotune_shape(int device, const Problem &p, int precision);
+// Cached tuned shape only (no tuning run); false when none is cached.
+bool autotune_lookup(int device, const Problem &p, int precision, Shape *out);
 
 // Assemble the reference's output quantities from the per-step slot sums.
 void assemble_outputs(const Problem &p, const std::vector<double> &jout, const double constpart[NSLOT],

@@ -601,23 +601,35 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
 }
 
 // ------------------------------------------------------- second pass
-// One warp per (solve, step): lanes 8g..8g+7 sum slots 0..7 over tiles
-// g, g+4, g+8, ... ; two fixed shuffles combine the four groups.
+// One CTA per (step, solve): its 8 warps split the tile rows into 8 fixed
+// contiguous ranges; within a warp, lanes 8g..8g+7 sum slots 0..7 over tiles
+// g, g+4, ... of the range and two fixed shuffles combine the four groups;
+// the 8 warp sums are added in warp order.  The order depends only on the
+// solve's tile count, so the sums are deterministic.
 __global__ void __launch_bounds__(256) reduce_tiles(const SolveDev *__restrict__ solves,
                                                     const int *__restrict__ solve_ids, int tick, int S)
 {
+    __shared__ double part[8][NSLOT];
     const SolveDev &sd = solves[solve_ids[blockIdx.y]];
     const int s0 = (tick - sd.admit_tick) * S;
-    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
+    const int j = blockIdx.x;
     if (s0 < 0 || j >= S || s0 + j >= sd.Nt) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int slot = lane & 7, g = lane >> 3, nt = sd.ntiles;
+    const int chunk = (nt + 7) / 8;
+    const int t0 = min(nt, warp * chunk), t1 = min(nt, t0 + chunk);
     const double *p = sd.partial + (size_t)j * nt * NSLOT;
     double acc = 0.0;
-    for (int t = g; t < nt; t += 4) acc += p[(size_t)t * NSLOT + slot];
+    for (int t = t0 + g; t < t1; t += 4) acc += p[(size_t)t * NSLOT + slot];
     acc += __shfl_xor_sync(0xffffffffu, acc, 8);
     acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-    if (lane < 8) sd.jout[(size_t)(s0 + j) * NSLOT + slot] = acc;
+    if (lane < 8) part[warp][lane] = acc;
+    __syncthreads();
+    if (threadIdx.x < NSLOT) {
+        double sum = 0.0;
+        for (int w = 0; w < 8; ++w) sum += part[w][threadIdx.x];
+        sd.jout[(size_t)(s0 + j) * NSLOT + threadIdx.x] = sum;
+    }
 }
 
 // ------------------------------------------------------------ set-up
@@ -884,9 +896,8 @@ cudaError_t launch_reduce(const SolveDev *solves, const int *solve_ids, int nsol
                           cudaStream_t stream)
 {
     if (nsolves <= 0) return cudaSuccess;
-    const int warps = 8;
-    dim3 grid((S + warps - 1) / warps, nsolves);
-    reduce_tiles<<<grid, warps * 32, 0, stream>>>(solves, solve_ids, tick, S);
+    dim3 grid(S, nsolves);
+    reduce_tiles<<<grid, 256, 0, stream>>>(solves, solve_ids, tick, S);
     return cudaGetLastError();
 }
 

@@ -60,6 +60,30 @@ bool autotune_enabled()
     return !(e && e[0] == '0');
 }
 
+static std::string tune_key(int device, const Problem &p, int precision);
+
+bool autotune_lookup(int device, const Problem &p, int precision, Shape *out)
+{
+    const std::string key = tune_key(device, p, precision);
+    std::lock_guard<std::mutex> lk(g_mu);
+    load_cache();
+    auto it = g_cache.find(key);
+    if (it == g_cache.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+static std::string tune_key(int device, const Problem &p, int precision)
+{
+    int sms = 0;
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device attribute");
+    const int bucket = (int)std::floor(2.0 * std::log2((double)std::max(p.ntotal(), 1)));
+    std::ostringstream ks;
+    ks << (p.gauge == GAUGE_VELOCITY ? "vg" : "lw") << '-' << (precision == PREC_FP64 ? "fp64" : "mixed") << "-rk"
+       << p.rk << "-t1" << (p.T1 > 1.0e-16 ? 1 : 0) << "-nk" << bucket << "-sm" << sms;
+    return ks.str();
+}
+
 Shape autotune_shape(int device, const Problem &p, int precision)
 {
     int sms = 0;
