@@ -16,6 +16,7 @@
 #include "sbe_engine.h"
 #include "sbe_handles.h"
 #include "sbe_kernels.h"
+#include "sbe_wansolve.h"
 
 using namespace sbe;
 
@@ -199,6 +200,7 @@ extern "C" void sbe_problem_destroy(sbe_problem *p) { delete p; }
 // ================================================================= solver
 struct sbe_solver {
     std::unique_ptr<Engine> eng;
+    std::unique_ptr<WannierSolve> wan;  // N-band Wannier problems
     cudaStream_t own = nullptr;
     cudaEvent_t ready = nullptr;
     int id = -1;
@@ -219,11 +221,16 @@ extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *op
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking), "stream create");
         cuda_check(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming), "event create");
-        s->eng = std::make_unique<Engine>(s->device, s->own, default_steps(opts));
-        s->id = s->eng->add(p->p, to_engine_opts(opts));
+        if (p->p.model == MODEL_SYNTHETIC_WANNIER) {
+            const int prec = (opts && opts->precision >= 0) ? opts->precision : p->p.precision;
+            s->wan = std::make_unique<WannierSolve>(p->p, prec, s->device, s->own);
+        } else {
+            s->eng = std::make_unique<Engine>(s->device, s->own, default_steps(opts));
+            s->id = s->eng->add(p->p, to_engine_opts(opts));
+            s->use_graph = opts && opts->use_graph && !opts->profile;
+            s->eng->set_profile(opts && opts->profile);
+        }
         cuda_check(cudaEventRecord(s->ready, s->own), "event record");
-        s->use_graph = opts && opts->use_graph && !opts->profile;
-        s->eng->set_profile(opts && opts->profile);
         *out = s.release();
         return SBE_OK;
     });
@@ -237,6 +244,12 @@ extern "C" sbe_status sbe_solver_run(sbe_solver *s, void *stream)
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->own;
         cuda_check(cudaStreamWaitEvent(st, s->ready, 0), "stream wait");
+        if (s->wan) {
+            s->wan->run(st);
+            s->launches = s->wan->launches();
+            s->ran = true;
+            return SBE_OK;
+        }
         s->eng->set_stream(st);
         run_engine(*s->eng, s->use_graph, &s->launches);
         s->eng->fetch_async(s->id);
@@ -251,7 +264,7 @@ extern "C" sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out)
     if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
-        SolveOutputs o = s->eng->outputs(s->id);
+        SolveOutputs o = s->wan ? s->wan->outputs() : s->eng->outputs(s->id);
         copy_out(o, out);
         return SBE_OK;
     });
@@ -263,6 +276,13 @@ extern "C" sbe_status sbe_solver_kernel_times(sbe_solver *s, double *pms, int *p
 {
     if (!s) return fail(SBE_INVALID_ARGUMENT, "null solver");
     return guard([&]() -> sbe_status {
+        if (!s->eng) {
+            if (pms) *pms = 0;
+            if (pn) *pn = 0;
+            if (rms) *rms = 0;
+            if (rn) *rn = 0;
+            return SBE_OK;
+        }
         s->eng->kernel_times(pms, pn, rms, rn);
         return SBE_OK;
     });
@@ -273,6 +293,7 @@ extern "C" void sbe_solver_destroy(sbe_solver *s)
     if (!s) return;
     cudaSetDevice(s->device);
     s->eng.reset();
+    s->wan.reset();
     if (s->ready) cudaEventDestroy(s->ready);
     if (s->own) {
         cudaStreamSynchronize(s->own);
@@ -334,8 +355,11 @@ extern "C" sbe_status sbe_batch_create(const sbe_problem *const *problems, int n
 {
     if (!problems || n <= 0 || !out) return fail(SBE_INVALID_ARGUMENT, "need at least one problem");
     *out = nullptr;
-    for (int i = 0; i < n; ++i)
+    for (int i = 0; i < n; ++i) {
         if (sbe_status st = check_problem(problems[i])) return st;
+        if (problems[i]->p.model != MODEL_HALDANE)
+            return fail(SBE_UNSUPPORTED, "Wannier models run through sbe_solver_* (one solve at a time)");
+    }
     return guard([&]() -> sbe_status {
         auto b = std::make_unique<sbe_batch>();
         b->device = opts ? opts->device : 0;
@@ -600,6 +624,8 @@ extern "C" sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, lon
 {
     if (!s) return fail(SBE_INVALID_ARGUMENT, "null server");
     if (sbe_status st = check_problem(p)) return st;
+    if (p->p.model != MODEL_HALDANE)
+        return fail(SBE_UNSUPPORTED, "Wannier models run through sbe_solver_* (one solve at a time)");
     auto r = std::make_unique<Request>();
     r->t_submit = Clock::now();
     r->prob = p->p;

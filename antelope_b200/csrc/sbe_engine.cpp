@@ -31,6 +31,18 @@ UploadRing::UploadRing(size_t bytes) : cap_(bytes)
     cuda_check(cudaMallocHost(&base_, cap_), "cudaMallocHost(upload ring)");
 }
 
+UploadRing &UploadRing::shared()
+{
+    static UploadRing *ring = new UploadRing(32u << 20);  // lives until exit
+    return *ring;
+}
+
+PinnedPool &PinnedPool::shared()
+{
+    static PinnedPool *pool = new PinnedPool();  // lives until exit
+    return *pool;
+}
+
 UploadRing::~UploadRing()
 {
     for (auto &sp : inflight_) {
@@ -44,6 +56,8 @@ UploadRing::~UploadRing()
 void UploadRing::upload(void *dst, const void *src, size_t bytes, cudaStream_t st)
 {
     if (bytes == 0) return;
+    std::unique_lock<std::mutex> lk(mu_, std::defer_lock);
+    if (bytes <= cap_) lk.lock();  // the split path below re-enters per piece
     if (bytes > cap_) {  // larger than the ring: stage it in pieces
         const char *s = static_cast<const char *>(src);
         char *d = static_cast<char *>(dst);
@@ -85,6 +99,7 @@ size_t PinnedPool::size_class(size_t b)
 
 void *PinnedPool::get(size_t bytes)
 {
+    std::lock_guard<std::mutex> lk(mu_);
     const size_t c = size_class(bytes);
     auto &v = free_[c];
     if (!v.empty()) {
@@ -99,6 +114,7 @@ void *PinnedPool::get(size_t bytes)
 
 void PinnedPool::put(void *p, size_t bytes)
 {
+    std::lock_guard<std::mutex> lk(mu_);
     if (p) free_[size_class(bytes)].push_back(p);
 }
 

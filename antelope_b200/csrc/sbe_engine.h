@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <mutex>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -41,8 +42,10 @@ public:
     explicit UploadRing(size_t bytes);
     ~UploadRing();
     void upload(void *dst, const void *src, size_t bytes, cudaStream_t st);
+    static UploadRing &shared();  // one per process, shared by all engines
 
 private:
+    std::mutex mu_;
     struct Span {
         size_t lo, hi;
         cudaEvent_t ev;
@@ -60,8 +63,10 @@ public:
     ~PinnedPool();
     void *get(size_t bytes);
     void put(void *p, size_t bytes);
+    static PinnedPool &shared();  // one per process, shared by all engines
 
 private:
+    std::mutex mu_;
     static size_t size_class(size_t b);
     std::map<size_t, std::vector<void *>> free_;
 };
@@ -153,8 +158,8 @@ private:
     SolveDev *h_solves_ = nullptr;   // host mirror of the descriptors
     int *d_ids_ = nullptr;
     std::vector<int> h_ids_;
-    UploadRing ring_{32u << 20};
-    PinnedPool pinned_;
+    UploadRing &ring_ = UploadRing::shared();
+    PinnedPool &pinned_ = PinnedPool::shared();
     int nids_ = 0;
     int status_dummy_ = 0;
     std::map<std::tuple<int, int, int, int, int, int>, std::unique_ptr<Group>> groups_;

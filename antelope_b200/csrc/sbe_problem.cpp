@@ -560,7 +560,8 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
         for (int i = 0; i < 3; ++i) p.bzorigin[i] = 0.0;
         if (custom)
             throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
-        unsup("SyntheticWannier models are not built on the GPU path yet");
+        if (p.gauge != GAUGE_LENGTH_WANNIER)
+            unsup("Wannier models run in the length gauge (LengthWannier) on the GPU path");
     } else if (p.target == "Haldane2L" || p.target == "KaneMele" || p.target == "WilsonMass" ||
                p.target == "Bi2Se3surf" || p.target == "TMDCs" || p.target == "XYHlattice" ||
                p.target == "SquareSBand" || p.target == "WDSM_TaAs" || p.target == "MultiWSM") {

@@ -1,0 +1,205 @@
+// Host side of the N-band Wannier solves (length gauge): device buffers,
+// model upload, the attempt/controller launch loop, and the assembly of the
+// reference's output quantities for N bands (antelope.cpp:514-548).
+#include "sbe_wansolve.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace sbe {
+
+namespace {
+template <class T> void dalloc(T **p, size_t bytes, cudaStream_t st, const char *what)
+{
+    cuda_check(cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st), what);
+}
+}  // namespace
+
+WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStream_t st)
+    : prob_(p), precision_(precision), device_(device), stream_(st)
+{
+    if (p.model != MODEL_SYNTHETIC_WANNIER) throw CfgError("not a Wannier problem");
+    if (p.gauge != GAUGE_LENGTH_WANNIER)
+        throw CfgError("Wannier models run in the length gauge (LengthWannier) on this path");
+    if (p.w_nR > WAN_MAXR) throw CfgError("SyntheticWannier: at most 64 lattice vectors");
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    const int N = p.nband, NN = N * N;
+    std::memset(&w_, 0, sizeof(w_));
+    w_.N = N;
+    w_.nval = p.nval;
+    w_.nR = p.w_nR;
+    w_.nk = p.ntotal();
+    w_.Nt = p.laser.Nt;
+    w_.ntiles = (w_.nk + WAN_WARPS - 1) / WAN_WARPS;
+    w_.rk = p.rk;
+    w_.inter_intra = p.inter_intra ? 1 : 0;
+    w_.use_fermi = p.use_fermi ? 1 : 0;
+    w_.has_dip = p.w_d.empty() ? 0 : 1;
+    w_.Ef = p.Ef;
+    w_.dt = p.dt;
+    w_.atmin = p.laser.atmin;
+    w_.tol = p.rk_tol;
+    w_.g1 = p.T1 > 1.0e-16 ? 1.0 / p.T1 : 0.0;  // SBEs.h:484-493
+    w_.g2 = p.T2 > 1.0e-16 ? 1.0 / p.T2 : 0.0;
+    for (int i = 0; i < 3; ++i) w_.Ngrid[i] = p.Nk[i];
+    for (int i = 0; i < 9; ++i) w_.axes[i] = p.bzaxes[i];
+    for (int i = 0; i < 3; ++i) w_.origin[i] = p.bzorigin[i];
+    for (int i = 0; i < 4; ++i) w_.lat[i] = p.w_lat[i];
+    LaserDev &L = w_.laser;
+    L.npulses = (int)p.laser.pulses.size();
+    if (L.npulses > 8) throw CfgError("at most 8 pulses");
+    for (int i = 0; i < L.npulses; ++i) {
+        const Pulse &q = p.laser.pulses[i];
+        PulseDev &d = L.p[i];
+        d.E0x = q.E0x; d.E0y = q.E0y; d.A0x = q.A0x; d.A0y = q.A0y; d.w0 = q.w0; d.cep = q.cep; d.t0 = q.t0;
+        d.twidth = q.twidth; d.twidth_clipped = q.twidth_clipped; d.envfactor = q.envfactor; d.env = q.env;
+        for (int j = 0; j < 3; ++j) { d.xdir[j] = q.xdir[j]; d.ydir[j] = q.ydir[j]; }
+    }
+    for (int j = 0; j < 3; ++j) { L.init_A[j] = p.laser.init_A[j]; L.init_E[j] = p.laser.init_E[j]; }
+
+    const size_t real = precision_ == 0 ? 8 : 4, cplx = 2 * real;
+    const size_t nk = (size_t)w_.nk;
+    int *R = nullptr;
+    void *h = nullptr, *d = nullptr;
+    dalloc(&R, sizeof(int) * p.w_R.size(), st, "alloc R");
+    dalloc(&h, cplx * p.w_h.size() / 2, st, "alloc h");
+    if (w_.has_dip) dalloc(&d, cplx * p.w_d.size() / 2, st, "alloc d");
+    for (int b = 0; b < 2; ++b) {
+        dalloc(&w_.rho[b], sizeof(double2) * nk * NN, st, "alloc rho");
+        dalloc(&w_.U[b], cplx * nk * NN, st, "alloc U");
+    }
+    dalloc(&w_.weight, sizeof(double) * nk, st, "alloc weights");
+    dalloc(&w_.tile_err, sizeof(double) * w_.ntiles, st, "alloc tile errors");
+    dalloc(&w_.cur_part, sizeof(double) * w_.ntiles * WAN_NSLOT, st, "alloc current partials");
+    dalloc(&w_.jout, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st, "alloc outputs");
+    dalloc(&w_.ctl, sizeof(WanCtl), st, "alloc control");
+    dalloc(&d_w_, sizeof(WanDev), st, "alloc descriptor");
+    w_.R = R;
+    w_.h = h;
+    w_.d = d;
+    UploadRing &ring = UploadRing::shared();
+    ring.upload(R, p.w_R.data(), sizeof(int) * p.w_R.size(), st);
+    auto up_real = [&](void *dst, const std::vector<double> &src) {
+        if (precision_ == 0) {
+            ring.upload(dst, src.data(), src.size() * 8, st);
+        } else {
+            std::vector<float> f(src.begin(), src.end());
+            ring.upload(dst, f.data(), f.size() * 4, st);
+        }
+    };
+    up_real(h, p.w_h);
+    if (w_.has_dip) up_real(d, p.w_d);
+    cuda_check(cudaMemsetAsync(w_.jout, 0, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st), "clear outputs");
+    // initial controller state: t = t_min, h = dt, currents first
+    WanCtl c{};
+    c.tc = w_.atmin;
+    c.h = w_.dt;
+    c.n = 0;
+    c.buf = 0;
+    c.need_current = 1;
+    const double tend = w_.atmin + w_.dt;
+    c.hs = c.h;
+    c.last = 0;
+    if (c.tc + c.hs >= tend - 1e-12 * w_.dt) {
+        c.hs = tend - c.tc;
+        c.last = 1;
+    }
+    ring.upload(w_.ctl, &c, sizeof(c), st);
+    ring.upload(d_w_, &w_, sizeof(w_), st);
+    cuda_check(launch_wan_init(w_, precision_, st), "Wannier init kernel");
+    cuda_check(cudaMallocHost(&h_ctl_, sizeof(WanCtl)), "cudaMallocHost(control)");
+}
+
+WannierSolve::~WannierSolve()
+{
+    cudaStreamSynchronize(stream_);
+    cudaFreeAsync((void *)w_.R, stream_);
+    cudaFreeAsync((void *)w_.h, stream_);
+    if (w_.d) cudaFreeAsync((void *)w_.d, stream_);
+    for (int b = 0; b < 2; ++b) {
+        cudaFreeAsync(w_.rho[b], stream_);
+        cudaFreeAsync(w_.U[b], stream_);
+    }
+    cudaFreeAsync(w_.weight, stream_);
+    cudaFreeAsync(w_.tile_err, stream_);
+    cudaFreeAsync(w_.cur_part, stream_);
+    cudaFreeAsync(w_.jout, stream_);
+    cudaFreeAsync(w_.ctl, stream_);
+    cudaFreeAsync(d_w_, stream_);
+    cudaStreamSynchronize(stream_);
+    if (h_ctl_) cudaFreeHost(h_ctl_);
+}
+
+void WannierSolve::run(cudaStream_t st)
+{
+    stream_ = st;
+    // attempts are launched in chunks; the controller makes surplus launches
+    // after the last step no-ops, and the host checks progress per chunk
+    const int chunk = 64;
+    const long long max_attempts = 64LL * w_.Nt + 1000;
+    long long launched = 0;
+    for (;;) {
+        for (int c = 0; c < chunk; ++c) {
+            cuda_check(launch_wan_attempt(w_, d_w_, precision_, st), "Wannier attempt kernel");
+            cuda_check(launch_wan_control(d_w_, st), "Wannier control kernel");
+        }
+        launched += chunk;
+        cuda_check(cudaMemcpyAsync(h_ctl_, w_.ctl, sizeof(WanCtl), cudaMemcpyDeviceToHost, st), "copy control");
+        cuda_check(cudaStreamSynchronize(st), "sync");
+        if (h_ctl_->done) break;
+        if (launched > max_attempts) throw CudaError("Wannier solve made no progress (step-size controller)");
+    }
+    if (h_ctl_->error) throw CudaError("Cash-Karp step size underflow: tolerance unreachable");
+    launches_ = (int)(2 * launched);
+}
+
+SolveOutputs WannierSolve::outputs()
+{
+    const Problem &p = prob_;
+    const int Nt = w_.Nt, N = p.nband, NN = N * N;
+    std::vector<double> j((size_t)Nt * WAN_NSLOT);
+    cuda_check(cudaMemcpyAsync(j.data(), w_.jout, j.size() * 8, cudaMemcpyDeviceToHost, stream_), "copy outputs");
+    cuda_check(cudaStreamSynchronize(stream_), "sync");
+    SolveOutputs o;
+    o.Nt = Nt;
+    o.nband = N;
+    o.inter.assign((size_t)Nt * 3, 0.0);
+    o.intra.assign((size_t)Nt * 3, 0.0);
+    o.occ.assign((size_t)Nt * (N + 1), 0.0);
+    o.coh.assign((size_t)Nt * 2, 0.0);
+    o.laser.assign((size_t)Nt * 7, 0.0);
+    const double dV = p.dV, Ntot = (double)p.ntotal();
+    const int e = p.nval * N + p.nval + 1, roff = e / NN;
+    for (int n = 0; n < Nt; ++n) {
+        const double *r = &j[(size_t)n * WAN_NSLOT];
+        const double t = p.laser.atmin + p.laser.dt * n;
+        double A[3], E[3];
+        p.laser.eval(t, A, E);
+        double *L = &o.laser[(size_t)n * 7];
+        L[0] = t;
+        for (int d = 0; d < 3; ++d) { L[1 + d] = E[d]; L[4 + d] = A[d]; }
+        for (int a = 0; a < 2; ++a) {
+            if (p.inter_intra) {
+                o.inter[(size_t)n * 3 + a] = r[a] * dV;
+                o.intra[(size_t)n * 3 + a] = r[2 + a] * dV;
+            } else {
+                o.inter[(size_t)n * 3 + a] = (r[a] + r[2 + a]) * dV;
+            }
+        }
+        double tot = 0.0;
+        for (int m = 0; m < N; ++m) {
+            o.occ[(size_t)n * (N + 1) + m] = r[4 + m] / Ntot;
+            tot += r[4 + m];
+        }
+        o.occ[(size_t)n * (N + 1) + N] = tot / Ntot;
+        const int row = n + roff;  // flat element Nval*N+Nval+1 (antelope.cpp:539-542)
+        if (row < Nt) {
+            o.coh[(size_t)n * 2] = j[(size_t)row * WAN_NSLOT + 4 + N] / Ntot;
+            o.coh[(size_t)n * 2 + 1] = j[(size_t)row * WAN_NSLOT + 5 + N] / Ntot;
+        }
+    }
+    return o;
+}
+
+}  // namespace sbe
