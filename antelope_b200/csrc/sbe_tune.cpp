@@ -105,9 +105,11 @@ Shape autotune_shape(int device, const Problem &p, int precision)
         if ((long long)threads * kpt > 2LL * nk && threads > 32) return;  // tiles far larger than the grid
         cand.push_back(Shape{threads * kpt, kpt, threads});
     };
-    for (int t : {32, 64, 128, 256}) addc(t, 1);
+    // every CTA size in warps: the best one balances occupancy against the
+    // quantisation of the tile count into waves of resident CTAs
+    for (int t = 32; t <= 256; t += 32) addc(t, 1);
     if (vg)
-        for (int t : {32, 64, 128, 256}) addc(t, 2);
+        for (int t = 32; t <= 256; t += 32) addc(t, 2);
     Problem q = p;
     const int S = 128;
     q.laser.Nt = std::min(p.laser.Nt, 3 * S);

@@ -289,11 +289,26 @@ template <class Real> __device__ void jacobi_round(WarpMem<Real> &w, int N, int 
     __syncwarp();
 }
 
-template <class Real> __device__ void jacobi_sweeps(WarpMem<Real> &w, int N, int sweeps, int lane)
+// Sweeps until the off-diagonal part of B is negligible against its diagonal
+// (|offdiag|^2 <= tol2 |diag|^2, warp-uniform test), at most max_sweeps.
+template <class Real>
+__device__ void jacobi_sweeps(WarpMem<Real> &w, int N, int max_sweeps, double tol2, int lane)
 {
     const int P = N + (N & 1);
-    for (int s = 0; s < sweeps; ++s)
+    for (int s = 0; s < max_sweeps; ++s) {
+        double off = 0.0, dia = 0.0;
+        for (int e = lane; e < N * N; e += 32) {
+            const double v = double(w.B[e].x) * double(w.B[e].x) + double(w.B[e].y) * double(w.B[e].y);
+            if (e / N == e % N) dia += v;
+            else off += v;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            dia += __shfl_xor_sync(0xffffffffu, dia, o);
+        }
+        if (off <= tol2 * dia) break;
         for (int r = 0; r < P - 1; ++r) jacobi_round<Real>(w, N, r, lane);
+    }
 }
 
 // Fourier sums at the phases w.ph: H0, D0, D1 and (optionally) S_a = sum R_a h_R e^{i(k+A)R}.
@@ -425,7 +440,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
     fourier<Real>(w, P, false, Rc, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
-    jacobi_sweeps<Real>(w, N, sizeof(Real) == 8 ? 12 : 8, lane);
+    jacobi_sweeps<Real>(w, N, 16, sizeof(Real) == 8 ? 1e-30 : 1e-13, lane);
     // occupations of the eigenstates: the Nval lowest filled, or Fermi-Dirac (SBEs.h:319-340)
     if (lane < N) {
         const Real ev = w.B[lane * N + lane].x;
@@ -581,7 +596,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
             __syncwarp();
             mat_mul<T>(w.B, w.U, w.Tm, N, true, lane);
             __syncwarp();
-            jacobi_sweeps<Real>(w, N, F64 ? 2 : 1, lane);
+            jacobi_sweeps<Real>(w, N, F64 ? 6 : 3, F64 ? 1e-30 : 1e-13, lane);
             // diag(U^dag Y U)
             mat_mul<T>(w.Tm, w.Y, w.U, N, false, lane);
             __syncwarp();
