@@ -104,8 +104,8 @@ def to_problem(case: dict, nthreads: int = 1):
     p.dt = calc.get("dt", 0.1)
     p.T1 = calc.get("T1", -1.0)
     p.T2 = calc.get("T2", -1.0)
-    rk = calc.get("rk", None)
-    p.rk = 45 if rk == "cashkarp45" else int(calc.get("RKorder", 5))
+    rk = calc.get("rk", None)   # extension key; overrides RKorder when present
+    p.rk = {"rk4": 4, "rk5": 5, "fehlberg5": 5, "cashkarp45": 45}[rk] if rk else int(calc.get("RKorder", 5))
     p.rk_tol = calc.get("tol", 1e-8)
     p.inter_intra = 1 if calc.get("InterIntra", False) else 0
     p.gauge = GAUGE.get(case.get("gauge", ""), 0)
