@@ -169,18 +169,23 @@ def run_ours(args):
                                         {"inter": out_fp64.inter, "intra": out_fp64.intra}, dims.dt, 0.014238)
 
     # e2e through the C ABI from host inputs to host outputs
-    e2e_s = []
+    e2e_s, phases = [], []
     text = cfgtext.dumps(case["mixed"])
     h2d = d2h = 0
-    for i in range(max(2, args.steps // 3)):
+    for i in range(max(3, args.steps // 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         p = ab.Problem.from_text(text)
+        t1 = time.perf_counter()
         s = Solver(p, precision="mixed")
+        t2 = time.perf_counter()
         s.run(0)
         o = s.get()
+        t3 = time.perf_counter()
         s.close()
-        e2e_s.append(time.perf_counter() - t0)
+        t4 = time.perf_counter()
+        e2e_s.append(t4 - t0)
+        phases.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
     nts = 3
     tile_k = args.tile_k or 128
     ntiles = -(-dims.ntotal // tile_k)
@@ -217,6 +222,8 @@ def run_ours(args):
                            "floor": "band power >= 1e-8 of the strongest", "vs": "fp64 run"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "seconds_per_solve": statistics.mean(e2e_s),
+                "phase_seconds": dict(zip(("parse", "create", "run_and_get", "destroy"),
+                                          [statistics.mean(x) for x in zip(*phases)])),
                 "path": "sbe_problem_from_string -> sbe_solver_create -> run -> sbe_solver_get"},
         "roofline": {"bound": "fp32 FMA pipe", "achieved": achieved, "peak": fp32_tf, "unit": "TFLOP/s",
                      "frac": achieved / fp32_tf, "traffic": traffic,

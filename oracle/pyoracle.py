@@ -132,22 +132,23 @@ def to_problem(case: dict, nthreads: int = 1):
         p.hal_a0_ang, p.hal_t1, p.hal_t2, p.hal_phi0 = mat["a0"], mat["t1"], mat["t2"], mat["phi0"]
         p.hal_M0 = mat["M0"] if "M0" in mat else mat["Mt2"] * mat["t2"]
     elif target == "SyntheticWannier":
-        from antelope_b200 import wannier  # pure-numpy model generator, shared definition
-
-        model = wannier.synthetic_model(mat)
-        p.model = 1
-        p.w_nband, p.w_nval, p.w_nR = model["nband"], model["nval"], len(model["R"])
-        R = np.ascontiguousarray(model["R"], dtype=np.int32)
-        h = np.ascontiguousarray(model["h"], dtype=np.complex128)
+        # explicit tight-binding tables of the cfg group (Nband, Nval, lattice,
+        # R pairs, h_re/h_im [nR][N][N], optional d_re/d_im [nR][2][N][N])
+        N = int(mat["Nband"])
+        R = np.ascontiguousarray(np.asarray(mat["R"], dtype=np.int32).reshape(-1, 2))
+        nR = len(R)
+        h = np.ascontiguousarray((np.asarray(mat["h_re"]) + 1j * np.asarray(mat["h_im"])).reshape(nR, N, N))
         keep += [R, h]
+        p.model = 1
+        p.w_nband, p.w_nval, p.w_nR = N, int(mat["Nval"]), nR
         p.w_R = R.ctypes.data_as(C.POINTER(C.c_int))
         p.w_h = h.ctypes.data_as(C.POINTER(C.c_double))
-        if model.get("d") is not None:
-            d = np.ascontiguousarray(model["d"], dtype=np.complex128)
+        if "d_re" in mat:
+            d = np.ascontiguousarray((np.asarray(mat["d_re"]) + 1j * np.asarray(mat["d_im"])).reshape(nR, 2, N, N))
             keep.append(d)
             p.w_d = d.ctypes.data_as(C.POINTER(C.c_double))
-        for i, v in enumerate(model["lattice"]):
-            p.w_lat[i] = v
+        for i, v in enumerate(mat["lattice"]):
+            p.w_lat[i] = float(v)
     else:
         raise ValueError(f"oracle has no model '{target}'")
     p.nthreads = nthreads
