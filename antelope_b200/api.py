@@ -133,6 +133,12 @@ class Solver:
     def kernel_times(self) -> dict:
         return _kernel_times(lib.sbe_solver_kernel_times, self._h)
 
+    def steps(self) -> dict:
+        """Accepted steps, attempts and rejected attempts of the finished run."""
+        v = [C.c_longlong() for _ in range(3)]
+        _check(lib.sbe_solver_steps(self._h, *[C.byref(x) for x in v]))
+        return {"steps": v[0].value, "attempts": v[1].value, "rejects": v[2].value}
+
     def close(self):
         if getattr(self, "_h", None):
             lib.sbe_solver_destroy(self._h)

@@ -60,6 +60,8 @@ def _load():
         "sbe_solver_run": (C.c_int, [P, C.c_void_p]),
         "sbe_solver_get": (C.c_int, [P, C.POINTER(COutputs)]),
         "sbe_solver_launches": (C.c_int, [P]),
+        "sbe_solver_steps": (C.c_int, [P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_longlong)]),
         "sbe_solver_destroy": (None, [P]),
         "sbe_solver_kernel_times": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_int),
                                               C.POINTER(C.c_double), C.POINTER(C.c_int)]),

@@ -208,6 +208,7 @@ struct sbe_solver {
     bool ran = false;
     int launches = 0;
     int device = 0;
+    long long nt = 0;  // fixed-step solves: steps taken
 };
 
 extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *opts, sbe_solver **out)
@@ -227,6 +228,7 @@ extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *op
         } else {
             s->eng = std::make_unique<Engine>(s->device, s->own, default_steps(opts));
             s->id = s->eng->add(p->p, to_engine_opts(opts));
+            s->nt = p->p.laser.Nt;  // antelope.cpp:297-338: one step per output time
             s->use_graph = opts && opts->use_graph && !opts->profile;
             s->eng->set_profile(opts && opts->profile);
         }
@@ -271,6 +273,26 @@ extern "C" sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out)
 }
 
 extern "C" int sbe_solver_launches(const sbe_solver *s) { return s ? s->launches : 0; }
+
+extern "C" sbe_status sbe_solver_steps(const sbe_solver *s, long long *steps, long long *attempts,
+                                       long long *rejects)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null solver");
+    if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
+    long long st = 0, at = 0, rj = 0;
+    if (s->wan) {
+        const WanCtl &c = s->wan->control();
+        st = c.steps;
+        at = c.attempts;
+        rj = c.rejects;
+    } else {
+        st = at = s->nt;
+    }
+    if (steps) *steps = st;
+    if (attempts) *attempts = at;
+    if (rejects) *rejects = rj;
+    return SBE_OK;
+}
 
 extern "C" sbe_status sbe_solver_kernel_times(sbe_solver *s, double *pms, int *pn, double *rms, int *rn)
 {

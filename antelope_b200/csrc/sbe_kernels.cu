@@ -112,7 +112,6 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b)
     return upk(d);
 }
 __device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
 
 template <class Real> struct V2;
 template <> struct V2<double> { using T = double2; };
@@ -175,26 +174,29 @@ struct TileReducer {
 };
 
 // ------------------------------------------------------ velocity gauge
+// The state is rho - rho0 in the band basis: (da, db, z) = (drho_00,
+// drho_11, rho_01).  Starting from rho = rho0, d(db)/dt = -d(da)/dt term by
+// term (SBEs.h:787-805 with Hermitian rho), and every floating-point
+// operation on db is the sign-mirrored operation on da; round-to-nearest is
+// symmetric under negation, so db == -da holds bit for bit at every stage.
+// The kernels therefore carry three components (da, Re z, Im z) and use -da
+// wherever the reference's arithmetic reads db.
+enum VgDof : int { D_DA = 0, D_ZR, D_ZI, D_N };
+
 template <class Real, bool G1>
-__device__ __forceinline__ void vg_rhs(const Real (&c)[VG_NCONST], typename V2<Real>::T A, const Real (&y)[4],
-                                       Real g1, Real g2, Real (&k)[4])
+__device__ __forceinline__ void vg_rhs(const Real (&c)[VG_NCONST], typename V2<Real>::T A, const Real (&y)[D_N],
+                                       Real g1, Real g2, Real (&k)[D_N])
 {
     const Real delta = fma(A.y, c[VG_DPY], fma(A.x, c[VG_DPX], c[VG_DE]));
     const Real wr = fma(A.y, c[VG_PYR], A.x * c[VG_PXR]);
     const Real wi = fma(A.y, c[VG_PYI], A.x * c[VG_PXI]);
-    const Real im2 = Real(2) * fma(wi, y[VG_ZR], -(wr * y[VG_ZI]));  // 2 Im(w z*)
-    if (G1) {
-        k[VG_DA] = fma(-g1, y[VG_DA], im2);
-        k[VG_DB] = fma(-g1, y[VG_DB], -im2);
-    } else {
-        k[VG_DA] = im2;
-        k[VG_DB] = -im2;
-    }
-    const Real bma = c[VG_C0] + (y[VG_DB] - y[VG_DA]);               // rho_11 - rho_00
-    const Real xr = fma(bma, wr, delta * y[VG_ZR]);
-    const Real xi = fma(bma, wi, delta * y[VG_ZI]);
-    k[VG_ZR] = fma(-g2, y[VG_ZR], xi);                                // -i X - g2 z
-    k[VG_ZI] = fma(-g2, y[VG_ZI], -xr);
+    const Real im2 = Real(2) * fma(wi, y[D_ZR], -(wr * y[D_ZI]));  // 2 Im(w z*)
+    k[D_DA] = G1 ? fma(-g1, y[D_DA], im2) : im2;
+    const Real bma = fma(Real(-2), y[D_DA], c[VG_C0]);             // rho_11 - rho_00 = c0 + db - da
+    const Real xr = fma(bma, wr, delta * y[D_ZR]);
+    const Real xi = fma(bma, wi, delta * y[D_ZI]);
+    k[D_ZR] = fma(-g2, y[D_ZR], xi);                                // -i X - g2 z
+    k[D_ZI] = fma(-g2, y[D_ZI], -xr);
 }
 
 template <class Real, int RK, int KPT, bool G1>
@@ -221,8 +223,9 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
     // the state (rho - rho0) is kept in FP64 in both methods; the mixed
     // method rounds it to FP32 once per step for the stage arithmetic and
     // adds the FP32 step increment back in FP64
+    constexpr int slot[D_N] = {VG_DA, VG_ZR, VG_ZI};
     Real c[KPT][VG_NCONST];
-    double y64[KPT][4];
+    double y64[KPT][D_N];
     int kidx[KPT];
     bool ok[KPT];
 #pragma unroll
@@ -233,16 +236,16 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 #pragma unroll
         for (int q = 0; q < VG_NCONST; ++q) c[j][q] = ok[j] ? kc[(size_t)q * nkp + kidx[j]] : Real(0);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) y64[j][q] = ok[j] ? st[(size_t)q * nkp + kidx[j]] : 0.0;
+        for (int q = 0; q < D_N; ++q) y64[j][q] = ok[j] ? st[(size_t)slot[q] * nkp + kidx[j]] : 0.0;
     }
     TileReducer red{red_s};
 
     for (int s = s0; s < s1; ++s) {
-        Real y0[KPT][4];
+        Real y0[KPT][D_N];
 #pragma unroll
         for (int j = 0; j < KPT; ++j)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) y0[j][q] = Real(y64[j][q]);
+            for (int q = 0; q < D_N; ++q) y0[j][q] = Real(y64[j][q]);
         // currents and occupations at t_s, before rho advances (antelope.cpp:309-334)
         double v[8];
 #pragma unroll
@@ -251,15 +254,16 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
         for (int j = 0; j < KPT; ++j) {
             const Real *cc = c[j];
             const Real *yy = y0[j];
-            v[0] += double(fma(yy[VG_ZR], cc[VG_WQXR], yy[VG_ZI] * cc[VG_WQXI]));
-            v[1] += double(fma(yy[VG_ZR], cc[VG_WQYR], yy[VG_ZI] * cc[VG_WQYI]));
-            v[2] += double(fma(yy[VG_DA], cc[VG_WPX0], yy[VG_DB] * cc[VG_WPX1]));
-            v[3] += double(fma(yy[VG_DA], cc[VG_WPY0], yy[VG_DB] * cc[VG_WPY1]));
-            v[4] += double(cc[VG_W] * yy[VG_DA]);
-            v[5] += double(cc[VG_W] * yy[VG_DB]);
-            v[6] += double(cc[VG_W] * yy[VG_ZR]);
-            v[7] += double(cc[VG_W] * yy[VG_ZI]);
+            const Real db = -yy[D_DA];
+            v[0] += double(fma(yy[D_ZR], cc[VG_WQXR], yy[D_ZI] * cc[VG_WQXI]));
+            v[1] += double(fma(yy[D_ZR], cc[VG_WQYR], yy[D_ZI] * cc[VG_WQYI]));
+            v[2] += double(fma(yy[D_DA], cc[VG_WPX0], db * cc[VG_WPX1]));
+            v[3] += double(fma(yy[D_DA], cc[VG_WPY0], db * cc[VG_WPY1]));
+            v[4] += double(cc[VG_W] * yy[D_DA]);
+            v[6] += double(cc[VG_W] * yy[D_ZR]);
+            v[7] += double(cc[VG_W] * yy[D_ZI]);
         }
+        v[5] = -v[4];
         const int r = (s - s0) % SUB;
         red.push(v, r);
         if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
@@ -272,13 +276,13 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
         for (int j = 0; j < KPT; ++j) {
             // FP64: acc = rho + sum_i dt b_i k_i in the reference's order
             // (SBEs.h:614-623); mixed: the sum is formed in FP32 first
-            Real kk[TB::S][4], y[4], acc[4];
+            Real kk[TB::S][D_N], y[D_N], acc[D_N];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = F64 ? y0[j][q] : Real(0);
+            for (int q = 0; q < D_N; ++q) acc[q] = F64 ? y0[j][q] : Real(0);
 #pragma unroll
             for (int i = 0; i < TB::S; ++i) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < D_N; ++q) {
                     Real t = y0[j][q];
 #pragma unroll
                     for (int m = 0; m < i; ++m)
@@ -288,18 +292,20 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
                 vg_rhs<Real, G1>(c[j], A[TB::ti(i)], y, g1, g2, kk[i]);
                 if (TB::b(i) != 0.0) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[q] = fma(Real(TB::b(i)), kk[i][q], acc[q]);
+                    for (int q = 0; q < D_N; ++q) acc[q] = fma(Real(TB::b(i)), kk[i][q], acc[q]);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) y64[j][q] = F64 ? double(acc[q]) : y64[j][q] + double(acc[q]);
+            for (int q = 0; q < D_N; ++q) y64[j][q] = F64 ? double(acc[q]) : y64[j][q] + double(acc[q]);
         }
     }
 #pragma unroll
     for (int j = 0; j < KPT; ++j)
-        if (ok[j])
+        if (ok[j]) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx[j]] = y64[j][q];
+            for (int q = 0; q < D_N; ++q) st[(size_t)slot[q] * nkp + kidx[j]] = y64[j][q];
+            st[(size_t)VG_DB * nkp + kidx[j]] = -y64[j][D_DA];
+        }
 }
 
 // Mixed method, velocity gauge, two k-points per thread packed into f32x2
@@ -331,28 +337,24 @@ __device__ __forceinline__ float warp_sum8f(const float (&v)[8], int lane)
     return y;  // lanes 4*i hold the sum of v[i]
 }
 
+// Packed right-hand side on (da, Re z, Im z) of two k-points.  The factor 2
+// of 2 Im(w z*) and of (rho_11 - rho_00) w is folded into w (cw = 2 w, hc0 =
+// c0 / 2: exact power-of-two scalings), and the Im z slope is produced with
+// the opposite sign (nzi = -dt dIm z/dt) so that no operand needs negating;
+// the stage and step combinations apply that sign through their coefficients.
 template <bool G1>
-__device__ __forceinline__ void vg_rhs2(const float2 (&c)[VG_NCONST], float2 A, const float2 (&y)[4], float2 ng1,
-                                        float2 ng2, float2 (&k)[4])
+__device__ __forceinline__ void vg_rhs2(const float2 (&c)[VG_NCONST], float2 A, const float2 (&y)[D_N], float2 ng1,
+                                        float2 ng2, float2 g2, float2 (&k)[D_N])
 {
     const float2 ax = bc2(A.x), ay = bc2(A.y);
     const float2 delta = fma2(ay, c[VG_DPY], fma2(ax, c[VG_DPX], c[VG_DE]));
-    const float2 wr = fma2(ay, c[VG_PYR], mul2(ax, c[VG_PXR]));
-    const float2 wi = fma2(ay, c[VG_PYI], mul2(ax, c[VG_PXI]));
-    const float2 im = fma2(wi, y[VG_ZR], neg2(mul2(wr, y[VG_ZI])));   // Im(w z*)
-    const float2 im2 = add2(im, im);
-    if (G1) {
-        k[VG_DA] = fma2(ng1, y[VG_DA], im2);
-        k[VG_DB] = fma2(ng1, y[VG_DB], neg2(im2));
-    } else {
-        k[VG_DA] = im2;
-        k[VG_DB] = neg2(im2);
-    }
-    const float2 bma = add2(c[VG_C0], sub2(y[VG_DB], y[VG_DA]));
-    const float2 xr = fma2(bma, wr, mul2(delta, y[VG_ZR]));
-    const float2 xi = fma2(bma, wi, mul2(delta, y[VG_ZI]));
-    k[VG_ZR] = fma2(ng2, y[VG_ZR], xi);
-    k[VG_ZI] = fma2(ng2, y[VG_ZI], neg2(xr));
+    const float2 cwr = fma2(ay, c[VG_PYR], mul2(ax, c[VG_PXR]));   // 2 Re w
+    const float2 cwi = fma2(ay, c[VG_PYI], mul2(ax, c[VG_PXI]));   // 2 Im w
+    const float2 im2 = sub2(mul2(cwi, y[D_ZR]), mul2(cwr, y[D_ZI]));  // 2 Im(w z*)
+    k[D_DA] = G1 ? fma2(ng1, y[D_DA], im2) : im2;
+    const float2 hbma = sub2(c[VG_C0], y[D_DA]);                     // (rho_11 - rho_00) / 2
+    k[D_ZR] = fma2(hbma, cwi, fma2(delta, y[D_ZI], mul2(ng2, y[D_ZR])));
+    k[D_ZI] = fma2(hbma, cwr, fma2(delta, y[D_ZR], mul2(g2, y[D_ZI])));  // negated slope
 }
 
 template <int RK, bool G1>
@@ -371,22 +373,32 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
     const float *__restrict__ kc = static_cast<const float *>(sd.kc);
     double *__restrict__ st = static_cast<double *>(sd.st);
     const float2 *__restrict__ tab = static_cast<const float2 *>(sd.tab);
-    const float2 ng1 = bc2(-float(sd.g1)), ng2 = bc2(-float(sd.g2));
+    const float2 ng1 = bc2(-float(sd.g1)), ng2 = bc2(-float(sd.g2)), g2 = bc2(float(sd.g2));
     double *partial = sd.partial;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int slot[D_N] = {VG_DA, VG_ZR, VG_ZI};
+    // sign of each component's slope as produced by vg_rhs2
+    constexpr float sg[D_N] = {1.f, 1.f, -1.f};
 
     const int l0 = threadIdx.x, l1 = threadIdx.x + blockDim.x;
     const bool ok0 = l0 < tl.kcount, ok1 = l1 < tl.kcount;
     const int k0 = tl.k0 + l0, k1 = tl.k0 + l1;
     float2 c[VG_NCONST];
-    double y64[2][4];
+    double y64[2][D_N];
 #pragma unroll
     for (int q = 0; q < VG_NCONST; ++q)
         c[q] = make_float2(ok0 ? kc[(size_t)q * nkp + k0] : 0.f, ok1 ? kc[(size_t)q * nkp + k1] : 0.f);
+    // derived constants: 2 w's coefficients, c0 / 2, and the intra-current
+    // weights of da alone (w P00 - w P11, since db = -da)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        y64[0][q] = ok0 ? st[(size_t)q * nkp + k0] : 0.0;
-        y64[1][q] = ok1 ? st[(size_t)q * nkp + k1] : 0.0;
+    for (int q = VG_PXR; q <= VG_PYI; ++q) c[q] = add2(c[q], c[q]);
+    c[VG_C0] = mul2(c[VG_C0], bc2(0.5f));
+    c[VG_WPX0] = sub2(c[VG_WPX0], c[VG_WPX1]);
+    c[VG_WPY0] = sub2(c[VG_WPY0], c[VG_WPY1]);
+#pragma unroll
+    for (int q = 0; q < D_N; ++q) {
+        y64[0][q] = ok0 ? st[(size_t)slot[q] * nkp + k0] : 0.0;
+        y64[1][q] = ok1 ? st[(size_t)slot[q] * nkp + k1] : 0.0;
     }
     float2 An[TB::NT];
 #pragma unroll
@@ -400,23 +412,25 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
 #pragma unroll
             for (int i = 0; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)(s + 1) * TB::NT + i);
         }
-        float2 y0[4];
+        float2 y0[D_N];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) y0[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+        for (int q = 0; q < D_N; ++q) y0[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
         // currents and occupations at t_s (antelope.cpp:309-334)
         {
-            float2 t[8];
-            t[0] = fma2(y0[VG_ZR], c[VG_WQXR], mul2(y0[VG_ZI], c[VG_WQXI]));
-            t[1] = fma2(y0[VG_ZR], c[VG_WQYR], mul2(y0[VG_ZI], c[VG_WQYI]));
-            t[2] = fma2(y0[VG_DA], c[VG_WPX0], mul2(y0[VG_DB], c[VG_WPX1]));
-            t[3] = fma2(y0[VG_DA], c[VG_WPY0], mul2(y0[VG_DB], c[VG_WPY1]));
-            t[4] = mul2(c[VG_W], y0[VG_DA]);
-            t[5] = mul2(c[VG_W], y0[VG_DB]);
-            t[6] = mul2(c[VG_W], y0[VG_ZR]);
-            t[7] = mul2(c[VG_W], y0[VG_ZI]);
+            float2 t[7];
+            t[0] = fma2(y0[D_ZR], c[VG_WQXR], mul2(y0[D_ZI], c[VG_WQXI]));
+            t[1] = fma2(y0[D_ZR], c[VG_WQYR], mul2(y0[D_ZI], c[VG_WQYI]));
+            t[2] = mul2(y0[D_DA], c[VG_WPX0]);
+            t[3] = mul2(y0[D_DA], c[VG_WPY0]);
+            t[4] = mul2(c[VG_W], y0[D_DA]);
+            t[5] = mul2(c[VG_W], y0[D_ZR]);
+            t[6] = mul2(c[VG_W], y0[D_ZI]);
             float v[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) v[q] = t[q].x + t[q].y;
+            for (int q = 0; q < 5; ++q) v[q] = t[q].x + t[q].y;
+            v[5] = -t[4].x - t[4].y;  // sum w db = -sum w da
+            v[6] = t[5].x + t[5].y;
+            v[7] = t[6].x + t[6].y;
             const float y = warp_sum8f(v, lane);
             const int r = (s - s0) % SUB;
             if ((lane & 3) == 0) red_s[r][warp][lane >> 2] = double(y);
@@ -426,36 +440,38 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
             }
         }
         // one RK step of both k-points
-        float2 kk[TB::S][4], yy[4], inc[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) inc[q] = make_float2(0.f, 0.f);
+        float2 kk[TB::S][D_N], yy[D_N], inc[D_N];
 #pragma unroll
         for (int i = 0; i < TB::S; ++i) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < D_N; ++q) {
                 float2 t = y0[q];
 #pragma unroll
                 for (int m = 0; m < i; ++m)
-                    if (TB::a(i, m) != 0.0) t = fma2(bc2(float(TB::a(i, m))), kk[m][q], t);
+                    if (TB::a(i, m) != 0.0) t = fma2(bc2(sg[q] * float(TB::a(i, m))), kk[m][q], t);
                 yy[q] = t;
             }
-            vg_rhs2<G1>(c, A[TB::ti(i)], yy, ng1, ng2, kk[i]);
-            if (TB::b(i) != 0.0) {
+            vg_rhs2<G1>(c, A[TB::ti(i)], yy, ng1, ng2, g2, kk[i]);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) inc[q] = fma2(bc2(float(TB::b(i))), kk[i][q], inc[q]);
+            for (int q = 0; q < D_N; ++q) {
+                const float2 bi = bc2(sg[q] * float(TB::b(i)));
+                if (i == 0) inc[q] = mul2(bi, kk[i][q]);
+                else if (TB::b(i) != 0.0) inc[q] = fma2(bi, kk[i][q], inc[q]);
             }
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < D_N; ++q) {
             y64[0][q] += double(inc[q].x);
             y64[1][q] += double(inc[q].y);
         }
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        if (ok0) st[(size_t)q * nkp + k0] = y64[0][q];
-        if (ok1) st[(size_t)q * nkp + k1] = y64[1][q];
+    for (int q = 0; q < D_N; ++q) {
+        if (ok0) st[(size_t)slot[q] * nkp + k0] = y64[0][q];
+        if (ok1) st[(size_t)slot[q] * nkp + k1] = y64[1][q];
     }
+    if (ok0) st[(size_t)VG_DB * nkp + k0] = -y64[0][D_DA];
+    if (ok1) st[(size_t)VG_DB * nkp + k1] = -y64[1][D_DA];
 }
 
 // -------------------------------------------------------- length gauge

@@ -15,9 +15,13 @@
 //      previous stage's U (the field moves k+A a little per stage),
 //   4. evaluates -i[H0 + E.D, rho] and the eigenbasis dephasing, written as
 //      g2 rho + (g1 - g2) U diag(U^dag rho U) U^dag (SBEs.h:831-861).
-// The state rho (Wannier basis) is FP64 in global memory between attempts;
-// Real is the precision of the stage arithmetic (double: plain method,
-// float: mixed method).
+// The state rho (Wannier basis) is FP64 in global memory between attempts.
+// Precision: the plain method is FP64 throughout; the mixed method does the
+// Fourier synthesis (the dominant work) in FP32 and the dynamics in FP64.
+// In the length gauge rho is O(1) (the valence projector moving with k+A), so
+// FP32 rounding of -i[H0, rho] or of the eigenbasis would add a field-
+// independent source that accumulates over the pulse; an FP32-synthesised H0
+// only perturbs the model itself, smoothly.
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -180,12 +184,14 @@ __device__ __forceinline__ void upper_mn(int u, int N, int &m, int &n)
     n = m + u;
 }
 
-// Per-warp shared-memory workspace (full N x N matrices, row-major).
-template <class Real> struct WarpMem {
+// Per-warp shared-memory workspace (full N x N matrices, row-major).  Real
+// is the precision of the dynamics, RF the precision of the Fourier sums.
+template <class Real, class RF> struct WarpMem {
     using T = typename Cx<Real>::T;
+    using TF = typename Cx<RF>::T;
     T Y[64], H0[64], HT[64], U[64], B[64], Tm[64], D0[64], D1[64], S0[64], S1[64];
-    T ph[WAN_MAXR];   // e^{i(k+A)R} of the current stage
-    T pk[WAN_MAXR];   // e^{ikR}
+    TF ph[WAN_MAXR];  // e^{i(k+A)R} of the current stage
+    TF pk[WAN_MAXR];  // e^{ikR}
     T dv[WAN_MAXN];   // diag(U^dag Y U)
     T rot[WAN_MAXN / 2 + 1];
     Real rc[WAN_MAXN / 2 + 1], rs[WAN_MAXN / 2 + 1];
@@ -208,7 +214,7 @@ template <class T> __device__ void mat_mul(T *C, const T *A, const T *B, int N, 
 
 // One parallel Jacobi round on (B, U): the round-robin pairs of round r are
 // disjoint, so their rotations are applied at once.  B <- J^dag B J, U <- U J.
-template <class Real> __device__ void jacobi_round(WarpMem<Real> &w, int N, int r, int lane)
+template <class Real, class RF> __device__ void jacobi_round(WarpMem<Real, RF> &w, int N, int r, int lane)
 {
     using T = typename Cx<Real>::T;
     const int P = N + (N & 1), np = P / 2;
@@ -291,8 +297,8 @@ template <class Real> __device__ void jacobi_round(WarpMem<Real> &w, int N, int 
 
 // Sweeps until the off-diagonal part of B is negligible against its diagonal
 // (|offdiag|^2 <= tol2 |diag|^2, warp-uniform test), at most max_sweeps.
-template <class Real>
-__device__ void jacobi_sweeps(WarpMem<Real> &w, int N, int max_sweeps, double tol2, int lane)
+template <class Real, class RF>
+__device__ void jacobi_sweeps(WarpMem<Real, RF> &w, int N, int max_sweeps, double tol2, int lane)
 {
     const int P = N + (N & 1);
     for (int s = 0; s < max_sweeps; ++s) {
@@ -307,25 +313,26 @@ __device__ void jacobi_sweeps(WarpMem<Real> &w, int N, int max_sweeps, double to
             dia += __shfl_xor_sync(0xffffffffu, dia, o);
         }
         if (off <= tol2 * dia) break;
-        for (int r = 0; r < P - 1; ++r) jacobi_round<Real>(w, N, r, lane);
+        for (int r = 0; r < P - 1; ++r) jacobi_round<Real, RF>(w, N, r, lane);
     }
 }
 
 // Fourier sums at the phases w.ph: H0, D0, D1 and (optionally) S_a = sum R_a h_R e^{i(k+A)R}.
-template <class Real>
-__device__ void fourier(WarpMem<Real> &w, const WanDev &P, bool with_S, const Real (*Rc)[2], int lane)
+template <class Real, class RF>
+__device__ void fourier(WarpMem<Real, RF> &w, const WanDev &P, bool with_S, const RF (*Rc)[2], int lane)
 {
     using T = typename Cx<Real>::T;
+    using TF = typename Cx<RF>::T;
     const int N = P.N, NN = N * N, NU = N * (N + 1) / 2;
-    const T *h = static_cast<const T *>(P.h);
-    const T *d = static_cast<const T *>(P.d);
+    const TF *h = static_cast<const TF *>(P.h);
+    const TF *d = static_cast<const TF *>(P.d);
     for (int u = lane; u < NU; u += 32) {
         int m, n;
         upper_mn(u, N, m, n);
         const int e = m * N + n;
-        T hs = cx<T>(0, 0), d0 = cx<T>(0, 0), d1 = cx<T>(0, 0), s0 = cx<T>(0, 0), s1 = cx<T>(0, 0);
+        TF hs = cx<TF>(0, 0), d0 = cx<TF>(0, 0), d1 = cx<TF>(0, 0), s0 = cx<TF>(0, 0), s1 = cx<TF>(0, 0);
         for (int r = 0; r < P.nR; ++r) {
-            const T t = cmul(h[(size_t)r * NN + e], w.ph[r]);
+            const TF t = cmul(h[(size_t)r * NN + e], w.ph[r]);
             hs.x += t.x;
             hs.y += t.y;
             if (with_S) {
@@ -339,15 +346,16 @@ __device__ void fourier(WarpMem<Real> &w, const WanDev &P, bool with_S, const Re
                 cfma(d1, d[((size_t)r * 2 + 1) * NN + e], w.ph[r]);
             }
         }
-        w.H0[e] = hs;
-        w.H0[n * N + m] = cconj(hs);
-        w.D0[e] = d0;
-        w.D0[n * N + m] = cconj(d0);
-        w.D1[e] = d1;
-        w.D1[n * N + m] = cconj(d1);
+        const T H = cx<T>(hs.x, hs.y), Dx = cx<T>(d0.x, d0.y), Dy = cx<T>(d1.x, d1.y);
+        w.H0[e] = H;
+        w.H0[n * N + m] = cconj(H);
+        w.D0[e] = Dx;
+        w.D0[n * N + m] = cconj(Dx);
+        w.D1[e] = Dy;
+        w.D1[n * N + m] = cconj(Dy);
         if (with_S) {
-            w.S0[e] = s0;
-            w.S1[e] = s1;
+            w.S0[e] = cx<T>(s0.x, s0.y);
+            w.S1[e] = cx<T>(s1.x, s1.y);
         }
     }
     if (with_S) {
@@ -367,19 +375,19 @@ __device__ void fourier(WarpMem<Real> &w, const WanDev &P, bool with_S, const Re
     __syncwarp();
 }
 
-template <class Real> struct BlockMem {
-    using T = typename Cx<Real>::T;
-    T cA[6][WAN_MAXR];          // e^{i A(t_s) R} per stage
-    Real Rc[WAN_MAXR][2];       // Cartesian lattice vectors
+template <class Real, class RF> struct BlockMem {
+    using TF = typename Cx<RF>::T;
+    TF cA[6][WAN_MAXR];         // e^{i A(t_s) R} per stage
+    RF Rc[WAN_MAXR][2];         // Cartesian lattice vectors
     double AE[6][6];            // A and E at the stage times
     double part[WAN_WARPS][WAN_NSLOT];
     double errw[WAN_WARPS];
     WTab tab;
 };
 
-template <class Real> constexpr size_t wan_smem_bytes()
+template <class Real, class RF> constexpr size_t wan_smem_bytes()
 {
-    return ((sizeof(BlockMem<Real>) + 15) / 16) * 16 + sizeof(WarpMem<Real>) * WAN_WARPS;
+    return ((sizeof(BlockMem<Real, RF>) + 15) / 16) * 16 + sizeof(WarpMem<Real, RF>) * WAN_WARPS;
 }
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -396,23 +404,25 @@ __device__ __forceinline__ double warp_max(double v)
 }  // namespace
 
 // ============================================================= init
-template <class Real>
+template <class Real, class RF>
 __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
 {
     using T = typename Cx<Real>::T;
+    using TF = typename Cx<RF>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockMem<Real> &bm = *reinterpret_cast<BlockMem<Real> *>(smem_raw);
-    WarpMem<Real> *wm = reinterpret_cast<WarpMem<Real> *>(smem_raw + ((sizeof(BlockMem<Real>) + 15) / 16) * 16);
-    Real(*Rc)[2] = bm.Rc;
+    BlockMem<Real, RF> &bm = *reinterpret_cast<BlockMem<Real, RF> *>(smem_raw);
+    WarpMem<Real, RF> *wm =
+        reinterpret_cast<WarpMem<Real, RF> *>(smem_raw + ((sizeof(BlockMem<Real, RF>) + 15) / 16) * 16);
+    RF(*Rc)[2] = bm.Rc;
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
     for (int r = threadIdx.x; r < P.nR; r += blockDim.x) {
-        Rc[r][0] = Real(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
-        Rc[r][1] = Real(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
+        Rc[r][0] = RF(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
+        Rc[r][1] = RF(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
     }
     __syncthreads();
     const int k = blockIdx.x * WAN_WARPS + wi;
     if (k >= P.nk) return;
-    WarpMem<Real> &w = wm[wi];
+    WarpMem<Real, RF> &w = wm[wi];
     const int N = P.N, NN = N * N;
     // k-grid point and trapezoid weight (momaxis.h:147-186, 349-383)
     const int N0 = P.Ngrid[0], N1 = P.Ngrid[1], N2 = P.Ngrid[2];
@@ -432,15 +442,15 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
         const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
         double s, c;
         sincos(kv[0] * Rx + kv[1] * Ry, &s, &c);
-        w.ph[r] = cx<T>(c, s);
+        w.ph[r] = cx<TF>(c, s);
     }
     for (int e = lane; e < NN; e += 32) w.U[e] = cx<T>((e / N) == (e % N) ? 1 : 0, 0);
     if (lane < WAN_MAXN + 1) { w.pidx[lane] = -1; w.mate[lane] = -1; }
     __syncwarp();
-    fourier<Real>(w, P, false, Rc, lane);
+    fourier<Real, RF>(w, P, false, Rc, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
-    jacobi_sweeps<Real>(w, N, 16, sizeof(Real) == 8 ? 1e-30 : 1e-13, lane);
+    jacobi_sweeps<Real, RF>(w, N, 16, 1e-30, lane);
     // occupations of the eigenstates: the Nval lowest filled, or Fermi-Dirac (SBEs.h:319-340)
     if (lane < N) {
         const Real ev = w.B[lane * N + lane].x;
@@ -477,16 +487,17 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
 }
 
 // ============================================================= attempt
-template <class Real>
+template <class Real, class RF>
 __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__restrict__ Pp)
 {
     using T = typename Cx<Real>::T;
-    constexpr bool F64 = std::is_same<Real, double>::value;
+    using TF = typename Cx<RF>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockMem<Real> &bm = *reinterpret_cast<BlockMem<Real> *>(smem_raw);
-    WarpMem<Real> *wm = reinterpret_cast<WarpMem<Real> *>(smem_raw + ((sizeof(BlockMem<Real>) + 15) / 16) * 16);
-    T(*cA)[WAN_MAXR] = bm.cA;
-    Real(*Rc)[2] = bm.Rc;
+    BlockMem<Real, RF> &bm = *reinterpret_cast<BlockMem<Real, RF> *>(smem_raw);
+    WarpMem<Real, RF> *wm =
+        reinterpret_cast<WarpMem<Real, RF> *>(smem_raw + ((sizeof(BlockMem<Real, RF>) + 15) / 16) * 16);
+    TF(*cA)[WAN_MAXR] = bm.cA;
+    RF(*Rc)[2] = bm.Rc;
     double(*AE)[6] = bm.AE;
     WTab &tab = bm.tab;
     const WanDev &P = *Pp;
@@ -499,8 +510,8 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
     const bool cur = ctl.need_current;
     if (threadIdx.x == 0) tableau(P.rk, tab);
     for (int r = threadIdx.x; r < P.nR; r += blockDim.x) {
-        Rc[r][0] = Real(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
-        Rc[r][1] = Real(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
+        Rc[r][0] = RF(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
+        Rc[r][1] = RF(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
     }
     __syncthreads();
     const int S = tab.S;
@@ -517,7 +528,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
         const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
         double sn, cs;
         sincos(AE[s][0] * Rx + AE[s][1] * Ry, &sn, &cs);
-        cA[s][r] = cx<T>(cs, sn);
+        cA[s][r] = cx<TF>(cs, sn);
     }
     for (int q = threadIdx.x; q < WAN_WARPS * WAN_NSLOT; q += blockDim.x) bm.part[q / WAN_NSLOT][q % WAN_NSLOT] = 0.0;
     if (threadIdx.x < WAN_WARPS) bm.errw[threadIdx.x] = 0.0;
@@ -526,7 +537,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
     const int k = blockIdx.x * WAN_WARPS + wi;
     double emax = 0.0;
     if (k < P.nk) {
-        WarpMem<Real> &w = wm[wi];
+        WarpMem<Real, RF> &w = wm[wi];
         if (lane < WAN_MAXN + 1) { w.pidx[lane] = -1; w.mate[lane] = -1; }
         // grid point (momaxis.h:349-383) and e^{ikR}
         const int N1 = P.Ngrid[1], N2 = P.Ngrid[2];
@@ -541,7 +552,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
             const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
             double sn, cs;
             sincos(kv[0] * Rx + kv[1] * Ry, &sn, &cs);
-            w.pk[r] = cx<T>(cs, sn);
+            w.pk[r] = cx<TF>(cs, sn);
         }
         const double2 *rho = P.rho[buf] + (size_t)k * NN;
         const T *Ug = static_cast<const T *>(P.U[buf]) + (size_t)k * NN;
@@ -580,7 +591,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
             for (int r = lane; r < P.nR; r += 32) w.ph[r] = cmul(w.pk[r], cA[s][r]);
             __syncwarp();
             const bool with_cur = cur && s == 0;
-            fourier<Real>(w, P, with_cur, Rc, lane);
+            fourier<Real, RF>(w, P, with_cur, Rc, lane);
             // H = H0 + E.D (SBEs.h:770-783)
             const Real Ex = Real(AE[s][3]), Ey = Real(AE[s][4]);
             for (int e = lane; e < NN; e += 32) {
@@ -596,7 +607,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
             __syncwarp();
             mat_mul<T>(w.B, w.U, w.Tm, N, true, lane);
             __syncwarp();
-            jacobi_sweeps<Real>(w, N, F64 ? 6 : 3, F64 ? 1e-30 : 1e-13, lane);
+            jacobi_sweeps<Real, RF>(w, N, 6, 1e-30, lane);
             // diag(U^dag Y U)
             mat_mul<T>(w.Tm, w.Y, w.U, N, false, lane);
             __syncwarp();
@@ -801,14 +812,14 @@ __global__ void __launch_bounds__(1024) wan_control(const WanDev *__restrict__ P
 }
 
 // ============================================================= launchers
-template <class Real> static cudaError_t allow_smem()
+template <class RF> static cudaError_t allow_smem()
 {
     static bool done = false;  // per process; the attribute applies to every device
     if (done) return cudaSuccess;
-    const int bytes = (int)wan_smem_bytes<Real>();
-    cudaError_t e = cudaFuncSetAttribute(wan_init<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    const int bytes = (int)wan_smem_bytes<double, RF>();
+    cudaError_t e = cudaFuncSetAttribute(wan_init<double, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(wan_attempt<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(wan_attempt<double, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     done = e == cudaSuccess;
     return e;
 }
@@ -818,8 +829,8 @@ cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st)
     const int grid = (w.nk + WAN_WARPS - 1) / WAN_WARPS;
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
-    if (precision == 0) wan_init<double><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double>(), st>>>(w);
-    else wan_init<float><<<grid, 32 * WAN_WARPS, wan_smem_bytes<float>(), st>>>(w);
+    if (precision == 0) wan_init<double, double><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, double>(), st>>>(w);
+    else wan_init<double, float><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, float>(), st>>>(w);
     return cudaGetLastError();
 }
 
@@ -828,8 +839,10 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
     const int grid = (w.nk + WAN_WARPS - 1) / WAN_WARPS;
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
-    if (precision == 0) wan_attempt<double><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double>(), st>>>(dw);
-    else wan_attempt<float><<<grid, 32 * WAN_WARPS, wan_smem_bytes<float>(), st>>>(dw);
+    if (precision == 0)
+        wan_attempt<double, double><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, double>(), st>>>(dw);
+    else
+        wan_attempt<double, float><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, float>(), st>>>(dw);
     return cudaGetLastError();
 }
 

@@ -49,10 +49,10 @@ struct WanDev {
     double lat[4];
     LaserDev laser;
     const int *R;           // [nR][2]
-    const void *h;          // [nR][N*N] complex Real
-    const void *d;          // [nR][2][N*N] complex Real (or null)
+    const void *h;          // [nR][N*N] complex, FP32 for the mixed method, FP64 otherwise
+    const void *d;          // [nR][2][N*N] complex, same precision (or null)
     double2 *rho[2];        // [nk][N*N] committed / trial state (Wannier basis, full matrix), FP64
-    void *U[2];             // [nk][N*N] tracked eigenbasis of H0(k+A), Real complex
+    void *U[2];             // [nk][N*N] tracked eigenbasis of H0(k+A), FP64 complex
     double *weight;         // [nk]
     double *tile_err;       // [ntiles]
     double *cur_part;       // [ntiles][WAN_NSLOT]

@@ -67,7 +67,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     if (w_.has_dip) dalloc(&d, cplx * p.w_d.size() / 2, st, "alloc d");
     for (int b = 0; b < 2; ++b) {
         dalloc(&w_.rho[b], sizeof(double2) * nk * NN, st, "alloc rho");
-        dalloc(&w_.U[b], cplx * nk * NN, st, "alloc U");
+        dalloc(&w_.U[b], sizeof(double2) * nk * NN, st, "alloc U");  // eigenbasis kept in FP64
     }
     dalloc(&w_.weight, sizeof(double) * nk, st, "alloc weights");
     dalloc(&w_.tile_err, sizeof(double) * w_.ntiles, st, "alloc tile errors");

@@ -107,6 +107,11 @@ sbe_status sbe_solver_run(sbe_solver *s, void *stream);
 sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out);
 /* Number of propagate kernel launches the last run issued. */
 int sbe_solver_launches(const sbe_solver *s);
+/* Time-stepping statistics of a finished run: accepted steps, attempted steps
+ * and rejected attempts.  Fixed-step methods (RKorder 4 / 5, SBEs.h:596-624)
+ * take Nt steps and reject none; the Cash-Karp extension reports its
+ * controller's counts (one step size per solve). */
+sbe_status sbe_solver_steps(const sbe_solver *s, long long *steps, long long *attempts, long long *rejects);
 /* With opts.profile = 1: total device time (ms) and count of the propagate
  * and reduce launches of the run (CUDA events on the launching stream). */
 sbe_status sbe_solver_kernel_times(sbe_solver *s, double *propagate_ms, int *propagate_launches,

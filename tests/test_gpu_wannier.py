@@ -71,11 +71,31 @@ def test_cash_karp_with_rejections():
 
 
 def test_mixed_close_to_fp64():
+    """The mixed method synthesises H0, D and dH/dk in FP32 (the dynamics stay
+    FP64).  FP32 rounding of the time-dependent phases e^{i(k+A)R} leaves a
+    broadband floor of ~1e-6 of max|J| in the currents: harmonics down to
+    1e-6 of the strongest band meet 1e-3; weaker bands reach that floor on
+    small grids, so the bar below is the measured one, not the 1e-8 range of
+    the two-band kernels."""
     c = wannier.wannier_case(seed=5, n=20, ncycles=2.0)
     c["laser"]["pulses"][0]["w0"] = 0.0285
     a = ab.solve(c, precision="fp64")
     b = ab.solve(c, precision="mixed")
     orders, err, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra},
-                                        {"inter": a.inter, "intra": a.intra}, 0.1, 0.0285)
+                                        {"inter": a.inter, "intra": a.intra}, 0.1, 0.0285, floor=1e-6)
     assert len(orders) > 5
     assert err.max() < 1e-3, (orders, err)
+    scale = max(np.abs(a.inter).max(), np.abs(a.intra).max())
+    for key in ("inter", "intra"):
+        assert np.abs(getattr(a, key) - getattr(b, key)).max() < 1e-5 * scale, key
+
+
+def test_step_statistics():
+    c = small_case("cashkarp45", tol=1e-13)
+    s = ab.api.Solver(ab.Problem.from_dict(c), precision="fp64")
+    s.run()
+    st = s.steps()
+    s.close()
+    ref = pyoracle.run(c)
+    assert st["steps"] == ref["steps"]
+    assert st["attempts"] == st["steps"] + st["rejects"]
