@@ -37,6 +37,14 @@ sys.path.insert(0, ROOT)
 METRIC = "HHG solves/hour & k·steps/s, batched FP32 vs plain FP64 at ≤1e-3 err; p99 lat"
 UNIT = "k·steps/s"
 FLOPS_PER_KSTEP = {4: 198.0, 5: 370.0}   # algorithmic flops per k-point step, 2-band velocity gauge
+
+
+def wannier_flops_per_rhs(N: int, nR: int) -> float:
+    """Algorithmic flops of one length-gauge RHS of an N-band Wannier model:
+    Fourier synthesis of H0, D_x, D_y at k+A over the Hermitian half
+    (3 nR N^2 8/2), the commutator (16 N^3) and the eigenbasis dephasing
+    rotations (4 x 8 N^3).  The eigensolver is not counted."""
+    return 3 * nR * N * N * 8 / 2 + 16 * N ** 3 + 4 * 8 * N ** 3
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -234,6 +242,8 @@ def run_ours(args):
         "gpu_launches": int(launches) * 2,   # propagate + reduce per launch tick, timed steps only
         "clocks": clocks,
     }
+    if args.wannier_grid > 0 and world == 1:
+        line["wannier"] = run_wannier(args, stream, fp64_tf)
     if args.scan_solves > 0:
         line["scan"] = run_scan(args, stream, rank, world)
     if args.serve_requests > 0 and world == 1:
@@ -244,6 +254,83 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_wannier(args, stream, fp64_tf):
+    """The N = 6 Wannier configuration (triangular lattice, 37 lattice
+    vectors, 3 valence bands, T2 = 220, 3.2 um sin2 pulse, Cash-Karp 4(5) at
+    tol 1e-8 with one step size per solve) on its full k-grid, over a bounded
+    part of the pulse (--wannier-cycles), plain FP64 and mixed.  k.steps
+    count accepted steps; the roofline counts attempted ones."""
+    import torch
+
+    import antelope_b200 as ab
+    from antelope_b200 import wannier
+    from antelope_b200.api import Solver
+    from antelope_b200.spectrum import per_harmonic_error
+
+    n = args.wannier_grid
+    case = wannier.wannier_case(seed=1, n=n, ncycles=args.wannier_cycles, rk="cashkarp45", tol=1e-8)
+    group = case["SyntheticWannier"]
+    N, nR = int(group["Nband"]), len(group["R"]) // 2
+    res, outs = {}, {}
+    for prec in ("fp64", "mixed"):
+        p = ab.Problem.from_dict(dict(case, calc=dict(case["calc"], precision=prec)))
+        s = Solver(p, precision=prec)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.run(stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = s.steps()
+        outs[prec] = s.get()
+        s.close()
+        nk = p.dims.ntotal
+        flops = wannier_flops_per_rhs(N, nR) * 6 * nk * st["attempts"]
+        res[prec] = {"ms": ms, "k_steps_per_s": nk * st["steps"] / (ms * 1e-3), **st,
+                     "achieved_tflops": flops / (ms * 1e-3) / 1e12}
+        res[prec]["roofline_frac_fp64"] = res[prec]["achieved_tflops"] / fp64_tf
+    a, b = outs["fp64"], outs["mixed"]
+    w0 = case["laser"]["pulses"][0]["w0"]
+    o6, e6, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra}, {"inter": a.inter, "intra": a.intra},
+                                   0.1, w0, floor=1e-6)
+    o8, e8, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra}, {"inter": a.inter, "intra": a.intra},
+                                   0.1, w0, floor=1e-8)
+    out = {"workload": f"SyntheticWannier N={N}, {nR} R, {n}x{n} k, length gauge, Cash-Karp tol 1e-8, "
+                        f"{args.wannier_cycles} of the 10-cycle pulse's cycles (a bounded part of the solve)",
+            "k_points": n * n, "output_steps": int(a.inter.shape[0]), "fp64": res["fp64"], "mixed": res["mixed"],
+            "mixed_over_fp64": res["mixed"]["k_steps_per_s"] / res["fp64"]["k_steps_per_s"],
+            "flops_per_rhs": wannier_flops_per_rhs(N, nR), "rhs_per_attempt": 6,
+            "spectral_error": {"max_floor_1e-6": float(e6.max()), "max_floor_1e-8": float(e8.max()),
+                               "vs": "fp64 run"}}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = wannier_cpu_baseline(args.wannier_cycles, budget_s=args.cpu_seconds / 2)
+    return out
+
+
+def wannier_cpu_baseline(ncycles: float, budget_s: float):
+    """The C restatement of the reference's length-gauge propagation with the
+    Wannier model form, on all host cores, on a k-subgrid of the same model and
+    pulse sized to ~budget_s (the reference itself has no compiled Wannier
+    model)."""
+    from antelope_b200 import wannier
+    from oracle import pyoracle
+
+    cores = os.cpu_count() or 1
+
+    def timed(g, cyc):
+        c = wannier.wannier_case(seed=1, n=g, ncycles=cyc, rk="cashkarp45", tol=1e-8)
+        t0 = time.perf_counter()
+        r = pyoracle.run(c, nthreads=cores)
+        return g * g * r["steps"] / (time.perf_counter() - t0), r["steps"]
+
+    rate, _ = timed(8, 0.02)
+    g = int(max(8, min(300, np.sqrt(rate * budget_s / 440.0 / max(ncycles, 0.05)))))
+    rate, steps = timed(g, min(ncycles, 0.05))
+    return {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"C oracle, same model, {g}x{g} k-subgrid, {steps} accepted steps, {cores} threads"}
 
 
 def _fp64_sequential(problems, stream):
@@ -496,6 +583,8 @@ def main():
     ap.add_argument("--scan-solves", dest="scan_solves", type=int, default=256)
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=600)
     ap.add_argument("--serve-rate", dest="serve_rate", type=float, default=40.0)
+    ap.add_argument("--wannier-grid", dest="wannier_grid", type=int, default=300)
+    ap.add_argument("--wannier-cycles", dest="wannier_cycles", type=float, default=0.5)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
