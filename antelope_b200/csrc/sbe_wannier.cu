@@ -8,11 +8,16 @@
 //
 // Work decomposition: one warp per k-point, the lanes own the upper-triangle
 // elements of the Hermitian N x N matrices, the full matrices of the warp live
-// in shared memory.  Per RK stage the warp
+// in shared memory sized to N and the number of lattice vectors.  The
+// controller kernel computes the stage fields A(t_s), E(t_s) and the factors
+// e^{iA(t_s)R} once per attempt for all blocks.  Per RK stage the warp
 //   1. forms the phases e^{i(k+A)R} (per-k e^{ikR} times per-stage e^{iAR}),
-//   2. sums H0(k+A), D_x, D_y over the lattice vectors (exact Fourier sums),
-//   3. tracks the eigenbasis U of H0(k+A) with Jacobi rounds started from the
-//      previous stage's U (the field moves k+A a little per stage),
+//   2. sums H0(k+A), D_x, D_y over the lattice vectors (exact Fourier sums,
+//      one (quantity, element) sum per lane task),
+//   3. tracks the eigenbasis U of H0(k+A) with parallel Jacobi rounds started
+//      from the previous stage's U (the field moves k+A a little per stage);
+//      a round applies its disjoint rotations to B = U^dag H0 U and U element
+//      by element in one pass,
 //   4. evaluates -i[H0 + E.D, rho] and the eigenbasis dephasing, written as
 //      g2 rho + (g1 - g2) U diag(U^dag rho U) U^dag (SBEs.h:831-861).
 // The state rho (Wannier basis) is FP64 in global memory between attempts.
@@ -184,26 +189,67 @@ __device__ __forceinline__ void upper_mn(int u, int N, int &m, int &n)
     n = m + u;
 }
 
-// Per-warp shared-memory workspace (full N x N matrices, row-major).  Real
-// is the precision of the dynamics, RF the precision of the Fourier sums.
-template <class Real, class RF> struct WarpMem {
-    using T = typename Cx<Real>::T;
+// Shared-memory layout, sized per solve from N and the number of lattice
+// vectors: a block head (stage fields, tableau, per-warp results), the
+// per-stage factors e^{iA(t_s)R} and the lattice vectors, then one workspace
+// per warp of full N x N complex matrices (row-major).
+constexpr int WAN_MAXU_ = WAN_MAXN * (WAN_MAXN + 1) / 2;
+struct BlockHead {
+    double AE[6][6];  // A and E at the stage times
+    double part[WAN_WARPS][WAN_NSLOT];
+    double errw[WAN_WARPS];
+    WTab tab;
+    unsigned char ut[WAN_MAXU_][2];  // upper-triangle element u -> (m, n)
+};
+constexpr int WAN_NMAT = 10;  // Y, H0, HT, U, B, Tm, D0, D1, S0, S1
+__host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) / 16 * 16; }
+struct WanSmem {
+    size_t cA, Rc, warp0, warp_bytes, total;
+};
+__host__ __device__ __forceinline__ WanSmem wan_smem(int N, int nR, int rf_bytes)
+{
+    WanSmem L;
+    L.cA = al16(sizeof(BlockHead));
+    L.Rc = L.cA + al16((size_t)6 * nR * 2 * rf_bytes);
+    L.warp0 = L.Rc + al16((size_t)nR * 2 * rf_bytes);
+    const size_t NN = (size_t)N * N;
+    L.warp_bytes = al16(WAN_NMAT * NN * 16 + (size_t)N * 16 + WAN_MAXN * 16 + 2 * WAN_MAXN * 8) +
+                   al16((size_t)2 * nR * 2 * rf_bytes);
+    L.total = L.warp0 + WAN_WARPS * L.warp_bytes;
+    return L;
+}
+
+// One warp's matrices; RF is the precision of the Fourier sums (phases).
+template <class RF> struct WarpView {
     using TF = typename Cx<RF>::T;
-    T Y[64], H0[64], HT[64], U[64], B[64], Tm[64], D0[64], D1[64], S0[64], S1[64];
-    TF ph[WAN_MAXR];  // e^{i(k+A)R} of the current stage
-    TF pk[WAN_MAXR];  // e^{ikR}
-    T dv[WAN_MAXN];   // diag(U^dag Y U)
-    T rot[WAN_MAXN / 2 + 1];
-    Real rc[WAN_MAXN / 2 + 1], rs[WAN_MAXN / 2 + 1];
-    int mate[WAN_MAXN + 1], role[WAN_MAXN + 1], pidx[WAN_MAXN + 1];
+    double2 *Y, *H0, *HT, *U, *B, *Tm, *D0, *D1, *S0, *S1;
+    double2 *dv;   // diag(U^dag Y U)
+    double2 *je;   // rotation phases of the current Jacobi round (by the pair's lower index)
+    double *jc, *js;
+    TF *ph;        // e^{i(k+A)R} of the current stage
+    TF *pk;        // e^{ikR}
+    __device__ WarpView(unsigned char *base, int N, int nR)
+    {
+        const int NN = N * N;
+        double2 *m = reinterpret_cast<double2 *>(base);
+        Y = m; H0 = m + NN; HT = m + 2 * NN; U = m + 3 * NN; B = m + 4 * NN;
+        Tm = m + 5 * NN; D0 = m + 6 * NN; D1 = m + 7 * NN; S0 = m + 8 * NN; S1 = m + 9 * NN;
+        dv = m + WAN_NMAT * NN;
+        je = dv + N;
+        jc = reinterpret_cast<double *>(je + WAN_MAXN);
+        js = jc + WAN_MAXN;
+        const size_t off = al16(WAN_NMAT * (size_t)NN * 16 + (size_t)N * 16 + WAN_MAXN * 16 + 2 * WAN_MAXN * 8);
+        ph = reinterpret_cast<TF *>(base + off);
+        pk = ph + nR;
+    }
 };
 
 // C = op(A) * B over the full matrices, lanes stride over the elements.
-template <class T> __device__ void mat_mul(T *C, const T *A, const T *B, int N, bool conjA, int lane)
+__device__ void mat_mul(double2 *C, const double2 *A, const double2 *B, int N, bool conjA, int lane)
 {
     for (int e = lane; e < N * N; e += 32) {
         const int m = e / N, n = e % N;
-        T acc = cx<T>(0, 0);
+        double2 acc = make_double2(0, 0);
         for (int l = 0; l < N; ++l) {
             if (conjA) cfmac(acc, A[l * N + m], B[l * N + n]);
             else cfma(acc, A[m * N + l], B[l * N + n]);
@@ -212,99 +258,155 @@ template <class T> __device__ void mat_mul(T *C, const T *A, const T *B, int N, 
     }
 }
 
-// One parallel Jacobi round on (B, U): the round-robin pairs of round r are
-// disjoint, so their rotations are applied at once.  B <- J^dag B J, U <- U J.
-template <class Real, class RF> __device__ void jacobi_round(WarpMem<Real, RF> &w, int N, int r, int lane)
+// Round-robin (circle method) schedule of the parallel Jacobi sweeps over P
+// (= N rounded up to even) indices: in round r index P-1 meets r and every
+// other i meets (2r - i) mod (P-1); partners >= N mean "no rotation".
+__device__ __forceinline__ int rr_mate(int i, int r, int P)
 {
-    using T = typename Cx<Real>::T;
-    const int P = N + (N & 1), np = P / 2;
-    if (lane < np) {
-        int p, q;
-        if (lane == 0) { p = P - 1; q = r; }
-        else { p = (r + lane) % (P - 1); q = (r - lane + (P - 1)) % (P - 1); }
-        if (p > q) { const int t = p; p = q; q = t; }
-        Real c = 1, s = 0;
-        T e = cx<T>(1, 0);
-        if (q < N) {
-            const T g = w.B[p * N + q];
-            const Real rr = sqrt(g.x * g.x + g.y * g.y);
-            const Real app = w.B[p * N + p].x, aqq = w.B[q * N + q].x;
-            if (rr > Real(0)) {
+    if (i == P - 1) return r;
+    if (i == r) return P - 1;
+    int m = (2 * r - i) % (P - 1);
+    return m < 0 ? m + P - 1 : m;
+}
+
+// Lane tasks: Fourier sums are (quantity, upper element) pairs and Jacobi
+// updates are B upper elements followed by U elements, dealt round-robin to
+// the lanes.  The upper-element coordinates come from a per-block table.
+constexpr int WAN_MAXJ = 4;  // ceil((36 + 64) / 32)
+
+__device__ void fill_upper(unsigned char (*ut)[2], int N)
+{
+    if (threadIdx.x == 0) {
+        int u = 0;
+        for (int m = 0; m < N; ++m)
+            for (int n = m; n < N; ++n, ++u) {
+                ut[u][0] = (unsigned char)m;
+                ut[u][1] = (unsigned char)n;
+            }
+    }
+}
+
+// Column j of the round's rotation matrix J: its nonzeros J_jj and J_mj,j.
+template <class RF>
+__device__ __forceinline__ void jcol(const WarpView<RF> &w, int j, int r, int P, int N, double2 &Jjj, double2 &Jmj,
+                                     int &mj)
+{
+    mj = rr_mate(j, r, P);
+    if (mj >= N) {
+        Jjj = make_double2(1, 0);
+        Jmj = make_double2(0, 0);
+        mj = j;
+        return;
+    }
+    const int p = min(j, mj);
+    const double c = w.jc[p], s = w.js[p];
+    const double2 e = w.je[p];
+    // J_pp = c, J_pq = s, J_qp = -s conj(e), J_qq = c conj(e)
+    if (j == p) {
+        Jjj = make_double2(c, 0);
+        Jmj = make_double2(-s * e.x, s * e.y);
+    } else {
+        Jjj = make_double2(c * e.x, -c * e.y);
+        Jmj = make_double2(s, 0);
+    }
+}
+
+// One parallel Jacobi round on (B, U): the pairs of round r are disjoint, so
+// B <- J^dag B J and U <- U J are applied element by element in one pass
+// (inputs read, then written).
+template <class RF>
+__device__ void jacobi_round(const WarpView<RF> &w, const unsigned char (*ut)[2], int N, int r, int lane)
+{
+    const int NU = N * (N + 1) / 2, nt = NU + N * N;
+    const int P = N + (N & 1);
+    if (lane < N) {
+        const int q = rr_mate(lane, r, P);
+        if (q < N && lane < q) {
+            const int p = lane;
+            const double2 g = w.B[p * N + q];
+            const double rr = sqrt(g.x * g.x + g.y * g.y);
+            double c = 1, s = 0;
+            double2 e = make_double2(1, 0);
+            if (rr > 0.0) {
+                const double app = w.B[p * N + p].x, aqq = w.B[q * N + q].x;
                 e.x = g.x / rr;
                 e.y = g.y / rr;
-                const Real zeta = (aqq - app) / (Real(2) * rr);
-                const Real t = (zeta >= 0 ? Real(1) : Real(-1)) / (fabs(zeta) + sqrt(zeta * zeta + Real(1)));
-                c = Real(1) / sqrt(t * t + Real(1));
+                const double zeta = (aqq - app) / (2.0 * rr);
+                const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(zeta * zeta + 1.0));
+                c = 1.0 / sqrt(t * t + 1.0);
                 s = t * c;
             }
-            w.mate[p] = q; w.role[p] = 0; w.pidx[p] = lane;
-            w.mate[q] = p; w.role[q] = 1; w.pidx[q] = lane;
-        } else {
-            if (p < N) { w.mate[p] = -1; }
+            w.jc[p] = c;
+            w.js[p] = s;
+            w.je[p] = e;
         }
-        w.rc[lane] = c;
-        w.rs[lane] = s;
-        w.rot[lane] = e;
     }
     __syncwarp();
-    // column operation on B and U: tasks (row i, pair k)
-    for (int task = lane; task < N * np; task += 32) {
-        const int i = task / np, k = task % np;
-        int p = -1, q = -1;
-        for (int x = 0; x < N; ++x)
-            if (w.pidx[x] == k && w.mate[x] >= 0 && w.role[x] == 0) { p = x; q = w.mate[x]; }
-        if (p < 0) continue;
-        const Real c = w.rc[k], s = w.rs[k];
-        const T e = w.rot[k];
-        // J_pp = c, J_pq = s, J_qp = -s conj(e), J_qq = c conj(e)
-        const T Jqp = cx<T>(-s * e.x, s * e.y), Jqq = cx<T>(c * e.x, -c * e.y);
-        T bp = w.B[i * N + p], bq = w.B[i * N + q];
-        T np_ = cx<T>(c * bp.x, c * bp.y), nq = cx<T>(s * bp.x, s * bp.y);
-        cfma(np_, bq, Jqp);
-        cfma(nq, bq, Jqq);
-        w.B[i * N + p] = np_;
-        w.B[i * N + q] = nq;
-        T up = w.U[i * N + p], uq = w.U[i * N + q];
-        T nup = cx<T>(c * up.x, c * up.y), nuq = cx<T>(s * up.x, s * up.y);
-        cfma(nup, uq, Jqp);
-        cfma(nuq, uq, Jqq);
-        w.U[i * N + p] = nup;
-        w.U[i * N + q] = nuq;
+    double2 out[WAN_MAXJ];
+#pragma unroll
+    for (int x = 0; x < WAN_MAXJ; ++x) {
+        const int t = lane + 32 * x;
+        if (t >= nt) break;
+        int i, j;
+        if (t < NU) {
+            i = ut[t][0];
+            j = ut[t][1];
+        } else {
+            i = -1 - (t - NU) / N;
+            j = (t - NU) % N;
+        }
+        double2 Jjj, Jmj;
+        int mj;
+        jcol(w, j, r, P, N, Jjj, Jmj, mj);
+        if (i >= 0) {  // B'_ij = sum_ab conj(J_ai) B_ab J_bj
+            double2 Jii, Jmi;
+            int mi;
+            jcol(w, i, r, P, N, Jii, Jmi, mi);
+            double2 t1 = cmul(w.B[i * N + j], Jjj), t2 = cmul(w.B[mi * N + j], Jjj);
+            cfma(t1, w.B[i * N + mj], Jmj);
+            cfma(t2, w.B[mi * N + mj], Jmj);
+            double2 o = make_double2(0, 0);
+            cfmac(o, Jii, t1);
+            cfmac(o, Jmi, t2);
+            out[x] = o;
+        } else {  // U'_ij = U_ij J_jj + U_i,mj J_mj,j
+            const int row = -1 - i;
+            double2 o = cmul(w.U[row * N + j], Jjj);
+            cfma(o, w.U[row * N + mj], Jmj);
+            out[x] = o;
+        }
     }
     __syncwarp();
-    // row operation on B: tasks (column j, pair k)
-    for (int task = lane; task < N * np; task += 32) {
-        const int j = task / np, k = task % np;
-        int p = -1, q = -1;
-        for (int x = 0; x < N; ++x)
-            if (w.pidx[x] == k && w.mate[x] >= 0 && w.role[x] == 0) { p = x; q = w.mate[x]; }
-        if (p < 0) continue;
-        const Real c = w.rc[k], s = w.rs[k];
-        const T e = w.rot[k];
-        const T Jqp = cx<T>(-s * e.x, s * e.y), Jqq = cx<T>(c * e.x, -c * e.y);
-        const T bp = w.B[p * N + j], bq = w.B[q * N + j];
-        // B'_pj = conj(J_pp) b_pj + conj(J_qp) b_qj ; B'_qj = conj(J_pq) b_pj + conj(J_qq) b_qj
-        T np_ = cx<T>(c * bp.x, c * bp.y), nq = cx<T>(s * bp.x, s * bp.y);
-        cfmac(np_, Jqp, bq);
-        cfmac(nq, Jqq, bq);
-        w.B[p * N + j] = np_;
-        w.B[q * N + j] = nq;
+#pragma unroll
+    for (int x = 0; x < WAN_MAXJ; ++x) {
+        const int t = lane + 32 * x;
+        if (t >= nt) break;
+        if (t < NU) {
+            const int i = ut[t][0], j = ut[t][1];
+            if (i == j) {
+                w.B[i * N + i] = make_double2(out[x].x, 0.0);
+            } else {
+                w.B[i * N + j] = out[x];
+                w.B[j * N + i] = cconj(out[x]);
+            }
+        } else {
+            w.U[t - NU] = out[x];
+        }
     }
-    __syncwarp();
-    if (lane < N) { w.pidx[lane] = -1; w.mate[lane] = -1; }
     __syncwarp();
 }
 
 // Sweeps until the off-diagonal part of B is negligible against its diagonal
 // (|offdiag|^2 <= tol2 |diag|^2, warp-uniform test), at most max_sweeps.
-template <class Real, class RF>
-__device__ void jacobi_sweeps(WarpMem<Real, RF> &w, int N, int max_sweeps, double tol2, int lane)
+template <class RF>
+__device__ void jacobi_sweeps(const WarpView<RF> &w, const unsigned char (*ut)[2], int N, int max_sweeps,
+                              double tol2, int lane)
 {
     const int P = N + (N & 1);
     for (int s = 0; s < max_sweeps; ++s) {
         double off = 0.0, dia = 0.0;
         for (int e = lane; e < N * N; e += 32) {
-            const double v = double(w.B[e].x) * double(w.B[e].x) + double(w.B[e].y) * double(w.B[e].y);
+            const double v = w.B[e].x * w.B[e].x + w.B[e].y * w.B[e].y;
             if (e / N == e % N) dia += v;
             else off += v;
         }
@@ -313,81 +415,59 @@ __device__ void jacobi_sweeps(WarpMem<Real, RF> &w, int N, int max_sweeps, doubl
             dia += __shfl_xor_sync(0xffffffffu, dia, o);
         }
         if (off <= tol2 * dia) break;
-        for (int r = 0; r < P - 1; ++r) jacobi_round<Real, RF>(w, N, r, lane);
+        for (int r = 0; r < P - 1; ++r) jacobi_round<RF>(w, ut, N, r, lane);
     }
 }
 
-// Fourier sums at the phases w.ph: H0, D0, D1 and (optionally) S_a = sum R_a h_R e^{i(k+A)R}.
-template <class Real, class RF>
-__device__ void fourier(WarpMem<Real, RF> &w, const WanDev &P, bool with_S, const RF (*Rc)[2], int lane)
+// Fourier sums at the phases w.ph: H0, D0, D1 and (optionally) S_a = sum R_a
+// h_R e^{i(k+A)R}, one (quantity, upper element) sum per lane task.
+template <class RF>
+__device__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], const WanDev &P, bool with_S,
+                        const RF *Rc, int lane)
 {
-    using T = typename Cx<Real>::T;
     using TF = typename Cx<RF>::T;
-    const int N = P.N, NN = N * N, NU = N * (N + 1) / 2;
+    const int N = P.N, NN = N * N, nR = P.nR, NU = N * (N + 1) / 2;
+    const int nt = (P.has_dip ? 3 : 1) * NU;
     const TF *h = static_cast<const TF *>(P.h);
     const TF *d = static_cast<const TF *>(P.d);
-    for (int u = lane; u < NU; u += 32) {
-        int m, n;
-        upper_mn(u, N, m, n);
-        const int e = m * N + n;
-        TF hs = cx<TF>(0, 0), d0 = cx<TF>(0, 0), d1 = cx<TF>(0, 0), s0 = cx<TF>(0, 0), s1 = cx<TF>(0, 0);
-        for (int r = 0; r < P.nR; ++r) {
-            const TF t = cmul(h[(size_t)r * NN + e], w.ph[r]);
-            hs.x += t.x;
-            hs.y += t.y;
-            if (with_S) {
-                s0.x = fma(Rc[r][0], t.x, s0.x);
-                s0.y = fma(Rc[r][0], t.y, s0.y);
-                s1.x = fma(Rc[r][1], t.x, s1.x);
-                s1.y = fma(Rc[r][1], t.y, s1.y);
+    for (int t = lane; t < nt; t += 32) {
+        const int q = t / NU, u = t - q * NU;
+        const int m = ut[u][0], n = ut[u][1];
+        const int e = m * N + n, l = n * N + m;
+        const TF *tb = q == 0 ? h + e : d + (size_t)(q - 1) * NN + e;
+        const int stride = q == 0 ? NN : 2 * NN;
+        TF acc = cx<TF>(0, 0), s0 = cx<TF>(0, 0), s1 = cx<TF>(0, 0);
+        if (q == 0 && with_S) {
+#pragma unroll 2
+            for (int r = 0; r < nR; ++r) {
+                const TF p = cmul(tb[(size_t)r * stride], w.ph[r]);
+                acc.x += p.x;
+                acc.y += p.y;
+                s0.x = fma(Rc[2 * r], p.x, s0.x);
+                s0.y = fma(Rc[2 * r], p.y, s0.y);
+                s1.x = fma(Rc[2 * r + 1], p.x, s1.x);
+                s1.y = fma(Rc[2 * r + 1], p.y, s1.y);
             }
-            if (P.has_dip) {
-                cfma(d0, d[((size_t)r * 2 + 0) * NN + e], w.ph[r]);
-                cfma(d1, d[((size_t)r * 2 + 1) * NN + e], w.ph[r]);
-            }
+        } else {
+#pragma unroll 2
+            for (int r = 0; r < nR; ++r) cfma(acc, tb[(size_t)r * stride], w.ph[r]);
         }
-        const T H = cx<T>(hs.x, hs.y), Dx = cx<T>(d0.x, d0.y), Dy = cx<T>(d1.x, d1.y);
-        w.H0[e] = H;
-        w.H0[n * N + m] = cconj(H);
-        w.D0[e] = Dx;
-        w.D0[n * N + m] = cconj(Dx);
-        w.D1[e] = Dy;
-        w.D1[n * N + m] = cconj(Dy);
-        if (with_S) {
-            w.S0[e] = cx<T>(s0.x, s0.y);
-            w.S1[e] = cx<T>(s1.x, s1.y);
-        }
-    }
-    if (with_S) {
-        // S_a = sum R_a h_R e^{iKR} is anti-Hermitian (h_{-R} = h_R^dag), so
-        // (S_a)_nm = -conj((S_a)_mn) and -i S_a = -dH/dk_a is Hermitian
-        __syncwarp();
-        for (int u = lane; u < NU; u += 32) {
-            int m, n;
-            upper_mn(u, N, m, n);
-            if (m != n) {
-                const T a = w.S0[m * N + n], b = w.S1[m * N + n];
-                w.S0[n * N + m] = cx<T>(-a.x, a.y);
-                w.S1[n * N + m] = cx<T>(-b.x, b.y);
+        const double2 v = make_double2(acc.x, acc.y);
+        double2 *M = q == 0 ? w.H0 : q == 1 ? w.D0 : w.D1;
+        M[e] = v;
+        M[l] = cconj(v);
+        if (q == 0 && with_S) {
+            // S_a = sum R_a h_R e^{iKR} is anti-Hermitian (h_{-R} = h_R^dag), so
+            // (S_a)_nm = -conj((S_a)_mn) and -i S_a = -dH/dk_a is Hermitian
+            w.S0[e] = make_double2(s0.x, s0.y);
+            w.S1[e] = make_double2(s1.x, s1.y);
+            if (l != e) {
+                w.S0[l] = make_double2(-s0.x, s0.y);
+                w.S1[l] = make_double2(-s1.x, s1.y);
             }
         }
     }
     __syncwarp();
-}
-
-template <class Real, class RF> struct BlockMem {
-    using TF = typename Cx<RF>::T;
-    TF cA[6][WAN_MAXR];         // e^{i A(t_s) R} per stage
-    RF Rc[WAN_MAXR][2];         // Cartesian lattice vectors
-    double AE[6][6];            // A and E at the stage times
-    double part[WAN_WARPS][WAN_NSLOT];
-    double errw[WAN_WARPS];
-    WTab tab;
-};
-
-template <class Real, class RF> constexpr size_t wan_smem_bytes()
-{
-    return ((sizeof(BlockMem<Real, RF>) + 15) / 16) * 16 + sizeof(WarpMem<Real, RF>) * WAN_WARPS;
 }
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -401,163 +481,153 @@ __device__ __forceinline__ double warp_max(double v)
     return v;
 }
 
-}  // namespace
-
-// ============================================================= init
-template <class Real, class RF>
-__global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
+// k-grid point (momaxis.h:147-186, 349-383) and its trapezoid weight
+__device__ void kpoint(const WanDev &P, int k, double kv[3], double &wt)
 {
-    using T = typename Cx<Real>::T;
-    using TF = typename Cx<RF>::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockMem<Real, RF> &bm = *reinterpret_cast<BlockMem<Real, RF> *>(smem_raw);
-    WarpMem<Real, RF> *wm =
-        reinterpret_cast<WarpMem<Real, RF> *>(smem_raw + ((sizeof(BlockMem<Real, RF>) + 15) / 16) * 16);
-    RF(*Rc)[2] = bm.Rc;
-    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-    for (int r = threadIdx.x; r < P.nR; r += blockDim.x) {
-        Rc[r][0] = RF(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
-        Rc[r][1] = RF(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
-    }
-    __syncthreads();
-    const int k = blockIdx.x * WAN_WARPS + wi;
-    if (k >= P.nk) return;
-    WarpMem<Real, RF> &w = wm[wi];
-    const int N = P.N, NN = N * N;
-    // k-grid point and trapezoid weight (momaxis.h:147-186, 349-383)
     const int N0 = P.Ngrid[0], N1 = P.Ngrid[1], N2 = P.Ngrid[2];
     const int ii[3] = {k / (N1 * N2), (k / N2) % N1, k % N2};
     const int NNg[3] = {N0, N1, N2};
-    double f[3], wt = 1.0;
+    double f[3];
+    wt = 1.0;
     for (int dd = 0; dd < 3; ++dd) {
         f[dd] = (NNg[dd] == 1) ? 0.0 : double(ii[dd]) / (NNg[dd] - 1) - 0.5;
         if (NNg[dd] != 1 && (ii[dd] == 0 || ii[dd] == NNg[dd] - 1)) wt /= 2;
     }
-    double kv[3];
     for (int dd = 0; dd < 3; ++dd)
         kv[dd] = P.origin[dd] + f[0] * P.axes[0 * 3 + dd] + f[1] * P.axes[1 * 3 + dd] + f[2] * P.axes[2 * 3 + dd];
-    if (lane == 0) P.weight[k] = wt;
+}
+
+template <class RF> __device__ void load_lattice(const WanDev &P, RF *Rc)
+{
+    for (int r = threadIdx.x; r < P.nR; r += blockDim.x) {
+        Rc[2 * r] = RF(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
+        Rc[2 * r + 1] = RF(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
+    }
+}
+
+template <class RF> __device__ void kphases(const WanDev &P, const double kv[3], typename Cx<RF>::T *pk, int lane)
+{
+    using TF = typename Cx<RF>::T;
     for (int r = lane; r < P.nR; r += 32) {
         const double Rx = P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2];
         const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
         double s, c;
         sincos(kv[0] * Rx + kv[1] * Ry, &s, &c);
-        w.ph[r] = cx<TF>(c, s);
+        pk[r] = cx<TF>(c, s);
     }
-    for (int e = lane; e < NN; e += 32) w.U[e] = cx<T>((e / N) == (e % N) ? 1 : 0, 0);
-    if (lane < WAN_MAXN + 1) { w.pidx[lane] = -1; w.mate[lane] = -1; }
+}
+
+}  // namespace
+
+// ============================================================= init
+template <class RF>
+__global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const WanSmem L = wan_smem(P.N, P.nR, sizeof(RF));
+    RF *Rc = reinterpret_cast<RF *>(smem_raw + L.Rc);
+    BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    load_lattice<RF>(P, Rc);
+    fill_upper(bh.ut, P.N);
+    __syncthreads();
+    const int k = blockIdx.x * WAN_WARPS + wi;
+    if (k >= P.nk) return;
+    const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, P.N, P.nR);
+    const unsigned char(*ut)[2] = bh.ut;
+    const int N = P.N, NN = N * N;
+    double kv[3], wt;
+    kpoint(P, k, kv, wt);
+    if (lane == 0) P.weight[k] = wt;
+    kphases<RF>(P, kv, w.ph, lane);
+    for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
     __syncwarp();
-    fourier<Real, RF>(w, P, false, Rc, lane);
+    fourier<RF>(w, ut, P, false, Rc, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
-    jacobi_sweeps<Real, RF>(w, N, 16, 1e-30, lane);
+    jacobi_sweeps<RF>(w, ut, N, 16, 1e-30, lane);
     // occupations of the eigenstates: the Nval lowest filled, or Fermi-Dirac (SBEs.h:319-340)
     if (lane < N) {
-        const Real ev = w.B[lane * N + lane].x;
+        const double ev = w.B[lane * N + lane].x;
         int rank = 0;
         for (int j = 0; j < N; ++j) {
-            const Real ej = w.B[j * N + j].x;
+            const double ej = w.B[j * N + j].x;
             rank += (ej < ev) || (ej == ev && j < lane);
         }
         double occ;
-        if (P.use_fermi) occ = 1.0 / (exp((double(ev) - P.Ef) / (300. / 3.15775024804e5)) + 1.0);
+        if (P.use_fermi) occ = 1.0 / (exp((ev - P.Ef) / (300. / 3.15775024804e5)) + 1.0);
         else occ = rank < P.nval ? 1.0 : 0.0;
-        w.dv[lane] = cx<T>(occ, 0);
+        w.dv[lane] = make_double2(occ, 0);
     }
     __syncwarp();
     if (P.use_fermi && lane == 0) {
         double s = 0;
-        for (int j = 0; j < N; ++j) s += double(w.dv[j].x);
-        for (int j = 0; j < N; ++j) w.dv[j] = cx<T>(double(w.dv[j].x) / s, 0);
+        for (int j = 0; j < N; ++j) s += w.dv[j].x;
+        for (int j = 0; j < N; ++j) w.dv[j] = make_double2(w.dv[j].x / s, 0);
     }
     __syncwarp();
-    // rho0 = U diag(f) U^dag (SBEs.h:352-356), FP64 state
+    // rho0 = U diag(f) U^dag (SBEs.h:352-356)
     for (int e = lane; e < NN; e += 32) {
         const int m = e / N, n = e % N;
         double2 acc = make_double2(0, 0);
         for (int p = 0; p < N; ++p) {
-            const T a = w.U[m * N + p], b = w.U[n * N + p];
-            const double fp = double(w.dv[p].x);
-            acc.x += fp * (double(a.x) * double(b.x) + double(a.y) * double(b.y));
-            acc.y += fp * (double(a.y) * double(b.x) - double(a.x) * double(b.y));
+            const double2 a = w.U[m * N + p], b = w.U[n * N + p];
+            const double fp = w.dv[p].x;
+            acc.x += fp * (a.x * b.x + a.y * b.y);
+            acc.y += fp * (a.y * b.x - a.x * b.y);
         }
         P.rho[0][(size_t)k * NN + e] = acc;
-        static_cast<T *>(P.U[0])[(size_t)k * NN + e] = w.U[e];
+        P.U[0][(size_t)k * NN + e] = w.U[e];
     }
 }
 
 // ============================================================= attempt
-template <class Real, class RF>
-__global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__restrict__ Pp)
+// Stage fields and e^{iA(t_s)R} of the attempt come precomputed (wan_control
+// / wan_prepare); each warp advances one k-point through all stages.
+template <class RF>
+__global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *__restrict__ Pp)
 {
-    using T = typename Cx<Real>::T;
     using TF = typename Cx<RF>::T;
+    using T = double2;
+    constexpr bool F32 = std::is_same<RF, float>::value;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockMem<Real, RF> &bm = *reinterpret_cast<BlockMem<Real, RF> *>(smem_raw);
-    WarpMem<Real, RF> *wm =
-        reinterpret_cast<WarpMem<Real, RF> *>(smem_raw + ((sizeof(BlockMem<Real, RF>) + 15) / 16) * 16);
-    TF(*cA)[WAN_MAXR] = bm.cA;
-    RF(*Rc)[2] = bm.Rc;
-    double(*AE)[6] = bm.AE;
-    WTab &tab = bm.tab;
     const WanDev &P = *Pp;
     const WanCtl ctl = *P.ctl;
     if (ctl.done) return;
+    const WanSmem L = wan_smem(P.N, P.nR, sizeof(RF));
+    BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
+    TF *cA = reinterpret_cast<TF *>(smem_raw + L.cA);
+    RF *Rc = reinterpret_cast<RF *>(smem_raw + L.Rc);
+    double(*AE)[6] = bh.AE;
+    WTab &tab = bh.tab;
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-    const int N = P.N, NN = N * N, NU = N * (N + 1) / 2;
-    const double h = ctl.hs, tc = ctl.tc;
+    const int N = P.N, NN = N * N, NU = N * (N + 1) / 2, nR = P.nR;
+    const double h = ctl.hs;
     const int buf = ctl.buf;
     const bool cur = ctl.need_current;
     if (threadIdx.x == 0) tableau(P.rk, tab);
-    for (int r = threadIdx.x; r < P.nR; r += blockDim.x) {
-        Rc[r][0] = RF(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
-        Rc[r][1] = RF(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
-    }
+    load_lattice<RF>(P, Rc);
+    fill_upper(bh.ut, N);
+    const unsigned char(*ut)[2] = bh.ut;
+    const TF *cAg = static_cast<const TF *>(P.stage_cA);
+    for (int i = threadIdx.x; i < 6 * nR; i += blockDim.x) cA[i] = cAg[i];
+    for (int i = threadIdx.x; i < 36; i += blockDim.x) AE[i / 6][i % 6] = P.stage_AE[i];
+    for (int q = threadIdx.x; q < WAN_WARPS * WAN_NSLOT; q += blockDim.x) bh.part[q / WAN_NSLOT][q % WAN_NSLOT] = 0.0;
+    if (threadIdx.x < WAN_WARPS) bh.errw[threadIdx.x] = 0.0;
     __syncthreads();
     const int S = tab.S;
-    if (threadIdx.x < S) {  // field at the stage times (SBEs.h:764-766)
-        double A[3], E[3];
-        const double ts = threadIdx.x == 0 ? tc : tc + tab.c[threadIdx.x] * h;
-        laser_eval(P.laser, ts, A, E);
-        for (int dd = 0; dd < 3; ++dd) { AE[threadIdx.x][dd] = A[dd]; AE[threadIdx.x][3 + dd] = E[dd]; }
-    }
-    __syncthreads();
-    for (int task = threadIdx.x; task < S * P.nR; task += blockDim.x) {
-        const int s = task / P.nR, r = task % P.nR;
-        const double Rx = P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2];
-        const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
-        double sn, cs;
-        sincos(AE[s][0] * Rx + AE[s][1] * Ry, &sn, &cs);
-        cA[s][r] = cx<TF>(cs, sn);
-    }
-    for (int q = threadIdx.x; q < WAN_WARPS * WAN_NSLOT; q += blockDim.x) bm.part[q / WAN_NSLOT][q % WAN_NSLOT] = 0.0;
-    if (threadIdx.x < WAN_WARPS) bm.errw[threadIdx.x] = 0.0;
-    __syncthreads();
 
     const int k = blockIdx.x * WAN_WARPS + wi;
     double emax = 0.0;
     if (k < P.nk) {
-        WarpMem<Real, RF> &w = wm[wi];
-        if (lane < WAN_MAXN + 1) { w.pidx[lane] = -1; w.mate[lane] = -1; }
-        // grid point (momaxis.h:349-383) and e^{ikR}
-        const int N1 = P.Ngrid[1], N2 = P.Ngrid[2];
-        const int ii[3] = {k / (N1 * N2), (k / N2) % N1, k % N2};
-        const int NNg[3] = {P.Ngrid[0], N1, N2};
-        double kv[3], f[3];
-        for (int dd = 0; dd < 3; ++dd) f[dd] = (NNg[dd] == 1) ? 0.0 : double(ii[dd]) / (NNg[dd] - 1) - 0.5;
-        for (int dd = 0; dd < 3; ++dd)
-            kv[dd] = P.origin[dd] + f[0] * P.axes[dd] + f[1] * P.axes[3 + dd] + f[2] * P.axes[6 + dd];
-        for (int r = lane; r < P.nR; r += 32) {
-            const double Rx = P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2];
-            const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
-            double sn, cs;
-            sincos(kv[0] * Rx + kv[1] * Ry, &sn, &cs);
-            w.pk[r] = cx<TF>(cs, sn);
-        }
+        const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, N, nR);
+        double kv[3], wk;
+        kpoint(P, k, kv, wk);
+        kphases<RF>(P, kv, w.pk, lane);
         const double2 *rho = P.rho[buf] + (size_t)k * NN;
-        const T *Ug = static_cast<const T *>(P.U[buf]) + (size_t)k * NN;
+        const T *Ug = P.U[buf] + (size_t)k * NN;
         for (int e = lane; e < NN; e += 32) w.U[e] = Ug[e];
-        // owned upper elements: committed state (FP64) and the stage slopes
+        // owned upper elements: committed state and the stage slopes
         constexpr int MAXO = 2;
         double2 r64[MAXO];
         T ks[6][MAXO];
@@ -571,14 +641,13 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
                 r64[o] = rho[om[o] * N + on[o]];
             }
         }
-        const double wk = P.weight[k];
         for (int s = 0; s < S; ++s) {
             // stage input Y = rho + h sum_j a_sj k_j (owned elements, mirrored)
             for (int o = 0; o < no; ++o) {
-                T y = cx<T>(r64[o].x, r64[o].y);
+                T y = r64[o];
                 for (int j = 0; j < s; ++j) {
-                    const Real a = Real(h * tab.a[s][j]);
-                    if (a != Real(0)) {
+                    const double a = h * tab.a[s][j];
+                    if (a != 0.0) {
                         y.x = fma(a, ks[j][o].x, y.x);
                         y.y = fma(a, ks[j][o].y, y.y);
                     }
@@ -588,12 +657,12 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
                 w.Y[m * N + n] = y;
                 w.Y[n * N + m] = cconj(y);
             }
-            for (int r = lane; r < P.nR; r += 32) w.ph[r] = cmul(w.pk[r], cA[s][r]);
+            for (int r = lane; r < nR; r += 32) w.ph[r] = cmul(w.pk[r], cA[s * nR + r]);
             __syncwarp();
             const bool with_cur = cur && s == 0;
-            fourier<Real, RF>(w, P, with_cur, Rc, lane);
+            fourier<RF>(w, ut, P, with_cur, Rc, lane);
             // H = H0 + E.D (SBEs.h:770-783)
-            const Real Ex = Real(AE[s][3]), Ey = Real(AE[s][4]);
+            const double Ex = AE[s][3], Ey = AE[s][4];
             for (int e = lane; e < NN; e += 32) {
                 T v = w.H0[e];
                 if (P.has_dip) {
@@ -603,16 +672,16 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
                 w.HT[e] = v;
             }
             // eigenbasis of H0(k+A): B = U^dag H0 U, then Jacobi rounds (warm start)
-            mat_mul<T>(w.Tm, w.H0, w.U, N, false, lane);
+            mat_mul(w.Tm, w.H0, w.U, N, false, lane);
             __syncwarp();
-            mat_mul<T>(w.B, w.U, w.Tm, N, true, lane);
+            mat_mul(w.B, w.U, w.Tm, N, true, lane);
             __syncwarp();
-            jacobi_sweeps<Real, RF>(w, N, 6, 1e-30, lane);
+            jacobi_sweeps<RF>(w, ut, N, 6, F32 ? 1e-20 : 1e-30, lane);
             // diag(U^dag Y U)
-            mat_mul<T>(w.Tm, w.Y, w.U, N, false, lane);
+            mat_mul(w.Tm, w.Y, w.U, N, false, lane);
             __syncwarp();
             if (lane < N) {
-                T acc = cx<T>(0, 0);
+                T acc = make_double2(0, 0);
                 for (int l = 0; l < N; ++l) cfmac(acc, w.U[l * N + lane], w.Tm[l * N + lane]);
                 w.dv[lane] = acc;
             }
@@ -627,7 +696,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
                     // J_a into B (B is free after the rounds above), then total = Re Tr(Y J_a)
                     for (int e = lane; e < NN; e += 32) {
                         const int m = e / N, n = e % N;
-                        T c = cx<T>(0, 0);
+                        T c = make_double2(0, 0);
                         for (int l = 0; l < N; ++l) {
                             cfma(c, Da[m * N + l], w.H0[l * N + n]);
                             const T t2 = cmul(w.H0[m * N + l], Da[l * N + n]);
@@ -635,52 +704,52 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
                             c.y -= t2.y;
                         }
                         // -i S + i c = (S.y - c.y, -S.x + c.x)
-                        w.B[e] = cx<T>(Sa[e].y - c.y, c.x - Sa[e].x);
+                        w.B[e] = make_double2(Sa[e].y - c.y, c.x - Sa[e].x);
                     }
                     __syncwarp();
                     double tot = 0.0;
                     for (int e = lane; e < NN; e += 32) {
                         const int m = e / N, n = e % N;
                         const T y = w.Y[e], j = w.B[n * N + m];
-                        tot += double(y.x) * double(j.x) - double(y.y) * double(j.y);
+                        tot += y.x * j.x - y.y * j.y;
                     }
                     tot = warp_sum(tot);
                     // intra = sum_n Re[(U^dag Y U)_nn (U^dag J_a U)_nn]
-                    mat_mul<T>(w.Tm, w.B, w.U, N, false, lane);
+                    mat_mul(w.Tm, w.B, w.U, N, false, lane);
                     __syncwarp();
                     double intra = 0.0;
                     if (lane < N) {
-                        T p = cx<T>(0, 0);
+                        T p = make_double2(0, 0);
                         for (int l = 0; l < N; ++l) cfmac(p, w.U[l * N + lane], w.Tm[l * N + lane]);
-                        intra = double(w.dv[lane].x) * double(p.x) - double(w.dv[lane].y) * double(p.y);
+                        intra = w.dv[lane].x * p.x - w.dv[lane].y * p.y;
                     }
                     intra = warp_sum(intra);
                     val[a] = wk * (tot - intra);
                     val[2 + a] = wk * intra;
                     __syncwarp();
                 }
-                for (int m = 0; m < N; ++m) val[4 + m] = wk * double(w.Y[m * N + m].x);
+                for (int m = 0; m < N; ++m) val[4 + m] = wk * w.Y[m * N + m].x;
                 const int ce = (P.nval * N + P.nval + 1) % NN;  // antelope.cpp:539-542
-                val[4 + N] = wk * double(w.Y[ce].x);
-                val[5 + N] = wk * double(w.Y[ce].y);
+                val[4 + N] = wk * w.Y[ce].x;
+                val[5 + N] = wk * w.Y[ce].y;
                 if (lane == 0)
-                    for (int q = 0; q < WAN_NSLOT; ++q) bm.part[wi][q] = val[q];
+                    for (int q = 0; q < WAN_NSLOT; ++q) bh.part[wi][q] = val[q];
                 __syncwarp();
             }
             // RHS for owned elements: -i[HT, Y] - (g2 Y + (g1-g2) U diag(dv) U^dag)
-            const Real g1 = Real(P.g1), g2 = Real(P.g2);
+            const double g1 = P.g1, g2 = P.g2;
             for (int o = 0; o < no; ++o) {
                 const int m = om[o], n = on[o];
-                T c = cx<T>(0, 0);
+                T c = make_double2(0, 0);
                 for (int l = 0; l < N; ++l) {
                     cfma(c, w.HT[m * N + l], w.Y[l * N + n]);
                     const T t2 = cmul(w.Y[m * N + l], w.HT[l * N + n]);
                     c.x -= t2.x;
                     c.y -= t2.y;
                 }
-                T kv2 = cx<T>(c.y, -c.x);  // -i [H, Y]
-                if (g1 != Real(0) || g2 != Real(0)) {
-                    T pr = cx<T>(0, 0);
+                T kv2 = make_double2(c.y, -c.x);  // -i [H, Y]
+                if (g1 != 0.0 || g2 != 0.0) {
+                    T pr = make_double2(0, 0);
                     for (int p = 0; p < N; ++p) {
                         const T um = w.U[m * N + p], un = w.U[n * N + p];
                         const T t2 = cmul(um, w.dv[p]);
@@ -697,49 +766,138 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_attempt(const WanDev *__re
         // trial state and error estimate
         double2 *rout = P.rho[1 - buf] + (size_t)k * NN;
         for (int o = 0; o < no; ++o) {
-            T inc = cx<T>(0, 0), er = cx<T>(0, 0);
+            T inc = make_double2(0, 0), er = make_double2(0, 0);
             for (int s = 0; s < S; ++s) {
-                const Real b = Real(h * tab.b[s]);
-                if (b != Real(0)) {
+                const double b = h * tab.b[s];
+                if (b != 0.0) {
                     inc.x = fma(b, ks[s][o].x, inc.x);
                     inc.y = fma(b, ks[s][o].y, inc.y);
                 }
-                const Real eb = Real(h * tab.e[s]);
-                if (eb != Real(0)) {
+                const double eb = h * tab.e[s];
+                if (eb != 0.0) {
                     er.x = fma(eb, ks[s][o].x, er.x);
                     er.y = fma(eb, ks[s][o].y, er.y);
                 }
             }
-            double2 v = make_double2(r64[o].x + double(inc.x), r64[o].y + double(inc.y));
+            double2 v = make_double2(r64[o].x + inc.x, r64[o].y + inc.y);
             const int m = om[o], n = on[o];
             if (m == n) v.y = 0.0;
             rout[m * N + n] = v;
             rout[n * N + m] = make_double2(v.x, -v.y);
-            emax = fmax(emax, sqrt(double(er.x) * double(er.x) + double(er.y) * double(er.y)));
+            emax = fmax(emax, sqrt(er.x * er.x + er.y * er.y));
         }
-        T *Uo = static_cast<T *>(P.U[1 - buf]) + (size_t)k * NN;
+        T *Uo = P.U[1 - buf] + (size_t)k * NN;
         for (int e = lane; e < NN; e += 32) Uo[e] = w.U[e];
         emax = warp_max(emax);
-        if (lane == 0) bm.errw[wi] = emax;
+        if (lane == 0) bh.errw[wi] = emax;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double m = 0.0;
-        for (int i = 0; i < WAN_WARPS; ++i) m = fmax(m, bm.errw[i]);
+        for (int i = 0; i < WAN_WARPS; ++i) m = fmax(m, bh.errw[i]);
         P.tile_err[blockIdx.x] = m;
     }
     if (cur && threadIdx.x < WAN_NSLOT) {
         double s = 0.0;
-        for (int i = 0; i < WAN_WARPS; ++i) s += bm.part[i][threadIdx.x];
+        for (int i = 0; i < WAN_WARPS; ++i) s += bh.part[i][threadIdx.x];
         P.cur_part[(size_t)blockIdx.x * WAN_NSLOT + threadIdx.x] = s;
     }
 }
 
+// Fields at the stage times of the next attempt and the per-stage factors
+// e^{iA(t_s)R} (SBEs.h:764-766), shared by every block of the attempt.
+template <class RF> __device__ void prepare_stages(const WanDev &P, const WanCtl &c)
+{
+    using TF = typename Cx<RF>::T;
+    __shared__ double AE[6][6];
+    __shared__ WTab tab;
+    if (threadIdx.x == 0) tableau(P.rk, tab);
+    __syncthreads();
+    const int S = tab.S;
+    if (threadIdx.x < S) {
+        double A[3], E[3];
+        const double ts = threadIdx.x == 0 ? c.tc : c.tc + tab.c[threadIdx.x] * c.hs;
+        laser_eval(P.laser, ts, A, E);
+        for (int dd = 0; dd < 3; ++dd) {
+            AE[threadIdx.x][dd] = A[dd];
+            AE[threadIdx.x][3 + dd] = E[dd];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 36) P.stage_AE[threadIdx.x] = AE[threadIdx.x / 6][threadIdx.x % 6];
+    TF *cA = static_cast<TF *>(P.stage_cA);
+    for (int task = threadIdx.x; task < S * P.nR; task += blockDim.x) {
+        const int s = task / P.nR, r = task % P.nR;
+        const double Rx = P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2];
+        const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
+        double sn, cs;
+        sincos(AE[s][0] * Rx + AE[s][1] * Ry, &sn, &cs);
+        cA[s * P.nR + r] = cx<TF>(cs, sn);
+    }
+}
+
+template <class RF> __global__ void __launch_bounds__(256) wan_prepare(const WanDev *__restrict__ Pp)
+{
+    const WanCtl c = *Pp->ctl;
+    prepare_stages<RF>(*Pp, c);
+}
+
 // ============================================================= control
 // One block: reduce the attempt's tile results (fixed order), record the
-// currents, accept or reject, and prepare the next attempt.  The step-size
-// rule is the oracle's (oracle/sbe_oracle.c, run_adaptive).
-__global__ void __launch_bounds__(1024) wan_control(const WanDev *__restrict__ Pp)
+// currents, accept or reject, and prepare the next attempt (its step, stage
+// fields and phase factors).  The step-size rule is the oracle's
+// (oracle/sbe_oracle.c, run_adaptive).
+__device__ void control_decide(const WanDev &P, WanCtl *ctl, double emax)
+{
+    ctl->attempts++;
+    ctl->need_current = 0;
+    ctl->emax = emax;
+    const double dt = P.dt, tend = P.atmin + dt * (ctl->n + 1);
+    bool accept = true;
+    if (P.rk == 45) {
+        if (emax <= P.tol) {
+            double fac = emax > 0 ? 0.9 * pow(P.tol / emax, 0.2) : 5.0;
+            if (fac > 5.0) fac = 5.0;
+            if (!ctl->last || fac < 1.0) ctl->h = ctl->hs * (fac < 0.2 ? 0.2 : fac);
+            if (ctl->h > dt) ctl->h = dt;
+        } else {
+            accept = false;
+            double fac = 0.9 * pow(P.tol / emax, 0.25);
+            ctl->h = ctl->hs * (fac < 0.1 ? 0.1 : fac);
+            ctl->rejects++;
+            if (!(ctl->h > 1e-12 * dt)) {
+                ctl->error = 1;
+                ctl->done = 1;
+                return;
+            }
+        }
+    }
+    if (accept) {
+        ctl->buf ^= 1;
+        ctl->steps++;
+        if (ctl->last) {
+            ctl->tc = tend;
+            ctl->n++;
+            if (ctl->n >= P.Nt) {
+                ctl->done = 1;
+                return;
+            }
+            ctl->need_current = 1;
+        } else {
+            ctl->tc = ctl->tc + ctl->hs;
+        }
+    }
+    // next attempt
+    const double tend2 = P.atmin + dt * (ctl->n + 1);
+    ctl->hs = ctl->h;
+    ctl->last = 0;
+    if (ctl->tc + ctl->hs >= tend2 - 1e-12 * dt) {
+        ctl->hs = tend2 - ctl->tc;
+        ctl->last = 1;
+    }
+}
+
+template <class RF> __global__ void __launch_bounds__(1024) wan_control(const WanDev *__restrict__ Pp)
 {
     __shared__ double red[1024];
     __shared__ double cs[WAN_NSLOT][64];
@@ -768,47 +926,10 @@ __global__ void __launch_bounds__(1024) wan_control(const WanDev *__restrict__ P
         P.jout[(size_t)ctl->n * WAN_NSLOT + t] = s;
     }
     __syncthreads();
-    if (t != 0) return;
-    const double emax = red[0];
-    ctl->attempts++;
-    ctl->need_current = 0;
-    ctl->emax = emax;
-    const double dt = P.dt, tend = P.atmin + dt * (ctl->n + 1);
-    bool accept = true;
-    if (P.rk == 45) {
-        if (emax <= P.tol) {
-            double fac = emax > 0 ? 0.9 * pow(P.tol / emax, 0.2) : 5.0;
-            if (fac > 5.0) fac = 5.0;
-            if (!ctl->last || fac < 1.0) ctl->h = ctl->hs * (fac < 0.2 ? 0.2 : fac);
-            if (ctl->h > dt) ctl->h = dt;
-        } else {
-            accept = false;
-            double fac = 0.9 * pow(P.tol / emax, 0.25);
-            ctl->h = ctl->hs * (fac < 0.1 ? 0.1 : fac);
-            ctl->rejects++;
-            if (!(ctl->h > 1e-12 * dt)) { ctl->error = 1; ctl->done = 1; return; }
-        }
-    }
-    if (accept) {
-        ctl->buf ^= 1;
-        ctl->steps++;
-        if (ctl->last) {
-            ctl->tc = tend;
-            ctl->n++;
-            if (ctl->n >= P.Nt) { ctl->done = 1; return; }
-            ctl->need_current = 1;
-        } else {
-            ctl->tc = ctl->tc + ctl->hs;
-        }
-    }
-    // next attempt
-    const double tend2 = P.atmin + dt * (ctl->n + 1);
-    ctl->hs = ctl->h;
-    ctl->last = 0;
-    if (ctl->tc + ctl->hs >= tend2 - 1e-12 * dt) {
-        ctl->hs = tend2 - ctl->tc;
-        ctl->last = 1;
-    }
+    if (t == 0) control_decide(P, ctl, red[0]);
+    __syncthreads();
+    const WanCtl c = *ctl;
+    if (!c.done) prepare_stages<RF>(P, c);
 }
 
 // ============================================================= launchers
@@ -816,12 +937,17 @@ template <class RF> static cudaError_t allow_smem()
 {
     static bool done = false;  // per process; the attribute applies to every device
     if (done) return cudaSuccess;
-    const int bytes = (int)wan_smem_bytes<double, RF>();
-    cudaError_t e = cudaFuncSetAttribute(wan_init<double, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    const int bytes = (int)wan_smem(WAN_MAXN, WAN_MAXR, sizeof(RF)).total;
+    cudaError_t e = cudaFuncSetAttribute(wan_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(wan_attempt<double, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(wan_attempt<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     done = e == cudaSuccess;
     return e;
+}
+
+size_t wan_smem_bytes(int N, int nR, int precision)
+{
+    return wan_smem(N, nR, precision == 0 ? 8 : 4).total;
 }
 
 cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st)
@@ -829,8 +955,16 @@ cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st)
     const int grid = (w.nk + WAN_WARPS - 1) / WAN_WARPS;
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
-    if (precision == 0) wan_init<double, double><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, double>(), st>>>(w);
-    else wan_init<double, float><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, float>(), st>>>(w);
+    const size_t sm = wan_smem_bytes(w.N, w.nR, precision);
+    if (precision == 0) wan_init<double><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
+    else wan_init<float><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st)
+{
+    if (precision == 0) wan_prepare<double><<<1, 256, 0, st>>>(dw);
+    else wan_prepare<float><<<1, 256, 0, st>>>(dw);
     return cudaGetLastError();
 }
 
@@ -839,16 +973,16 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
     const int grid = (w.nk + WAN_WARPS - 1) / WAN_WARPS;
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
-    if (precision == 0)
-        wan_attempt<double, double><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, double>(), st>>>(dw);
-    else
-        wan_attempt<double, float><<<grid, 32 * WAN_WARPS, wan_smem_bytes<double, float>(), st>>>(dw);
+    const size_t sm = wan_smem_bytes(w.N, w.nR, precision);
+    if (precision == 0) wan_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    else wan_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wan_control(const WanDev *dw, cudaStream_t st)
+cudaError_t launch_wan_control(const WanDev *dw, int precision, cudaStream_t st)
 {
-    wan_control<<<1, 1024, 0, st>>>(dw);
+    if (precision == 0) wan_control<double><<<1, 1024, 0, st>>>(dw);
+    else wan_control<float><<<1, 1024, 0, st>>>(dw);
     return cudaGetLastError();
 }
 

@@ -3,7 +3,8 @@
 // 297-387 model form).  One warp advances one k-point; a launch performs one
 // attempted step of every k-point of the solve; a one-block controller kernel
 // accepts or rejects it (Cash-Karp, one step size per solve) or always
-// accepts (fixed-step RK4 / Fehlberg-5).
+// accepts (fixed-step RK4 / Fehlberg-5) and prepares the next attempt's stage
+// fields.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -52,16 +53,20 @@ struct WanDev {
     const void *h;          // [nR][N*N] complex, FP32 for the mixed method, FP64 otherwise
     const void *d;          // [nR][2][N*N] complex, same precision (or null)
     double2 *rho[2];        // [nk][N*N] committed / trial state (Wannier basis, full matrix), FP64
-    void *U[2];             // [nk][N*N] tracked eigenbasis of H0(k+A), FP64 complex
+    double2 *U[2];          // [nk][N*N] tracked eigenbasis of H0(k+A), FP64
     double *weight;         // [nk]
     double *tile_err;       // [ntiles]
     double *cur_part;       // [ntiles][WAN_NSLOT]
     double *jout;           // [Nt][WAN_NSLOT]
     WanCtl *ctl;
+    double *stage_AE;       // [6][6] A and E at the stage times of the next attempt
+    void *stage_cA;         // [6][nR] e^{i A(t_s) R} of the next attempt (Fourier precision)
 };
 
+size_t wan_smem_bytes(int N, int nR, int precision);
 cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st);
+cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st);
 cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st);
-cudaError_t launch_wan_control(const WanDev *dw, cudaStream_t st);
+cudaError_t launch_wan_control(const WanDev *dw, int precision, cudaStream_t st);
 
 }  // namespace sbe

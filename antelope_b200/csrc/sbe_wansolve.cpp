@@ -67,13 +67,15 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     if (w_.has_dip) dalloc(&d, cplx * p.w_d.size() / 2, st, "alloc d");
     for (int b = 0; b < 2; ++b) {
         dalloc(&w_.rho[b], sizeof(double2) * nk * NN, st, "alloc rho");
-        dalloc(&w_.U[b], sizeof(double2) * nk * NN, st, "alloc U");  // eigenbasis kept in FP64
+        dalloc(&w_.U[b], sizeof(double2) * nk * NN, st, "alloc U");
     }
     dalloc(&w_.weight, sizeof(double) * nk, st, "alloc weights");
     dalloc(&w_.tile_err, sizeof(double) * w_.ntiles, st, "alloc tile errors");
     dalloc(&w_.cur_part, sizeof(double) * w_.ntiles * WAN_NSLOT, st, "alloc current partials");
     dalloc(&w_.jout, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st, "alloc outputs");
     dalloc(&w_.ctl, sizeof(WanCtl), st, "alloc control");
+    dalloc(&w_.stage_AE, sizeof(double) * 36, st, "alloc stage fields");
+    dalloc(&w_.stage_cA, cplx * 6 * (size_t)w_.nR, st, "alloc stage phases");
     dalloc(&d_w_, sizeof(WanDev), st, "alloc descriptor");
     w_.R = R;
     w_.h = h;
@@ -108,6 +110,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     ring.upload(w_.ctl, &c, sizeof(c), st);
     ring.upload(d_w_, &w_, sizeof(w_), st);
     cuda_check(launch_wan_init(w_, precision_, st), "Wannier init kernel");
+    cuda_check(launch_wan_prepare(d_w_, precision_, st), "Wannier stage preparation");
     cuda_check(cudaMallocHost(&h_ctl_, sizeof(WanCtl)), "cudaMallocHost(control)");
 }
 
@@ -126,6 +129,8 @@ WannierSolve::~WannierSolve()
     cudaFreeAsync(w_.cur_part, stream_);
     cudaFreeAsync(w_.jout, stream_);
     cudaFreeAsync(w_.ctl, stream_);
+    cudaFreeAsync(w_.stage_AE, stream_);
+    cudaFreeAsync(w_.stage_cA, stream_);
     cudaFreeAsync(d_w_, stream_);
     cudaStreamSynchronize(stream_);
     if (h_ctl_) cudaFreeHost(h_ctl_);
@@ -142,7 +147,7 @@ void WannierSolve::run(cudaStream_t st)
     for (;;) {
         for (int c = 0; c < chunk; ++c) {
             cuda_check(launch_wan_attempt(w_, d_w_, precision_, st), "Wannier attempt kernel");
-            cuda_check(launch_wan_control(d_w_, st), "Wannier control kernel");
+            cuda_check(launch_wan_control(d_w_, precision_, st), "Wannier control kernel");
         }
         launched += chunk;
         cuda_check(cudaMemcpyAsync(h_ctl_, w_.ctl, sizeof(WanCtl), cudaMemcpyDeviceToHost, st), "copy control");
