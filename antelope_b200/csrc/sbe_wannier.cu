@@ -200,6 +200,7 @@ struct BlockHead {
     double errw[WAN_WARPS];
     WTab tab;
     unsigned char ut[WAN_MAXU_][2];  // upper-triangle element u -> (m, n)
+    signed char mate[WAN_MAXN - 1][WAN_MAXN];  // Jacobi round r: partner of i (>= N: none)
 };
 constexpr int WAN_NMAT = 10;  // Y, H0, HT, U, B, Tm, D0, D1, S0, S1
 __host__ __device__ __forceinline__ size_t al16(size_t x) { return (x + 15) / 16 * 16; }
@@ -249,12 +250,22 @@ __device__ void mat_mul(double2 *C, const double2 *A, const double2 *B, int N, b
 {
     for (int e = lane; e < N * N; e += 32) {
         const int m = e / N, n = e % N;
-        double2 acc = make_double2(0, 0);
-        for (int l = 0; l < N; ++l) {
-            if (conjA) cfmac(acc, A[l * N + m], B[l * N + n]);
-            else cfma(acc, A[m * N + l], B[l * N + n]);
+        double2 a0 = make_double2(0, 0), a1 = make_double2(0, 0);  // even / odd l
+        int l = 0;
+        for (; l + 2 <= N; l += 2) {
+            if (conjA) {
+                cfmac(a0, A[l * N + m], B[l * N + n]);
+                cfmac(a1, A[(l + 1) * N + m], B[(l + 1) * N + n]);
+            } else {
+                cfma(a0, A[m * N + l], B[l * N + n]);
+                cfma(a1, A[m * N + l + 1], B[(l + 1) * N + n]);
+            }
         }
-        C[e] = acc;
+        if (l < N) {
+            if (conjA) cfmac(a0, A[l * N + m], B[l * N + n]);
+            else cfma(a0, A[m * N + l], B[l * N + n]);
+        }
+        C[e] = make_double2(a0.x + a1.x, a0.y + a1.y);
     }
 }
 
@@ -274,24 +285,27 @@ __device__ __forceinline__ int rr_mate(int i, int r, int P)
 // the lanes.  The upper-element coordinates come from a per-block table.
 constexpr int WAN_MAXJ = 4;  // ceil((36 + 64) / 32)
 
-__device__ void fill_upper(unsigned char (*ut)[2], int N)
+__device__ void fill_tables(BlockHead &bh, int N)
 {
     if (threadIdx.x == 0) {
         int u = 0;
         for (int m = 0; m < N; ++m)
             for (int n = m; n < N; ++n, ++u) {
-                ut[u][0] = (unsigned char)m;
-                ut[u][1] = (unsigned char)n;
+                bh.ut[u][0] = (unsigned char)m;
+                bh.ut[u][1] = (unsigned char)n;
             }
+        const int P = N + (N & 1);
+        for (int r = 0; r < P - 1; ++r)
+            for (int i = 0; i < N; ++i) bh.mate[r][i] = (signed char)rr_mate(i, r, P);
     }
 }
 
 // Column j of the round's rotation matrix J: its nonzeros J_jj and J_mj,j.
 template <class RF>
-__device__ __forceinline__ void jcol(const WarpView<RF> &w, int j, int r, int P, int N, double2 &Jjj, double2 &Jmj,
-                                     int &mj)
+__device__ __forceinline__ void jcol(const WarpView<RF> &w, const signed char *mt, int j, int N, double2 &Jjj,
+                                     double2 &Jmj, int &mj)
 {
-    mj = rr_mate(j, r, P);
+    mj = mt[j];
     if (mj >= N) {
         Jjj = make_double2(1, 0);
         Jmj = make_double2(0, 0);
@@ -315,26 +329,30 @@ __device__ __forceinline__ void jcol(const WarpView<RF> &w, int j, int r, int P,
 // B <- J^dag B J and U <- U J are applied element by element in one pass
 // (inputs read, then written).
 template <class RF>
-__device__ void jacobi_round(const WarpView<RF> &w, const unsigned char (*ut)[2], int N, int r, int lane)
+__device__ void jacobi_round(const WarpView<RF> &w, const BlockHead &bh, int N, int r, int lane)
 {
+    const unsigned char(*ut)[2] = bh.ut;
+    const signed char *mt = bh.mate[r];
     const int NU = N * (N + 1) / 2, nt = NU + N * N;
-    const int P = N + (N & 1);
     if (lane < N) {
-        const int q = rr_mate(lane, r, P);
+        const int q = mt[lane];
         if (q < N && lane < q) {
             const int p = lane;
             const double2 g = w.B[p * N + q];
-            const double rr = sqrt(g.x * g.x + g.y * g.y);
+            const double r2 = g.x * g.x + g.y * g.y;
             double c = 1, s = 0;
             double2 e = make_double2(1, 0);
-            if (rr > 0.0) {
-                const double app = w.B[p * N + p].x, aqq = w.B[q * N + q].x;
-                e.x = g.x / rr;
-                e.y = g.y / rr;
-                const double zeta = (aqq - app) / (2.0 * rr);
-                const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(zeta * zeta + 1.0));
-                c = 1.0 / sqrt(t * t + 1.0);
+            if (r2 > 0.0) {
+                // t = tan(theta) = sign(d) 2|g| / (|d| + sqrt(d^2 + 4|g|^2)), d = a_qq - a_pp
+                // (the smaller root of t^2 + (d/|g|) t - 1 = 0); c = 1/sqrt(1 + t^2)
+                const double d = w.B[q * N + q].x - w.B[p * N + p].x;
+                const double ir = rsqrt(r2);
+                const double hh = sqrt(fma(d, d, 4.0 * r2));
+                const double t = copysign(2.0 * r2 * ir, d) / (fabs(d) + hh);
+                c = rsqrt(fma(t, t, 1.0));
                 s = t * c;
+                e.x = g.x * ir;
+                e.y = g.y * ir;
             }
             w.jc[p] = c;
             w.js[p] = s;
@@ -357,11 +375,11 @@ __device__ void jacobi_round(const WarpView<RF> &w, const unsigned char (*ut)[2]
         }
         double2 Jjj, Jmj;
         int mj;
-        jcol(w, j, r, P, N, Jjj, Jmj, mj);
+        jcol(w, mt, j, N, Jjj, Jmj, mj);
         if (i >= 0) {  // B'_ij = sum_ab conj(J_ai) B_ab J_bj
             double2 Jii, Jmi;
             int mi;
-            jcol(w, i, r, P, N, Jii, Jmi, mi);
+            jcol(w, mt, i, N, Jii, Jmi, mi);
             double2 t1 = cmul(w.B[i * N + j], Jjj), t2 = cmul(w.B[mi * N + j], Jjj);
             cfma(t1, w.B[i * N + mj], Jmj);
             cfma(t2, w.B[mi * N + mj], Jmj);
@@ -399,8 +417,8 @@ __device__ void jacobi_round(const WarpView<RF> &w, const unsigned char (*ut)[2]
 // Sweeps until the off-diagonal part of B is negligible against its diagonal
 // (|offdiag|^2 <= tol2 |diag|^2, warp-uniform test), at most max_sweeps.
 template <class RF>
-__device__ void jacobi_sweeps(const WarpView<RF> &w, const unsigned char (*ut)[2], int N, int max_sweeps,
-                              double tol2, int lane)
+__device__ void jacobi_sweeps(const WarpView<RF> &w, const BlockHead &bh, int N, int max_sweeps, double tol2,
+                              int lane)
 {
     const int P = N + (N & 1);
     for (int s = 0; s < max_sweeps; ++s) {
@@ -415,7 +433,7 @@ __device__ void jacobi_sweeps(const WarpView<RF> &w, const unsigned char (*ut)[2
             dia += __shfl_xor_sync(0xffffffffu, dia, o);
         }
         if (off <= tol2 * dia) break;
-        for (int r = 0; r < P - 1; ++r) jacobi_round<RF>(w, ut, N, r, lane);
+        for (int r = 0; r < P - 1; ++r) jacobi_round<RF>(w, bh, N, r, lane);
     }
 }
 
@@ -435,12 +453,13 @@ __device__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], con
         const int m = ut[u][0], n = ut[u][1];
         const int e = m * N + n, l = n * N + m;
         const TF *tb = q == 0 ? h + e : d + (size_t)(q - 1) * NN + e;
-        const int stride = q == 0 ? NN : 2 * NN;
+        const size_t stride = q == 0 ? NN : 2 * NN;
+        // two independent partial sums (even / odd r) and four table loads in
+        // flight per iteration
         TF acc = cx<TF>(0, 0), s0 = cx<TF>(0, 0), s1 = cx<TF>(0, 0);
-        if (q == 0 && with_S) {
-#pragma unroll 2
+        if (q == 0 && with_S) {  // once per output step: one chain
             for (int r = 0; r < nR; ++r) {
-                const TF p = cmul(tb[(size_t)r * stride], w.ph[r]);
+                const TF p = cmul(tb[r * stride], w.ph[r]);
                 acc.x += p.x;
                 acc.y += p.y;
                 s0.x = fma(Rc[2 * r], p.x, s0.x);
@@ -449,8 +468,14 @@ __device__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], con
                 s1.y = fma(Rc[2 * r + 1], p.y, s1.y);
             }
         } else {
-#pragma unroll 2
-            for (int r = 0; r < nR; ++r) cfma(acc, tb[(size_t)r * stride], w.ph[r]);
+            TF a2[2] = {cx<TF>(0, 0), cx<TF>(0, 0)};
+            int r = 0;
+            for (; r + 4 <= nR; r += 4) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cfma(a2[j & 1], tb[(r + j) * stride], w.ph[r + j]);
+            }
+            for (int j = 0; r < nR; ++r, ++j) cfma(a2[j & 1], tb[r * stride], w.ph[r]);
+            acc = cx<TF>(a2[0].x + a2[1].x, a2[0].y + a2[1].y);
         }
         const double2 v = make_double2(acc.x, acc.y);
         double2 *M = q == 0 ? w.H0 : q == 1 ? w.D0 : w.D1;
@@ -529,7 +554,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
     BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
     load_lattice<RF>(P, Rc);
-    fill_upper(bh.ut, P.N);
+    fill_tables(bh, P.N);
     __syncthreads();
     const int k = blockIdx.x * WAN_WARPS + wi;
     if (k >= P.nk) return;
@@ -545,7 +570,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
     fourier<RF>(w, ut, P, false, Rc, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
-    jacobi_sweeps<RF>(w, ut, N, 16, 1e-30, lane);
+    jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
     // occupations of the eigenstates: the Nval lowest filled, or Fermi-Dirac (SBEs.h:319-340)
     if (lane < N) {
         const double ev = w.B[lane * N + lane].x;
@@ -607,7 +632,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
     const bool cur = ctl.need_current;
     if (threadIdx.x == 0) tableau(P.rk, tab);
     load_lattice<RF>(P, Rc);
-    fill_upper(bh.ut, N);
+    fill_tables(bh, N);
     const unsigned char(*ut)[2] = bh.ut;
     const TF *cAg = static_cast<const TF *>(P.stage_cA);
     for (int i = threadIdx.x; i < 6 * nR; i += blockDim.x) cA[i] = cAg[i];
@@ -676,7 +701,13 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
             __syncwarp();
             mat_mul(w.B, w.U, w.Tm, N, true, lane);
             __syncwarp();
-            jacobi_sweeps<RF>(w, ut, N, 6, F32 ? 1e-20 : 1e-30, lane);
+            jacobi_sweeps<RF>(w, bh, N, 6, F32 ? 1e-20 : 1e-30, lane);
+            // the eigenbasis at t + h (c = 1) warm-starts the next attempt,
+            // whose first stage is at that time once this step is accepted
+            if (tab.c[s] == 1.0) {
+                T *Uo = P.U[1 - buf] + (size_t)k * NN;
+                for (int e = lane; e < NN; e += 32) Uo[e] = w.U[e];
+            }
             // diag(U^dag Y U)
             mat_mul(w.Tm, w.Y, w.U, N, false, lane);
             __syncwarp();
@@ -740,13 +771,13 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
             const double g1 = P.g1, g2 = P.g2;
             for (int o = 0; o < no; ++o) {
                 const int m = om[o], n = on[o];
-                T c = make_double2(0, 0);
+                T c = make_double2(0, 0), c2 = make_double2(0, 0);  // (H Y)_mn and (Y H)_mn
                 for (int l = 0; l < N; ++l) {
                     cfma(c, w.HT[m * N + l], w.Y[l * N + n]);
-                    const T t2 = cmul(w.Y[m * N + l], w.HT[l * N + n]);
-                    c.x -= t2.x;
-                    c.y -= t2.y;
+                    cfma(c2, w.Y[m * N + l], w.HT[l * N + n]);
                 }
+                c.x -= c2.x;
+                c.y -= c2.y;
                 T kv2 = make_double2(c.y, -c.x);  // -i [H, Y]
                 if (g1 != 0.0 || g2 != 0.0) {
                     T pr = make_double2(0, 0);
@@ -786,8 +817,6 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
             rout[n * N + m] = make_double2(v.x, -v.y);
             emax = fmax(emax, sqrt(er.x * er.x + er.y * er.y));
         }
-        T *Uo = P.U[1 - buf] + (size_t)k * NN;
-        for (int e = lane; e < NN; e += 32) Uo[e] = w.U[e];
         emax = warp_max(emax);
         if (lane == 0) bh.errw[wi] = emax;
     }
