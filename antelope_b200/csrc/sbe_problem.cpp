@@ -551,6 +551,11 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
                         throw CfgError("SyntheticWannier: h_{-R} must equal h_R^dagger");
                 }
         }
+        p.w_vec.resize(2 * (size_t)p.w_nR);
+        for (int r = 0; r < p.w_nR; ++r) {
+            p.w_vec[2 * r] = p.w_R[2 * r] * p.w_lat[0] + p.w_R[2 * r + 1] * p.w_lat[2];
+            p.w_vec[2 * r + 1] = p.w_R[2 * r] * p.w_lat[1] + p.w_R[2 * r + 1] * p.w_lat[3];
+        }
         // reciprocal basis b_i . a_j = 2 pi delta_ij (Wannier90.h:489-502)
         const double det = p.w_lat[0] * p.w_lat[3] - p.w_lat[1] * p.w_lat[2];
         if (det == 0.0) throw CfgError("SyntheticWannier.lattice is singular");

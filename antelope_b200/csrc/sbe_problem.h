@@ -88,9 +88,12 @@ struct Problem {
     // D_a(k) = sum_R d_{a,R} e^{ik.R}, R = n1 a1 + n2 a2
     int w_nR = 0;
     double w_lat[4] = {0, 0, 0, 0};   // a1 = (w_lat[0], w_lat[1]), a2 = (w_lat[2], w_lat[3])
-    std::vector<int> w_R;             // [nR][2] lattice coordinates
+    std::vector<int> w_R;             // [nR][2] lattice coordinates (SyntheticWannier input)
+    std::vector<double> w_vec;        // [nR][2] hopping vectors, Cartesian (bohr)
     std::vector<double> w_h;          // [nR][N][N] complex, interleaved
     std::vector<double> w_d;          // [nR][2][N][N] complex, interleaved (empty: no dipoles)
+    std::vector<double> w_j;          // [nR][2][N][N] complex current-operator tables (empty:
+                                      // J_a = -dH/dk_a + i[D_a, H], BaseMaterial.h:62-68)
 
     // derived grid quantities (momaxis.h:192-240)
     int ntotal() const { return Nk[0] * Nk[1] * Nk[2]; }

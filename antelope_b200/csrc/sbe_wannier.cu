@@ -213,9 +213,9 @@ __host__ __device__ __forceinline__ WanSmem wan_smem(int N, int nR, int rf_bytes
     L.cA = al16(sizeof(BlockHead));
     L.Rc = L.cA + al16((size_t)6 * nR * 2 * rf_bytes);
     L.warp0 = L.Rc + al16((size_t)nR * 2 * rf_bytes);
-    const size_t NN = (size_t)N * N;
+    const size_t NN = (size_t)N * N, NU = (size_t)N * (N + 1) / 2;
     L.warp_bytes = al16(WAN_NMAT * NN * 16 + (size_t)N * 16 + WAN_MAXN * 16 + 2 * WAN_MAXN * 8) +
-                   al16((size_t)2 * nR * 2 * rf_bytes);
+                   al16((size_t)2 * nR * 2 * rf_bytes) + 6 * NU * 16;
     L.total = L.warp0 + WAN_WARPS * L.warp_bytes;
     return L;
 }
@@ -229,6 +229,7 @@ template <class RF> struct WarpView {
     double *jc, *js;
     TF *ph;        // e^{i(k+A)R} of the current stage
     TF *pk;        // e^{ikR}
+    double2 *ks;   // [6][NU] stage slopes of the upper-triangle elements
     __device__ WarpView(unsigned char *base, int N, int nR)
     {
         const int NN = N * N;
@@ -242,6 +243,7 @@ template <class RF> struct WarpView {
         const size_t off = al16(WAN_NMAT * (size_t)NN * 16 + (size_t)N * 16 + WAN_MAXN * 16 + 2 * WAN_MAXN * 8);
         ph = reinterpret_cast<TF *>(base + off);
         pk = ph + nR;
+        ks = reinterpret_cast<double2 *>(base + off + al16((size_t)2 * nR * sizeof(TF)));
     }
 };
 
@@ -445,19 +447,33 @@ __device__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], con
 {
     using TF = typename Cx<RF>::T;
     const int N = P.N, NN = N * N, nR = P.nR, NU = N * (N + 1) / 2;
-    const int nt = (P.has_dip ? 3 : 1) * NU;
+    const bool jt = with_S && P.has_jtab;  // current operator from its own tables
+    const bool sS = with_S && !P.has_jtab;  // current operator from S_a = sum R_a h_R e^{iKR}
+    const int nh = (P.has_dip ? 3 : 1) * NU, nt = nh + (jt ? 2 * NN : 0);
     const TF *h = static_cast<const TF *>(P.h);
     const TF *d = static_cast<const TF *>(P.d);
+    const TF *j = static_cast<const TF *>(P.jt);
     for (int t = lane; t < nt; t += 32) {
-        const int q = t / NU, u = t - q * NU;
-        const int m = ut[u][0], n = ut[u][1];
-        const int e = m * N + n, l = n * N + m;
-        const TF *tb = q == 0 ? h + e : d + (size_t)(q - 1) * NN + e;
-        const size_t stride = q == 0 ? NN : 2 * NN;
+        int q, e, l;
+        const TF *tb;
+        size_t stride;
+        if (t < nh) {  // H0, D_x, D_y: Hermitian, upper triangle
+            q = t / NU;
+            const int u = t - q * NU, m = ut[u][0], n = ut[u][1];
+            e = m * N + n;
+            l = n * N + m;
+            tb = q == 0 ? h + e : d + (size_t)(q - 1) * NN + e;
+            stride = q == 0 ? NN : 2 * NN;
+        } else {  // J_x, J_y: every element (the tables need not be Hermitian)
+            q = 3 + (t - nh) / NN;
+            e = l = (t - nh) % NN;
+            tb = j + (size_t)(q - 3) * NN + e;
+            stride = 2 * NN;
+        }
         // two independent partial sums (even / odd r) and four table loads in
         // flight per iteration
         TF acc = cx<TF>(0, 0), s0 = cx<TF>(0, 0), s1 = cx<TF>(0, 0);
-        if (q == 0 && with_S) {  // once per output step: one chain
+        if (q == 0 && sS) {  // once per output step: one chain
             for (int r = 0; r < nR; ++r) {
                 const TF p = cmul(tb[r * stride], w.ph[r]);
                 acc.x += p.x;
@@ -472,16 +488,20 @@ __device__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], con
             int r = 0;
             for (; r + 4 <= nR; r += 4) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) cfma(a2[j & 1], tb[(r + j) * stride], w.ph[r + j]);
+                for (int x = 0; x < 4; ++x) cfma(a2[x & 1], tb[(r + x) * stride], w.ph[r + x]);
             }
-            for (int j = 0; r < nR; ++r, ++j) cfma(a2[j & 1], tb[r * stride], w.ph[r]);
+            for (int x = 0; r < nR; ++r, ++x) cfma(a2[x & 1], tb[r * stride], w.ph[r]);
             acc = cx<TF>(a2[0].x + a2[1].x, a2[0].y + a2[1].y);
         }
         const double2 v = make_double2(acc.x, acc.y);
+        if (q >= 3) {
+            (q == 3 ? w.S0 : w.S1)[e] = v;
+            continue;
+        }
         double2 *M = q == 0 ? w.H0 : q == 1 ? w.D0 : w.D1;
         M[e] = v;
         M[l] = cconj(v);
-        if (q == 0 && with_S) {
+        if (q == 0 && sS) {
             // S_a = sum R_a h_R e^{iKR} is anti-Hermitian (h_{-R} = h_R^dag), so
             // (S_a)_nm = -conj((S_a)_mn) and -i S_a = -dH/dk_a is Hermitian
             w.S0[e] = make_double2(s0.x, s0.y);
@@ -525,8 +545,8 @@ __device__ void kpoint(const WanDev &P, int k, double kv[3], double &wt)
 template <class RF> __device__ void load_lattice(const WanDev &P, RF *Rc)
 {
     for (int r = threadIdx.x; r < P.nR; r += blockDim.x) {
-        Rc[2 * r] = RF(P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2]);
-        Rc[2 * r + 1] = RF(P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3]);
+        Rc[2 * r] = RF(P.V[2 * r]);
+        Rc[2 * r + 1] = RF(P.V[2 * r + 1]);
     }
 }
 
@@ -534,10 +554,8 @@ template <class RF> __device__ void kphases(const WanDev &P, const double kv[3],
 {
     using TF = typename Cx<RF>::T;
     for (int r = lane; r < P.nR; r += 32) {
-        const double Rx = P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2];
-        const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
         double s, c;
-        sincos(kv[0] * Rx + kv[1] * Ry, &s, &c);
+        sincos(kv[0] * P.V[2 * r] + kv[1] * P.V[2 * r + 1], &s, &c);
         pk[r] = cx<TF>(c, s);
     }
 }
@@ -652,10 +670,9 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
         const double2 *rho = P.rho[buf] + (size_t)k * NN;
         const T *Ug = P.U[buf] + (size_t)k * NN;
         for (int e = lane; e < NN; e += 32) w.U[e] = Ug[e];
-        // owned upper elements: committed state and the stage slopes
+        // owned upper elements u = lane + 32 o: committed state; stage slopes in w.ks
         constexpr int MAXO = 2;
         double2 r64[MAXO];
-        T ks[6][MAXO];
         int om[MAXO], on[MAXO];
         const int no = (NU + 31 - lane) / 32;
         for (int o = 0; o < MAXO; ++o) {
@@ -673,8 +690,9 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
                 for (int j = 0; j < s; ++j) {
                     const double a = h * tab.a[s][j];
                     if (a != 0.0) {
-                        y.x = fma(a, ks[j][o].x, y.x);
-                        y.y = fma(a, ks[j][o].y, y.y);
+                        const T kj = w.ks[j * NU + lane + 32 * o];
+                        y.x = fma(a, kj.x, y.x);
+                        y.y = fma(a, kj.y, y.y);
                     }
                 }
                 const int m = om[o], n = on[o];
@@ -718,14 +736,18 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
             }
             __syncwarp();
             if (with_cur) {
-                // currents at k + A(t_n) (SBEs.h:694-760): J_a = -i S_a + i[D_a, H0]
-                double val[WAN_NSLOT];
-                for (int q = 0; q < WAN_NSLOT; ++q) val[q] = 0.0;
+                // currents at k + A(t_n) (SBEs.h:694-760): J_a = -i S_a + i[D_a, H0];
+                // lane 0 records this k's weighted values in its warp's slot row
+                double *val = bh.part[wi];
                 for (int a = 0; a < 2; ++a) {
                     T *Da = a == 0 ? w.D0 : w.D1;
                     T *Sa = a == 0 ? w.S0 : w.S1;
                     // J_a into B (B is free after the rounds above), then total = Re Tr(Y J_a)
                     for (int e = lane; e < NN; e += 32) {
+                        if (P.has_jtab) {  // the model's own current operator at k + A
+                            w.B[e] = Sa[e];
+                            continue;
+                        }
                         const int m = e / N, n = e % N;
                         T c = make_double2(0, 0);
                         for (int l = 0; l < N; ++l) {
@@ -755,30 +777,33 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
                         intra = w.dv[lane].x * p.x - w.dv[lane].y * p.y;
                     }
                     intra = warp_sum(intra);
-                    val[a] = wk * (tot - intra);
-                    val[2 + a] = wk * intra;
+                    if (lane == 0) {
+                        val[a] = wk * (tot - intra);
+                        val[2 + a] = wk * intra;
+                    }
                     __syncwarp();
                 }
-                for (int m = 0; m < N; ++m) val[4 + m] = wk * w.Y[m * N + m].x;
+                if (lane < N) val[4 + lane] = wk * w.Y[lane * N + lane].x;
                 const int ce = (P.nval * N + P.nval + 1) % NN;  // antelope.cpp:539-542
-                val[4 + N] = wk * w.Y[ce].x;
-                val[5 + N] = wk * w.Y[ce].y;
-                if (lane == 0)
-                    for (int q = 0; q < WAN_NSLOT; ++q) bh.part[wi][q] = val[q];
+                if (lane == 0) {
+                    val[4 + N] = wk * w.Y[ce].x;
+                    val[5 + N] = wk * w.Y[ce].y;
+                }
                 __syncwarp();
             }
-            // RHS for owned elements: -i[HT, Y] - (g2 Y + (g1-g2) U diag(dv) U^dag)
+            // RHS for owned elements: -i((HY) - (HY)^dag) (SBEs.h:808-819)
+            // - (g2 Y + (g1-g2) U diag(dv) U^dag)
             const double g1 = P.g1, g2 = P.g2;
             for (int o = 0; o < no; ++o) {
                 const int m = om[o], n = on[o];
-                T c = make_double2(0, 0), c2 = make_double2(0, 0);  // (H Y)_mn and (Y H)_mn
+                T c = make_double2(0, 0), c2 = make_double2(0, 0);  // (H Y)_mn and (H Y)_nm
                 for (int l = 0; l < N; ++l) {
                     cfma(c, w.HT[m * N + l], w.Y[l * N + n]);
-                    cfma(c2, w.Y[m * N + l], w.HT[l * N + n]);
+                    cfma(c2, w.HT[n * N + l], w.Y[l * N + m]);
                 }
                 c.x -= c2.x;
-                c.y -= c2.y;
-                T kv2 = make_double2(c.y, -c.x);  // -i [H, Y]
+                c.y += c2.y;
+                T kv2 = make_double2(c.y, -c.x);  // -i (HY - (HY)^dag)
                 if (g1 != 0.0 || g2 != 0.0) {
                     T pr = make_double2(0, 0);
                     for (int p = 0; p < N; ++p) {
@@ -790,7 +815,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
                     kv2.x -= g2 * y.x + (g1 - g2) * pr.x;
                     kv2.y -= g2 * y.y + (g1 - g2) * pr.y;
                 }
-                ks[s][o] = kv2;
+                w.ks[s * NU + lane + 32 * o] = kv2;
             }
             __syncwarp();
         }
@@ -799,15 +824,16 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
         for (int o = 0; o < no; ++o) {
             T inc = make_double2(0, 0), er = make_double2(0, 0);
             for (int s = 0; s < S; ++s) {
+                const T kv = w.ks[s * NU + lane + 32 * o];
                 const double b = h * tab.b[s];
                 if (b != 0.0) {
-                    inc.x = fma(b, ks[s][o].x, inc.x);
-                    inc.y = fma(b, ks[s][o].y, inc.y);
+                    inc.x = fma(b, kv.x, inc.x);
+                    inc.y = fma(b, kv.y, inc.y);
                 }
                 const double eb = h * tab.e[s];
                 if (eb != 0.0) {
-                    er.x = fma(eb, ks[s][o].x, er.x);
-                    er.y = fma(eb, ks[s][o].y, er.y);
+                    er.x = fma(eb, kv.x, er.x);
+                    er.y = fma(eb, kv.y, er.y);
                 }
             }
             double2 v = make_double2(r64[o].x + inc.x, r64[o].y + inc.y);
@@ -857,10 +883,8 @@ template <class RF> __device__ void prepare_stages(const WanDev &P, const WanCtl
     TF *cA = static_cast<TF *>(P.stage_cA);
     for (int task = threadIdx.x; task < S * P.nR; task += blockDim.x) {
         const int s = task / P.nR, r = task % P.nR;
-        const double Rx = P.R[2 * r] * P.lat[0] + P.R[2 * r + 1] * P.lat[2];
-        const double Ry = P.R[2 * r] * P.lat[1] + P.R[2 * r + 1] * P.lat[3];
         double sn, cs;
-        sincos(AE[s][0] * Rx + AE[s][1] * Ry, &sn, &cs);
+        sincos(AE[s][0] * P.V[2 * r] + AE[s][1] * P.V[2 * r + 1], &sn, &cs);
         cA[s * P.nR + r] = cx<TF>(cs, sn);
     }
 }

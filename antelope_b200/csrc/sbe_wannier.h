@@ -43,15 +43,16 @@ struct WanCtl {
 };
 
 struct WanDev {
-    int N, nval, nR, nk, Nt, ntiles, rk, inter_intra, use_fermi, has_dip;
+    int N, nval, nR, nk, Nt, ntiles, rk, inter_intra, use_fermi, has_dip, has_jtab;
     double Ef, dt, atmin, tol, g1, g2;  // g1 = 1/T1, g2 = 1/T2 (0 when disabled)
     int Ngrid[3];
     double axes[9], origin[3];
-    double lat[4];
     LaserDev laser;
-    const int *R;           // [nR][2]
+    const double *V;        // [nR][2] hopping vectors, Cartesian (bohr)
     const void *h;          // [nR][N*N] complex, FP32 for the mixed method, FP64 otherwise
     const void *d;          // [nR][2][N*N] complex, same precision (or null)
+    const void *jt;         // [nR][2][N*N] current-operator tables, same precision (or null:
+                            // J_a = -dH/dk_a + i[D_a, H])
     double2 *rho[2];        // [nk][N*N] committed / trial state (Wannier basis, full matrix), FP64
     double2 *U[2];          // [nk][N*N] tracked eigenbasis of H0(k+A), FP64
     double *weight;         // [nk]

@@ -22,7 +22,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     if (p.model != MODEL_SYNTHETIC_WANNIER) throw CfgError("not a Wannier problem");
     if (p.gauge != GAUGE_LENGTH_WANNIER)
         throw CfgError("Wannier models run in the length gauge (LengthWannier) on this path");
-    if (p.w_nR > WAN_MAXR) throw CfgError("SyntheticWannier: at most 64 lattice vectors");
+    if (p.w_nR > WAN_MAXR) throw CfgError("tight-binding model: at most 64 hopping vectors");
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
     const int N = p.nband, NN = N * N;
     std::memset(&w_, 0, sizeof(w_));
@@ -36,6 +36,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     w_.inter_intra = p.inter_intra ? 1 : 0;
     w_.use_fermi = p.use_fermi ? 1 : 0;
     w_.has_dip = p.w_d.empty() ? 0 : 1;
+    w_.has_jtab = p.w_j.empty() ? 0 : 1;
     w_.Ef = p.Ef;
     w_.dt = p.dt;
     w_.atmin = p.laser.atmin;
@@ -45,7 +46,6 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     for (int i = 0; i < 3; ++i) w_.Ngrid[i] = p.Nk[i];
     for (int i = 0; i < 9; ++i) w_.axes[i] = p.bzaxes[i];
     for (int i = 0; i < 3; ++i) w_.origin[i] = p.bzorigin[i];
-    for (int i = 0; i < 4; ++i) w_.lat[i] = p.w_lat[i];
     LaserDev &L = w_.laser;
     L.npulses = (int)p.laser.pulses.size();
     if (L.npulses > 8) throw CfgError("at most 8 pulses");
@@ -60,11 +60,12 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
 
     const size_t real = precision_ == 0 ? 8 : 4, cplx = 2 * real;
     const size_t nk = (size_t)w_.nk;
-    int *R = nullptr;
-    void *h = nullptr, *d = nullptr;
-    dalloc(&R, sizeof(int) * p.w_R.size(), st, "alloc R");
+    double *V = nullptr;
+    void *h = nullptr, *d = nullptr, *j = nullptr;
+    dalloc(&V, sizeof(double) * p.w_vec.size(), st, "alloc hopping vectors");
     dalloc(&h, cplx * p.w_h.size() / 2, st, "alloc h");
     if (w_.has_dip) dalloc(&d, cplx * p.w_d.size() / 2, st, "alloc d");
+    if (w_.has_jtab) dalloc(&j, cplx * p.w_j.size() / 2, st, "alloc current tables");
     for (int b = 0; b < 2; ++b) {
         dalloc(&w_.rho[b], sizeof(double2) * nk * NN, st, "alloc rho");
         dalloc(&w_.U[b], sizeof(double2) * nk * NN, st, "alloc U");
@@ -77,11 +78,12 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     dalloc(&w_.stage_AE, sizeof(double) * 36, st, "alloc stage fields");
     dalloc(&w_.stage_cA, cplx * 6 * (size_t)w_.nR, st, "alloc stage phases");
     dalloc(&d_w_, sizeof(WanDev), st, "alloc descriptor");
-    w_.R = R;
+    w_.V = V;
     w_.h = h;
     w_.d = d;
+    w_.jt = j;
     UploadRing &ring = UploadRing::shared();
-    ring.upload(R, p.w_R.data(), sizeof(int) * p.w_R.size(), st);
+    ring.upload(V, p.w_vec.data(), sizeof(double) * p.w_vec.size(), st);
     auto up_real = [&](void *dst, const std::vector<double> &src) {
         if (precision_ == 0) {
             ring.upload(dst, src.data(), src.size() * 8, st);
@@ -92,6 +94,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     };
     up_real(h, p.w_h);
     if (w_.has_dip) up_real(d, p.w_d);
+    if (w_.has_jtab) up_real(j, p.w_j);
     cuda_check(cudaMemsetAsync(w_.jout, 0, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st), "clear outputs");
     // initial controller state: t = t_min, h = dt, currents first
     WanCtl c{};
@@ -117,9 +120,10 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
 WannierSolve::~WannierSolve()
 {
     cudaStreamSynchronize(stream_);
-    cudaFreeAsync((void *)w_.R, stream_);
+    cudaFreeAsync((void *)w_.V, stream_);
     cudaFreeAsync((void *)w_.h, stream_);
     if (w_.d) cudaFreeAsync((void *)w_.d, stream_);
+    if (w_.jt) cudaFreeAsync((void *)w_.jt, stream_);
     for (int b = 0; b < 2; ++b) {
         cudaFreeAsync(w_.rho[b], stream_);
         cudaFreeAsync(w_.U[b], stream_);
