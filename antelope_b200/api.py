@@ -104,6 +104,25 @@ class Problem:
         _check(lib.sbe_problem_laser(self._h, out.ctypes.data))
         return out
 
+    def model_tables(self) -> dict:
+        """The tight-binding tables of a table model (``sbe_problem_model``):
+        vectors [nvec, 2], h [nvec, N, N], optional d / j [nvec, 2, N, N]
+        (complex), the material's Brillouin-zone axes bz [9], nband, nval."""
+        from .capi import Model
+        m = Model()
+        _check(lib.sbe_problem_model(self._h, C.byref(m)))
+        N, nv = m.nband, m.nvec
+        out = {"nband": N, "nval": m.nval, "vec": np.zeros((nv, 2)), "h": np.zeros((nv, N, N), complex),
+               "d": np.zeros((nv, 2, N, N), complex) if m.has_dipoles else None,
+               "j": np.zeros((nv, 2, N, N), complex) if m.has_current_tables else None, "bz": np.zeros(9)}
+        m.vec, m.h, m.bz = out["vec"].ctypes.data, out["h"].ctypes.data, out["bz"].ctypes.data
+        if out["d"] is not None:
+            m.d = out["d"].ctypes.data
+        if out["j"] is not None:
+            m.j = out["j"].ctypes.data
+        _check(lib.sbe_problem_model(self._h, C.byref(m)))
+        return out
+
     def __del__(self):
         if getattr(self, "_h", None):
             lib.sbe_problem_destroy(self._h)

@@ -29,6 +29,11 @@ class Opts(C.Structure):
                 ("profile", C.c_int)]
 
 
+class Model(C.Structure):
+    _fields_ = [("nband", C.c_int), ("nval", C.c_int), ("nvec", C.c_int), ("has_dipoles", C.c_int),
+                ("has_current_tables", C.c_int)] + [(n, C.c_void_p) for n in ("vec", "h", "d", "j", "bz")]
+
+
 class COutputs(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("inter", "intra", "occ", "coh", "laser")]
 
@@ -55,6 +60,7 @@ def _load():
         "sbe_problem_from_string": (C.c_int, [C.c_char_p, C.POINTER(P)]),
         "sbe_problem_dims": (C.c_int, [P, C.POINTER(Dims)]),
         "sbe_problem_laser": (C.c_int, [P, C.c_void_p]),
+        "sbe_problem_model": (C.c_int, [P, C.POINTER(Model)]),
         "sbe_problem_destroy": (None, [P]),
         "sbe_solver_create": (C.c_int, [P, C.POINTER(Opts), C.POINTER(P)]),
         "sbe_solver_run": (C.c_int, [P, C.c_void_p]),

@@ -195,6 +195,24 @@ extern "C" sbe_status sbe_problem_laser(const sbe_problem *p, double *laser)
     return SBE_OK;
 }
 
+extern "C" sbe_status sbe_problem_model(const sbe_problem *p, sbe_model *m)
+{
+    if (!p || !m) return fail(SBE_INVALID_ARGUMENT, "null argument");
+    const Problem &q = p->p;
+    if (q.model == MODEL_HALDANE) return fail(SBE_INVALID_ARGUMENT, "the Haldane model has no tables");
+    m->nband = q.nband;
+    m->nval = q.nval;
+    m->nvec = q.w_nR;
+    m->has_dipoles = q.w_d.empty() ? 0 : 1;
+    m->has_current_tables = q.w_j.empty() ? 0 : 1;
+    if (m->vec) std::copy(q.w_vec.begin(), q.w_vec.end(), m->vec);
+    if (m->h) std::copy(q.w_h.begin(), q.w_h.end(), m->h);
+    if (m->d && !q.w_d.empty()) std::copy(q.w_d.begin(), q.w_d.end(), m->d);
+    if (m->j && !q.w_j.empty()) std::copy(q.w_j.begin(), q.w_j.end(), m->j);
+    if (m->bz) std::copy(q.bz_model, q.bz_model + 9, m->bz);
+    return SBE_OK;
+}
+
 extern "C" void sbe_problem_destroy(sbe_problem *p) { delete p; }
 
 // ================================================================= solver
@@ -222,7 +240,7 @@ extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *op
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking), "stream create");
         cuda_check(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming), "event create");
-        if (p->p.model == MODEL_SYNTHETIC_WANNIER) {
+        if (p->p.model != MODEL_HALDANE) {
             const int prec = (opts && opts->precision >= 0) ? opts->precision : p->p.precision;
             s->wan = std::make_unique<WannierSolve>(p->p, prec, s->device, s->own);
         } else {

@@ -1,0 +1,368 @@
+// The reference's analytic tight-binding materials (src/GeneralModel/Materials)
+// restated as Fourier tables: H(k) = sum_v h_v e^{ik.v} and the current
+// operator the material's GenJMatrix returns, J_a(k) = sum_v j_{a,v} e^{ik.v},
+// over a small set of Cartesian vectors v.  Every cos / sin / exp term of the
+// reference's formulas becomes one or two table entries, so the tables
+// reproduce its H and J -- including where its J is not -dH/dk (noted per
+// material) -- and the N-band length- and velocity-gauge kernels run them
+// unchanged.  Parameter keys, defaults, unit conversions, Brillouin-zone axes
+// and error texts follow each material's constructor.
+#include <array>
+#include <cmath>
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "sbe_problem.h"
+
+namespace sbe {
+
+namespace {
+
+using cplx = std::complex<double>;
+const cplx I1(0.0, 1.0);
+
+// Accumulates table entries on a set of vectors (entries on the same vector
+// are merged; vectors are compared with a relative tolerance of 1e-12).
+struct TBBuilder {
+    int N;
+    std::vector<std::array<double, 2>> v;
+    std::vector<cplx> h, j;  // [nv][N*N], [nv][2][N*N]
+    explicit TBBuilder(int n) : N(n) {}
+
+    int vec(double x, double y)
+    {
+        for (size_t i = 0; i < v.size(); ++i) {
+            const double s = 1e-12 * (1.0 + std::fabs(x) + std::fabs(y));
+            if (std::fabs(v[i][0] - x) <= s && std::fabs(v[i][1] - y) <= s) return (int)i;
+        }
+        v.push_back({x, y});
+        h.resize(v.size() * N * N);
+        j.resize(v.size() * 2 * N * N);
+        return (int)v.size() - 1;
+    }
+    // c e^{ik.v} into H(m, n), or into J_a(m, n) for a = 0, 1
+    void exp_(int a, int m, int n, double vx, double vy, cplx c)
+    {
+        if (c == cplx(0.0)) return;
+        const int r = vec(vx, vy);
+        if (a < 0) h[(size_t)r * N * N + m * N + n] += c;
+        else j[((size_t)r * 2 + a) * N * N + m * N + n] += c;
+    }
+    // c cos(k.v) and c sin(k.v) as two exponentials
+    void cos_(int a, int m, int n, double vx, double vy, cplx c)
+    {
+        exp_(a, m, n, vx, vy, 0.5 * c);
+        exp_(a, m, n, -vx, -vy, 0.5 * c);
+    }
+    void sin_(int a, int m, int n, double vx, double vy, cplx c)
+    {
+        exp_(a, m, n, vx, vy, -0.5 * I1 * c);
+        exp_(a, m, n, -vx, -vy, 0.5 * I1 * c);
+    }
+    void const_(int a, int m, int n, cplx c) { exp_(a, m, n, 0.0, 0.0, c); }
+
+    void to_problem(Problem &p) const
+    {
+        p.nband = N;
+        p.w_nR = (int)v.size();
+        p.w_vec.resize(2 * v.size());
+        for (size_t i = 0; i < v.size(); ++i) {
+            p.w_vec[2 * i] = v[i][0];
+            p.w_vec[2 * i + 1] = v[i][1];
+        }
+        p.w_h.resize(2 * h.size());
+        for (size_t i = 0; i < h.size(); ++i) {
+            p.w_h[2 * i] = h[i].real();
+            p.w_h[2 * i + 1] = h[i].imag();
+        }
+        p.w_j.resize(2 * j.size());
+        for (size_t i = 0; i < j.size(); ++i) {
+            p.w_j[2 * i] = j[i].real();
+            p.w_j[2 * i + 1] = j[i].imag();
+        }
+        p.w_d.clear();
+    }
+};
+
+void set_bz(Problem &p, double kxMax, double kyMax)
+{
+    const double axes[9] = {2 * kxMax, 0, 0, 0, 2 * kyMax, 0, 0, 0, 0};
+    for (int i = 0; i < 9; ++i) p.bzaxes[i] = axes[i];
+    for (int i = 0; i < 3; ++i) p.bzorigin[i] = 0.0;
+}
+
+// Honeycomb nearest- and next-nearest-neighbour vectors (SetBasis of
+// Haldane.h:134-143, KaneMele.h, Haldane2L.h)
+void honeycomb(double a, double va[3][2], double vb[3][2])
+{
+    const double r3 = std::sqrt(3.);
+    const double A[3][2] = {{0., a}, {-r3 / 2 * a, -0.5 * a}, {r3 / 2 * a, -0.5 * a}};
+    const double B[3][2] = {{r3 * a, 0.}, {-r3 / 2 * a, 3. / 2. * a}, {-r3 / 2 * a, -3. / 2. * a}};
+    for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 2; ++c) {
+            va[i][c] = A[i][c];
+            vb[i][c] = B[i][c];
+        }
+}
+
+// One Haldane block on rows/columns (o, o+1) of H:
+//   B0 = 2 t2 cos(phi) sum cos(k.b), B1 = t1 sum cos(k.a), B2 = t1 sum sin(k.a),
+//   B3 = M0 - f3 sum sin(k.b)  with f3 = 2 t2 sin(phi) (GenBcomp),
+//   H = [[B0 + B3, B1 - s i B2], [B1 + s i B2, B0 - B3]]   (s = B2 sign).
+// b3const / b3sin allow the Haldane2L bottom-layer form of B3.
+void haldane_block_h(TBBuilder &tb, int o, double va[3][2], double vb[3][2], double t1, double c0, double b3const,
+                     double b3sin, double s)
+{
+    for (int i = 0; i < 3; ++i) {
+        const double *a = va[i], *b = vb[i];
+        // B0 on both diagonal entries
+        tb.cos_(-1, o, o, b[0], b[1], c0);
+        tb.cos_(-1, o + 1, o + 1, b[0], b[1], c0);
+        // +/- B3 (sin part)
+        tb.sin_(-1, o, o, b[0], b[1], -b3sin);
+        tb.sin_(-1, o + 1, o + 1, b[0], b[1], b3sin);
+        // B1 -/+ s i B2
+        tb.cos_(-1, o, o + 1, a[0], a[1], t1);
+        tb.sin_(-1, o, o + 1, a[0], a[1], -s * I1 * t1);
+        tb.cos_(-1, o + 1, o, a[0], a[1], t1);
+        tb.sin_(-1, o + 1, o, a[0], a[1], s * I1 * t1);
+    }
+    tb.const_(-1, o, o, b3const);
+    tb.const_(-1, o + 1, o + 1, -b3const);
+}
+
+// -d/dk of that block (GenJMatrix of Haldane.h:94-127 and the layered forms):
+//   xder0 = -c0 sum b_x sin(k.b), xder1 = -t1 sum a_x sin(k.a),
+//   xder2 = t1 sum a_x cos(k.a),  xder3 = -f3 sum b_x cos(k.b),
+//   J = -[[x0 + x3, x1 - s i x2], [x1 + s i x2, x0 - x3]]
+// (sw swaps the roles of +x3 / -x3 on the diagonal: Kane-Mele's lower block).
+void haldane_block_j(TBBuilder &tb, int o, double va[3][2], double vb[3][2], double t1, double c0, double f3,
+                     double s, bool sw)
+{
+    for (int ax = 0; ax < 2; ++ax)
+        for (int i = 0; i < 3; ++i) {
+            const double *a = va[i], *b = vb[i];
+            // x0 = -c0 b sin(k.b): -x0 on both diagonal entries
+            tb.sin_(ax, o, o, b[0], b[1], c0 * b[ax]);
+            tb.sin_(ax, o + 1, o + 1, b[0], b[1], c0 * b[ax]);
+            // x3 = -f3 b cos(k.b): -x3 on (o,o), +x3 on (o+1,o+1) (swapped when sw)
+            const double d3 = sw ? -1.0 : 1.0;
+            tb.cos_(ax, o, o, b[0], b[1], d3 * f3 * b[ax]);
+            tb.cos_(ax, o + 1, o + 1, b[0], b[1], -d3 * f3 * b[ax]);
+            // x1 = -t1 a sin(k.a), x2 = t1 a cos(k.a): -(x1 -/+ s i x2)
+            tb.sin_(ax, o, o + 1, a[0], a[1], t1 * a[ax]);
+            tb.cos_(ax, o, o + 1, a[0], a[1], s * I1 * t1 * a[ax]);
+            tb.sin_(ax, o + 1, o, a[0], a[1], t1 * a[ax]);
+            tb.cos_(ax, o + 1, o, a[0], a[1], -s * I1 * t1 * a[ax]);
+        }
+}
+
+// ------------------------------------------------------------ WilsonMass
+// WilsonMass.h: 2 bands, B1 = delta sin(a0 kx), B2 = delta sin(a1 ky),
+// B3 = -2t (cos(a0 kx) + cos(a1 ky)) - mu; J = -dH/dk.  Lengths in bohr.
+void wilson_mass(const CfgValue *mat, Problem &p)
+{
+    double t, delta, mu, a0, a1;
+    if (!(mat && get_double(mat, "t", t) && get_double(mat, "delta", delta) && get_double(mat, "mu", mu) &&
+          get_double(mat, "a0", a0)))
+        throw CfgError("Some Haldane paramters are missing");  // the reference's text
+    if (!get_double(mat, "a1", a1)) a1 = a0;
+    TBBuilder tb(2);
+    // H = [[B3, B1 - i B2], [B1 + i B2, -B3]]
+    tb.cos_(-1, 0, 0, a0, 0, -2 * t);
+    tb.cos_(-1, 0, 0, 0, a1, -2 * t);
+    tb.const_(-1, 0, 0, -mu);
+    tb.cos_(-1, 1, 1, a0, 0, 2 * t);
+    tb.cos_(-1, 1, 1, 0, a1, 2 * t);
+    tb.const_(-1, 1, 1, mu);
+    tb.sin_(-1, 0, 1, a0, 0, delta);
+    tb.sin_(-1, 0, 1, 0, a1, -I1 * delta);
+    tb.sin_(-1, 1, 0, a0, 0, delta);
+    tb.sin_(-1, 1, 0, 0, a1, I1 * delta);
+    // J (WilsonMass.h GenJMatrix): x: [-2t a0 s, -a0 d c; -a0 d c, 2t a0 s] with s, c of a0 kx
+    tb.sin_(0, 0, 0, a0, 0, -2 * t * a0);
+    tb.sin_(0, 1, 1, a0, 0, 2 * t * a0);
+    tb.cos_(0, 0, 1, a0, 0, -a0 * delta);
+    tb.cos_(0, 1, 0, a0, 0, -a0 * delta);
+    tb.sin_(1, 0, 0, 0, a1, -2 * t * a1);
+    tb.sin_(1, 1, 1, 0, a1, 2 * t * a1);
+    tb.cos_(1, 0, 1, 0, a1, I1 * a1 * delta);
+    tb.cos_(1, 1, 0, 0, a1, -I1 * a1 * delta);
+    tb.to_problem(p);
+    p.nval = 1;
+    set_bz(p, PI / a0, PI / a1);
+}
+
+// ------------------------------------------------------------ KaneMele
+// KaneMele.h: two Haldane blocks with phi0 and -phi0 and a Rashba coupling
+// between them.  Reference specifics kept: J's Rashba entries are +dH/dk
+// (the Haldane blocks are -dH/dk), and its (3,0) entry is not multiplied by
+// i tR (the scaling loop stops at index 2).
+void kane_mele(const CfgValue *mat, Problem &p)
+{
+    double t1, t2, tR, M0, phi0, a0;
+    if (!(mat && get_double(mat, "t1", t1) && get_double(mat, "t2", t2) && get_double(mat, "tR", tR) &&
+          get_double(mat, "Mt2", M0) && get_double(mat, "phi0", phi0) && get_double(mat, "a0", a0)))
+        throw CfgError("Some KaneMele paramters are missing");
+    a0 /= AU_ANGSTROM;
+    M0 *= t2;
+    double va[3][2], vb[3][2];
+    honeycomb(a0, va, vb);
+    const double cR[3][2] = {{1., 0.}, {-0.5, std::sqrt(3.) / 2}, {-0.5, -std::sqrt(3.) / 2}};
+    TBBuilder tb(4);
+    // upper block: phi0; lower block: -phi0 (cos unchanged, sin flips)
+    haldane_block_h(tb, 0, va, vb, t1, 2. * t2 * std::cos(phi0), M0, 2. * t2 * std::sin(phi0), 1.0);
+    haldane_block_h(tb, 2, va, vb, t1, 2. * t2 * std::cos(-phi0), M0, 2. * t2 * std::sin(-phi0), 1.0);
+    // the reference's lower-block J takes the upper block's derivatives with
+    // x3 swapped between the diagonal entries (KaneMele.h GenJMatrix)
+    haldane_block_j(tb, 0, va, vb, t1, 2. * t2 * std::cos(phi0), 2. * t2 * std::sin(phi0), 1.0, false);
+    haldane_block_j(tb, 2, va, vb, t1, 2. * t2 * std::cos(phi0), 2. * t2 * std::sin(phi0), 1.0, true);
+    for (int i = 0; i < 3; ++i) {
+        const double *a = va[i];
+        const cplx cm(cR[i][0], -cR[i][1]), cp(cR[i][0], cR[i][1]);
+        // H(0,3) = i tR sum cm e^{ik.a}, H(1,2) = i tR sum cm e^{-ik.a},
+        // H(2,1) = conj(H(1,2)), H(3,0) = conj(H(0,3))
+        tb.exp_(-1, 0, 3, a[0], a[1], I1 * tR * cm);
+        tb.exp_(-1, 1, 2, -a[0], -a[1], I1 * tR * cm);
+        tb.exp_(-1, 2, 1, a[0], a[1], -I1 * tR * cp);
+        tb.exp_(-1, 3, 0, -a[0], -a[1], -I1 * tR * cp);
+        for (int ax = 0; ax < 2; ++ax) {
+            tb.exp_(ax, 0, 3, a[0], a[1], I1 * tR * cm * (I1 * a[ax]));
+            tb.exp_(ax, 1, 2, -a[0], -a[1], I1 * tR * cm * (-I1 * a[ax]));
+            tb.exp_(ax, 2, 1, a[0], a[1], I1 * tR * (-cp) * (I1 * a[ax]));
+            tb.exp_(ax, 3, 0, -a[0], -a[1], (-cp) * (-I1 * a[ax]));
+        }
+    }
+    tb.to_problem(p);
+    p.nval = 2;
+    set_bz(p, PI / std::sqrt(3.) / a0, 2. * PI / 3. / a0);
+}
+
+// ------------------------------------------------------------ Haldane2L
+// Haldane2L.h: two Haldane layers (4 bands) with a stacking-dependent
+// interlayer hopping t11.  Reference specifics kept: the bottom-layer
+// parameters t1_bottom / t2_bottom / phi0_bottom are read with a
+// short-circuiting OR (after the first one found, the others keep the top
+// values); with distinct layers, the bottom B3 is M0_b - 2 t2_b sin(phi0_b)
+// times the top layer's B3 (not its own sine sum) while J uses the bottom
+// layer's own derivatives.
+void haldane_2l(const CfgValue *mat, Problem &p)
+{
+    double t1[2], t2[2], phi0[2], M0[2], a0, t11;
+    std::string polytype;
+    if (!(mat && get_double(mat, "t1", t1[0]) && get_double(mat, "t2", t2[0]) &&
+          get_double(mat, "phi0", phi0[0]) && get_double(mat, "a0", a0) && get_double(mat, "t11", t11) &&
+          get_string(mat, "polytype", polytype)))
+        throw CfgError("Some Haldane2L paramters are missing");
+    a0 /= AU_ANGSTROM;
+    if (!get_double(mat, "M0", M0[0])) {
+        if (get_double(mat, "Mt2", M0[0])) M0[0] *= t2[0];
+        else throw CfgError("M0 param missing");
+    }
+    bool same = true;
+    t1[1] = t1[0];
+    t2[1] = t2[0];
+    phi0[1] = phi0[0];
+    M0[1] = M0[0];
+    if (get_double(mat, "t1_bottom", t1[1]) || get_double(mat, "t2_bottom", t2[1]) ||
+        get_double(mat, "phi0_bottom", phi0[1]))
+        same = false;
+    if (get_double(mat, "M0_bottom", M0[1])) {
+        same = false;
+    } else if (get_double(mat, "Mt2_bottom", M0[1])) {
+        M0[1] *= t2[1];
+        same = false;
+    }
+    double B2sign[2] = {1., 1.}, hi[4] = {0, 0, 0, 0};
+    if (polytype == "AA") { hi[0] = t11; hi[3] = t11; }
+    else if (polytype == "AB" || polytype == "AB1") { hi[1] = t11; }
+    else if (polytype == "AB2" || polytype == "3R") { hi[2] = t11; }
+    else if (polytype == "AA'" || polytype == "2H") { hi[1] = t11; hi[2] = t11; B2sign[1] = -1.; }
+    else if (polytype == "A'B") { hi[3] = t11; B2sign[0] = -1.; }
+    else if (polytype == "AB'") { hi[0] = t11; B2sign[1] = -1.; }
+    else throw CfgError("Undefined polytype");
+    double va[3][2], vb[3][2];
+    honeycomb(a0, va, vb);
+    TBBuilder tb(4);
+    const double f3t = 2. * t2[0] * std::sin(phi0[0]);
+    haldane_block_h(tb, 0, va, vb, t1[0], 2. * t2[0] * std::cos(phi0[0]), M0[0], f3t, B2sign[0]);
+    if (same) {
+        haldane_block_h(tb, 2, va, vb, t1[0], 2. * t2[0] * std::cos(phi0[0]), M0[0], f3t, B2sign[1]);
+    } else {
+        // B3_b = M0_b - f3b * (M0_t - f3t sum sin(k.b))
+        const double f3b = 2. * t2[1] * std::sin(phi0[1]);
+        haldane_block_h(tb, 2, va, vb, t1[1], 2. * t2[1] * std::cos(phi0[1]), M0[1] - f3b * M0[0], -f3b * f3t,
+                        B2sign[1]);
+    }
+    haldane_block_j(tb, 0, va, vb, t1[0], 2. * t2[0] * std::cos(phi0[0]), f3t, B2sign[0], false);
+    haldane_block_j(tb, 2, va, vb, t1[1], 2. * t2[1] * std::cos(phi0[1]), 2. * t2[1] * std::sin(phi0[1]),
+                    B2sign[1], false);
+    // interlayer: H(0,2) = hi0, (0,3) = hi1, (1,2) = hi2, (1,3) = hi3 and their conjugates
+    const int im[4][2] = {{0, 2}, {0, 3}, {1, 2}, {1, 3}};
+    for (int i = 0; i < 4; ++i) {
+        tb.const_(-1, im[i][0], im[i][1], hi[i]);
+        tb.const_(-1, im[i][1], im[i][0], hi[i]);
+    }
+    tb.to_problem(p);
+    p.nval = 2;
+    set_bz(p, PI / std::sqrt(3.) / a0, 2. * PI / 3. / a0);
+}
+
+// ------------------------------------------------------------ XYHlattice
+// XYHlattice.h: 4 bands, phases e^{-ik.a_i} of three bond vectors,
+// alpha_+- = e^{-ik.a_0} +- e^{-ik.a_1}, beta = e^{-ik.a_2}.  Reference
+// specific kept: its J is +dH/dk.
+void xyh_lattice(const CfgValue *mat, Problem &p)
+{
+    double tl, tr, lambda, a0;
+    if (!(mat && get_double(mat, "tl", tl) && get_double(mat, "tr", tr) && get_double(mat, "lambda", lambda) &&
+          get_double(mat, "a0", a0)))
+        throw CfgError("Some XYHlattice paramters are missing");
+    a0 /= AU_ANGSTROM;
+    const double r3 = std::sqrt(3.);
+    const double va[3][2] = {{0., a0 / r3}, {-0.5 * a0, -0.5 * a0 / r3}, {0.5 * a0, -0.5 * a0 / r3}};
+    TBBuilder tb(4);
+    tb.const_(-1, 0, 0, lambda);
+    tb.const_(-1, 1, 1, lambda);
+    tb.const_(-1, 2, 2, -lambda);
+    tb.const_(-1, 3, 3, -lambda);
+    // upper blocks as coefficients of e^{-ik.a_i}, i = 0, 1, 2
+    const double c02[3] = {0.75 * tl + 0.25 * tr, 0.75 * tl + 0.25 * tr, tr};
+    const double c03[3] = {r3 / 4 * (tl - tr), -r3 / 4 * (tl - tr), 0.};
+    const double c13[3] = {0.25 * tl + 0.75 * tr, 0.25 * tl + 0.75 * tr, tl};
+    const double *cs[3] = {c02, c03, c13};
+    // (row, col) of the three independent entries; (1,2) equals (0,3)
+    const int ent[4][3] = {{0, 2, 0}, {0, 3, 1}, {1, 2, 1}, {1, 3, 2}};
+    for (int e = 0; e < 4; ++e) {
+        const int m = ent[e][0], n = ent[e][1];
+        const double *c = cs[ent[e][2]];
+        for (int i = 0; i < 3; ++i) {
+            const double *a = va[i];
+            tb.exp_(-1, m, n, -a[0], -a[1], c[i]);
+            tb.exp_(-1, n, m, a[0], a[1], c[i]);  // conjugate entry
+            for (int ax = 0; ax < 2; ++ax) {
+                tb.exp_(ax, m, n, -a[0], -a[1], c[i] * (-I1 * a[ax]));
+                tb.exp_(ax, n, m, a[0], a[1], c[i] * (I1 * a[ax]));
+            }
+        }
+    }
+    tb.to_problem(p);
+    p.nval = 2;
+    set_bz(p, PI / a0, 2. * PI / r3 / a0);
+}
+
+}  // namespace
+
+bool build_material(const std::string &target, const CfgValue *mat, Problem &p)
+{
+    if (target == "WilsonMass") wilson_mass(mat, p);
+    else if (target == "KaneMele") kane_mele(mat, p);
+    else if (target == "Haldane2L") haldane_2l(mat, p);
+    else if (target == "XYHlattice") xyh_lattice(mat, p);
+    else return false;
+    p.model = MODEL_TB;
+    return true;
+}
+
+}  // namespace sbe

@@ -11,10 +11,8 @@
 
 namespace sbe {
 
-namespace {
-const double PI = 4.0 * std::atan(1.0);   // constant.h:19
-const double AU_ANGSTROM = 0.529177210903;  // constant.h:32
-}  // namespace
+extern const double PI = 4.0 * std::atan(1.0);   // constant.h:19
+extern const double AU_ANGSTROM = 0.529177210903;  // constant.h:32
 
 // ================================================================= parser
 const CfgValue *CfgValue::get(const std::string &key) const
@@ -174,6 +172,8 @@ void parse_value(Lexer &L, CfgValue &out)
     }
 }
 
+}  // namespace
+
 // ---- typed access with libconfig's strict rules (no auto-conversion)
 bool get_double(const CfgValue *g, const char *key, double &v)
 {
@@ -203,6 +203,8 @@ bool get_string(const CfgValue *g, const char *key, std::string &v)
     v = x->sval;
     return true;
 }
+
+namespace {
 // element i of an array/list setting as a float (type error otherwise)
 double elem_double(const CfgValue &arr, size_t i, const char *err)
 {
@@ -565,17 +567,18 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
         for (int i = 0; i < 3; ++i) p.bzorigin[i] = 0.0;
         if (custom)
             throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
-        if (p.gauge != GAUGE_LENGTH_WANNIER)
-            unsup("Wannier models run in the length gauge (LengthWannier) on the GPU path");
-    } else if (p.target == "Haldane2L" || p.target == "KaneMele" || p.target == "WilsonMass" ||
-               p.target == "Bi2Se3surf" || p.target == "TMDCs" || p.target == "XYHlattice" ||
-               p.target == "SquareSBand" || p.target == "WDSM_TaAs" || p.target == "MultiWSM") {
+    } else if (build_material(p.target, mat, p)) {
+        if (custom)
+            throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
+    } else if (p.target == "Bi2Se3surf" || p.target == "TMDCs" || p.target == "SquareSBand" ||
+               p.target == "WDSM_TaAs" || p.target == "MultiWSM") {
         unsup("material '" + p.target + "' is not built on the GPU path");
         return p;
     } else {
         throw CfgError("Undefined Material");
     }
     // ksfactor scaling and BZ overrides (SBEs.h:221-241)
+    for (int i = 0; i < 9; ++i) p.bz_model[i] = p.bzaxes[i];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) p.bzaxes[3 * i + j] *= p.ksfactor[i];
     if (const CfgValue *bz = calc->get("BZaxes"))
@@ -588,8 +591,8 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
 
     if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) unsup("gauge LengthHamiltonian is not implemented in the reference either");
     if (p.shot_number > 0) unsup("density snapshots (calc.shotNumber > 0) are not built");
-    if (p.rk == 45 && p.model != MODEL_SYNTHETIC_WANNIER)
-        unsup("adaptive Cash-Karp steps are built for Wannier models only");
+    if (p.rk == 45 && p.model == MODEL_HALDANE)
+        unsup("adaptive Cash-Karp steps are built for the N-band (table) models only");
     return p;
 }
 

@@ -61,7 +61,11 @@ struct Laser {
 
 // ---------------------------------------------------------------- problem
 enum Gauge { GAUGE_LENGTH_WANNIER = 0, GAUGE_LENGTH_HAMILTONIAN = 1, GAUGE_VELOCITY = 2 };
-enum Model { MODEL_HALDANE = 0, MODEL_SYNTHETIC_WANNIER = 1 };
+enum Model {
+    MODEL_HALDANE = 0,
+    MODEL_SYNTHETIC_WANNIER = 1,  // tight-binding tables given in the cfg
+    MODEL_TB = 2,                 // an analytic material restated as tables (sbe_materials.cpp)
+};
 
 struct Problem {
     std::string target;
@@ -76,6 +80,7 @@ struct Problem {
     int Nk[3] = {1, 1, 1};
     double ksfactor[3] = {1.0, 1.0, 1.0};
     double bzaxes[9] = {0}, bzorigin[3] = {0};
+    double bz_model[9] = {0};  // the material's own axes, before ksfactor and calc.BZaxes
     int precision = 0;        // 0 = FP64 (plain), 1 = mixed FP32/FP64 (extension)
     int model = MODEL_HALDANE;
     int nband = 2, nval = 1;
@@ -105,6 +110,17 @@ struct Problem {
 // reference's own diagnostic for the condition (where it has one).
 // `unsupported` is set instead of throwing when the input is valid for the
 // reference but names something this library does not build.
+// libconfig-typed lookups (no auto-conversion) and the material tables
+bool get_double(const CfgValue *g, const char *key, double &v);
+bool get_int(const CfgValue *g, const char *key, int &v);
+bool get_bool(const CfgValue *g, const char *key, bool &v);
+bool get_string(const CfgValue *g, const char *key, std::string &v);
+// Fills nband, nval, the tables and the Brillouin zone for an analytic
+// material of the reference; false if `target` is not one of them.
+bool build_material(const std::string &target, const CfgValue *mat, Problem &p);
+extern const double PI;           // constant.h:19
+extern const double AU_ANGSTROM;  // constant.h:32
+
 Problem problem_from_cfg(const CfgValue &root, std::string *unsupported);
 
 // Stage-time tables for the kernels.

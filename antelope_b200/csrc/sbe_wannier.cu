@@ -859,6 +859,269 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
     }
 }
 
+// ============================================================= velocity gauge
+// N-band velocity gauge (SBEs.h:284-373, 787-805, 862-871): rho in the band
+// basis of H(k), H = diag(eps) + sum_a A_a P_a with P_a = U^dag J_a U fixed
+// per k, dephasing Gamma o (rho - rho0) element-wise.  Set-up: H(k) and J_a(k)
+// from the tables, Jacobi from the identity, eigenpairs sorted ascending (the
+// band order the written occupations and coherence follow, as zheevr's).
+template <class RF>
+__global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
+{
+    using T = double2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const WanSmem L = wan_smem(P.N, P.nR, sizeof(RF));
+    RF *Rc = reinterpret_cast<RF *>(smem_raw + L.Rc);
+    BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    load_lattice<RF>(P, Rc);
+    fill_tables(bh, P.N);
+    __syncthreads();
+    const int k = blockIdx.x * WAN_WARPS + wi;
+    if (k >= P.nk) return;
+    const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, P.N, P.nR);
+    const int N = P.N, NN = N * N;
+    double kv[3], wt;
+    kpoint(P, k, kv, wt);
+    if (lane == 0) P.weight[k] = wt;
+    kphases<RF>(P, kv, w.ph, lane);
+    for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
+    __syncwarp();
+    fourier<RF>(w, bh.ut, P, true, Rc, lane);
+    for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
+    __syncwarp();
+    jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
+    // ascending order: column n of U goes to position rank(n)
+    if (lane < N) {
+        const double ev = w.B[lane * N + lane].x;
+        int rank = 0;
+        for (int j = 0; j < N; ++j) {
+            const double ej = w.B[j * N + j].x;
+            rank += (ej < ev) || (ej == ev && j < lane);
+        }
+        for (int i = 0; i < N; ++i) w.Tm[i * N + rank] = w.U[i * N + lane];
+        w.dv[rank] = make_double2(ev, 0);
+    }
+    __syncwarp();
+    for (int e = lane; e < NN; e += 32) w.U[e] = w.Tm[e];
+    // occupations: the Nval lowest bands, or Fermi-Dirac at 300 K (SBEs.h:319-340)
+    if (lane < N) {
+        double f;
+        if (P.use_fermi) f = 1.0 / (exp((w.dv[lane].x - P.Ef) / (300. / 3.15775024804e5)) + 1.0);
+        else f = lane < P.nval ? 1.0 : 0.0;
+        w.dv[lane].y = f;
+    }
+    __syncwarp();
+    if (P.use_fermi && lane == 0) {
+        double s = 0;
+        for (int j = 0; j < N; ++j) s += w.dv[j].y;
+        for (int j = 0; j < N; ++j) w.dv[j].y /= s;
+    }
+    __syncwarp();
+    if (lane < N) {
+        P.vg_eps[(size_t)k * N + lane] = w.dv[lane].x;
+        P.vg_f[(size_t)k * N + lane] = w.dv[lane].y;
+    }
+    // P_a = U^dag J_a U (SBEs.h:366-372)
+    for (int a = 0; a < 2; ++a) {
+        T *Sa = a == 0 ? w.S0 : w.S1;
+        T *Da = a == 0 ? w.D0 : w.D1;
+        for (int e = lane; e < NN; e += 32) {
+            if (P.has_jtab) {
+                w.B[e] = Sa[e];
+                continue;
+            }
+            const int m = e / N, n = e % N;
+            T c = make_double2(0, 0);
+            for (int l = 0; l < N; ++l) {
+                cfma(c, Da[m * N + l], w.H0[l * N + n]);
+                const T t2 = cmul(w.H0[m * N + l], Da[l * N + n]);
+                c.x -= t2.x;
+                c.y -= t2.y;
+            }
+            w.B[e] = make_double2(Sa[e].y - c.y, c.x - Sa[e].x);
+        }
+        __syncwarp();
+        mat_mul(w.Tm, w.B, w.U, N, false, lane);
+        __syncwarp();
+        mat_mul(w.B, w.U, w.Tm, N, true, lane);
+        __syncwarp();
+        for (int e = lane; e < NN; e += 32) P.vg_P[((size_t)k * 2 + a) * NN + e] = w.B[e];
+        __syncwarp();
+    }
+    // rho = rho0 = diag(f) in the band basis
+    for (int e = lane; e < NN; e += 32) {
+        const int m = e / N, n = e % N;
+        P.rho[0][(size_t)k * NN + e] = make_double2(m == n ? w.dv[m].y : 0.0, 0.0);
+    }
+}
+
+template <class RF>
+__global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev *__restrict__ Pp)
+{
+    using T = double2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const WanDev &P = *Pp;
+    const WanCtl ctl = *P.ctl;
+    if (ctl.done) return;
+    const WanSmem L = wan_smem(P.N, P.nR, sizeof(RF));
+    BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
+    double(*AE)[6] = bh.AE;
+    WTab &tab = bh.tab;
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    const int N = P.N, NN = N * N, NU = N * (N + 1) / 2;
+    const double h = ctl.hs;
+    const int buf = ctl.buf;
+    const bool cur = ctl.need_current;
+    if (threadIdx.x == 0) tableau(P.rk, tab);
+    fill_tables(bh, N);
+    for (int i = threadIdx.x; i < 36; i += blockDim.x) AE[i / 6][i % 6] = P.stage_AE[i];
+    for (int q = threadIdx.x; q < WAN_WARPS * WAN_NSLOT; q += blockDim.x) bh.part[q / WAN_NSLOT][q % WAN_NSLOT] = 0.0;
+    if (threadIdx.x < WAN_WARPS) bh.errw[threadIdx.x] = 0.0;
+    __syncthreads();
+    const int S = tab.S;
+    const int k = blockIdx.x * WAN_WARPS + wi;
+    double emax = 0.0;
+    if (k < P.nk) {
+        const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, N, P.nR);
+        double kv[3], wk;
+        kpoint(P, k, kv, wk);
+        for (int e = lane; e < NN; e += 32) {
+            w.D0[e] = P.vg_P[((size_t)k * 2 + 0) * NN + e];
+            w.D1[e] = P.vg_P[((size_t)k * 2 + 1) * NN + e];
+        }
+        if (lane < N) w.dv[lane] = make_double2(P.vg_eps[(size_t)k * N + lane], P.vg_f[(size_t)k * N + lane]);
+        const double2 *rho = P.rho[buf] + (size_t)k * NN;
+        constexpr int MAXO = 2;
+        double2 r64[MAXO];
+        int om[MAXO], on[MAXO];
+        const int no = (NU + 31 - lane) / 32;
+        for (int o = 0; o < MAXO; ++o) {
+            om[o] = on[o] = 0;
+            r64[o] = make_double2(0, 0);
+            if (o < no) {
+                upper_mn(lane + 32 * o, N, om[o], on[o]);
+                r64[o] = rho[om[o] * N + on[o]];
+            }
+        }
+        __syncwarp();
+        for (int s = 0; s < S; ++s) {
+            for (int o = 0; o < no; ++o) {
+                T y = r64[o];
+                for (int j = 0; j < s; ++j) {
+                    const double a = h * tab.a[s][j];
+                    if (a != 0.0) {
+                        const T kj = w.ks[j * NU + lane + 32 * o];
+                        y.x = fma(a, kj.x, y.x);
+                        y.y = fma(a, kj.y, y.y);
+                    }
+                }
+                const int m = om[o], n = on[o];
+                if (m == n) y.y = 0;
+                w.Y[m * N + n] = y;
+                w.Y[n * N + m] = cconj(y);
+            }
+            // H = diag(eps) + A.P (SBEs.h:787-805)
+            const double Ax = AE[s][0], Ay = AE[s][1];
+            for (int e = lane; e < NN; e += 32) {
+                T v;
+                v.x = fma(Ax, w.D0[e].x, Ay * w.D1[e].x);
+                v.y = fma(Ax, w.D0[e].y, Ay * w.D1[e].y);
+                if (e / N == e % N) v.x += w.dv[e / N].x;
+                w.HT[e] = v;
+            }
+            __syncwarp();
+            if (cur && s == 0) {
+                // currents at k (SBEs.h:694-760): Re sum_ij rho_ij P_a,ji, diagonal -> intra
+                double *val = bh.part[wi];
+                for (int a = 0; a < 2; ++a) {
+                    const T *Pa = a == 0 ? w.D0 : w.D1;
+                    double tot = 0.0, intra = 0.0;
+                    for (int e = lane; e < NN; e += 32) {
+                        const int m = e / N, n = e % N;
+                        const T y = w.Y[e], p = Pa[n * N + m];
+                        const double v = y.x * p.x - y.y * p.y;
+                        tot += v;
+                        if (m == n) intra += v;
+                    }
+                    tot = warp_sum(tot);
+                    intra = warp_sum(intra);
+                    if (lane == 0) {
+                        val[a] = wk * (tot - intra);
+                        val[2 + a] = wk * intra;
+                    }
+                }
+                if (lane < N) val[4 + lane] = wk * w.Y[lane * N + lane].x;
+                const int ce = (P.nval * N + P.nval + 1) % NN;  // antelope.cpp:539-542
+                if (lane == 0) {
+                    val[4 + N] = wk * w.Y[ce].x;
+                    val[5 + N] = wk * w.Y[ce].y;
+                }
+                __syncwarp();
+            }
+            // -i((HY) - (HY)^dag) - Gamma o (Y - rho0)   (SBEs.h:808-819, 862-871)
+            const double g1 = P.g1, g2 = P.g2;
+            for (int o = 0; o < no; ++o) {
+                const int m = om[o], n = on[o];
+                T c = make_double2(0, 0), c2 = make_double2(0, 0);
+                for (int l = 0; l < N; ++l) {
+                    cfma(c, w.HT[m * N + l], w.Y[l * N + n]);
+                    cfma(c2, w.HT[n * N + l], w.Y[l * N + m]);
+                }
+                c.x -= c2.x;
+                c.y += c2.y;
+                T kv2 = make_double2(c.y, -c.x);
+                const T y = w.Y[m * N + n];
+                if (m == n) {
+                    kv2.x -= g1 * (y.x - w.dv[m].y);
+                    kv2.y -= g1 * y.y;
+                } else {
+                    kv2.x -= g2 * y.x;
+                    kv2.y -= g2 * y.y;
+                }
+                w.ks[s * NU + lane + 32 * o] = kv2;
+            }
+            __syncwarp();
+        }
+        double2 *rout = P.rho[1 - buf] + (size_t)k * NN;
+        for (int o = 0; o < no; ++o) {
+            T inc = make_double2(0, 0), er = make_double2(0, 0);
+            for (int s = 0; s < S; ++s) {
+                const T kv = w.ks[s * NU + lane + 32 * o];
+                const double b = h * tab.b[s];
+                if (b != 0.0) {
+                    inc.x = fma(b, kv.x, inc.x);
+                    inc.y = fma(b, kv.y, inc.y);
+                }
+                const double eb = h * tab.e[s];
+                if (eb != 0.0) {
+                    er.x = fma(eb, kv.x, er.x);
+                    er.y = fma(eb, kv.y, er.y);
+                }
+            }
+            double2 v = make_double2(r64[o].x + inc.x, r64[o].y + inc.y);
+            const int m = om[o], n = on[o];
+            if (m == n) v.y = 0.0;
+            rout[m * N + n] = v;
+            rout[n * N + m] = make_double2(v.x, -v.y);
+            emax = fmax(emax, sqrt(er.x * er.x + er.y * er.y));
+        }
+        emax = warp_max(emax);
+        if (lane == 0) bh.errw[wi] = emax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int i = 0; i < WAN_WARPS; ++i) m = fmax(m, bh.errw[i]);
+        P.tile_err[blockIdx.x] = m;
+    }
+    if (cur && threadIdx.x < WAN_NSLOT) {
+        double s = 0.0;
+        for (int i = 0; i < WAN_WARPS; ++i) s += bh.part[i][threadIdx.x];
+        P.cur_part[(size_t)blockIdx.x * WAN_NSLOT + threadIdx.x] = s;
+    }
+}
+
 // Fields at the stage times of the next attempt and the per-stage factors
 // e^{iA(t_s)R} (SBEs.h:764-766), shared by every block of the attempt.
 template <class RF> __device__ void prepare_stages(const WanDev &P, const WanCtl &c)
@@ -994,6 +1257,10 @@ template <class RF> static cudaError_t allow_smem()
     cudaError_t e = cudaFuncSetAttribute(wan_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(wan_attempt<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(wan_vg_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(wan_vg_attempt<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     done = e == cudaSuccess;
     return e;
 }
@@ -1009,8 +1276,13 @@ cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st)
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
     const size_t sm = wan_smem_bytes(w.N, w.nR, precision);
-    if (precision == 0) wan_init<double><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
-    else wan_init<float><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
+    if (w.vg) {
+        if (precision == 0) wan_vg_init<double><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
+        else wan_vg_init<float><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
+    } else {
+        if (precision == 0) wan_init<double><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
+        else wan_init<float><<<grid, 32 * WAN_WARPS, sm, st>>>(w);
+    }
     return cudaGetLastError();
 }
 
@@ -1027,8 +1299,15 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
     const size_t sm = wan_smem_bytes(w.N, w.nR, precision);
-    if (precision == 0) wan_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-    else wan_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    if (w.vg) {
+        // the stage arithmetic is FP64 in both methods (no per-stage Fourier
+        // sums); the instantiation must match the layout `sm` was sized for
+        if (precision == 0) wan_vg_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+        else wan_vg_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    } else {
+        if (precision == 0) wan_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+        else wan_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    }
     return cudaGetLastError();
 }
 

@@ -44,6 +44,7 @@ struct WanCtl {
 
 struct WanDev {
     int N, nval, nR, nk, Nt, ntiles, rk, inter_intra, use_fermi, has_dip, has_jtab;
+    int vg;                 // 1: velocity gauge (band basis), 0: length gauge (Wannier basis)
     double Ef, dt, atmin, tol, g1, g2;  // g1 = 1/T1, g2 = 1/T2 (0 when disabled)
     int Ngrid[3];
     double axes[9], origin[3];
@@ -60,6 +61,9 @@ struct WanDev {
     double *cur_part;       // [ntiles][WAN_NSLOT]
     double *jout;           // [Nt][WAN_NSLOT]
     WanCtl *ctl;
+    double *vg_eps;         // velocity gauge: [nk][N] band energies (ascending)
+    double *vg_f;           // velocity gauge: [nk][N] initial occupations
+    double2 *vg_P;          // velocity gauge: [nk][2][N*N] P_a = U^dag J_a U
     double *stage_AE;       // [6][6] A and E at the stage times of the next attempt
     void *stage_cA;         // [6][nR] e^{i A(t_s) R} of the next attempt (Fourier precision)
 };

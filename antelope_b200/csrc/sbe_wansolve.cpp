@@ -19,9 +19,9 @@ template <class T> void dalloc(T **p, size_t bytes, cudaStream_t st, const char 
 WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStream_t st)
     : prob_(p), precision_(precision), device_(device), stream_(st)
 {
-    if (p.model != MODEL_SYNTHETIC_WANNIER) throw CfgError("not a Wannier problem");
-    if (p.gauge != GAUGE_LENGTH_WANNIER)
-        throw CfgError("Wannier models run in the length gauge (LengthWannier) on this path");
+    if (p.model != MODEL_SYNTHETIC_WANNIER && p.model != MODEL_TB) throw CfgError("not a tight-binding problem");
+    if (p.gauge != GAUGE_LENGTH_WANNIER && p.gauge != GAUGE_VELOCITY)
+        throw CfgError("tight-binding models run in the LengthWannier or Velocity gauge");
     if (p.w_nR > WAN_MAXR) throw CfgError("tight-binding model: at most 64 hopping vectors");
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
     const int N = p.nband, NN = N * N;
@@ -37,6 +37,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     w_.use_fermi = p.use_fermi ? 1 : 0;
     w_.has_dip = p.w_d.empty() ? 0 : 1;
     w_.has_jtab = p.w_j.empty() ? 0 : 1;
+    w_.vg = p.gauge == GAUGE_VELOCITY ? 1 : 0;
     w_.Ef = p.Ef;
     w_.dt = p.dt;
     w_.atmin = p.laser.atmin;
@@ -71,6 +72,11 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
         dalloc(&w_.U[b], sizeof(double2) * nk * NN, st, "alloc U");
     }
     dalloc(&w_.weight, sizeof(double) * nk, st, "alloc weights");
+    if (w_.vg) {
+        dalloc(&w_.vg_eps, sizeof(double) * nk * N, st, "alloc band energies");
+        dalloc(&w_.vg_f, sizeof(double) * nk * N, st, "alloc occupations");
+        dalloc(&w_.vg_P, sizeof(double2) * nk * 2 * NN, st, "alloc momentum matrices");
+    }
     dalloc(&w_.tile_err, sizeof(double) * w_.ntiles, st, "alloc tile errors");
     dalloc(&w_.cur_part, sizeof(double) * w_.ntiles * WAN_NSLOT, st, "alloc current partials");
     dalloc(&w_.jout, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st, "alloc outputs");
@@ -129,6 +135,9 @@ WannierSolve::~WannierSolve()
         cudaFreeAsync(w_.U[b], stream_);
     }
     cudaFreeAsync(w_.weight, stream_);
+    if (w_.vg_eps) cudaFreeAsync(w_.vg_eps, stream_);
+    if (w_.vg_f) cudaFreeAsync(w_.vg_f, stream_);
+    if (w_.vg_P) cudaFreeAsync(w_.vg_P, stream_);
     cudaFreeAsync(w_.tile_err, stream_);
     cudaFreeAsync(w_.cur_part, stream_);
     cudaFreeAsync(w_.jout, stream_);
@@ -179,6 +188,8 @@ SolveOutputs WannierSolve::outputs()
     o.coh.assign((size_t)Nt * 2, 0.0);
     o.laser.assign((size_t)Nt * 7, 0.0);
     const double dV = p.dV, Ntot = (double)p.ntotal();
+    // velocity gauge: intra_a += Nval A_a(t) per k (SBEs.h:750-757), i.e. Nval A_a sum_k w_k
+    const double nvw = w_.vg ? p.nval * p.total_weight : 0.0;
     const int e = p.nval * N + p.nval + 1, roff = e / NN;
     for (int n = 0; n < Nt; ++n) {
         const double *r = &j[(size_t)n * WAN_NSLOT];
@@ -188,12 +199,13 @@ SolveOutputs WannierSolve::outputs()
         double *L = &o.laser[(size_t)n * 7];
         L[0] = t;
         for (int d = 0; d < 3; ++d) { L[1 + d] = E[d]; L[4 + d] = A[d]; }
-        for (int a = 0; a < 2; ++a) {
+        for (int a = 0; a < 3; ++a) {  // in-plane models: no z current besides Nval A_z
+            const double ie = a < 2 ? r[a] : 0.0, ia = (a < 2 ? r[2 + a] : 0.0) + nvw * A[a];
             if (p.inter_intra) {
-                o.inter[(size_t)n * 3 + a] = r[a] * dV;
-                o.intra[(size_t)n * 3 + a] = r[2 + a] * dV;
-            } else {
-                o.inter[(size_t)n * 3 + a] = (r[a] + r[2 + a]) * dV;
+                o.inter[(size_t)n * 3 + a] = ie * dV;
+                o.intra[(size_t)n * 3 + a] = ia * dV;
+            } else {  // GenCurrent: the total current goes to the inter column (antelope.cpp:316-324)
+                o.inter[(size_t)n * 3 + a] = (ie + ia) * dV;
             }
         }
         double tot = 0.0;

@@ -96,6 +96,22 @@ sbe_status sbe_problem_dims(const sbe_problem *p, sbe_dims *out);
 /* Host-only: the columns of outlaserdata.dat (t, E[3], A[3]) into laser[Nt*7]
  * (antelope.cpp:208-235; laser.h:278-322).  Needs no GPU. */
 sbe_status sbe_problem_laser(const sbe_problem *p, double *laser);
+
+/* The tight-binding tables a table model runs on: the SyntheticWannier cfg
+ * group, or an analytic material of the reference (KaneMele, Haldane2L,
+ * WilsonMass, XYHlattice) restated as H(k) = sum_v h_v e^{ik.v} and its
+ * GenJMatrix as J_a(k) = sum_v j_{a,v} e^{ik.v}.  Call once with the array
+ * pointers NULL to read the sizes, then with caller-owned arrays:
+ *   vec[nvec*2] Cartesian vectors (bohr), h[nvec*N*N*2], d and j
+ *   [nvec*2*N*N*2] (complex interleaved; d / j only when the flags say so),
+ *   bz[9] Brillouin-zone axes before ksfactor / BZaxes overrides.
+ * The Haldane model has closed-form kernels and no tables:
+ * SBE_INVALID_ARGUMENT. */
+typedef struct sbe_model {
+    int nband, nval, nvec, has_dipoles, has_current_tables;
+    double *vec, *h, *d, *j, *bz;
+} sbe_model;
+sbe_status sbe_problem_model(const sbe_problem *p, sbe_model *m);
 void sbe_problem_destroy(sbe_problem *p);
 
 /* One solve (replaces SBEs + the driver loop of antelope.cpp:297-548). */

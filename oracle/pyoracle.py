@@ -50,6 +50,7 @@ class OrcProblem(C.Structure):
         ("w_nband", C.c_int), ("w_nval", C.c_int), ("w_nR", C.c_int),
         ("w_R", C.POINTER(C.c_int)), ("w_lat", C.c_double * 4),
         ("w_h", C.POINTER(C.c_double)), ("w_d", C.POINTER(C.c_double)),
+        ("w_vec", C.POINTER(C.c_double)), ("w_j", C.POINTER(C.c_double)), ("w_bz", C.c_double * 9),
         ("nthreads", C.c_int),
     ]
 
@@ -80,6 +81,9 @@ def lib():
 
 def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
+
+
+MATERIAL_TABLES = ("KaneMele", "Haldane2L", "WilsonMass", "XYHlattice")
 
 
 def to_problem(case: dict, nthreads: int = 1):
@@ -149,6 +153,26 @@ def to_problem(case: dict, nthreads: int = 1):
             p.w_d = d.ctypes.data_as(C.POINTER(C.c_double))
         for i, v in enumerate(mat["lattice"]):
             p.w_lat[i] = float(v)
+    elif target in MATERIAL_TABLES:
+        # an analytic material (Materials/*.h): its H and GenJMatrix as Fourier
+        # tables, read from the product's cfg front end (sbe_problem_model).
+        # The tables are checked end to end against the reference's own runs
+        # of the same cfgs (tests/golden), so the oracle's engine and the
+        # restated material are pinned together.
+        from antelope_b200 import Problem
+        t = Problem.from_dict(case).model_tables()
+        N, nR = t["nband"], len(t["vec"])
+        vec = np.ascontiguousarray(t["vec"])
+        h = np.ascontiguousarray(t["h"])
+        j = np.ascontiguousarray(t["j"])
+        keep += [vec, h, j]
+        p.model = 1
+        p.w_nband, p.w_nval, p.w_nR = N, t["nval"], nR
+        p.w_vec = vec.ctypes.data_as(C.POINTER(C.c_double))
+        p.w_h = h.ctypes.data_as(C.POINTER(C.c_double))
+        p.w_j = j.ctypes.data_as(C.POINTER(C.c_double))
+        for i in range(9):
+            p.w_bz[i] = t["bz"][i]
     else:
         raise ValueError(f"oracle has no model '{target}'")
     p.nthreads = nthreads

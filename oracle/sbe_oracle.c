@@ -178,7 +178,7 @@ typedef struct {
     /* Wannier */
     int nR;
     double (*Rc)[2];        /* Cartesian R vectors */
-    const double *h, *d;
+    const double *h, *d, *j; /* j: explicit current-operator tables or NULL */
     double bzaxes[9], bzorigin[3];
 } model_t;
 
@@ -203,10 +203,16 @@ static int model_build(model_t *m, const orc_problem *p)
         return 0;
     }
     if (p->model == ORC_MODEL_WANNIER) {
-        if (p->w_nband < 1 || p->w_nband > ORC_MAX_BANDS || p->w_nR < 1 || !p->w_R || !p->w_h) return -1;
+        if (p->w_nband < 1 || p->w_nband > ORC_MAX_BANDS || p->w_nR < 1 || (!p->w_R && !p->w_vec) || !p->w_h)
+            return -1;
         m->N = p->w_nband; m->nval = p->w_nval; m->dipole = p->w_d != NULL;
-        m->nR = p->w_nR; m->h = p->w_h; m->d = p->w_d;
+        m->nR = p->w_nR; m->h = p->w_h; m->d = p->w_d; m->j = p->w_j;
         m->Rc = malloc(sizeof(double[2]) * (size_t)m->nR);
+        if (p->w_vec) {
+            for (int r = 0; r < m->nR; ++r) { m->Rc[r][0] = p->w_vec[2 * r]; m->Rc[r][1] = p->w_vec[2 * r + 1]; }
+            for (int i = 0; i < 9; ++i) m->bzaxes[i] = p->w_bz[i];
+            return 0;
+        }
         for (int r = 0; r < m->nR; ++r) {
             m->Rc[r][0] = p->w_R[2 * r] * p->w_lat[0] + p->w_R[2 * r + 1] * p->w_lat[2];
             m->Rc[r][1] = p->w_R[2 * r] * p->w_lat[1] + p->w_R[2 * r + 1] * p->w_lat[3];
@@ -262,7 +268,8 @@ static void haldane_J(const model_t *m, const double *k, cplx *J /* [3][4] */)
 
 /* Wannier model form (Materials/Wannier90.h:297-387, exact Fourier sums):
  * H = sum_R h_R e^{ikR}; D_a = sum_R d_aR e^{ikR};
- * J_a = -dH/dk_a + i[D_a, H] (BaseMaterial.h:62-68). */
+ * J_a = -dH/dk_a + i[D_a, H] (BaseMaterial.h:62-68), or, for a material's
+ * tables, J_a = sum_v j_{a,v} e^{ikv} (its GenJMatrix). */
 static void wannier_HDJ(const model_t *m, const double *k, cplx *H, cplx *D, cplx *J)
 {
     int N = m->N, NN = N * N;
@@ -289,7 +296,17 @@ static void wannier_HDJ(const model_t *m, const double *k, cplx *H, cplx *D, cpl
                     D[a * NN + i] += (dr[2 * (a * NN + i)] + I * dr[2 * (a * NN + i) + 1]) * e;
         }
     }
-    if (J) {
+    if (J && m->j) {
+        for (int i = 0; i < 3 * NN; ++i) J[i] = 0;
+        for (int r = 0; r < m->nR; ++r) {
+            double ph = k[0] * m->Rc[r][0] + k[1] * m->Rc[r][1];
+            cplx e = cos(ph) + I * sin(ph);
+            const double *jr = m->j + (size_t)r * 2 * NN * 2;
+            for (int a = 0; a < 2; ++a)
+                for (int i = 0; i < NN; ++i)
+                    J[a * NN + i] += (jr[2 * (a * NN + i)] + I * jr[2 * (a * NN + i) + 1]) * e;
+        }
+    } else if (J) {
         for (int a = 0; a < 2; ++a)
             for (int i = 0; i < N; ++i)
                 for (int j = 0; j < N; ++j) {

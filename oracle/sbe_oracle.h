@@ -63,6 +63,13 @@ typedef struct {
     double w_lat[4];     /* a1 = (w_lat[0], w_lat[1]), a2 = (w_lat[2], w_lat[3]) in bohr */
     const double *w_h;   /* [nR][N][N] complex, interleaved re/im */
     const double *w_d;   /* [nR][2][N][N] complex, interleaved re/im, or NULL for no dipoles */
+    /* Table models of analytic materials: Cartesian vectors instead of
+     * R = n1 a1 + n2 a2, the material's own current operator
+     * J_a(k) = sum_v j_{a,v} e^{ik.v} (its GenJMatrix) instead of
+     * -dH/dk + i[D, H], and the material's Brillouin-zone axes. */
+    const double *w_vec; /* [nR][2] Cartesian vectors (bohr), or NULL */
+    const double *w_j;   /* [nR][2][N][N] complex, interleaved re/im, or NULL */
+    double w_bz[9];      /* used when w_vec != NULL */
     int nthreads;        /* k-range split as ParaRange (utility.h:104-115); 1 = sequential */
 } orc_problem;
 

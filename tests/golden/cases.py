@@ -67,5 +67,40 @@ GOLDEN_CASES = {
                                       if k != "gauge"},
 }
 
+# The reference's other analytic materials (Materials/*.h), run on the GPU as
+# Fourier tables of H(k) and of their GenJMatrix (antelope_b200/csrc/
+# sbe_materials.cpp); each in both gauges on a small grid.
+MATERIALS = {
+    "WilsonMass": {"t": 0.02, "delta": 0.015, "mu": -0.03, "a0": 5.0, "a1": 6.0},
+    "KaneMele": {"t1": 0.075, "t2": 0.025, "tR": 0.01, "Mt2": 1.5, "phi0": 1.16, "a0": 1.44},
+    "Haldane2L": {"t1": 0.075, "t2": 0.025, "phi0": 1.16, "a0": 1.44, "t11": 0.01, "polytype": "AB",
+                  "Mt2": 2.0, "t2_bottom": 0.02, "Mt2_bottom": 1.0},
+    "XYHlattice": {"tl": 0.05, "tr": 0.03, "lambda": 0.01, "a0": 2.5},
+}
+
+
+def material(name, gauge, **kw):
+    c = variant(top__gauge=gauge, calc__Npoints=[6, 5], **kw)
+    del c["Haldane"]
+    c["target"] = name
+    c[name] = dict(MATERIALS[name])
+    return c
+
+
+MATERIAL_CASES = {f"{m.lower()}_{g[0].lower()}": material(m, g) for m in MATERIALS for g in ("Velocity", "Wannier")}
+# reference specifics exercised on purpose: WilsonMass without a1 (a1 = a0);
+# Haldane2L stackings with a flipped B2 sign and t1_bottom read first (the
+# OR short-circuit leaves t2_bottom unread); Kane-Mele with T1 and no Rashba
+_h2l = material("Haldane2L", "Wannier", calc__T1=300.0)
+_h2l["Haldane2L"].update(polytype="AA'", t1_bottom=0.07, t2_bottom=0.03)
+_wm = material("WilsonMass", "Velocity", pulse__ellip=0.4)
+del _wm["WilsonMass"]["a1"]
+_km = material("KaneMele", "Velocity", calc__T1=150.0)
+_km["KaneMele"]["tR"] = 0.0
+_h2lv = material("Haldane2L", "Velocity")
+_h2lv["Haldane2L"].update(polytype="A'B", M0=0.01)
+MATERIAL_CASES.update({"haldane2l_w_2h_t1bottom": _h2l, "wilsonmass_v_default_a1": _wm,
+                       "kanemele_v_t1_no_rashba": _km, "haldane2l_v_apb_m0": _h2lv})
+
 # A one-cycle case whose output files are kept verbatim (byte format pin).
 TEXT_CASE = variant(pulse__ncycles=1.0, pulse__w0=0.114, calc__Npoints=[5, 6])

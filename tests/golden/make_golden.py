@@ -2,9 +2,10 @@
 
 Runs the unmodified reference (oracle/_ref/exec_hhg_ref, built by
 ``make -C oracle ref`` from the reference sources with the stand-in headers of
-oracle/refshim) on every case of cases.GOLDEN_CASES and stores its output files
-as arrays in golden_<name>.npz; TEXT_CASE's files are also kept verbatim in
-text_case/.  Usage:  python tests/golden/make_golden.py
+oracle/refshim) on every case of cases.GOLDEN_CASES and cases.MATERIAL_CASES
+and stores its output files as arrays in golden_<name>.npz; TEXT_CASE's files
+are also kept verbatim in text_case/.
+Usage:  python tests/golden/make_golden.py [case names]   (default: all)
 """
 import os
 import shutil
@@ -18,7 +19,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from cases import GOLDEN_CASES, TEXT_CASE  # noqa: E402
+from cases import GOLDEN_CASES, MATERIAL_CASES, TEXT_CASE  # noqa: E402
 from oracle import pyoracle  # noqa: E402
 from antelope_b200 import cfgtext  # noqa: E402
 
@@ -26,12 +27,15 @@ FILES = ["interband_dipole_full_evol.dat", "intraband_current_full_evol.dat",
          "occupation__full__evol.dat", "coherence__full__evol.dat", "outlaserdata.dat"]
 
 
-def main():
-    for name, case in GOLDEN_CASES.items():
+def main(names):
+    cases = {**GOLDEN_CASES, **MATERIAL_CASES}
+    for name in names or cases:
         with tempfile.TemporaryDirectory() as d:
-            out = pyoracle.run_reference(case, d)
+            out = pyoracle.run_reference(cases[name], d)
         np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **out)
         print(name, out["inter"].shape)
+    if names:
+        return
     tdir = os.path.join(HERE, "text_case")
     os.makedirs(tdir, exist_ok=True)
     with tempfile.TemporaryDirectory() as d:
@@ -43,4 +47,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

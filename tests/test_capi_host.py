@@ -12,7 +12,7 @@ import pytest
 from antelope_b200 import Problem, SbeError, capi
 from antelope_b200.api import Outputs, write_outputs
 from antelope_b200 import cfgtext
-from cases import BASE, GOLDEN_CASES, TEXT_CASE, variant
+from cases import BASE, GOLDEN_CASES, MATERIAL_CASES, TEXT_CASE, variant
 from oracle import pyoracle
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -80,7 +80,12 @@ def _err(case_or_text):
     (lambda c: c["Haldane"].pop("t1"), "SBE_BAD_CONFIG", "Some Haldane paramters are missing"),
     (lambda c: c["Haldane"].pop("Mt2"), "SBE_BAD_CONFIG", "M0 param missing"),
     (lambda c: c.__setitem__("target", "Graphene"), "SBE_BAD_CONFIG", "Undefined Material"),
-    (lambda c: c.__setitem__("target", "KaneMele"), "SBE_UNSUPPORTED", "not built"),
+    (lambda c: c.__setitem__("target", "TMDCs"), "SBE_UNSUPPORTED", "not built"),
+    (lambda c: c.__setitem__("target", "KaneMele"), "SBE_BAD_CONFIG", "Some KaneMele paramters are missing"),
+    (lambda c: c.__setitem__("target", "WilsonMass"), "SBE_BAD_CONFIG", "Some Haldane paramters are missing"),
+    (lambda c: (c.__setitem__("target", "Haldane2L"),
+                c.__setitem__("Haldane2L", dict(c["Haldane"], t11=0.01, polytype="ABC"))),
+     "SBE_BAD_CONFIG", "Undefined polytype"),
     (lambda c: c["calc"].__setitem__("shotNumber", 4), "SBE_UNSUPPORTED", "snapshots"),
     (lambda c: c.__setitem__("gauge", "Hamiltonian"), "SBE_UNSUPPORTED", "LengthHamiltonian"),
 ])
@@ -148,3 +153,27 @@ def test_writers_reproduce_reference_bytes(tmp_path):
         with open(os.path.join(tdir, f), "rb") as a, open(os.path.join(tmp_path, f), "rb") as b:
             assert a.read() == b.read(), f
     assert os.path.getsize(os.path.join(tmp_path, "laserParameters.dat")) == 0
+
+
+@pytest.mark.parametrize("name", sorted(MATERIAL_CASES))
+def test_material_tables_are_hermitian_and_sized(name):
+    """sbe_problem_model exports the tables the N-band kernels run on; H(k)
+    built from them is Hermitian at any k (the reference's GenJMatrix need not
+    be -dH/dk, so J is only checked for size)."""
+    case = MATERIAL_CASES[name]
+    p = Problem.from_dict(case)
+    t = p.model_tables()
+    N = t["nband"]
+    assert t["h"].shape == (len(t["vec"]), N, N) and t["j"].shape == (len(t["vec"]), 2, N, N)
+    assert t["d"] is None and p.dims.nband == N
+    rng = np.random.default_rng(3)
+    for k in rng.normal(size=(5, 2)):
+        ph = np.exp(1j * t["vec"] @ k)
+        H = np.einsum("r,rij->ij", ph, t["h"])
+        assert np.abs(H - H.conj().T).max() < 1e-14 * max(1.0, np.abs(H).max())
+
+
+def test_haldane_has_no_tables():
+    with pytest.raises(SbeError) as e:
+        Problem.from_dict(BASE).model_tables()
+    assert e.value.name == "SBE_INVALID_ARGUMENT"

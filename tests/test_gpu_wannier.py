@@ -49,6 +49,18 @@ def test_fixed_step_fp64_matches_oracle(rk):
     check(out, ref, FP64_TOL)
 
 
+@pytest.mark.parametrize("rk", [None, "cashkarp45"])
+def test_velocity_gauge_fp64_matches_oracle(rk):
+    c = small_case(rk, T1=400.0)
+    c["gauge"] = "Velocity"
+    if rk is None:
+        c["calc"].pop("rk", None)
+        c["calc"]["RKorder"] = 4
+    out = ab.solve(c, precision="fp64")
+    ref = pyoracle.run(c)
+    check(out, ref, FP64_TOL)
+
+
 def test_cash_karp_fp64_matches_oracle():
     c = small_case("cashkarp45", tol=1e-8, T1=500.0)
     out = ab.solve(c, precision="fp64")

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from cases import GOLDEN_CASES
+from cases import GOLDEN_CASES, MATERIAL_CASES
 from oracle import pyoracle
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -34,6 +34,21 @@ def test_oracle_matches_reference_outputs(name):
     # laser file: time axis and the A/E columns
     t = out["dims"]["atmin"] + case["calc"].get("dt", 0.1) * np.arange(out["dims"]["Nt"])
     assert np.allclose(ref["laser"][:, 0], t, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("name", sorted(MATERIAL_CASES))
+def test_material_tables_reproduce_reference_outputs(name):
+    """The analytic materials as Fourier tables (read from the product's cfg
+    front end) run through the oracle's engine against the reference's own
+    run of the same cfg: the tables reproduce each material's H and GenJMatrix
+    and the engine its propagation, to summation-order rounding."""
+    case = MATERIAL_CASES[name]
+    ref = np.load(os.path.join(GOLDEN, f"golden_{name}.npz"))
+    out = pyoracle.run(case)
+    N = out["dims"]["nband"]
+    assert _rel(out["inter"], ref["inter"]) < 1e-12
+    assert _rel(out["intra"], ref["intra"]) < 1e-12
+    assert np.abs(out["occ"] - ref["occ_file"][:, :N]).max() < 1e-13
 
 
 def test_oracle_threads_match_sequential():

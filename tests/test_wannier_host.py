@@ -39,10 +39,11 @@ def test_rejects_non_hermitian_model():
     assert e.value.name == "SBE_BAD_CONFIG" and "dagger" in str(e.value)
 
 
-def test_velocity_gauge_wannier_is_unsupported():
+def test_velocity_gauge_wannier_parses():
+    """Wannier models also run in the velocity gauge (band basis of H(k),
+    P = U^dag J U with J = -dH/dk + i[D, H]); the dims follow the tables."""
     c = wannier.wannier_case(seed=2, n=9, ncycles=1.0, gauge="Velocity")
     p = ab.Problem.from_dict(c)
-    from antelope_b200.api import Solver
-    with pytest.raises(SbeError) as e:
-        Solver(p)
-    assert e.value.name == "SBE_UNSUPPORTED"
+    assert p.dims.nband == 6 and p.dims.gauge == 2
+    t = p.model_tables()
+    assert t["d"] is not None and t["j"] is None
