@@ -352,6 +352,212 @@ void xyh_lattice(const CfgValue *mat, Problem &p)
     set_bz(p, PI / a0, 2. * PI / r3 / a0);
 }
 
+// ------------------------------------------------------------ TMDCs
+// TMDCs.h: the three-band (d_z2, d_xy, d_x2-y2) tight-binding model of
+// monolayer MX2 with up to third-neighbour hoppings (G.-B. Liu et al.,
+// Phys. Rev. B 88, 085433 (2013), GGA parameters), optionally doubled with
+// on-site spin-orbit coupling (6 bands).  H is a trigonometric polynomial in
+// alpha = kx a/2 and beta = ky a sqrt(3)/2; its entries are expanded here on
+// the vectors (p a/2, q a sqrt(3)/2).  Reference specific kept: its J is the
+// written derivative +dH/dk of each entry (GenJMatrix), transcribed term by
+// term.
+struct FPoly {  // sum over (p, q) of c e^{i (p alpha + q beta)}
+    std::vector<std::array<int, 2>> pq;
+    std::vector<cplx> c;
+    void add(int p, int q, cplx v)
+    {
+        for (size_t i = 0; i < pq.size(); ++i)
+            if (pq[i][0] == p && pq[i][1] == q) {
+                c[i] += v;
+                return;
+            }
+        pq.push_back({p, q});
+        c.push_back(v);
+    }
+};
+FPoly operator+(FPoly a, const FPoly &b)
+{
+    for (size_t i = 0; i < b.pq.size(); ++i) a.add(b.pq[i][0], b.pq[i][1], b.c[i]);
+    return a;
+}
+FPoly operator*(cplx s, FPoly a)
+{
+    for (auto &v : a.c) v *= s;
+    return a;
+}
+FPoly operator-(const FPoly &a, const FPoly &b) { return a + cplx(-1.0) * b; }
+FPoly operator*(const FPoly &a, const FPoly &b)
+{
+    FPoly r;
+    for (size_t i = 0; i < a.pq.size(); ++i)
+        for (size_t j = 0; j < b.pq.size(); ++j)
+            r.add(a.pq[i][0] + b.pq[j][0], a.pq[i][1] + b.pq[j][1], a.c[i] * b.c[j]);
+    return r;
+}
+FPoly fconst(cplx v)
+{
+    FPoly r;
+    r.add(0, 0, v);
+    return r;
+}
+// cos(n x), sin(n x) of x = alpha (axis 0) or beta (axis 1)
+FPoly fcos(int axis, int n)
+{
+    FPoly r;
+    r.add(axis == 0 ? n : 0, axis == 1 ? n : 0, 0.5);
+    r.add(axis == 0 ? -n : 0, axis == 1 ? -n : 0, 0.5);
+    return r;
+}
+FPoly fsin(int axis, int n)
+{
+    FPoly r;
+    r.add(axis == 0 ? n : 0, axis == 1 ? n : 0, -0.5 * I1);
+    r.add(axis == 0 ? -n : 0, axis == 1 ? -n : 0, 0.5 * I1);
+    return r;
+}
+
+void tmdcs(const CfgValue *mat, Problem &p)
+{
+    bool soc = false;
+    std::string name;
+    if (mat) {
+        get_bool(mat, "isSOCEnabled", soc);
+        get_string(mat, "Material", name);
+    }
+    // GGA parameters (eV) e1 e2 t0 t1 t2 t11 t12 t22 r0 r1 r2 r11 r12 u0 u1 u2 u11 u12 u22
+    // of MoS2, WS2, MoSe2, WSe2, MoTe2, WTe2 (Liu et al. 2013, Table III; TMDCs.h)
+    static const double gga[6][19] = {
+        {0.683, 1.707, -0.146, -0.114, 0.506, 0.085, 0.162, 0.073, 0.060, -0.236, 0.067, 0.016, 0.087, -0.038,
+         0.046, 0.001, 0.266, -0.176, -0.150},
+        {0.717, 1.916, -0.152, -0.097, 0.590, 0.047, 0.178, 0.016, 0.069, -0.261, 0.107, -0.003, 0.109, -0.054,
+         0.045, 0.002, 0.325, -0.206, -0.163},
+        {0.684, 1.546, -0.146, -0.130, 0.432, 0.144, 0.117, 0.075, 0.039, -0.209, 0.069, 0.052, 0.060, -0.042,
+         0.036, 0.008, 0.272, -0.172, -0.150},
+        {0.728, 1.655, -0.146, -0.124, 0.507, 0.117, 0.127, 0.015, 0.036, -0.234, 0.107, 0.044, 0.075, -0.061,
+         0.032, 0.007, 0.329, -0.202, -0.164},
+        {0.588, 1.303, -0.226, -0.234, 0.036, 0.400, 0.098, 0.017, 0.003, -0.025, -0.169, 0.082, 0.051, 0.057,
+         0.103, 0.187, -0.045, -0.141, 0.087},
+        {0.697, 1.380, -0.109, -0.164, 0.368, 0.204, 0.093, 0.038, -0.015, -0.209, 0.107, 0.115, 0.009, -0.066,
+         0.011, -0.013, 0.312, -0.177, -0.132}};
+    static const char *names[6] = {"MoS2", "WS2", "MoSe2", "WSe2", "MoTe2", "WTe2"};
+    static const double lat[6] = {3.190, 3.191, 3.326, 3.325, 3.557, 3.560};   // Angstrom
+    static const double socp[6] = {0.073, 0.211, 0.091, 0.228, 0.107, 0.237};  // eV
+    int mi = -1;
+    for (int i = 0; i < 6; ++i)
+        if (name == names[i]) mi = i;
+    if (mi < 0) throw CfgError("Unknowm material: " + name);
+    const double AU_EV = 27.211386245988;  // constant.h:35
+    double P[19];
+    for (int i = 0; i < 19; ++i) P[i] = gga[mi][i] / AU_EV;
+    const double a0 = lat[mi] / AU_ANGSTROM, sp = socp[mi] / AU_EV;
+    const double e1 = P[0], e2 = P[1], t0 = P[2], t1 = P[3], t2 = P[4], t11 = P[5], t12 = P[6], t22 = P[7];
+    const double r0 = P[8], r1 = P[9], r2 = P[10], r11 = P[11], r12 = P[12];
+    const double u0 = P[13], u1 = P[14], u2 = P[15], u11 = P[16], u12 = P[17], u22 = P[18];
+    const double r3 = std::sqrt(3.);
+    auto ca = [](int i) { return fcos(0, i + 1); };
+    auto sa = [](int i) { return fsin(0, i + 1); };
+    auto cb = [](int i) { return fcos(1, i + 1); };
+    auto sb = [](int i) { return fsin(1, i + 1); };
+    auto C = [](double v) { return fconst(v); };
+    const cplx i1 = I1;
+    // GenHamiltonian
+    const FPoly V0 = C(e1) + C(2 * t0) * (C(2) * ca(0) * cb(0) + ca(1)) + C(2 * r0) * (C(2) * ca(2) * cb(0) + cb(1)) +
+                     C(2 * u0) * (C(2) * ca(1) * cb(1) + ca(3));
+    const FPoly V1 = (C(-2 * r3 * t2) * sa(0) * sb(0) + C(2 * (r1 + r2)) * sa(2) * sb(0) - C(2 * r3 * u2) * sa(1) * sb(1)) +
+                     i1 * (C(2 * t1) * sa(0) * (C(2) * ca(0) + cb(0)) + C(2 * (r1 - r2)) * sa(2) * cb(0) +
+                           C(2 * u1) * sa(1) * (C(2) * ca(1) + cb(1)));
+    const FPoly V2 = (C(2 * t2) * (ca(1) - ca(0) * cb(0)) - C(2 / r3 * (r1 + r2)) * (ca(2) * cb(0) - cb(1)) +
+                      C(2 * u2) * (ca(3) - ca(1) * cb(1))) +
+                     i1 * (C(2 * r3 * t1) * ca(0) * sb(0) + C(2 / r3) * sb(0) * C(r1 - r2) * (ca(2) + C(2) * cb(0)) +
+                           C(2 * r3 * u1) * ca(1) * sb(1));
+    const FPoly V11 = C(e2) + C(t11 + 3 * t22) * ca(0) * cb(0) + C(2 * t11) * ca(1) + C(4 * r11) * ca(2) * cb(0) +
+                      C(2 * (r11 + r3 * r12)) * cb(1) + C(u11 + 3 * u22) * ca(1) * cb(1) + C(2 * u11) * ca(3);
+    const FPoly V12 = (C(r3 * (t22 - t11)) * sa(0) * sb(0) + C(4 * r12) * sa(2) * sb(0) +
+                       C(r3 * (u22 - u11)) * sa(1) * sb(1)) +
+                      i1 * (C(4 * t12) * sa(0) * (ca(0) - cb(0)) + C(4 * u12) * sa(1) * (ca(1) - cb(1)));
+    const FPoly V22 = C(e2) + C(3 * t11 + t22) * ca(0) * cb(0) + C(2 * t22) * ca(1) +
+                      C(2 * r11) * (C(2) * ca(2) * cb(0) + cb(1)) + C(2 / r3 * r12) * (C(4) * ca(2) * cb(0) - cb(1)) +
+                      C(3 * u11 + u22) * ca(1) * cb(1) + C(2 * u22) * ca(3);
+    // GenJMatrix: d/dkx of cos/sin((i+1) alpha) and d/dky of cos/sin((i+1) beta)
+    const double da = a0 / 2, db = a0 * r3 / 2;
+    auto dca = [&](int i) { return C(-(i + 1) * da) * sa(i); };
+    auto dsa = [&](int i) { return C((i + 1) * da) * ca(i); };
+    auto dcb = [&](int i) { return C(-(i + 1) * db) * sb(i); };
+    auto dsb = [&](int i) { return C((i + 1) * db) * cb(i); };
+    const FPoly dxV0 = C(2 * t0) * (C(2) * dca(0) * cb(0) + dca(1)) + C(2 * r0) * (C(2) * dca(2) * cb(0)) +
+                       C(2 * u0) * (C(2) * dca(1) * cb(1) + dca(3));
+    const FPoly dxV1 =
+        (C(-2 * r3 * t2) * dsa(0) * sb(0) + C(2 * (r1 + r2)) * dsa(2) * sb(0) - C(2 * r3 * u2) * dsa(1) * sb(1)) +
+        i1 * (C(2 * t1) * dsa(0) * (C(2) * ca(0) + cb(0)) + C(2 * t1) * sa(0) * (C(2) * dca(0)) +
+              C(2 * (r1 - r2)) * dsa(2) * cb(0) + C(2 * u1) * dsa(1) * (C(2) * ca(1) + cb(1)) +
+              C(2 * u1) * sa(1) * (C(2) * dca(1)));
+    const FPoly dxV2 = (C(2 * t2) * (dca(1) - dca(0) * cb(0)) - C(2 / r3 * (r1 + r2)) * (dca(2) * cb(0)) +
+                        C(2 * u2) * (dca(3) - dca(1) * cb(1))) +
+                       i1 * (C(2 * r3 * t1) * dca(0) * sb(0) + C(2 / r3) * sb(0) * C(r1 - r2) * dca(2) +
+                             C(2 * r3 * u1) * dca(1) * sb(1));
+    const FPoly dxV11 = C(t11 + 3 * t22) * dca(0) * cb(0) + C(2 * t11) * dca(1) + C(4 * r11) * dca(2) * cb(0) +
+                        C(u11 + 3 * u22) * dca(1) * cb(1) + C(2 * u11) * dca(3);
+    const FPoly dxV12 = (C(r3 * (t22 - t11)) * dsa(0) * sb(0) + C(4 * r12) * dsa(2) * sb(0) +
+                         C(r3 * (u22 - u11)) * dsa(1) * sb(1)) +
+                        i1 * (C(4 * t12) * dsa(0) * (ca(0) - cb(0)) + C(4 * t12) * sa(0) * dca(0) +
+                              C(4 * u12) * dsa(1) * (ca(1) - cb(1)) + C(4 * u12) * sa(1) * dca(1));
+    const FPoly dxV22 = C(3 * t11 + t22) * dca(0) * cb(0) + C(2 * t22) * dca(1) + C(2 * r11) * (C(2) * dca(2) * cb(0)) +
+                        C(2 / r3 * r12) * (C(4) * dca(2) * cb(0)) + C(3 * u11 + u22) * dca(1) * cb(1) +
+                        C(2 * u22) * dca(3);
+    const FPoly dyV0 = C(2 * t0) * (C(2) * ca(0) * dcb(0)) + C(2 * r0) * (C(2) * ca(2) * dcb(0) + dcb(1)) +
+                       C(2 * u0) * (C(2) * ca(1) * dcb(1));
+    const FPoly dyV1 =
+        (C(-2 * r3 * t2) * sa(0) * dsb(0) + C(2 * (r1 + r2)) * sa(2) * dsb(0) - C(2 * r3 * u2) * sa(1) * dsb(1)) +
+        i1 * (C(2 * t1) * sa(0) * dcb(0) + C(2 * (r1 - r2)) * sa(2) * dcb(0) + C(2 * u1) * sa(1) * dcb(1));
+    const FPoly dyV2 = (C(2 * t2) * (C(-1) * ca(0) * dcb(0)) - C(2 / r3 * (r1 + r2)) * (ca(2) * dcb(0) - dcb(1)) +
+                        C(2 * u2) * (C(-1) * ca(1) * dcb(1))) +
+                       i1 * (C(2 * r3 * t1) * ca(0) * dsb(0) + C(2 / r3) * dsb(0) * C(r1 - r2) * (ca(2) + C(2) * cb(0)) +
+                             C(2 / r3) * sb(0) * C(r1 - r2) * (C(2) * dcb(0)) + C(2 * r3 * u1) * ca(1) * dsb(1));
+    const FPoly dyV11 = C(t11 + 3 * t22) * ca(0) * dcb(0) + C(4 * r11) * ca(2) * dcb(0) +
+                        C(2 * (r11 + r3 * r12)) * dcb(1) + C(u11 + 3 * u22) * ca(1) * dcb(1);
+    const FPoly dyV12 = (C(r3 * (t22 - t11)) * sa(0) * dsb(0) + C(4 * r12) * sa(2) * dsb(0) +
+                         C(r3 * (u22 - u11)) * sa(1) * dsb(1)) +
+                        i1 * (C(4 * t12) * sa(0) * (C(-1) * dcb(0)) + C(4 * u12) * sa(1) * (C(-1) * dcb(1)));
+    const FPoly dyV22 = C(3 * t11 + t22) * ca(0) * dcb(0) + C(2 * r11) * (C(2) * ca(2) * dcb(0) + dcb(1)) +
+                        C(2 / r3 * r12) * (C(4) * ca(2) * dcb(0) - dcb(1)) + C(3 * u11 + u22) * ca(1) * dcb(1);
+    auto conjp = [](FPoly a) {  // conj(sum c e^{i(p,q)}) = sum conj(c) e^{-i(p,q)}
+        for (auto &x : a.pq) x = {-x[0], -x[1]};
+        for (auto &v : a.c) v = std::conj(v);
+        return a;
+    };
+    const int N = soc ? 6 : 3;
+    TBBuilder tb(N);
+    auto put = [&](int a, int m, int n, const FPoly &f) {
+        for (size_t i = 0; i < f.pq.size(); ++i) tb.exp_(a, m, n, f.pq[i][0] * da, f.pq[i][1] * db, f.c[i]);
+    };
+    // one 3x3 block at offset o; s = +1 / -1: sign of the soc term on (1,2) / (2,1)
+    auto block = [&](int o, double s) {
+        const FPoly *H[3][3] = {{&V0, &V1, &V2}, {nullptr, &V11, &V12}, {nullptr, nullptr, &V22}};
+        const FPoly *Jx[3][3] = {{&dxV0, &dxV1, &dxV2}, {nullptr, &dxV11, &dxV12}, {nullptr, nullptr, &dxV22}};
+        const FPoly *Jy[3][3] = {{&dyV0, &dyV1, &dyV2}, {nullptr, &dyV11, &dyV12}, {nullptr, nullptr, &dyV22}};
+        for (int m = 0; m < 3; ++m)
+            for (int n = m; n < 3; ++n) {
+                put(-1, o + m, o + n, *H[m][n]);
+                put(0, o + m, o + n, *Jx[m][n]);
+                put(1, o + m, o + n, *Jy[m][n]);
+                if (n != m) {
+                    put(-1, o + n, o + m, conjp(*H[m][n]));
+                    put(0, o + n, o + m, conjp(*Jx[m][n]));
+                    put(1, o + n, o + m, conjp(*Jy[m][n]));
+                }
+            }
+        if (soc) {
+            tb.const_(-1, o + 1, o + 2, s * sp * I1);
+            tb.const_(-1, o + 2, o + 1, -s * sp * I1);
+        }
+    };
+    block(0, 1.0);
+    if (soc) block(3, -1.0);
+    tb.to_problem(p);
+    p.nval = soc ? 2 : 1;
+    set_bz(p, PI / a0, 2. * PI / r3 / a0);
+}
+
 }  // namespace
 
 bool build_material(const std::string &target, const CfgValue *mat, Problem &p)
@@ -360,6 +566,7 @@ bool build_material(const std::string &target, const CfgValue *mat, Problem &p)
     else if (target == "KaneMele") kane_mele(mat, p);
     else if (target == "Haldane2L") haldane_2l(mat, p);
     else if (target == "XYHlattice") xyh_lattice(mat, p);
+    else if (target == "TMDCs") tmdcs(mat, p);
     else return false;
     p.model = MODEL_TB;
     return true;

@@ -76,6 +76,7 @@ MATERIALS = {
     "Haldane2L": {"t1": 0.075, "t2": 0.025, "phi0": 1.16, "a0": 1.44, "t11": 0.01, "polytype": "AB",
                   "Mt2": 2.0, "t2_bottom": 0.02, "Mt2_bottom": 1.0},
     "XYHlattice": {"tl": 0.05, "tr": 0.03, "lambda": 0.01, "a0": 2.5},
+    "TMDCs": {"Material": "MoS2"},
 }
 
 
@@ -99,8 +100,22 @@ _km = material("KaneMele", "Velocity", calc__T1=150.0)
 _km["KaneMele"]["tR"] = 0.0
 _h2lv = material("Haldane2L", "Velocity")
 _h2lv["Haldane2L"].update(polytype="A'B", M0=0.01)
+_soc = {g: material("TMDCs", g) for g in ("Velocity", "Wannier")}
+for g, c in _soc.items():
+    c["TMDCs"] = {"Material": "WSe2", "isSOCEnabled": True}
 MATERIAL_CASES.update({"haldane2l_w_2h_t1bottom": _h2l, "wilsonmass_v_default_a1": _wm,
-                       "kanemele_v_t1_no_rashba": _km, "haldane2l_v_apb_m0": _h2lv})
+                       "kanemele_v_t1_no_rashba": _km, "haldane2l_v_apb_m0": _h2lv,
+                       "tmdcs_v_wse2_soc": _soc["Velocity"], "tmdcs_w_wse2_soc": _soc["Wannier"]})
+
+# Bands degenerate at grid points: per-band values there depend on the basis
+# chosen inside the degenerate subspace (LAPACK zheevr's in the reference,
+# unpinned; a rounding-level change of H(k) changes the Jacobi solvers'
+# choice), so band-basis occupations are compared summed over each group.
+# Kane-Mele without Rashba: two uncoupled Haldane blocks (phi0, -phi0) whose
+# valence bands coincide on the ky = 0 row; WSe2 with spin-orbit coupling:
+# spin pairs meet where the splitting vanishes.
+BAND_GROUPS = {"kanemele_v_t1_no_rashba": [[0, 1], [2, 3]],
+               "tmdcs_v_wse2_soc": [[0, 1], [2, 3], [4, 5]]}
 
 # A one-cycle case whose output files are kept verbatim (byte format pin).
 TEXT_CASE = variant(pulse__ncycles=1.0, pulse__w0=0.114, calc__Npoints=[5, 6])

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import antelope_b200 as ab
-from cases import MATERIAL_CASES
+from cases import BAND_GROUPS, MATERIAL_CASES
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -21,13 +21,6 @@ def rel_series(a, b, scale):
     # differences (~1e-13 of it) are rounding of the large terms they sum
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-3 * scale)
 
-
-# Bands degenerate by symmetry at grid points: Kane-Mele without Rashba has
-# two uncoupled Haldane blocks (phi0, -phi0) whose valence bands coincide on
-# the ky = 0 row.  Per-band values there depend on the basis chosen inside the
-# degenerate pair (LAPACK zheevr's in the reference, unpinned), so the
-# occupations are compared summed over each pair.
-BAND_GROUPS = {"kanemele_v_t1_no_rashba": [[0, 1], [2, 3]]}
 
 
 @pytest.mark.parametrize("name", sorted(MATERIAL_CASES))
