@@ -352,6 +352,33 @@ void xyh_lattice(const CfgValue *mat, Problem &p)
     set_bz(p, PI / a0, 2. * PI / r3 / a0);
 }
 
+// ------------------------------------------------------------ SquareSBand
+// SquareSBand.h: H = [[M0, B1], [B1, -M0]], B1 = 2 t1 (cos(a kx) + cos(a ky)).
+// Reference specific kept: its GenJMatrix sets only the (0,1) entries,
+// J_x(0,1) = 2 t1 a sin(a kx), J_y(0,1) = 2 t1 a sin(a ky) -- a
+// non-Hermitian current operator.  The kernels use full J tables and the
+// reference's -i(HY - (HY)^dag) commutator, so the velocity-gauge
+// H = diag(eps) + A.P it implies is propagated as the reference does.
+void square_sband(const CfgValue *mat, Problem &p)
+{
+    double t1, M0, a0;
+    if (!(mat && get_double(mat, "t1", t1) && get_double(mat, "M0", M0) && get_double(mat, "a0", a0)))
+        throw CfgError("Some SquareSBand paramters are missing");
+    a0 /= AU_ANGSTROM;
+    TBBuilder tb(2);
+    tb.const_(-1, 0, 0, M0);
+    tb.const_(-1, 1, 1, -M0);
+    for (int m = 0; m < 2; ++m) {
+        tb.cos_(-1, m, 1 - m, a0, 0, 2 * t1);
+        tb.cos_(-1, m, 1 - m, 0, a0, 2 * t1);
+    }
+    tb.sin_(0, 0, 1, a0, 0, 2 * t1 * a0);
+    tb.sin_(1, 0, 1, 0, a0, 2 * t1 * a0);
+    tb.to_problem(p);
+    p.nval = 1;
+    set_bz(p, PI / a0, PI / a0);
+}
+
 // ------------------------------------------------------------ TMDCs
 // TMDCs.h: the three-band (d_z2, d_xy, d_x2-y2) tight-binding model of
 // monolayer MX2 with up to third-neighbour hoppings (G.-B. Liu et al.,
@@ -567,6 +594,7 @@ bool build_material(const std::string &target, const CfgValue *mat, Problem &p)
     else if (target == "Haldane2L") haldane_2l(mat, p);
     else if (target == "XYHlattice") xyh_lattice(mat, p);
     else if (target == "TMDCs") tmdcs(mat, p);
+    else if (target == "SquareSBand") square_sband(mat, p);
     else return false;
     p.model = MODEL_TB;
     return true;

@@ -83,7 +83,7 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-MATERIAL_TABLES = ("KaneMele", "Haldane2L", "WilsonMass", "XYHlattice", "TMDCs")
+MATERIAL_TABLES = ("KaneMele", "Haldane2L", "WilsonMass", "XYHlattice", "TMDCs", "SquareSBand")
 
 
 def to_problem(case: dict, nthreads: int = 1):

@@ -77,6 +77,7 @@ MATERIALS = {
                   "Mt2": 2.0, "t2_bottom": 0.02, "Mt2_bottom": 1.0},
     "XYHlattice": {"tl": 0.05, "tr": 0.03, "lambda": 0.01, "a0": 2.5},
     "TMDCs": {"Material": "MoS2"},
+    "SquareSBand": {"t1": 0.02, "M0": 0.03, "a0": 2.0},
 }
 
 
