@@ -403,6 +403,19 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
     float2 An[TB::NT];
 #pragma unroll
     for (int i = 0; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)s0 * TB::NT + i);
+    // The FP64 state is y64 = (rounded to FP32: yhi) and the FP32 sum `acc` of
+    // the increments since the last fold; every FOLD steps acc is added to
+    // y64 in FP64.  The stage input yhi + acc is rounded once, as float(y64)
+    // would be, and acc holds only a few increments, so the state keeps its
+    // FP64 accumulation while the f64<->f32 conversions drop FOLD-fold.
+    constexpr int FOLD = 8;
+    float2 yhi[D_N], acc[D_N];
+#pragma unroll
+    for (int q = 0; q < D_N; ++q) {
+        yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+        acc[q] = make_float2(0.f, 0.f);
+    }
+    int since = 0;
 
     for (int s = s0; s < s1; ++s) {
         float2 A[TB::NT];
@@ -414,7 +427,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
         }
         float2 y0[D_N];
 #pragma unroll
-        for (int q = 0; q < D_N; ++q) y0[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+        for (int q = 0; q < D_N; ++q) y0[q] = add2(yhi[q], acc[q]);
         // currents and occupations at t_s (antelope.cpp:309-334)
         {
             float2 t[7];
@@ -460,9 +473,16 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
             }
         }
 #pragma unroll
-        for (int q = 0; q < D_N; ++q) {
-            y64[0][q] += double(inc[q].x);
-            y64[1][q] += double(inc[q].y);
+        for (int q = 0; q < D_N; ++q) acc[q] = add2(acc[q], inc[q]);
+        if (++since == FOLD || s == s1 - 1) {
+#pragma unroll
+            for (int q = 0; q < D_N; ++q) {
+                y64[0][q] += double(acc[q].x);
+                y64[1][q] += double(acc[q].y);
+                yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+                acc[q] = make_float2(0.f, 0.f);
+            }
+            since = 0;
         }
     }
 #pragma unroll
