@@ -152,6 +152,13 @@ class Solver:
     def kernel_times(self) -> dict:
         return _kernel_times(lib.sbe_solver_kernel_times, self._h)
 
+    def harmonics(self, w0: float, hmax: int) -> np.ndarray:
+        """Band powers of harmonic orders 1..hmax, computed on the GPU
+        (``sbe_solver_harmonics``; the analysis-script convention)."""
+        out = np.zeros(hmax)
+        _check(lib.sbe_solver_harmonics(self._h, C.c_double(w0), hmax, out.ctypes.data))
+        return out
+
     def steps(self) -> dict:
         """Accepted steps, attempts and rejected attempts of the finished run."""
         v = [C.c_longlong() for _ in range(3)]
@@ -212,6 +219,12 @@ class Batch:
     def get(self, i: int) -> Outputs:
         out = Outputs.empty(self.problems[i].dims)
         _check(lib.sbe_batch_get(self._h, i, C.byref(out.c())))
+        return out
+
+    def harmonics(self, i: int, w0: float, hmax: int) -> np.ndarray:
+        """Band powers of harmonic orders 1..hmax of solve i, on the GPU."""
+        out = np.zeros(hmax)
+        _check(lib.sbe_batch_harmonics(self._h, i, C.c_double(w0), hmax, out.ctypes.data))
         return out
 
     @property

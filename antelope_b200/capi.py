@@ -66,6 +66,8 @@ def _load():
         "sbe_solver_run": (C.c_int, [P, C.c_void_p]),
         "sbe_solver_get": (C.c_int, [P, C.POINTER(COutputs)]),
         "sbe_solver_launches": (C.c_int, [P]),
+        "sbe_solver_harmonics": (C.c_int, [P, C.c_double, C.c_int, C.c_void_p]),
+        "sbe_batch_harmonics": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_void_p]),
         "sbe_solver_steps": (C.c_int, [P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                        C.POINTER(C.c_longlong)]),
         "sbe_solver_destroy": (None, [P]),

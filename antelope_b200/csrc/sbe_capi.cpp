@@ -328,6 +328,18 @@ extern "C" sbe_status sbe_solver_kernel_times(sbe_solver *s, double *pms, int *p
     });
 }
 
+extern "C" sbe_status sbe_solver_harmonics(sbe_solver *s, double w0, int hmax, double *band_power)
+{
+    if (!s || !band_power) return fail(SBE_INVALID_ARGUMENT, "null argument");
+    if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        if (s->wan) s->wan->harmonics(w0, hmax, band_power);
+        else s->eng->harmonics(s->id, w0, hmax, band_power);
+        return SBE_OK;
+    });
+}
+
 extern "C" void sbe_solver_destroy(sbe_solver *s)
 {
     if (!s) return;
@@ -448,6 +460,18 @@ extern "C" sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
         copy_out(b->eng->outputs(b->ids[index]), out);
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_batch_harmonics(sbe_batch *b, int index, double w0, int hmax, double *band_power)
+{
+    if (!b || index < 0 || index >= (int)b->ids.size() || !band_power)
+        return fail(SBE_INVALID_ARGUMENT, "bad batch index or null output");
+    if (!b->ran) return fail(SBE_NOT_READY, "sbe_batch_run has not been called");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+        b->eng->harmonics(b->ids[index], w0, hmax, band_power);
         return SBE_OK;
     });
 }

@@ -1,6 +1,7 @@
 // Host engine: device buffers of resident solves, launch lists, per-launch
 // stepping, output assembly and the reference's file writers.
 #include "sbe_engine.h"
+#include "sbe_spectrum.h"
 
 #include <algorithm>
 #include <cmath>
@@ -534,6 +535,38 @@ void Engine::raw_outputs(int id, std::vector<double> &jout, double cp[NSLOT])
     for (int t = 0; t < s.ntiles; ++t)
         for (int q = 0; q < NSLOT; ++q) cp[q] += s.h_const[(size_t)t * NSLOT + q];
     jout.assign(s.h_jout, s.h_jout + (size_t)s.Nt * NSLOT);
+}
+
+void Engine::harmonics(int id, double w0, int hmax, double *band_power)
+{
+    Solve &s = get(id);
+    const Problem &p = s.prob;
+    HarmonicsInput in;
+    in.jout = s.jout;
+    in.stride = NSLOT;
+    in.nt = s.Nt;
+    in.dt = p.laser.dt;
+    in.dV = p.dV;
+    double *A = nullptr;
+    if (p.gauge == GAUGE_VELOCITY) {  // intra += rho0 parts (per tile) + Nval A(t_n) sum_k w_k
+        in.cp = s.constpart;
+        in.ntiles = s.ntiles;
+        in.cp_stride = NSLOT;
+        in.cp_slot = 2;
+        std::vector<double> a(2 * (size_t)s.Nt);
+        for (int n = 0; n < s.Nt; ++n) {
+            double A3[3], E3[3];
+            p.laser.eval(p.laser.atmin + p.laser.dt * n, A3, E3);
+            a[2 * (size_t)n] = A3[0];
+            a[2 * (size_t)n + 1] = A3[1];
+        }
+        cuda_check(cudaMallocAsync(reinterpret_cast<void **>(&A), a.size() * 8, stream_), "alloc A table");
+        UploadRing::shared().upload(A, a.data(), a.size() * 8, stream_);
+        in.A = A;
+        in.nvw = p.nval * p.total_weight;
+    }
+    harmonics_on_device(in, w0, hmax, band_power, stream_);
+    if (A) cudaFreeAsync(A, stream_);
 }
 
 SolveOutputs Engine::outputs(int id)

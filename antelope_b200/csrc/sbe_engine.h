@@ -118,6 +118,9 @@ public:
     // fetched solve (waits for the copy); assemble_outputs() turns them into
     // the output arrays.
     void raw_outputs(int id, std::vector<double> &jout, double cp[NSLOT]);
+    // harmonic band powers h = 1..hmax of a finished solve, from its
+    // device-resident sums (sbe_spectrum.h); synchronises the stream
+    void harmonics(int id, double w0, int hmax, double *band_power);
     void remove(int id);
     int nresident() const { return (int)live_.size(); }
     int tick() const { return tick_; }

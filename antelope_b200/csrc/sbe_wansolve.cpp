@@ -3,6 +3,8 @@
 // reference's output quantities for N bands (antelope.cpp:514-548).
 #include "sbe_wansolve.h"
 
+#include "sbe_spectrum.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -170,6 +172,33 @@ void WannierSolve::run(cudaStream_t st)
     }
     if (h_ctl_->error) throw CudaError("Cash-Karp step size underflow: tolerance unreachable");
     launches_ = (int)(2 * launched);
+}
+
+void WannierSolve::harmonics(double w0, int hmax, double *band_power)
+{
+    const Problem &p = prob_;
+    HarmonicsInput in;
+    in.jout = w_.jout;
+    in.stride = WAN_NSLOT;
+    in.nt = w_.Nt;
+    in.dt = p.laser.dt;
+    in.dV = p.dV;
+    double *A = nullptr;
+    if (w_.vg) {  // intra += Nval A(t_n) sum_k w_k
+        std::vector<double> a(2 * (size_t)w_.Nt);
+        for (int n = 0; n < w_.Nt; ++n) {
+            double A3[3], E3[3];
+            p.laser.eval(p.laser.atmin + p.laser.dt * n, A3, E3);
+            a[2 * (size_t)n] = A3[0];
+            a[2 * (size_t)n + 1] = A3[1];
+        }
+        cuda_check(cudaMallocAsync(reinterpret_cast<void **>(&A), a.size() * 8, stream_), "alloc A table");
+        UploadRing::shared().upload(A, a.data(), a.size() * 8, stream_);
+        in.A = A;
+        in.nvw = p.nval * p.total_weight;
+    }
+    harmonics_on_device(in, w0, hmax, band_power, stream_);
+    if (A) cudaFreeAsync(A, stream_);
 }
 
 SolveOutputs WannierSolve::outputs()

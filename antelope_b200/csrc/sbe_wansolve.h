@@ -17,6 +17,8 @@ public:
     // Run every attempted step on `st` (returns when the solve is done).
     void run(cudaStream_t st);
     SolveOutputs outputs();
+    // harmonic band powers h = 1..hmax from the device-resident sums
+    void harmonics(double w0, int hmax, double *band_power);
     int launches() const { return launches_; }
     const WanCtl &control() const { return *h_ctl_; }
 

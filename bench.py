@@ -211,6 +211,10 @@ def run_ours(args):
     prop64 = sum(k["propagate_ms"] for k in kt_fp64)
     ach64 = FLOPS_PER_KSTEP[4] * kst * len(kt_fp64) / (prop64 * 1e-3) / 1e12
     traffic = read_traffic()
+    shapes = read_tune_cache()
+    kpt_mixed = args.kpt or next((v["k_per_thread"] for k, v in shapes.items() if k.startswith("vg-mixed")), 2)
+    kernel_name = "propagate_vg_x2<4> (2 k-points per thread, packed f32x2)" if kpt_mixed == 2 \
+        else "propagate_vg<float,4,1>"
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -236,9 +240,9 @@ def run_ours(args):
         "roofline": {"bound": "fp32 FMA pipe", "achieved": achieved, "peak": fp32_tf, "unit": "TFLOP/s",
                      "frac": achieved / fp32_tf, "traffic": traffic,
                      "peak_source": "measured FMA-chain microbenchmark (MEASURED_PEAKS.json has no FP32/FP64)",
-                     "flops_per_kstep": FLOPS_PER_KSTEP[4], "kernel": "propagate_vg<float,4>",
+                     "flops_per_kstep": FLOPS_PER_KSTEP[4], "kernel": kernel_name,
                      "kernel_share": prop_ms / (prop_ms + red_ms)},
-        "launch_shapes": read_tune_cache(),
+        "launch_shapes": shapes,
         "gpu_launches": int(launches) * 2,   # propagate + reduce per launch tick, timed steps only
         "clocks": clocks,
     }
@@ -389,6 +393,11 @@ def run_scan(args, stream, rank, world):
         _, e, _ = per_harmonic_error({"inter": o.inter, "intra": o.intra},
                                      {"inter": fp64_out[j].inter, "intra": fp64_out[j].intra}, 0.1, w0)
         errs.append(float(e.max()))
+    # harmonic band powers of every solve, on the GPU from the resident results
+    t_h = time.perf_counter()
+    for i in range(len(probs)):
+        batch.harmonics(i, cases[a + i]["laser"]["pulses"][0]["w0"], 30)
+    t_h = time.perf_counter() - t_h
     launches = batch.launches
     batch.close()
     nsolves = sum_over_ranks(len(probs))
@@ -400,7 +409,8 @@ def run_scan(args, stream, rank, world):
             "batched_mixed_over_sequential_fp64": sph / sph64,
             "fp64_sequential_sample": f"{len(sub)} of {len(probs)} solves (every 4th)",
             "max_per_harmonic_error_vs_fp64": max(errs), "error_sample": f"{len(errs)} solves",
-            "setup_s": t_create, "launches": launches, "graph": True, "steps_per_launch": 256}
+            "setup_s": t_create, "launches": launches, "graph": True, "steps_per_launch": 256,
+            "harmonics_s_all_solves": t_h, "harmonics": "30 band powers per solve on the GPU (sbe_batch_harmonics)"}
 
 
 def run_serve(args):

@@ -134,6 +134,15 @@ sbe_status sbe_solver_kernel_times(sbe_solver *s, double *propagate_ms, int *pro
                                    double *reduce_ms, int *reduce_launches);
 void sbe_solver_destroy(sbe_solver *s);
 
+/* Harmonic band powers of a finished solve, computed on the GPU from its
+ * device-resident results, in the convention of the reference's analysis
+ * script (AlsisPythonShort/AnalysisReader_PyDir.py:252-354: Blackman window
+ * over the record, FFT times dt, times -i*omega, |.|^2 summed over x and y,
+ * with J = interband + intraband current; band h = the bins with
+ * h - 1/2 <= omega / w0 < h + 1/2 as IntegrateSpectrumOrder.py:57-70).
+ * w0: the fundamental angular frequency (a.u.); band_power[hmax]. */
+sbe_status sbe_solver_harmonics(sbe_solver *s, double w0, int hmax, double *band_power);
+
 /* Write the reference's six output files into `dir` (antelope.cpp:176-184,
  * 208-235, 514-548) from arrays filled by a get call. */
 sbe_status sbe_write_outputs(const sbe_problem *p, const sbe_outputs *o, const char *dir);
@@ -148,6 +157,7 @@ sbe_status sbe_batch_create(const sbe_problem *const *problems, int n, const sbe
 sbe_status sbe_batch_run(sbe_batch *b, void *stream);
 sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *out);
 int sbe_batch_launches(const sbe_batch *b);
+sbe_status sbe_batch_harmonics(sbe_batch *b, int i, double w0, int hmax, double *band_power);
 sbe_status sbe_batch_kernel_times(sbe_batch *b, double *propagate_ms, int *propagate_launches,
                                   double *reduce_ms, int *reduce_launches);
 void sbe_batch_destroy(sbe_batch *b);
