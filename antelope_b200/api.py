@@ -130,12 +130,17 @@ class Problem:
 
 
 class Solver:
-    """One solve on the GPU (``sbe_solver_*``)."""
+    """One solve on the GPU (``sbe_solver_*``); ``k_slice=(k_begin, k_end)``
+    restricts it to a block of the k-grid (``sbe_solver_create_slice``)."""
 
-    def __init__(self, problem: Problem, **opts):
+    def __init__(self, problem: Problem, k_slice: tuple[int, int] | None = None, **opts):
         self.problem = problem
         self._h = P()
-        _check(lib.sbe_solver_create(problem._h, C.byref(_opts(**opts)), C.byref(self._h)))
+        if k_slice is None:
+            _check(lib.sbe_solver_create(problem._h, C.byref(_opts(**opts)), C.byref(self._h)))
+        else:
+            _check(lib.sbe_solver_create_slice(problem._h, C.byref(_opts(**opts)), int(k_slice[0]),
+                                               int(k_slice[1]), C.byref(self._h)))
 
     def run(self, stream: int = 0):
         _check(lib.sbe_solver_run(self._h, C.c_void_p(stream)))
@@ -151,6 +156,13 @@ class Solver:
 
     def kernel_times(self) -> dict:
         return _kernel_times(lib.sbe_solver_kernel_times, self._h)
+
+    def sums(self) -> np.ndarray:
+        """Per-step k-sums of this solver's k-points, (Nt + 1) x width,
+        additive over k-slices (``sbe_solver_sums``)."""
+        out = np.zeros((self.problem.dims.Nt + 1, lib.sbe_sums_width(self.problem._h)))
+        _check(lib.sbe_solver_sums(self._h, out.ctypes.data))
+        return out
 
     def harmonics(self, w0: float, hmax: int) -> np.ndarray:
         """Band powers of harmonic orders 1..hmax, computed on the GPU
@@ -171,6 +183,17 @@ class Solver:
             self._h = None
 
     __del__ = close
+
+
+def assemble(problem: Problem, sums: np.ndarray) -> "Outputs":
+    """Output arrays from k-sums added over all slices (``sbe_assemble``,
+    host only)."""
+    sums = np.ascontiguousarray(sums, dtype=np.float64)
+    if sums.shape != (problem.dims.Nt + 1, lib.sbe_sums_width(problem._h)):
+        raise ValueError("sums has the wrong shape")
+    out = Outputs.empty(problem.dims)
+    _check(lib.sbe_assemble(problem._h, sums.ctypes.data, C.byref(out.c())))
+    return out
 
 
 def solve(problem, **opts) -> Outputs:

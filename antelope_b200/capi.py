@@ -67,6 +67,10 @@ def _load():
         "sbe_solver_get": (C.c_int, [P, C.POINTER(COutputs)]),
         "sbe_solver_launches": (C.c_int, [P]),
         "sbe_solver_harmonics": (C.c_int, [P, C.c_double, C.c_int, C.c_void_p]),
+        "sbe_solver_create_slice": (C.c_int, [P, C.POINTER(Opts), C.c_int, C.c_int, C.POINTER(P)]),
+        "sbe_sums_width": (C.c_int, [P]),
+        "sbe_solver_sums": (C.c_int, [P, C.c_void_p]),
+        "sbe_assemble": (C.c_int, [P, C.c_void_p, C.POINTER(COutputs)]),
         "sbe_batch_harmonics": (C.c_int, [P, C.c_int, C.c_double, C.c_int, C.c_void_p]),
         "sbe_solver_steps": (C.c_int, [P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                        C.POINTER(C.c_longlong)]),

@@ -229,7 +229,8 @@ struct sbe_solver {
     long long nt = 0;  // fixed-step solves: steps taken
 };
 
-extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *opts, sbe_solver **out)
+namespace {
+sbe_status create_solver(const sbe_problem *p, const sbe_opts *opts, int kb, int ke, sbe_solver **out)
 {
     if (sbe_status st = check_problem(p)) return st;
     if (!out) return fail(SBE_INVALID_ARGUMENT, "null output pointer");
@@ -242,16 +243,81 @@ extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *op
         cuda_check(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming), "event create");
         if (p->p.model != MODEL_HALDANE) {
             const int prec = (opts && opts->precision >= 0) ? opts->precision : p->p.precision;
-            s->wan = std::make_unique<WannierSolve>(p->p, prec, s->device, s->own);
+            s->wan = std::make_unique<WannierSolve>(p->p, prec, s->device, s->own, kb, ke);
         } else {
             s->eng = std::make_unique<Engine>(s->device, s->own, default_steps(opts));
-            s->id = s->eng->add(p->p, to_engine_opts(opts));
+            EngineOptions eo = to_engine_opts(opts);
+            eo.k_begin = kb;
+            eo.k_end = ke;
+            s->id = s->eng->add(p->p, eo);
             s->nt = p->p.laser.Nt;  // antelope.cpp:297-338: one step per output time
             s->use_graph = opts && opts->use_graph && !opts->profile;
             s->eng->set_profile(opts && opts->profile);
         }
         cuda_check(cudaEventRecord(s->ready, s->own), "event record");
         *out = s.release();
+        return SBE_OK;
+    });
+}
+}  // namespace
+
+extern "C" sbe_status sbe_solver_create(const sbe_problem *p, const sbe_opts *opts, sbe_solver **out)
+{
+    return create_solver(p, opts, 0, 0, out);
+}
+
+extern "C" sbe_status sbe_solver_create_slice(const sbe_problem *p, const sbe_opts *opts, int k_begin, int k_end,
+                                              sbe_solver **out)
+{
+    if (p && (k_begin < 0 || k_end > p->p.ntotal() || k_begin >= k_end))
+        return fail(SBE_INVALID_ARGUMENT, "k-slice outside the grid");
+    return create_solver(p, opts, k_begin, k_end, out);
+}
+
+extern "C" int sbe_sums_width(const sbe_problem *p)
+{
+    if (!p) return 0;
+    return p->p.model == MODEL_HALDANE ? NSLOT : WAN_NSLOT;
+}
+
+extern "C" sbe_status sbe_solver_sums(sbe_solver *s, double *sums)
+{
+    if (!s || !sums) return fail(SBE_INVALID_ARGUMENT, "null argument");
+    if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        if (s->wan) {
+            const std::vector<double> j = s->wan->sums();
+            std::copy(j.begin(), j.end(), sums);
+            const int Nt = (int)(j.size() / WAN_NSLOT);
+            std::fill(sums + (size_t)Nt * WAN_NSLOT, sums + (size_t)(Nt + 1) * WAN_NSLOT, 0.0);
+        } else {
+            std::vector<double> j;
+            double cp[NSLOT];
+            s->eng->raw_outputs(s->id, j, cp);
+            std::copy(j.begin(), j.end(), sums);
+            std::copy(cp, cp + NSLOT, sums + j.size());
+        }
+        return SBE_OK;
+    });
+}
+
+extern "C" sbe_status sbe_assemble(const sbe_problem *p, const double *sums, const sbe_outputs *out)
+{
+    if (sbe_status st = check_problem(p)) return st;
+    if (!sums || !out) return fail(SBE_INVALID_ARGUMENT, "null argument");
+    return guard([&]() -> sbe_status {
+        const Problem &q = p->p;
+        const int Nt = q.laser.Nt;
+        SolveOutputs o;
+        if (q.model == MODEL_HALDANE) {
+            std::vector<double> j(sums, sums + (size_t)Nt * NSLOT);
+            assemble_outputs(q, j, sums + (size_t)Nt * NSLOT, o);
+        } else {
+            std::vector<double> j(sums, sums + (size_t)Nt * WAN_NSLOT);
+            assemble_table_outputs(q, j, o);
+        }
+        copy_out(o, out);
         return SBE_OK;
     });
 }

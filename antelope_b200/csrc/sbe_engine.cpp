@@ -244,7 +244,9 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     s->precision = o.precision >= 0 ? o.precision : p.precision;
     s->variant = p.gauge == GAUGE_VELOCITY ? VAR_HALDANE_VG : VAR_HALDANE_LW;
     s->shape = shape_for(p, o);
-    s->nk = p.ntotal();
+    const int kb = o.k_end > 0 ? o.k_begin : 0, ke = o.k_end > 0 ? o.k_end : p.ntotal();
+    if (kb < 0 || ke > p.ntotal() || kb >= ke) throw CfgError("k-slice outside the grid");
+    s->nk = ke - kb;
     s->ntiles = ceil_div(s->nk, s->shape.tile_k);
     s->nk_pad = s->ntiles * s->shape.tile_k;
     s->Nt = p.laser.Nt;
@@ -297,6 +299,7 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     }
     InitArgs ia{};
     ia.nk = s->nk;
+    ia.k_offset = kb;
     ia.nk_pad = s->nk_pad;
     ia.tile_k = s->shape.tile_k;
     ia.variant = s->variant;

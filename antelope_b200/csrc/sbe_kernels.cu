@@ -707,9 +707,10 @@ __global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restric
     const int k1 = min(k0 + ia.tile_k, ia.nk);
     double cp[4] = {0, 0, 0, 0};  // sum w rho0 P00/P11 (x, y), sum w rho0_00, sum w rho0_11
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-        // momaxis grid point and weight
+        // momaxis grid point and weight (of flat index k_offset + k)
         const int N0 = ia.N[0], N1 = ia.N[1], N2 = ia.N[2];
-        const int ii[3] = {k / (N1 * N2), (k / N2) % N1, k % N2};
+        const int kg = ia.k_offset + k;
+        const int ii[3] = {kg / (N1 * N2), (kg / N2) % N1, kg % N2};
         const int NN[3] = {N0, N1, N2};
         double f[3], w = 1.0;
 #pragma unroll

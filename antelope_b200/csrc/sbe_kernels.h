@@ -20,6 +20,7 @@ struct LaunchArgs {
 
 struct InitArgs {
     int nk, nk_pad, tile_k, variant, nval, use_fermi;
+    int k_offset;  // flat grid index of local k-point 0 (a k-slice of the grid)
     int N[3];
     double axes[9], origin[3];
     double t1, t2, M0, phi0, va[3][2], vb[3][2];

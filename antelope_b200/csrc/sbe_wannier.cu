@@ -527,9 +527,10 @@ __device__ __forceinline__ double warp_max(double v)
 }
 
 // k-grid point (momaxis.h:147-186, 349-383) and its trapezoid weight
-__device__ void kpoint(const WanDev &P, int k, double kv[3], double &wt)
+__device__ void kpoint(const WanDev &P, int kl, double kv[3], double &wt)
 {
     const int N0 = P.Ngrid[0], N1 = P.Ngrid[1], N2 = P.Ngrid[2];
+    const int k = P.k_offset + kl;  // local index -> flat grid index
     const int ii[3] = {k / (N1 * N2), (k / N2) % N1, k % N2};
     const int NNg[3] = {N0, N1, N2};
     double f[3];

@@ -45,6 +45,7 @@ struct WanCtl {
 struct WanDev {
     int N, nval, nR, nk, Nt, ntiles, rk, inter_intra, use_fermi, has_dip, has_jtab;
     int vg;                 // 1: velocity gauge (band basis), 0: length gauge (Wannier basis)
+    int k_offset;           // flat grid index of local k-point 0 (a k-slice of the grid)
     double Ef, dt, atmin, tol, g1, g2;  // g1 = 1/T1, g2 = 1/T2 (0 when disabled)
     int Ngrid[3];
     double axes[9], origin[3];

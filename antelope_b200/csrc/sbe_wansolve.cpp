@@ -18,7 +18,7 @@ template <class T> void dalloc(T **p, size_t bytes, cudaStream_t st, const char 
 }
 }  // namespace
 
-WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStream_t st)
+WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStream_t st, int k_begin, int k_end)
     : prob_(p), precision_(precision), device_(device), stream_(st)
 {
     if (p.model != MODEL_SYNTHETIC_WANNIER && p.model != MODEL_TB) throw CfgError("not a tight-binding problem");
@@ -31,7 +31,10 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     w_.N = N;
     w_.nval = p.nval;
     w_.nR = p.w_nR;
-    w_.nk = p.ntotal();
+    const int kb = k_end > 0 ? k_begin : 0, ke = k_end > 0 ? k_end : p.ntotal();
+    if (kb < 0 || ke > p.ntotal() || kb >= ke) throw CfgError("k-slice outside the grid");
+    w_.nk = ke - kb;
+    w_.k_offset = kb;
     w_.Nt = p.laser.Nt;
     w_.ntiles = (w_.nk + WAN_WARPS - 1) / WAN_WARPS;
     w_.rk = p.rk;
@@ -201,14 +204,25 @@ void WannierSolve::harmonics(double w0, int hmax, double *band_power)
     if (A) cudaFreeAsync(A, stream_);
 }
 
-SolveOutputs WannierSolve::outputs()
+std::vector<double> WannierSolve::sums()
 {
-    const Problem &p = prob_;
-    const int Nt = w_.Nt, N = p.nband, NN = N * N;
-    std::vector<double> j((size_t)Nt * WAN_NSLOT);
+    std::vector<double> j((size_t)w_.Nt * WAN_NSLOT);
     cuda_check(cudaMemcpyAsync(j.data(), w_.jout, j.size() * 8, cudaMemcpyDeviceToHost, stream_), "copy outputs");
     cuda_check(cudaStreamSynchronize(stream_), "sync");
+    return j;
+}
+
+SolveOutputs WannierSolve::outputs()
+{
     SolveOutputs o;
+    assemble_table_outputs(prob_, sums(), o);
+    return o;
+}
+
+void assemble_table_outputs(const Problem &p, const std::vector<double> &j, SolveOutputs &o)
+{
+    const int Nt = p.laser.Nt, N = p.nband, NN = N * N;
+    const bool vg = p.gauge == GAUGE_VELOCITY;
     o.Nt = Nt;
     o.nband = N;
     o.inter.assign((size_t)Nt * 3, 0.0);
@@ -218,7 +232,7 @@ SolveOutputs WannierSolve::outputs()
     o.laser.assign((size_t)Nt * 7, 0.0);
     const double dV = p.dV, Ntot = (double)p.ntotal();
     // velocity gauge: intra_a += Nval A_a(t) per k (SBEs.h:750-757), i.e. Nval A_a sum_k w_k
-    const double nvw = w_.vg ? p.nval * p.total_weight : 0.0;
+    const double nvw = vg ? p.nval * p.total_weight : 0.0;
     const int e = p.nval * N + p.nval + 1, roff = e / NN;
     for (int n = 0; n < Nt; ++n) {
         const double *r = &j[(size_t)n * WAN_NSLOT];
@@ -249,7 +263,6 @@ SolveOutputs WannierSolve::outputs()
             o.coh[(size_t)n * 2 + 1] = j[(size_t)row * WAN_NSLOT + 5 + N] / Ntot;
         }
     }
-    return o;
 }
 
 }  // namespace sbe

@@ -10,13 +10,16 @@ namespace sbe {
 
 class WannierSolve {
 public:
-    WannierSolve(const Problem &p, int precision, int device, cudaStream_t st);
+    // k_begin/k_end: a k-slice [k_begin, k_end) of the grid (0, 0: all of it)
+    WannierSolve(const Problem &p, int precision, int device, cudaStream_t st, int k_begin = 0, int k_end = 0);
     ~WannierSolve();
     WannierSolve(const WannierSolve &) = delete;
     WannierSolve &operator=(const WannierSolve &) = delete;
     // Run every attempted step on `st` (returns when the solve is done).
     void run(cudaStream_t st);
     SolveOutputs outputs();
+    // per-step sums [Nt][WAN_NSLOT] of this solve's k-points (host copy)
+    std::vector<double> sums();
     // harmonic band powers h = 1..hmax from the device-resident sums
     void harmonics(double w0, int hmax, double *band_power);
     int launches() const { return launches_; }
@@ -31,5 +34,9 @@ private:
     WanCtl *h_ctl_ = nullptr;
     int launches_ = 0;
 };
+
+// The reference's output arrays of a table model from its per-step sums
+// [Nt][WAN_NSLOT] (possibly summed over k-slices; antelope.cpp:514-548).
+void assemble_table_outputs(const Problem &p, const std::vector<double> &sums, SolveOutputs &o);
 
 }  // namespace sbe

@@ -143,6 +143,22 @@ void sbe_solver_destroy(sbe_solver *s);
  * w0: the fundamental angular frequency (a.u.); band_power[hmax]. */
 sbe_status sbe_solver_harmonics(sbe_solver *s, double w0, int hmax, double *band_power);
 
+/* k-sharding of one solve over several GPUs or processes (the reference's
+ * ParaRange split of the k-grid over MPI ranks, utility.h:104-115, and the
+ * MPI_Reduce of antelope.cpp:482-512):
+ *   sbe_solver_create_slice  a solver for flat k-points [k_begin, k_end);
+ *   sbe_solver_sums          its per-step k-sums, (Nt + 1) rows of
+ *                            sbe_sums_width(p) doubles (the last row holds the
+ *                            time-independent parts), additive over slices;
+ *   sbe_assemble             the output arrays from sums added over all slices
+ *                            (host only, no GPU).
+ * The slices' sums are combined by the caller (an NCCL all-reduce, say). */
+sbe_status sbe_solver_create_slice(const sbe_problem *p, const sbe_opts *opts, int k_begin, int k_end,
+                                   sbe_solver **out);
+int sbe_sums_width(const sbe_problem *p);
+sbe_status sbe_solver_sums(sbe_solver *s, double *sums);
+sbe_status sbe_assemble(const sbe_problem *p, const double *sums, const sbe_outputs *out);
+
 /* Write the reference's six output files into `dir` (antelope.cpp:176-184,
  * 208-235, 514-548) from arrays filled by a get call. */
 sbe_status sbe_write_outputs(const sbe_problem *p, const sbe_outputs *o, const char *dir);
