@@ -39,9 +39,11 @@ namespace sbe {
 // ------------------------------------------------------------ RK tableaux
 // Butcher tableaux of SBEs.h:395-416.  The stage slopes carry the factor dt
 // (all per-k constants are dt-scaled), so only the pure coefficients appear.
+// ti(i): the field-table column of stage i; END: the column at t + dt, whose
+// field terms are the next step's terms at its own start.
 template <int RK> struct Tableau;
 template <> struct Tableau<4> {
-    static constexpr int S = 4, NT = 3;
+    static constexpr int S = 4, NT = 3, END = 2;
     __device__ static constexpr double a(int i, int j)
     {
         return (i == 1 && j == 0) ? 0.5 : (i == 2 && j == 1) ? 0.5 : (i == 3 && j == 2) ? 1.0 : 0.0;
@@ -53,7 +55,7 @@ template <> struct Tableau<4> {
     __device__ static constexpr int ti(int i) { return i == 0 ? 0 : (i == 3 ? 2 : 1); }
 };
 template <> struct Tableau<5> {  // Fehlberg tableau with its 5th-order weights
-    static constexpr int S = 6, NT = 6;
+    static constexpr int S = 6, NT = 6, END = 4;
     __device__ static constexpr double a(int i, int j)
     {
         return i == 1 ? (j == 0 ? 1.0 / 4.0 : 0.0)
@@ -151,13 +153,23 @@ constexpr int MAX_WARPS = 8;
 // Per-step tile reduction staged through shared memory: each warp deposits
 // its 8 sums per step; every SUB steps (and at the end of the launch) the
 // block sums over warps and writes one row of the partial buffer per step.
+// The staging area has two halves used in turn, so one barrier per flush
+// suffices: a warp writes a half again only after the next flush's barrier,
+// which every thread reaches after finishing its reads of that half.
+using RedStage = double[2][SUB][MAX_WARPS][NSLOT];
+
 struct TileReducer {
-    double (*red)[MAX_WARPS][NSLOT];
-    __device__ __forceinline__ void push(const double (&v)[8], int r)
+    double (*red)[SUB][MAX_WARPS][NSLOT];
+    int half;
+    __device__ __forceinline__ explicit TileReducer(RedStage &s) : red(s), half(0) {}
+    __device__ __forceinline__ void put(double y, int r)
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        double y = warp_sum8(v, lane);
-        if ((lane & 3) == 0) red[r][warp][lane >> 2] = y;
+        if ((lane & 3) == 0) red[half][r][warp][lane >> 2] = y;
+    }
+    __device__ __forceinline__ void push(const double (&v)[8], int r)
+    {
+        put(warp_sum8(v, threadIdx.x & 31), r);
     }
     __device__ __forceinline__ void flush(int nrows, int row0, int ntiles, int tile, double *partial)
     {
@@ -166,10 +178,10 @@ struct TileReducer {
         for (int idx = threadIdx.x; idx < nrows * NSLOT; idx += blockDim.x) {
             const int row = idx / NSLOT, slot = idx % NSLOT;
             double acc = 0.0;
-            for (int w = 0; w < nwarp; ++w) acc += red[row][w][slot];
+            for (int w = 0; w < nwarp; ++w) acc += red[half][row][w][slot];
             partial[((size_t)(row0 + row) * ntiles + tile) * NSLOT + slot] = acc;
         }
-        __syncthreads();
+        half ^= 1;
     }
 };
 
@@ -183,19 +195,42 @@ struct TileReducer {
 // wherever the reference's arithmetic reads db.
 enum VgDof : int { D_DA = 0, D_ZR, D_ZI, D_N };
 
-template <class Real, bool G1>
-__device__ __forceinline__ void vg_rhs(const Real (&c)[VG_NCONST], typename V2<Real>::T A, const Real (&y)[D_N],
-                                       Real g1, Real g2, Real (&k)[D_N])
+// Field terms of the velocity-gauge Hamiltonian at one stage time:
+// dt (h0 - h1) and dt w = dt A.P01 (SBEs.h:787-805 with H = diag eps + A.P).
+// They depend on the stage time only through A, so a step evaluates them once
+// per distinct stage time (RK4: t, t + dt/2, t + dt), and the terms at t + dt
+// serve again as the next step's terms at its start.
+template <class Real> struct VgField { Real d, wr, wi; };
+
+// Table entry of the field at the start of step s0: step 0 starts at t_min;
+// every later step s starts with the field of step s-1 at t_{s-1} + dt, which
+// the host evaluated at that sum (SBEs.h:612) -- the reference's own start
+// time t_s = t_min + s dt (antelope.cpp:299) differs from it by at most an
+// ulp of t.  Loading that same entry when a launch begins at s0 makes the
+// result independent of where launches split the time loop.
+template <class TB>
+__device__ __forceinline__ size_t vg_start_row(int s0)
 {
-    const Real delta = fma(A.y, c[VG_DPY], fma(A.x, c[VG_DPX], c[VG_DE]));
-    const Real wr = fma(A.y, c[VG_PYR], A.x * c[VG_PXR]);
-    const Real wi = fma(A.y, c[VG_PYI], A.x * c[VG_PXI]);
-    const Real im2 = Real(2) * fma(wi, y[D_ZR], -(wr * y[D_ZI]));  // 2 Im(w z*)
+    return s0 == 0 ? 0 : (size_t)(s0 - 1) * TB::NT + TB::END;
+}
+
+template <class Real>
+__device__ __forceinline__ VgField<Real> vg_field(const Real (&c)[VG_NCONST], typename V2<Real>::T A)
+{
+    return {fma(A.y, c[VG_DPY], fma(A.x, c[VG_DPX], c[VG_DE])), fma(A.y, c[VG_PYR], A.x * c[VG_PXR]),
+            fma(A.y, c[VG_PYI], A.x * c[VG_PXI])};
+}
+
+template <class Real, bool G1>
+__device__ __forceinline__ void vg_rhs(const VgField<Real> &h, Real c0, const Real (&y)[D_N], Real g1, Real g2,
+                                       Real (&k)[D_N])
+{
+    const Real im2 = Real(2) * fma(h.wi, y[D_ZR], -(h.wr * y[D_ZI]));  // 2 Im(w z*)
     k[D_DA] = G1 ? fma(-g1, y[D_DA], im2) : im2;
-    const Real bma = fma(Real(-2), y[D_DA], c[VG_C0]);             // rho_11 - rho_00 = c0 + db - da
-    const Real xr = fma(bma, wr, delta * y[D_ZR]);
-    const Real xi = fma(bma, wi, delta * y[D_ZI]);
-    k[D_ZR] = fma(-g2, y[D_ZR], xi);                                // -i X - g2 z
+    const Real bma = fma(Real(-2), y[D_DA], c0);                       // rho_11 - rho_00 = c0 + db - da
+    const Real xr = fma(bma, h.wr, h.d * y[D_ZR]);
+    const Real xi = fma(bma, h.wi, h.d * y[D_ZI]);
+    k[D_ZR] = fma(-g2, y[D_ZR], xi);                                   // -i X - g2 z
     k[D_ZI] = fma(-g2, y[D_ZI], -xr);
 }
 
@@ -206,7 +241,7 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
     using T2 = typename V2<Real>::T;
     using TB = Tableau<RK>;
     constexpr bool F64 = std::is_same<Real, double>::value;
-    __shared__ double red_s[SUB][MAX_WARPS][NSLOT];
+    __shared__ RedStage red_s;
     const TileDev tl = tiles[blockIdx.x];
     const SolveDev &sd = solves[tl.solve];
     const int s0 = (tick - sd.admit_tick) * S;
@@ -238,7 +273,14 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 #pragma unroll
         for (int q = 0; q < D_N; ++q) y64[j][q] = ok[j] ? st[(size_t)slot[q] * nkp + kidx[j]] : 0.0;
     }
-    TileReducer red{red_s};
+    TileReducer red(red_s);
+    // field terms at the start of the launch's first step (see vg_start_row)
+    VgField<Real> hstart[KPT];
+    {
+        const T2 A0 = __ldg(tab + vg_start_row<TB>(s0));
+#pragma unroll
+        for (int j = 0; j < KPT; ++j) hstart[j] = vg_field<Real>(c[j], A0);
+    }
 
     for (int s = s0; s < s1; ++s) {
         Real y0[KPT][D_N];
@@ -266,14 +308,18 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
         v[5] = -v[4];
         const int r = (s - s0) % SUB;
         red.push(v, r);
-        if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
 
         // one RK step
         T2 A[TB::NT];
 #pragma unroll
-        for (int i = 0; i < TB::NT; ++i) A[i] = __ldg(tab + (size_t)s * TB::NT + i);
+        for (int i = 1; i < TB::NT; ++i) A[i] = __ldg(tab + (size_t)s * TB::NT + i);
 #pragma unroll
         for (int j = 0; j < KPT; ++j) {
+            VgField<Real> h[TB::NT];
+            h[0] = hstart[j];
+#pragma unroll
+            for (int i = 1; i < TB::NT; ++i) h[i] = vg_field<Real>(c[j], A[i]);
+            hstart[j] = h[TB::END];
             // FP64: acc = rho + sum_i dt b_i k_i in the reference's order
             // (SBEs.h:614-623); mixed: the sum is formed in FP32 first
             Real kk[TB::S][D_N], y[D_N], acc[D_N];
@@ -289,7 +335,7 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
                         if (TB::a(i, m) != 0.0) t = fma(Real(TB::a(i, m)), kk[m][q], t);
                     y[q] = t;
                 }
-                vg_rhs<Real, G1>(c[j], A[TB::ti(i)], y, g1, g2, kk[i]);
+                vg_rhs<Real, G1>(h[TB::ti(i)], c[j][VG_C0], y, g1, g2, kk[i]);
                 if (TB::b(i) != 0.0) {
 #pragma unroll
                     for (int q = 0; q < D_N; ++q) acc[q] = fma(Real(TB::b(i)), kk[i][q], acc[q]);
@@ -298,6 +344,9 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 #pragma unroll
             for (int q = 0; q < D_N; ++q) y64[j][q] = F64 ? double(acc[q]) : y64[j][q] + double(acc[q]);
         }
+        // the staged sums reach the partial buffer after the step's arithmetic,
+        // so the warp reduction above can overlap it
+        if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
     }
 #pragma unroll
     for (int j = 0; j < KPT; ++j)
@@ -337,24 +386,30 @@ __device__ __forceinline__ float warp_sum8f(const float (&v)[8], int lane)
     return y;  // lanes 4*i hold the sum of v[i]
 }
 
-// Packed right-hand side on (da, Re z, Im z) of two k-points.  The factor 2
-// of 2 Im(w z*) and of (rho_11 - rho_00) w is folded into w (cw = 2 w, hc0 =
-// c0 / 2: exact power-of-two scalings), and the Im z slope is produced with
-// the opposite sign (nzi = -dt dIm z/dt) so that no operand needs negating;
-// the stage and step combinations apply that sign through their coefficients.
-template <bool G1>
-__device__ __forceinline__ void vg_rhs2(const float2 (&c)[VG_NCONST], float2 A, const float2 (&y)[D_N], float2 ng1,
-                                        float2 ng2, float2 g2, float2 (&k)[D_N])
+// Packed field terms and right-hand side on (da, Re z, Im z) of two
+// k-points.  The factor 2 of 2 Im(w z*) and of (rho_11 - rho_00) w is folded
+// into w (cw = 2 w, hc0 = c0 / 2: exact power-of-two scalings), and the Im z
+// slope is produced with the opposite sign (nzi = -dt dIm z/dt) so that no
+// operand needs negating; the stage and step combinations apply that sign
+// through their coefficients.
+struct VgField2 { float2 d, cwr, cwi; };   // dt (h0 - h1), 2 dt Re w, 2 dt Im w
+
+__device__ __forceinline__ VgField2 vg_field2(const float2 (&c)[VG_NCONST], float2 A)
 {
     const float2 ax = bc2(A.x), ay = bc2(A.y);
-    const float2 delta = fma2(ay, c[VG_DPY], fma2(ax, c[VG_DPX], c[VG_DE]));
-    const float2 cwr = fma2(ay, c[VG_PYR], mul2(ax, c[VG_PXR]));   // 2 Re w
-    const float2 cwi = fma2(ay, c[VG_PYI], mul2(ax, c[VG_PXI]));   // 2 Im w
-    const float2 im2 = sub2(mul2(cwi, y[D_ZR]), mul2(cwr, y[D_ZI]));  // 2 Im(w z*)
+    return {fma2(ay, c[VG_DPY], fma2(ax, c[VG_DPX], c[VG_DE])), fma2(ay, c[VG_PYR], mul2(ax, c[VG_PXR])),
+            fma2(ay, c[VG_PYI], mul2(ax, c[VG_PXI]))};
+}
+
+template <bool G1>
+__device__ __forceinline__ void vg_rhs2(const VgField2 &h, float2 hc0, const float2 (&y)[D_N], float2 ng1,
+                                        float2 ng2, float2 g2, float2 (&k)[D_N])
+{
+    const float2 im2 = sub2(mul2(h.cwi, y[D_ZR]), mul2(h.cwr, y[D_ZI]));  // 2 Im(w z*)
     k[D_DA] = G1 ? fma2(ng1, y[D_DA], im2) : im2;
-    const float2 hbma = sub2(c[VG_C0], y[D_DA]);                     // (rho_11 - rho_00) / 2
-    k[D_ZR] = fma2(hbma, cwi, fma2(delta, y[D_ZI], mul2(ng2, y[D_ZR])));
-    k[D_ZI] = fma2(hbma, cwr, fma2(delta, y[D_ZR], mul2(g2, y[D_ZI])));  // negated slope
+    const float2 hbma = sub2(hc0, y[D_DA]);                               // (rho_11 - rho_00) / 2
+    k[D_ZR] = fma2(hbma, h.cwi, fma2(h.d, y[D_ZI], mul2(ng2, y[D_ZR])));
+    k[D_ZI] = fma2(hbma, h.cwr, fma2(h.d, y[D_ZR], mul2(g2, y[D_ZI])));  // negated slope
 }
 
 template <int RK, bool G1>
@@ -362,7 +417,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
                                                        const SolveDev *__restrict__ solves, int tick, int S)
 {
     using TB = Tableau<RK>;
-    __shared__ double red_s[SUB][MAX_WARPS][NSLOT];
+    __shared__ RedStage red_s;
     const TileDev tl = tiles[blockIdx.x];
     const SolveDev &sd = solves[tl.solve];
     const int s0 = (tick - sd.admit_tick) * S;
@@ -375,7 +430,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
     const float2 *__restrict__ tab = static_cast<const float2 *>(sd.tab);
     const float2 ng1 = bc2(-float(sd.g1)), ng2 = bc2(-float(sd.g2)), g2 = bc2(float(sd.g2));
     double *partial = sd.partial;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     constexpr int slot[D_N] = {VG_DA, VG_ZR, VG_ZI};
     // sign of each component's slope as produced by vg_rhs2
     constexpr float sg[D_N] = {1.f, 1.f, -1.f};
@@ -400,9 +455,12 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
         y64[0][q] = ok0 ? st[(size_t)slot[q] * nkp + k0] : 0.0;
         y64[1][q] = ok1 ? st[(size_t)slot[q] * nkp + k1] : 0.0;
     }
+    // field terms at the start of the first step (see vg_start_row);
+    // afterwards the terms at t_s + dt of step s serve as step s+1's
+    VgField2 hstart = vg_field2(c, __ldg(tab + vg_start_row<TB>(s0)));
     float2 An[TB::NT];
 #pragma unroll
-    for (int i = 0; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)s0 * TB::NT + i);
+    for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)s0 * TB::NT + i);
     // The FP64 state is y64 = (rounded to FP32: yhi) and the FP32 sum `acc` of
     // the increments since the last fold; every FOLD steps acc is added to
     // y64 in FP64.  The stage input yhi + acc is rounded once, as float(y64)
@@ -416,19 +474,23 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
         acc[q] = make_float2(0.f, 0.f);
     }
     int since = 0;
+    TileReducer red(red_s);
 
     for (int s = s0; s < s1; ++s) {
-        float2 A[TB::NT];
+        VgField2 h[TB::NT];
+        h[0] = hstart;
 #pragma unroll
-        for (int i = 0; i < TB::NT; ++i) A[i] = An[i];
+        for (int i = 1; i < TB::NT; ++i) h[i] = vg_field2(c, An[i]);
+        hstart = h[TB::END];
         if (s + 1 < s1) {
 #pragma unroll
-            for (int i = 0; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)(s + 1) * TB::NT + i);
+            for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)(s + 1) * TB::NT + i);
         }
         float2 y0[D_N];
 #pragma unroll
         for (int q = 0; q < D_N; ++q) y0[q] = add2(yhi[q], acc[q]);
         // currents and occupations at t_s (antelope.cpp:309-334)
+        const int r = (s - s0) % SUB;
         {
             float2 t[7];
             t[0] = fma2(y0[D_ZR], c[VG_WQXR], mul2(y0[D_ZI], c[VG_WQXI]));
@@ -444,13 +506,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
             v[5] = -t[4].x - t[4].y;  // sum w db = -sum w da
             v[6] = t[5].x + t[5].y;
             v[7] = t[6].x + t[6].y;
-            const float y = warp_sum8f(v, lane);
-            const int r = (s - s0) % SUB;
-            if ((lane & 3) == 0) red_s[r][warp][lane >> 2] = double(y);
-            if (r == SUB - 1 || s == s1 - 1) {
-                TileReducer red{red_s};
-                red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
-            }
+            red.put(double(warp_sum8f(v, lane)), r);
         }
         // one RK step of both k-points
         float2 kk[TB::S][D_N], yy[D_N], inc[D_N];
@@ -464,7 +520,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
                     if (TB::a(i, m) != 0.0) t = fma2(bc2(sg[q] * float(TB::a(i, m))), kk[m][q], t);
                 yy[q] = t;
             }
-            vg_rhs2<G1>(c, A[TB::ti(i)], yy, ng1, ng2, g2, kk[i]);
+            vg_rhs2<G1>(h[TB::ti(i)], c[VG_C0], yy, ng1, ng2, g2, kk[i]);
 #pragma unroll
             for (int q = 0; q < D_N; ++q) {
                 const float2 bi = bc2(sg[q] * float(TB::b(i)));
@@ -484,6 +540,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
             }
             since = 0;
         }
+        if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
     }
 #pragma unroll
     for (int q = 0; q < D_N; ++q) {
@@ -536,7 +593,7 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
                                                     const SolveDev *__restrict__ solves, int tick, int S)
 {
     using TB = Tableau<RK>;
-    __shared__ double red_s[SUB][MAX_WARPS][NSLOT];
+    __shared__ RedStage red_s;
     const TileDev tl = tiles[blockIdx.x];
     const SolveDev &sd = solves[tl.solve];
     const int s0 = (tick - sd.admit_tick) * S;
@@ -567,7 +624,7 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
 #pragma unroll
     for (int q = 0; q < 4; ++q) y64[q] = ok ? st[(size_t)q * nkp + kidx] : 0.0;
     if (!ok) c[LW_CA0] = c[LW_CB0] = Real(1);  // padding lanes: a harmless k = 0 point, weight 0
-    TileReducer red{red_s};
+    TileReducer red(red_s);
 
     for (int s = s0; s < s1; ++s) {
         const Real *row = tab + (size_t)s * TB::NT * LW_NPHASE;
@@ -605,9 +662,7 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
             v[5] = w * (al - sz);
             v[6] = w * sx;
             v[7] = -w * sy;
-            const int r = (s - s0) % SUB;
-            red.push(v, r);
-            if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, sd.partial);
+            red.push(v, (s - s0) % SUB);
         }
         Real kk[TB::S][4], y[4], acc[4];
 #pragma unroll
@@ -630,6 +685,8 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) y64[q] = F64 ? double(acc[q]) : y64[q] + double(acc[q]);
+        const int r = (s - s0) % SUB;
+        if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, sd.partial);
     }
     if (ok)
 #pragma unroll
