@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <type_traits>
 
 #include "sbe_dev.h"
@@ -358,33 +359,21 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 }
 
 // Mixed method, velocity gauge, two k-points per thread packed into f32x2
-// registers: every RK instruction advances both.  The per-step current sums
-// are added across the pair and over the warp in FP32 (one conversion to
-// FP64 per lane per step instead of eight), then staged and summed over
-// warps in FP64 as in propagate_vg.  The state stays FP64.
-__device__ __forceinline__ float warp_sum8f(const float (&v)[8], int lane)
-{
-    const bool h4 = lane & 16, h2 = lane & 8, h1 = lane & 4;
-    float u[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        float send = h4 ? v[i] : v[i + 4];
-        float keep = h4 ? v[i + 4] : v[i];
-        u[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-    float x[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        float send = h2 ? u[i] : u[i + 2];
-        float keep = h2 ? u[i + 2] : u[i];
-        x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-    float send = h1 ? x[0] : x[1];
-    float y = (h1 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
-    y += __shfl_xor_sync(0xffffffffu, y, 2);
-    y += __shfl_xor_sync(0xffffffffu, y, 1);
-    return y;  // lanes 4*i hold the sum of v[i]
-}
+// registers: every RK instruction advances both.  The state stays FP64.
+//
+// The per-step current sums are reduced over the warp through shared memory
+// instead of a shuffle butterfly: each lane writes its 7 pair-summed values
+// (FP32) for the step into the warp's stage, and every XSTEP steps the warp
+// sums the staged rows -- lane l owns row (l & 15) >> 1, slot group l & 1,
+// and half l >> 4 of the source lanes, adds its 16 sources in FP32 (starting
+// at source l & 15, so the 8 lanes of each 16-byte load phase read 8
+// different bank groups), one shuffle adds the halves (64 k-points per FP32 sum, as a
+// warp butterfly would), and the FP64 value goes to the block stage that is
+// summed over warps every SUB steps.  Per step that costs two 16-byte stores
+// instead of 9 shuffles, 9 adds and 14 selects.
+constexpr int XSTEP = 8;                                // steps per warp-stage flush
+constexpr int XSTAGE_F4 = XSTEP * 2 * 32;               // float4s per warp stage
+constexpr int xstage_bytes(int threads) { return (threads / 32) * XSTAGE_F4 * 16; }
 
 // Packed field terms and right-hand side on (da, Re z, Im z) of two
 // k-points.  The factor 2 of 2 Im(w z*) and of (rho_11 - rho_00) w is folded
@@ -418,6 +407,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
 {
     using TB = Tableau<RK>;
     __shared__ RedStage red_s;
+    extern __shared__ float4 xstage_all[];
     const TileDev tl = tiles[blockIdx.x];
     const SolveDev &sd = solves[tl.solve];
     const int s0 = (tick - sd.admit_tick) * S;
@@ -430,7 +420,8 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
     const float2 *__restrict__ tab = static_cast<const float2 *>(sd.tab);
     const float2 ng1 = bc2(-float(sd.g1)), ng2 = bc2(-float(sd.g2)), g2 = bc2(float(sd.g2));
     double *partial = sd.partial;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float4 *const xst = xstage_all + warp * XSTAGE_F4;   // this warp's stage [XSTEP][2][32]
     constexpr int slot[D_N] = {VG_DA, VG_ZR, VG_ZI};
     // sign of each component's slope as produced by vg_rhs2
     constexpr float sg[D_N] = {1.f, 1.f, -1.f};
@@ -458,89 +449,113 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
     // field terms at the start of the first step (see vg_start_row);
     // afterwards the terms at t_s + dt of step s serve as step s+1's
     VgField2 hstart = vg_field2(c, __ldg(tab + vg_start_row<TB>(s0)));
+    const float2 *arow = tab + (size_t)s0 * TB::NT;   // field-table row of the current step
     float2 An[TB::NT];
 #pragma unroll
-    for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)s0 * TB::NT + i);
+    for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(arow + i);
     // The FP64 state is y64 = (rounded to FP32: yhi) and the FP32 sum `acc` of
-    // the increments since the last fold; every FOLD steps acc is added to
+    // the increments since the last fold; every XSTEP steps acc is added to
     // y64 in FP64.  The stage input yhi + acc is rounded once, as float(y64)
     // would be, and acc holds only a few increments, so the state keeps its
-    // FP64 accumulation while the f64<->f32 conversions drop FOLD-fold.
-    constexpr int FOLD = 8;
+    // FP64 accumulation while the f64<->f32 conversions drop XSTEP-fold.
     float2 yhi[D_N], acc[D_N];
 #pragma unroll
     for (int q = 0; q < D_N; ++q) {
         yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
         acc[q] = make_float2(0.f, 0.f);
     }
-    int since = 0;
     TileReducer red(red_s);
+    // warp-stage reduction role of this lane (see above)
+    const int xrow = (lane & 15) >> 1, xgrp = lane & 1, xsrc = (lane >> 4) * 16, xrot = lane & 15;
 
-    for (int s = s0; s < s1; ++s) {
-        VgField2 h[TB::NT];
-        h[0] = hstart;
+    for (int sb = s0; sb < s1; sb += SUB) {
+        const int nb = min(SUB, s1 - sb);
+#pragma unroll 1
+        for (int r = 0; r < nb; ++r) {
+            VgField2 h[TB::NT];
+            h[0] = hstart;
 #pragma unroll
-        for (int i = 1; i < TB::NT; ++i) h[i] = vg_field2(c, An[i]);
-        hstart = h[TB::END];
-        if (s + 1 < s1) {
+            for (int i = 1; i < TB::NT; ++i) h[i] = vg_field2(c, An[i]);
+            hstart = h[TB::END];
+            arow += TB::NT;
+            if (sb + r + 1 < s1) {
 #pragma unroll
-            for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(tab + (size_t)(s + 1) * TB::NT + i);
-        }
-        float2 y0[D_N];
-#pragma unroll
-        for (int q = 0; q < D_N; ++q) y0[q] = add2(yhi[q], acc[q]);
-        // currents and occupations at t_s (antelope.cpp:309-334)
-        const int r = (s - s0) % SUB;
-        {
-            float2 t[7];
-            t[0] = fma2(y0[D_ZR], c[VG_WQXR], mul2(y0[D_ZI], c[VG_WQXI]));
-            t[1] = fma2(y0[D_ZR], c[VG_WQYR], mul2(y0[D_ZI], c[VG_WQYI]));
-            t[2] = mul2(y0[D_DA], c[VG_WPX0]);
-            t[3] = mul2(y0[D_DA], c[VG_WPY0]);
-            t[4] = mul2(c[VG_W], y0[D_DA]);
-            t[5] = mul2(c[VG_W], y0[D_ZR]);
-            t[6] = mul2(c[VG_W], y0[D_ZI]);
-            float v[8];
-#pragma unroll
-            for (int q = 0; q < 5; ++q) v[q] = t[q].x + t[q].y;
-            v[5] = -t[4].x - t[4].y;  // sum w db = -sum w da
-            v[6] = t[5].x + t[5].y;
-            v[7] = t[6].x + t[6].y;
-            red.put(double(warp_sum8f(v, lane)), r);
-        }
-        // one RK step of both k-points
-        float2 kk[TB::S][D_N], yy[D_N], inc[D_N];
-#pragma unroll
-        for (int i = 0; i < TB::S; ++i) {
-#pragma unroll
-            for (int q = 0; q < D_N; ++q) {
-                float2 t = y0[q];
-#pragma unroll
-                for (int m = 0; m < i; ++m)
-                    if (TB::a(i, m) != 0.0) t = fma2(bc2(sg[q] * float(TB::a(i, m))), kk[m][q], t);
-                yy[q] = t;
+                for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(arow + i);
             }
-            vg_rhs2<G1>(h[TB::ti(i)], c[VG_C0], yy, ng1, ng2, g2, kk[i]);
+            float2 y0[D_N];
 #pragma unroll
-            for (int q = 0; q < D_N; ++q) {
-                const float2 bi = bc2(sg[q] * float(TB::b(i)));
-                if (i == 0) inc[q] = mul2(bi, kk[i][q]);
-                else if (TB::b(i) != 0.0) inc[q] = fma2(bi, kk[i][q], inc[q]);
+            for (int q = 0; q < D_N; ++q) y0[q] = add2(yhi[q], acc[q]);
+            const int xr = r & (XSTEP - 1);
+            // currents and occupations at t_s (antelope.cpp:309-334), summed
+            // over the pair and staged for the warp reduction
+            {
+                const float2 t0 = fma2(y0[D_ZR], c[VG_WQXR], mul2(y0[D_ZI], c[VG_WQXI]));
+                const float2 t1 = fma2(y0[D_ZR], c[VG_WQYR], mul2(y0[D_ZI], c[VG_WQYI]));
+                const float2 t2 = mul2(y0[D_DA], c[VG_WPX0]);
+                const float2 t3 = mul2(y0[D_DA], c[VG_WPY0]);
+                const float2 t4 = mul2(c[VG_W], y0[D_DA]);
+                const float2 t5 = mul2(c[VG_W], y0[D_ZR]);
+                const float2 t6 = mul2(c[VG_W], y0[D_ZI]);
+                xst[(xr * 2 + 0) * 32 + lane] = make_float4(t0.x + t0.y, t1.x + t1.y, t2.x + t2.y, t3.x + t3.y);
+                xst[(xr * 2 + 1) * 32 + lane] = make_float4(t4.x + t4.y, t5.x + t5.y, t6.x + t6.y, 0.f);
+            }
+            // one RK step of both k-points
+            float2 kk[TB::S][D_N], yy[D_N], inc[D_N];
+#pragma unroll
+            for (int i = 0; i < TB::S; ++i) {
+#pragma unroll
+                for (int q = 0; q < D_N; ++q) {
+                    float2 t = y0[q];
+#pragma unroll
+                    for (int m = 0; m < i; ++m)
+                        if (TB::a(i, m) != 0.0) t = fma2(bc2(sg[q] * float(TB::a(i, m))), kk[m][q], t);
+                    yy[q] = t;
+                }
+                vg_rhs2<G1>(h[TB::ti(i)], c[VG_C0], yy, ng1, ng2, g2, kk[i]);
+#pragma unroll
+                for (int q = 0; q < D_N; ++q) {
+                    const float2 bi = bc2(sg[q] * float(TB::b(i)));
+                    if (i == 0) inc[q] = mul2(bi, kk[i][q]);
+                    else if (TB::b(i) != 0.0) inc[q] = fma2(bi, kk[i][q], inc[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < D_N; ++q) acc[q] = add2(acc[q], inc[q]);
+            if (xr == XSTEP - 1 || r == nb - 1) {
+                // fold the FP32 increments into the FP64 state
+#pragma unroll
+                for (int q = 0; q < D_N; ++q) {
+                    y64[0][q] += double(acc[q].x);
+                    y64[1][q] += double(acc[q].y);
+                    yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+                    acc[q] = make_float2(0.f, 0.f);
+                }
+                // warp sums of the staged rows 0..xr
+                __syncwarp();
+                float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 *src = xst + (xrow * 2 + xgrp) * 32 + xsrc;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float4 b = src[(i + xrot) & 15];
+                    a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
+                }
+                a.x += __shfl_xor_sync(0xffffffffu, a.x, 16);
+                a.y += __shfl_xor_sync(0xffffffffu, a.y, 16);
+                a.z += __shfl_xor_sync(0xffffffffu, a.z, 16);
+                a.w += __shfl_xor_sync(0xffffffffu, a.w, 16);
+                __syncwarp();
+                if (lane < 16 && xrow <= xr) {
+                    double *dst = red.red[red.half][(r - xr) + xrow][warp];
+                    if (xgrp == 0) {
+                        dst[0] = double(a.x); dst[1] = double(a.y); dst[2] = double(a.z); dst[3] = double(a.w);
+                    } else {
+                        dst[4] = double(a.x); dst[5] = -double(a.x);   // sum w db = -sum w da
+                        dst[6] = double(a.y); dst[7] = double(a.z);
+                    }
+                }
             }
         }
-#pragma unroll
-        for (int q = 0; q < D_N; ++q) acc[q] = add2(acc[q], inc[q]);
-        if (++since == FOLD || s == s1 - 1) {
-#pragma unroll
-            for (int q = 0; q < D_N; ++q) {
-                y64[0][q] += double(acc[q].x);
-                y64[1][q] += double(acc[q].y);
-                yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
-                acc[q] = make_float2(0.f, 0.f);
-            }
-            since = 0;
-        }
-        if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, partial);
+        red.flush(nb, sb - s0, ntiles, tl.tile, partial);
     }
 #pragma unroll
     for (int q = 0; q < D_N; ++q) {
@@ -932,12 +947,33 @@ static cudaError_t launch_vg_t(const LaunchArgs &la, bool g1)
     SBE_CHECK_LAUNCH();
 }
 
+// The packed kernel's warp stages live in dynamic shared memory (64 KiB at
+// 256 threads, above the 48 KiB default): the limit is raised once per device
+// and kernel instance.
+template <int RK, bool G1>
+static cudaError_t launch_vg_x2_t(const LaunchArgs &la)
+{
+    constexpr int kMaxDev = 64;
+    static std::atomic<int> raised[kMaxDev];
+    const int bytes = xstage_bytes(la.threads);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+    if (raised[dev].load(std::memory_order_acquire) == 0) {
+        e = cudaFuncSetAttribute(propagate_vg_x2<RK, G1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 xstage_bytes(256));
+        if (e != cudaSuccess) return e;
+        raised[dev].store(1, std::memory_order_release);
+    }
+    propagate_vg_x2<RK, G1><<<la.ntiles, la.threads, bytes, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+    SBE_CHECK_LAUNCH();
+}
+
 template <int RK>
 static cudaError_t launch_vg_x2(const LaunchArgs &la, bool g1)
 {
-    if (g1) propagate_vg_x2<RK, true><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
-    else propagate_vg_x2<RK, false><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
-    SBE_CHECK_LAUNCH();
+    return g1 ? launch_vg_x2_t<RK, true>(la) : launch_vg_x2_t<RK, false>(la);
 }
 
 template <class Real, int RK>
