@@ -365,14 +365,15 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 // instead of a shuffle butterfly: each lane writes its 7 pair-summed values
 // (FP32) for the step into the warp's stage, and every XSTEP steps the warp
 // sums the staged rows -- lane l owns row (l & 15) >> 1, slot group l & 1,
-// and half l >> 4 of the source lanes, adds its 16 sources in FP32 (starting
-// at source l & 15, so the 8 lanes of each 16-byte load phase read 8
+// and half l >> 4 of the source lanes, adds its 16 sources in FP32 (stage
+// rows are 33 float4s long, so the 8 lanes of each 16-byte load phase read 8
 // different bank groups), one shuffle adds the halves (64 k-points per FP32 sum, as a
 // warp butterfly would), and the FP64 value goes to the block stage that is
 // summed over warps every SUB steps.  Per step that costs two 16-byte stores
 // instead of 9 shuffles, 9 adds and 14 selects.
 constexpr int XSTEP = 8;                                // steps per warp-stage flush
-constexpr int XSTAGE_F4 = XSTEP * 2 * 32;               // float4s per warp stage
+constexpr int XROW = 33;                                // float4s per stage row (32 lanes + 1 pad)
+constexpr int XSTAGE_F4 = XSTEP * 2 * XROW;             // float4s per warp stage
 constexpr int xstage_bytes(int threads) { return (threads / 32) * XSTAGE_F4 * 16; }
 
 // Packed field terms and right-hand side on (da, Re z, Im z) of two
@@ -454,8 +455,8 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
 #pragma unroll
     for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(arow + i);
     // The FP64 state is y64 = (rounded to FP32: yhi) and the FP32 sum `acc` of
-    // the increments since the last fold; every XSTEP steps acc is added to
-    // y64 in FP64.  The stage input yhi + acc is rounded once, as float(y64)
+    // the increments since the last fold (each step's b_i k_i are added onto
+    // it directly); every XSTEP steps acc is added to y64 in FP64.  The stage input yhi + acc is rounded once, as float(y64)
     // would be, and acc holds only a few increments, so the state keeps its
     // FP64 accumulation while the f64<->f32 conversions drop XSTEP-fold.
     float2 yhi[D_N], acc[D_N];
@@ -466,92 +467,98 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
     }
     TileReducer red(red_s);
     // warp-stage reduction role of this lane (see above)
-    const int xrow = (lane & 15) >> 1, xgrp = lane & 1, xsrc = (lane >> 4) * 16, xrot = lane & 15;
+    const int xrow = (lane & 15) >> 1, xgrp = lane & 1;
+    const float4 *const xsrc = xst + (lane & 15) * XROW + (lane >> 4) * 16;
+
+    // one time step s, staged in row j of the warp stage
+    auto step = [&](int j, int s) {
+        VgField2 h[TB::NT];
+        h[0] = hstart;
+#pragma unroll
+        for (int i = 1; i < TB::NT; ++i) h[i] = vg_field2(c, An[i]);
+        hstart = h[TB::END];
+        arow += TB::NT;
+        if (s + 1 < s1) {
+#pragma unroll
+            for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(arow + i);
+        }
+        float2 y0[D_N];
+#pragma unroll
+        for (int q = 0; q < D_N; ++q) y0[q] = add2(yhi[q], acc[q]);
+        // currents and occupations at t_s (antelope.cpp:309-334), summed
+        // over the pair and staged for the warp reduction
+        {
+            const float2 t0 = fma2(y0[D_ZR], c[VG_WQXR], mul2(y0[D_ZI], c[VG_WQXI]));
+            const float2 t1 = fma2(y0[D_ZR], c[VG_WQYR], mul2(y0[D_ZI], c[VG_WQYI]));
+            const float2 t2 = mul2(y0[D_DA], c[VG_WPX0]);
+            const float2 t3 = mul2(y0[D_DA], c[VG_WPY0]);
+            const float2 t4 = mul2(c[VG_W], y0[D_DA]);
+            const float2 t5 = mul2(c[VG_W], y0[D_ZR]);
+            const float2 t6 = mul2(c[VG_W], y0[D_ZI]);
+            xst[(j * 2 + 0) * XROW + lane] = make_float4(t0.x + t0.y, t1.x + t1.y, t2.x + t2.y, t3.x + t3.y);
+            xst[(j * 2 + 1) * XROW + lane] = make_float4(t4.x + t4.y, t5.x + t5.y, t6.x + t6.y, 0.f);
+        }
+        // one RK step of both k-points
+        float2 kk[TB::S][D_N], yy[D_N];
+#pragma unroll
+        for (int i = 0; i < TB::S; ++i) {
+#pragma unroll
+            for (int q = 0; q < D_N; ++q) {
+                float2 t = y0[q];
+#pragma unroll
+                for (int m = 0; m < i; ++m)
+                    if (TB::a(i, m) != 0.0) t = fma2(bc2(sg[q] * float(TB::a(i, m))), kk[m][q], t);
+                yy[q] = t;
+            }
+            vg_rhs2<G1>(h[TB::ti(i)], c[VG_C0], yy, ng1, ng2, g2, kk[i]);
+            // the step increment sum_i b_i k_i goes straight onto acc
+#pragma unroll
+            for (int q = 0; q < D_N; ++q)
+                if (TB::b(i) != 0.0) acc[q] = fma2(bc2(sg[q] * float(TB::b(i))), kk[i][q], acc[q]);
+        }
+    };
 
     for (int sb = s0; sb < s1; sb += SUB) {
         const int nb = min(SUB, s1 - sb);
+        for (int r8 = 0; r8 < nb; r8 += XSTEP) {
+            const int m = min(XSTEP, nb - r8);
+            if (m == XSTEP) {
+#pragma unroll
+                for (int j = 0; j < XSTEP; ++j) step(j, sb + r8 + j);
+            } else {
 #pragma unroll 1
-        for (int r = 0; r < nb; ++r) {
-            VgField2 h[TB::NT];
-            h[0] = hstart;
-#pragma unroll
-            for (int i = 1; i < TB::NT; ++i) h[i] = vg_field2(c, An[i]);
-            hstart = h[TB::END];
-            arow += TB::NT;
-            if (sb + r + 1 < s1) {
-#pragma unroll
-                for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(arow + i);
+                for (int j = 0; j < m; ++j) step(j, sb + r8 + j);
             }
-            float2 y0[D_N];
+            // fold the FP32 increments into the FP64 state
 #pragma unroll
-            for (int q = 0; q < D_N; ++q) y0[q] = add2(yhi[q], acc[q]);
-            const int xr = r & (XSTEP - 1);
-            // currents and occupations at t_s (antelope.cpp:309-334), summed
-            // over the pair and staged for the warp reduction
-            {
-                const float2 t0 = fma2(y0[D_ZR], c[VG_WQXR], mul2(y0[D_ZI], c[VG_WQXI]));
-                const float2 t1 = fma2(y0[D_ZR], c[VG_WQYR], mul2(y0[D_ZI], c[VG_WQYI]));
-                const float2 t2 = mul2(y0[D_DA], c[VG_WPX0]);
-                const float2 t3 = mul2(y0[D_DA], c[VG_WPY0]);
-                const float2 t4 = mul2(c[VG_W], y0[D_DA]);
-                const float2 t5 = mul2(c[VG_W], y0[D_ZR]);
-                const float2 t6 = mul2(c[VG_W], y0[D_ZI]);
-                xst[(xr * 2 + 0) * 32 + lane] = make_float4(t0.x + t0.y, t1.x + t1.y, t2.x + t2.y, t3.x + t3.y);
-                xst[(xr * 2 + 1) * 32 + lane] = make_float4(t4.x + t4.y, t5.x + t5.y, t6.x + t6.y, 0.f);
+            for (int q = 0; q < D_N; ++q) {
+                y64[0][q] += double(acc[q].x);
+                y64[1][q] += double(acc[q].y);
+                yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+                acc[q] = make_float2(0.f, 0.f);
             }
-            // one RK step of both k-points
-            float2 kk[TB::S][D_N], yy[D_N], inc[D_N];
+            // warp sums of the m staged rows
+            __syncwarp();
+            float2 alo = make_float2(0.f, 0.f), ahi = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int i = 0; i < TB::S; ++i) {
-#pragma unroll
-                for (int q = 0; q < D_N; ++q) {
-                    float2 t = y0[q];
-#pragma unroll
-                    for (int m = 0; m < i; ++m)
-                        if (TB::a(i, m) != 0.0) t = fma2(bc2(sg[q] * float(TB::a(i, m))), kk[m][q], t);
-                    yy[q] = t;
-                }
-                vg_rhs2<G1>(h[TB::ti(i)], c[VG_C0], yy, ng1, ng2, g2, kk[i]);
-#pragma unroll
-                for (int q = 0; q < D_N; ++q) {
-                    const float2 bi = bc2(sg[q] * float(TB::b(i)));
-                    if (i == 0) inc[q] = mul2(bi, kk[i][q]);
-                    else if (TB::b(i) != 0.0) inc[q] = fma2(bi, kk[i][q], inc[q]);
-                }
+            for (int i = 0; i < 16; ++i) {
+                const float4 b = xsrc[i];
+                alo = add2(alo, make_float2(b.x, b.y));
+                ahi = add2(ahi, make_float2(b.z, b.w));
             }
-#pragma unroll
-            for (int q = 0; q < D_N; ++q) acc[q] = add2(acc[q], inc[q]);
-            if (xr == XSTEP - 1 || r == nb - 1) {
-                // fold the FP32 increments into the FP64 state
-#pragma unroll
-                for (int q = 0; q < D_N; ++q) {
-                    y64[0][q] += double(acc[q].x);
-                    y64[1][q] += double(acc[q].y);
-                    yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
-                    acc[q] = make_float2(0.f, 0.f);
-                }
-                // warp sums of the staged rows 0..xr
-                __syncwarp();
-                float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-                const float4 *src = xst + (xrow * 2 + xgrp) * 32 + xsrc;
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float4 b = src[(i + xrot) & 15];
-                    a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
-                }
-                a.x += __shfl_xor_sync(0xffffffffu, a.x, 16);
-                a.y += __shfl_xor_sync(0xffffffffu, a.y, 16);
-                a.z += __shfl_xor_sync(0xffffffffu, a.z, 16);
-                a.w += __shfl_xor_sync(0xffffffffu, a.w, 16);
-                __syncwarp();
-                if (lane < 16 && xrow <= xr) {
-                    double *dst = red.red[red.half][(r - xr) + xrow][warp];
-                    if (xgrp == 0) {
-                        dst[0] = double(a.x); dst[1] = double(a.y); dst[2] = double(a.z); dst[3] = double(a.w);
-                    } else {
-                        dst[4] = double(a.x); dst[5] = -double(a.x);   // sum w db = -sum w da
-                        dst[6] = double(a.y); dst[7] = double(a.z);
-                    }
+            float4 a = make_float4(alo.x, alo.y, ahi.x, ahi.y);
+            a.x += __shfl_xor_sync(0xffffffffu, a.x, 16);
+            a.y += __shfl_xor_sync(0xffffffffu, a.y, 16);
+            a.z += __shfl_xor_sync(0xffffffffu, a.z, 16);
+            a.w += __shfl_xor_sync(0xffffffffu, a.w, 16);
+            __syncwarp();
+            if (lane < 16 && xrow < m) {
+                double *dst = red.red[red.half][r8 + xrow][warp];
+                if (xgrp == 0) {
+                    dst[0] = double(a.x); dst[1] = double(a.y); dst[2] = double(a.z); dst[3] = double(a.w);
+                } else {
+                    dst[4] = double(a.x); dst[5] = -double(a.x);   // sum w db = -sum w da
+                    dst[6] = double(a.y); dst[7] = double(a.z);
                 }
             }
         }
