@@ -72,6 +72,9 @@ def lib():
         _lib.orc_get_dims.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcDims)]
         _lib.orc_run.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.POINTER(C.c_long)]
+        _lib.orc_run_shots.argtypes = [C.POINTER(OrcProblem), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_long), C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_shot_dims.argtypes = [C.POINTER(OrcProblem), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         _lib.orc_laser_eval.argtypes = [C.POINTER(OrcProblem), C.c_double, C.c_void_p, C.c_void_p]
         _lib.orc_kgrid.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p]
         _lib.orc_model_hj.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p, C.c_void_p]
@@ -188,10 +191,22 @@ def dims(case: dict) -> dict:
     return {f: getattr(d, f) for f, _ in OrcDims._fields_}
 
 
+def shot_dims(case: dict):
+    """(interval F, number of snapshots) for the case's calc.shotNumber."""
+    p = to_problem(case)
+    every, n = C.c_int(0), C.c_int(0)
+    rc = lib().orc_shot_dims(C.byref(p), int(case["calc"].get("shotNumber", 0)), C.byref(every), C.byref(n))
+    if rc != 0:
+        raise ValueError(f"no snapshot interval for this case ({rc})")
+    return every.value, n.value
+
+
 def run(case: dict, nthreads: int = 1) -> dict:
     """Propagate a case on the CPU.  Returns the arrays the reference writes:
     ``inter``/``intra`` [Nt,3] (already times dV), ``occ`` [Nt,N] and the raw
-    weighted density-matrix integral ``dmi`` [Nt,N,N] (complex)."""
+    weighted density-matrix integral ``dmi`` [Nt,N,N] (complex).  With
+    calc.shotNumber > 0 also the snapshots: ``occ1d`` [nshots,N0] and the
+    per-k ``nc`` [nshots,Ntotal] and ``pi`` [nshots,Ntotal] (complex)."""
     p = to_problem(case, nthreads)
     d = dims(case)
     Nt, N = d["Nt"], d["nband"]
@@ -199,12 +214,24 @@ def run(case: dict, nthreads: int = 1) -> dict:
     intra = np.zeros((Nt, 3))
     dmi = np.zeros((Nt, N, N), dtype=np.complex128)
     steps = C.c_long(0)
-    rc = lib().orc_run(C.byref(p), _ptr(inter), _ptr(intra), _ptr(dmi), C.byref(steps))
+    shots = int(case["calc"].get("shotNumber", 0))
+    out = {}
+    if shots > 0:
+        _, ns = shot_dims(case)
+        n0 = int(case["calc"]["Npoints"][0])
+        occ1d = np.zeros((ns, n0))
+        nc = np.zeros((ns, d["ntotal"]))
+        pi = np.zeros((ns, d["ntotal"]), dtype=np.complex128)
+        rc = lib().orc_run_shots(C.byref(p), shots, _ptr(inter), _ptr(intra), _ptr(dmi), C.byref(steps),
+                                 _ptr(occ1d), _ptr(nc), _ptr(pi))
+        out = {"occ1d": occ1d, "nc": nc, "pi": pi}
+    else:
+        rc = lib().orc_run(C.byref(p), _ptr(inter), _ptr(intra), _ptr(dmi), C.byref(steps))
     if rc != 0:
         raise RuntimeError(f"oracle run failed ({rc})")
     occ = np.real(np.einsum("tii->ti", dmi)) / d["ntotal"]
     return {"inter": inter, "intra": intra, "dmi": dmi, "occ": occ, "dims": d,
-            "steps": steps.value}
+            "steps": steps.value, **out}
 
 
 def laser_eval(case: dict, t: float):
@@ -263,11 +290,20 @@ def run_reference(case: dict, workdir: str, env: dict | None = None, timeout: fl
 
 
 def read_outputs(workdir: str) -> dict:
+    """The reference's output files as arrays; the snapshot files
+    (antelope.cpp:288-292, 416-421) when they exist: ``occ1d`` [nshots,N0]
+    (text), ``nc`` (binary doubles) and ``pi`` (binary complex doubles) as flat
+    arrays of nshots * Ntotal values."""
     def load(name):
         return np.loadtxt(os.path.join(workdir, name), ndmin=2)
 
-    return {"inter": load("interband_dipole_full_evol.dat"),
-            "intra": load("intraband_current_full_evol.dat"),
-            "occ_file": load("occupation__full__evol.dat"),
-            "coh_file": load("coherence__full__evol.dat"),
-            "laser": load("outlaserdata.dat")}
+    out = {"inter": load("interband_dipole_full_evol.dat"),
+           "intra": load("intraband_current_full_evol.dat"),
+           "occ_file": load("occupation__full__evol.dat"),
+           "coh_file": load("coherence__full__evol.dat"),
+           "laser": load("outlaserdata.dat")}
+    if os.path.exists(os.path.join(workdir, "occupation_1d_integration.dat")):
+        out["occ1d"] = load("occupation_1d_integration.dat")
+        out["nc"] = np.fromfile(os.path.join(workdir, "fisrt_conduction.dat"), dtype=np.float64)
+        out["pi"] = np.fromfile(os.path.join(workdir, "fisrt_coherence.dat"), dtype=np.complex128)
+    return out

@@ -542,6 +542,11 @@ typedef struct {
     cplx *dmi;             /* [Nt][NN] */
     long steps;
     int err;
+    /* density snapshots (antelope.cpp:340-422): every shot_every steps */
+    int shot_every;
+    double *occ1d;         /* this worker's partial sums [nshots][N0] */
+    double *nc;            /* [nshots][Ntotal], shared, written at global k */
+    double *pi;            /* [nshots][Ntotal][2], shared */
 } worker_t;
 
 /* SBEs::GenDifferentialDM (SBEs.h:762-872) */
@@ -683,6 +688,50 @@ static void init_k(worker_t *W, int kl)
     }
 }
 
+/* Snapshot of step n (antelope.cpp:340-422), taken after every k of the
+ * worker has advanced past t_n.  The conduction occupation rho'[Nval][Nval]
+ * and the coherence rho'[Nval][Nval-1] are read from rho' = rho in the band
+ * basis (velocity gauge) or rho' = U^dag rho U with U the eigenvectors of
+ * H0(k + A(t_n)) (length gauge: SBEs::WannierToHamiltonian, SBEs.h:927-940,
+ * evaluated at the time of the step's start, as the reference calls it).
+ * The 1-D integration adds w rho'_cc into the bin of the first k index
+ * (antelope.cpp:343-370).  The per-k values are stored at each k's own index:
+ * the reference's own loop (antelope.cpp:384-400) indexes them with a stale
+ * k index, so its binary files hold one k-point's value (velocity gauge) or
+ * unset memory (length gauge) everywhere but at the last k of each rank. */
+static void snapshot(worker_t *W, int n)
+{
+    int N = W->N, NN = N * N, nk = W->k1 - W->k0, nv = W->m->nval;
+    const grid_t *g = W->g;
+    int shot = n / W->shot_every;
+    double t = W->L->atmin + W->L->dt * n, A[3];
+    laser_AE(W->L, t, A, NULL);
+    for (int kl = 0; kl < nk; ++kl) {
+        const cplx *rho = W->rho + (size_t)kl * NN;
+        cplx r[MAXNN];
+        if (W->gauge == ORC_GAUGE_LENGTH_WANNIER) {
+            const double *k = W->kpt + 3 * kl;
+            double kt[3] = {k[0] + A[0], k[1] + A[1], k[2] + A[2]};
+            cplx H0[MAXNN], U[MAXNN], Uh[MAXNN], tmp[MAXNN];
+            double ev[ORC_MAX_BANDS];
+            model_H(W->m, kt, H0);
+            eigh(N, H0, ev, U);
+            dagger(Uh, U, N);
+            matmul(tmp, rho, U, N);
+            matmul(r, Uh, tmp, N);
+        } else {
+            memcpy(r, rho, sizeof(cplx) * NN);
+        }
+        int kg = W->k0 + kl;
+        double cc = creal(r[nv * N + nv]);
+        cplx cv = r[nv * N + nv - 1];
+        W->occ1d[(size_t)shot * g->N[0] + kg / (g->N[1] * g->N[2])] += cc * W->wgt[kl];
+        W->nc[(size_t)shot * g->Ntotal + kg] = cc;
+        W->pi[2 * ((size_t)shot * g->Ntotal + kg)] = creal(cv);
+        W->pi[2 * ((size_t)shot * g->Ntotal + kg) + 1] = cimag(cv);
+    }
+}
+
 /* SBEs::RunSBEs (SBEs.h:596-624) for one k and one step of size h */
 static void rk_step(const worker_t *W, int kl, double t, double h, cplx *rho, cplx *errv)
 {
@@ -729,6 +778,7 @@ static void *worker_run(void *arg)
             for (int i = 0; i < NN; ++i) W->dmi[(size_t)n * NN + i] += rho[i] * w;
             rk_step(W, kl, t, W->L->dt, rho, NULL);
         }
+        if (W->shot_every > 0 && n % W->shot_every == 0) snapshot(W, n);
     }
     W->steps = W->Nt;
     return NULL;
@@ -792,6 +842,7 @@ static int run_adaptive(worker_t *W)
             }
         }
         if (guard >= 100000) { free(trial); return -1; }
+        if (W->shot_every > 0 && n % W->shot_every == 0) snapshot(W, n);
     }
     W->steps = steps;
     free(trial);
@@ -826,7 +877,32 @@ static void para_range(int total, int size, int rank, int *s, int *e)   /* utili
     *e = *s + w1 + (w2 > rank ? 1 : 0);
 }
 
+/* shotFrequency of antelope.cpp:274-278: steps between snapshots, from the
+ * first pulse's period (laser.h:75) */
+static int shot_every(const laser_t *L, int shot_number)
+{
+    if (shot_number <= 0) return 0;
+    return (int)(L->p[0].period0 / shot_number / L->dt);
+}
+
+int orc_shot_dims(const orc_problem *p, int shot_number, int *every, int *nshots)
+{
+    laser_t L;
+    if (laser_build(&L, p)) return -1;
+    int F = shot_every(&L, shot_number);
+    if (shot_number > 0 && F <= 0) return -3;   /* ktime % 0 in the reference */
+    if (every) *every = F;
+    if (nshots) *nshots = F > 0 ? (L.Nt - 1) / F + 1 : 0;
+    return 0;
+}
+
 int orc_run(const orc_problem *p, double *inter, double *intra, double *dmi, long *steps_taken)
+{
+    return orc_run_shots(p, 0, inter, intra, dmi, steps_taken, NULL, NULL, NULL);
+}
+
+int orc_run_shots(const orc_problem *p, int shot_number, double *inter, double *intra, double *dmi,
+                  long *steps_taken, double *occ1d, double *nc, double *pi)
 {
     laser_t L;
     model_t m;
@@ -834,8 +910,11 @@ int orc_run(const orc_problem *p, double *inter, double *intra, double *dmi, lon
     tableau_t T;
     if (laser_build(&L, p) || model_build(&m, p) || tableau_build(&T, p->rk)) return -1;
     if (p->gauge == ORC_GAUGE_LENGTH_HAMILTONIAN) { model_free(&m); return -2; } /* SBEs.h:806-810 */
+    const int F = shot_every(&L, shot_number);
+    if (shot_number > 0 && (F <= 0 || !occ1d || !nc || !pi)) { model_free(&m); return -3; }
     grid_build(&g, p, &m);
     int N = m.N, NN = N * N, Nt = L.Nt;
+    const int nshots = F > 0 ? (Nt - 1) / F + 1 : 0;
     int nth = T.adaptive ? 1 : (p->nthreads > 0 ? p->nthreads : 1);
     if (nth > g.Ntotal) nth = g.Ntotal;
     worker_t *W = calloc((size_t)nth, sizeof(worker_t));
@@ -858,6 +937,10 @@ int orc_run(const orc_problem *p, double *inter, double *intra, double *dmi, lon
         w->inter = calloc((size_t)Nt * 3, sizeof(double));
         w->intra = calloc((size_t)Nt * 3, sizeof(double));
         w->dmi = calloc((size_t)Nt * NN, sizeof(cplx));
+        w->shot_every = F;
+        w->occ1d = calloc((size_t)nshots * g.N[0] + 1, sizeof(double));
+        w->nc = nc;
+        w->pi = pi;
     }
     if (T.adaptive) rc = run_adaptive(&W[0]);
     else {
@@ -881,10 +964,18 @@ int orc_run(const orc_problem *p, double *inter, double *intra, double *dmi, lon
             dmi[2 * ((size_t)n * NN + i) + 1] = cimag(s);
         }
     }
+    /* 1-D integrated occupation: rank-ordered sum, real part over Nk[1]
+     * (antelope.cpp:354-370) */
+    for (int sh = 0; sh < nshots; ++sh)
+        for (int i = 0; i < g.N[0]; ++i) {
+            double s = 0;
+            for (int r = 0; r < nth; ++r) s += W[r].occ1d[(size_t)sh * g.N[0] + i];
+            occ1d[(size_t)sh * g.N[0] + i] = s / (double)g.N[1];
+        }
     if (steps_taken) *steps_taken = W[0].steps;
     for (int r = 0; r < nth; ++r) {
         free(W[r].rho); free(W[r].init); free(W[r].P); free(W[r].eps); free(W[r].kpt);
-        free(W[r].wgt); free(W[r].inter); free(W[r].intra); free(W[r].dmi);
+        free(W[r].wgt); free(W[r].inter); free(W[r].intra); free(W[r].dmi); free(W[r].occ1d);
     }
     free(W);
     free(th);

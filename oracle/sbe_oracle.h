@@ -90,6 +90,20 @@ int orc_get_dims(const orc_problem *p, orc_dims *out);
  * Returns 0 on success, nonzero on a bad problem. */
 int orc_run(const orc_problem *p, double *inter, double *intra, double *dmi, long *steps_taken);
 
+/* Density snapshots (calc.shotNumber > 0, antelope.cpp:267-422): every
+ * F = int(period0 / shot_number / dt) steps (period0 of the first pulse), after
+ * the step n with n % F == 0:
+ *   occ1d[nshots*N0]  occupation_1d_integration.dat: Re sum_k w_k rho'_cc over the
+ *                     k with first index i, divided by Nk[1];
+ *   nc[nshots*Ntotal] fisrt_conduction.dat: rho'_cc per k (each k's own value);
+ *   pi[nshots*Ntotal*2] fisrt_coherence.dat: rho'[Nval][Nval-1] per k, complex;
+ * rho' = rho (velocity gauge, band basis) or U^dag rho U at k + A(t_n) (length
+ * gauge).  nshots = (Nt - 1) / F + 1.  orc_shot_dims returns -3 when F is 0
+ * (the reference then takes ktime % 0). */
+int orc_shot_dims(const orc_problem *p, int shot_number, int *every, int *nshots);
+int orc_run_shots(const orc_problem *p, int shot_number, double *inter, double *intra, double *dmi,
+                  long *steps_taken, double *occ1d, double *nc, double *pi);
+
 /* Building blocks exported for unit tests. */
 void orc_laser_eval(const orc_problem *p, double t, double *A3, double *E3);
 int orc_kgrid(const orc_problem *p, double *k3, double *w);

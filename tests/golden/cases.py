@@ -118,5 +118,16 @@ MATERIAL_CASES.update({"haldane2l_w_2h_t1bottom": _h2l, "wilsonmass_v_default_a1
 BAND_GROUPS = {"kanemele_v_t1_no_rashba": [[0, 1], [2, 3]],
                "tmdcs_v_wse2_soc": [[0, 1], [2, 3], [4, 5]]}
 
+# Density snapshots (calc.shotNumber, antelope.cpp:267-422): the 1-D integrated
+# conduction occupation and the per-k conduction occupation and coherence
+# every int(period0 / shotNumber / dt) steps.
+_km_shots = material("KaneMele", "Wannier", calc__shotNumber=2)
+SNAPSHOT_CASES = {
+    "vg_shots": variant(calc__shotNumber=4),
+    "lw_shots": variant(top__gauge="Wannier", calc__shotNumber=3, calc__Npoints=[7, 6]),
+    "vg_shots_fermi_t1": variant(Haldane__Ef=0.0, calc__T1=150.0, calc__shotNumber=5, pulse__ellip=0.3),
+    "kanemele_w_shots": _km_shots,
+}
+
 # A one-cycle case whose output files are kept verbatim (byte format pin).
 TEXT_CASE = variant(pulse__ncycles=1.0, pulse__w0=0.114, calc__Npoints=[5, 6])
