@@ -123,10 +123,33 @@ class Problem:
         _check(lib.sbe_problem_model(self._h, C.byref(m)))
         return out
 
+    def snapshot_dims(self) -> dict:
+        """Snapshot interval (steps), number of snapshots and Npoints[0]
+        (``sbe_problem_snapshots``; zeros when calc.shotNumber <= 0)."""
+        v = [C.c_int() for _ in range(3)]
+        _check(lib.sbe_problem_snapshots(self._h, *[C.byref(x) for x in v]))
+        return {"interval": v[0].value, "nshots": v[1].value, "n0": v[2].value}
+
     def __del__(self):
         if getattr(self, "_h", None):
             lib.sbe_problem_destroy(self._h)
             self._h = None
+
+
+def _snapshot_arrays(problem: "Problem", nk: int):
+    sd = problem.snapshot_dims()
+    ns = sd["nshots"]
+    return (np.zeros((ns, sd["n0"])), np.zeros((ns, nk)), np.zeros((ns, nk), dtype=np.complex128))
+
+
+def write_snapshots(problem: "Problem", snaps: dict, out_dir: str):
+    """The reference's snapshot files from ``snapshots()`` arrays
+    (``sbe_write_snapshots``)."""
+    occ1d = np.ascontiguousarray(snaps["occ1d"], dtype=np.float64)
+    nc = np.ascontiguousarray(snaps["nc"], dtype=np.float64)
+    pi = np.ascontiguousarray(snaps["pi"], dtype=np.complex128)
+    _check(lib.sbe_write_snapshots(problem._h, occ1d.ctypes.data, nc.ctypes.data, pi.ctypes.data,
+                                   os.fsencode(out_dir)))
 
 
 class Solver:
@@ -135,6 +158,7 @@ class Solver:
 
     def __init__(self, problem: Problem, k_slice: tuple[int, int] | None = None, **opts):
         self.problem = problem
+        self._k_slice = k_slice
         self._h = P()
         if k_slice is None:
             _check(lib.sbe_solver_create(problem._h, C.byref(_opts(**opts)), C.byref(self._h)))
@@ -163,6 +187,15 @@ class Solver:
         out = np.zeros((self.problem.dims.Nt + 1, lib.sbe_sums_width(self.problem._h)))
         _check(lib.sbe_solver_sums(self._h, out.ctypes.data))
         return out
+
+    def snapshots(self) -> dict:
+        """Density snapshots of the finished run (``sbe_solver_snapshots``):
+        occ1d [nshots, Npoints[0]], per-k nc [nshots, nk] and pi [nshots, nk]
+        (complex)."""
+        nk = self._k_slice[1] - self._k_slice[0] if self._k_slice else self.problem.ntotal
+        occ1d, nc, pi = _snapshot_arrays(self.problem, nk)
+        _check(lib.sbe_solver_snapshots(self._h, occ1d.ctypes.data, nc.ctypes.data, pi.ctypes.data))
+        return {"occ1d": occ1d, "nc": nc, "pi": pi}
 
     def harmonics(self, w0: float, hmax: int) -> np.ndarray:
         """Band powers of harmonic orders 1..hmax, computed on the GPU
@@ -243,6 +276,12 @@ class Batch:
         out = Outputs.empty(self.problems[i].dims)
         _check(lib.sbe_batch_get(self._h, i, C.byref(out.c())))
         return out
+
+    def snapshots(self, i: int) -> dict:
+        """Density snapshots of solve i (``sbe_batch_snapshots``)."""
+        occ1d, nc, pi = _snapshot_arrays(self.problems[i], self.problems[i].ntotal)
+        _check(lib.sbe_batch_snapshots(self._h, i, occ1d.ctypes.data, nc.ctypes.data, pi.ctypes.data))
+        return {"occ1d": occ1d, "nc": nc, "pi": pi}
 
     def harmonics(self, i: int, w0: float, hmax: int) -> np.ndarray:
         """Band powers of harmonic orders 1..hmax of solve i, on the GPU."""

@@ -61,7 +61,11 @@ def _load():
         "sbe_problem_dims": (C.c_int, [P, C.POINTER(Dims)]),
         "sbe_problem_laser": (C.c_int, [P, C.c_void_p]),
         "sbe_problem_model": (C.c_int, [P, C.POINTER(Model)]),
+        "sbe_problem_snapshots": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "sbe_problem_destroy": (None, [P]),
+        "sbe_solver_snapshots": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "sbe_batch_snapshots": (C.c_int, [P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "sbe_write_snapshots": (C.c_int, [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p]),
         "sbe_solver_create": (C.c_int, [P, C.POINTER(Opts), C.POINTER(P)]),
         "sbe_solver_run": (C.c_int, [P, C.c_void_p]),
         "sbe_solver_get": (C.c_int, [P, C.POINTER(COutputs)]),

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <fstream>
@@ -213,6 +214,15 @@ extern "C" sbe_status sbe_problem_model(const sbe_problem *p, sbe_model *m)
     return SBE_OK;
 }
 
+extern "C" sbe_status sbe_problem_snapshots(const sbe_problem *p, int *interval, int *nshots, int *n0)
+{
+    if (!p) return fail(SBE_INVALID_ARGUMENT, "null problem");
+    if (interval) *interval = p->p.shot_every();
+    if (nshots) *nshots = p->p.nshots();
+    if (n0) *n0 = p->p.Nk[0];
+    return SBE_OK;
+}
+
 extern "C" void sbe_problem_destroy(sbe_problem *p) { delete p; }
 
 // ================================================================= solver
@@ -394,6 +404,19 @@ extern "C" sbe_status sbe_solver_kernel_times(sbe_solver *s, double *pms, int *p
     });
 }
 
+extern "C" sbe_status sbe_solver_snapshots(sbe_solver *s, double *occ1d, double *nc, double *pi)
+{
+    if (!s) return fail(SBE_INVALID_ARGUMENT, "null solver");
+    if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
+    return guard([&]() -> sbe_status {
+        if (!s->eng) return fail(SBE_UNSUPPORTED, "density snapshots are built for the Haldane model");
+        cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
+        if (s->eng->snapshots(s->id, occ1d, nc, pi) == 0)
+            return fail(SBE_INVALID_ARGUMENT, "the problem takes no snapshots (calc.shotNumber <= 0)");
+        return SBE_OK;
+    });
+}
+
 extern "C" sbe_status sbe_solver_harmonics(sbe_solver *s, double w0, int hmax, double *band_power)
 {
     if (!s || !band_power) return fail(SBE_INVALID_ARGUMENT, "null argument");
@@ -441,6 +464,37 @@ extern "C" sbe_status sbe_write_outputs(const sbe_problem *p, const sbe_outputs 
     });
 }
 
+// The snapshot files of antelope.cpp:288-292, 365-368, 416-421:
+// occupation_1d_integration.dat rows of "%16e    " values, the binary
+// fisrt_conduction.dat (doubles) and fisrt_coherence.dat (complex doubles),
+// and snapshot_log.dat, which the reference opens and never writes.
+extern "C" sbe_status sbe_write_snapshots(const sbe_problem *p, const double *occ1d, const double *nc,
+                                          const double *pi, const char *dir)
+{
+    if (!p || !occ1d || !nc || !pi) return fail(SBE_INVALID_ARGUMENT, "all three snapshot arrays are needed");
+    const Problem &q = p->p;
+    const int ns = q.nshots();
+    if (ns == 0) return fail(SBE_INVALID_ARGUMENT, "the problem takes no snapshots (calc.shotNumber <= 0)");
+    const std::string d = (dir && *dir) ? std::string(dir) + "/" : std::string();
+    FILE *f1 = fopen((d + "occupation_1d_integration.dat").c_str(), "w");
+    FILE *f2 = fopen((d + "fisrt_conduction.dat").c_str(), "w");
+    FILE *f3 = fopen((d + "fisrt_coherence.dat").c_str(), "w");
+    FILE *f4 = fopen((d + "snapshot_log.dat").c_str(), "w");
+    const bool ok = f1 && f2 && f3 && f4;
+    if (ok) {
+        const size_t nt = (size_t)q.ntotal();
+        for (int k = 0; k < ns; ++k) {
+            for (int m = 0; m < q.Nk[0]; ++m) fprintf(f1, "%16e    ", occ1d[(size_t)k * q.Nk[0] + m]);
+            fprintf(f1, "\n");
+            fwrite(nc + (size_t)k * nt, sizeof(double), nt, f2);
+            fwrite(pi + (size_t)k * nt * 2, sizeof(double), nt * 2, f3);
+        }
+    }
+    for (FILE *f : {f1, f2, f3, f4})
+        if (f) fclose(f);
+    return ok ? SBE_OK : fail(SBE_INVALID_ARGUMENT, "cannot open the snapshot files in " + d);
+}
+
 extern "C" sbe_status sbe_run_cfg(const char *cfg_path, const char *out_dir, const sbe_opts *opts)
 {
     sbe_problem *p = nullptr;
@@ -455,7 +509,14 @@ extern "C" sbe_status sbe_run_cfg(const char *cfg_path, const char *out_dir, con
     std::vector<double> inter(Nt * 3), intra(Nt * 3), occ(Nt * (N + 1)), coh(Nt * 2), laser(Nt * 7);
     sbe_outputs o{inter.data(), intra.data(), occ.data(), coh.data(), laser.data()};
     if (sbe_status st = sbe_solver_get(s, &o)) return st;
-    return sbe_write_outputs(p, &o, out_dir);
+    if (sbe_status st = sbe_write_outputs(p, &o, out_dir)) return st;
+    if (q.nshots() > 0) {   // density snapshots (antelope.cpp:267-422)
+        const size_t ns = q.nshots(), nt = q.ntotal();
+        std::vector<double> occ1d(ns * q.Nk[0]), nc(ns * nt), pi(ns * nt * 2);
+        if (sbe_status st = sbe_solver_snapshots(s, occ1d.data(), nc.data(), pi.data())) return st;
+        return sbe_write_snapshots(p, occ1d.data(), nc.data(), pi.data(), out_dir);
+    }
+    return SBE_OK;
 }
 
 // ================================================================= batch
@@ -542,6 +603,18 @@ extern "C" sbe_status sbe_batch_harmonics(sbe_batch *b, int index, double w0, in
     });
 }
 
+extern "C" sbe_status sbe_batch_snapshots(sbe_batch *b, int index, double *occ1d, double *nc, double *pi)
+{
+    if (!b || index < 0 || index >= (int)b->ids.size()) return fail(SBE_INVALID_ARGUMENT, "bad batch index");
+    if (!b->ran) return fail(SBE_NOT_READY, "sbe_batch_run has not been called");
+    return guard([&]() -> sbe_status {
+        cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
+        if (b->eng->snapshots(b->ids[index], occ1d, nc, pi) == 0)
+            return fail(SBE_INVALID_ARGUMENT, "the problem takes no snapshots (calc.shotNumber <= 0)");
+        return SBE_OK;
+    });
+}
+
 extern "C" int sbe_batch_launches(const sbe_batch *b) { return b ? b->launches : 0; }
 
 extern "C" sbe_status sbe_batch_kernel_times(sbe_batch *b, double *pms, int *pn, double *rms, int *rn)
@@ -612,6 +685,7 @@ void sbe_server::loop()
     eo.tile_k = opts.tile_k;
     eo.kpt = opts.k_per_thread;
     eo.allow_tuning = false;  // never stall the serving loop on a tuning run
+    eo.snapshots = false;     // requests return the file outputs only (sbe_server_wait)
     std::vector<cudaEvent_t> pool;
     for (;;) {
         std::unique_lock<std::mutex> lk(mu);

@@ -44,9 +44,16 @@ enum VgConst : int {
     VG_WPX0, VG_WPX1, VG_WPY0, VG_WPY1,  // w*P00, w*P11 for x, y
     VG_WQXR, VG_WQXI, VG_WQYR, VG_WQYI,  // 2*w*P01 for x, y (re, im)
     VG_W,          // w (trapezoid weight)
-    VG_NCONST
+    VG_NCONST      // constants the propagate kernels hold in registers
 };
+// One more per-k value stored after those (not loaded by the propagate
+// kernels): rho0_11, read only when a density snapshot is taken.
+constexpr int VG_R11 = VG_NCONST, VG_NCONST_ALL = VG_NCONST + 1;
 enum VgState : int { VG_DA = 0, VG_DB, VG_ZR, VG_ZI, VG_NSTATE };
+// Three more FP64 rows after those: the packed mixed kernel's FP32 sum of the
+// increments not yet folded into the state (folds happen at absolute step
+// multiples of 8, so a run split into launches anywhere gives the same bits).
+constexpr int VG_ACC = VG_NSTATE, VG_NSTATE_ALL = VG_NSTATE + 3;
 
 // Length gauge, Haldane: per-k cos/sin of k.a_i and k.b_i, and the weight.
 enum LwConst : int {
@@ -72,6 +79,14 @@ struct SolveDev {
     double t1, t2c, t2s;          // t1, 2*t2*cos(phi0), 2*t2*sin(phi0)
     double va[3][2], vb[3][2];    // NN and NNN vectors (bohr)
     int *status;                  // device status word (0 = ok)
+    // density snapshots (antelope.cpp:340-422): after every step s with
+    // s % shot_every == 0 the kernels store, per k, the conduction occupation
+    // snap_nc[s / shot_every][k] and the coherence snap_pi[..][k] (re, im) of
+    // rho in the band basis (VG) or in the eigenbasis of H0(k + A(t_s)) (LW);
+    // shot_every = 0: none
+    int shot_every;
+    double *snap_nc;   // [nshots][nk]
+    double *snap_pi;   // [nshots][nk][2]
 };
 
 struct TileDev {

@@ -133,6 +133,8 @@ struct Engine::Solve {
     bool g1 = false;
     void *kc = nullptr, *st = nullptr, *tab = nullptr;
     double *partial = nullptr, *jout = nullptr, *constpart = nullptr;
+    double *snap_nc = nullptr, *snap_pi = nullptr;  // density snapshots (or null)
+    int nshots = 0, k_begin = 0;
     double *h_jout = nullptr, *h_const = nullptr;  // pinned
     cudaEvent_t ev = nullptr;
     bool fetched = false;
@@ -175,6 +177,8 @@ Engine::~Engine()
         cudaFreeAsync(s.partial, stream_);
         cudaFreeAsync(s.jout, stream_);
         cudaFreeAsync(s.constpart, stream_);
+        if (s.snap_nc) cudaFreeAsync(s.snap_nc, stream_);
+        if (s.snap_pi) cudaFreeAsync(s.snap_pi, stream_);
         if (s.ev) {
             cudaEventSynchronize(s.ev);
             cudaEventDestroy(s.ev);
@@ -227,10 +231,12 @@ size_t Engine::bytes_needed(const Problem &p, const EngineOptions &o) const
     const size_t nk_pad = (size_t)ntiles * sh.tile_k;
     const int nts = (int)stage_fractions(p.rk).size();
     const bool vg = p.gauge == GAUGE_VELOCITY;
-    const size_t nc = vg ? (size_t)VG_NCONST : (size_t)LW_NCONST, ns = 4;
+    const size_t nc = vg ? (size_t)VG_NCONST_ALL : (size_t)LW_NCONST, ns = vg ? VG_NSTATE_ALL : LW_NSTATE;
     const size_t tab = (size_t)p.laser.Nt * nts * (vg ? 2 : LW_NPHASE) * real;
+    const size_t nk = o.k_end > 0 ? (size_t)(o.k_end - o.k_begin) : (size_t)p.ntotal();
+    const size_t snap = o.snapshots ? (size_t)p.nshots() * nk * 24 : 0;
     return nc * nk_pad * real + ns * nk_pad * 8 + tab + (size_t)S_ * ntiles * NSLOT * 8 + (size_t)p.laser.Nt * NSLOT * 8 +
-           (size_t)ntiles * NSLOT * 8;
+           (size_t)ntiles * NSLOT * 8 + snap;
 }
 
 int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<double> *atab_in)
@@ -256,8 +262,12 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     if (free_slots_.empty()) throw OomError("too many resident solves (descriptor slots exhausted)");
     const size_t real = s->precision == PREC_FP64 ? 8 : 4;
     const bool vg = s->variant == VAR_HALDANE_VG;
-    const size_t nc = vg ? (size_t)VG_NCONST : (size_t)LW_NCONST;
-    const size_t kc_b = nc * s->nk_pad * real, st_b = 4 * (size_t)s->nk_pad * 8;  // state is FP64 in both methods
+    const size_t nc = vg ? (size_t)VG_NCONST_ALL : (size_t)LW_NCONST;
+    const size_t ns = vg ? (size_t)VG_NSTATE_ALL : (size_t)LW_NSTATE;
+    const size_t kc_b = nc * s->nk_pad * real, st_b = ns * s->nk_pad * 8;  // state is FP64 in both methods
+    s->k_begin = kb;
+    s->nshots = o.snapshots ? p.nshots() : 0;
+    const size_t snap_n = (size_t)s->nshots * s->nk;
     const size_t tab_n = (size_t)s->Nt * s->nts * (vg ? 2 : LW_NPHASE);
     const size_t part_b = (size_t)S_ * s->ntiles * NSLOT * 8, jout_b = (size_t)s->Nt * NSLOT * 8;
     const size_t cp_b = (size_t)s->ntiles * NSLOT * 8;
@@ -270,6 +280,8 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
             cudaFreeAsync(s->tab, stream_);
             cudaFreeAsync(s->partial, stream_);
             cudaFreeAsync(s->jout, stream_);
+            cudaFreeAsync(s->constpart, stream_);
+            if (s->snap_nc) cudaFreeAsync(s->snap_nc, stream_);
             cuda_check(e, what);
         }
     };
@@ -279,7 +291,11 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     alloc((void **)&s->partial, part_b, "alloc partials");
     alloc((void **)&s->jout, jout_b, "alloc outputs");
     alloc((void **)&s->constpart, cp_b, "alloc constant parts");
-    s->bytes = kc_b + st_b + tab_n * real + part_b + jout_b + cp_b;
+    if (snap_n > 0) {
+        alloc((void **)&s->snap_nc, snap_n * 8, "alloc snapshots");
+        alloc((void **)&s->snap_pi, snap_n * 16, "alloc snapshots");
+    }
+    s->bytes = kc_b + st_b + tab_n * real + part_b + jout_b + cp_b + snap_n * 24;
     s->h_jout = static_cast<double *>(pinned_.get(jout_b));
     s->h_const = static_cast<double *>(pinned_.get(cp_b));
     cuda_check(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate");
@@ -337,6 +353,9 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     d.tab = s->tab;
     d.partial = s->partial;
     d.jout = s->jout;
+    d.shot_every = s->nshots > 0 ? p.shot_every() : 0;
+    d.snap_nc = s->snap_nc;
+    d.snap_pi = s->snap_pi;
     d.g1 = p.T1 > 1.0e-16 ? p.dt / p.T1 : 0.0;   // SBEs.h:484-493
     d.g2 = p.T2 > 1.0e-16 ? p.dt / p.T2 : 0.0;
     const double t2c = 2.0 * p.hal_t2 * std::cos(p.hal_phi0), t2s = 2.0 * p.hal_t2 * std::sin(p.hal_phi0);
@@ -540,6 +559,27 @@ void Engine::raw_outputs(int id, std::vector<double> &jout, double cp[NSLOT])
     jout.assign(s.h_jout, s.h_jout + (size_t)s.Nt * NSLOT);
 }
 
+int Engine::snapshots(int id, double *occ1d, double *nc, double *pi)
+{
+    Solve &s = get(id);
+    if (s.nshots == 0) return 0;
+    const Problem &p = s.prob;
+    const size_t n = (size_t)s.nshots * s.nk;
+    if (occ1d) {
+        double *d_occ = nullptr;
+        const size_t b = (size_t)s.nshots * p.Nk[0] * 8;
+        cuda_check(cudaMallocAsync(reinterpret_cast<void **>(&d_occ), b, stream_), "alloc snapshot bins");
+        cudaError_t e = launch_snapshot_bins(s.snap_nc, s.nk, s.k_begin, p.Nk, s.nshots, d_occ, stream_);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(occ1d, d_occ, b, cudaMemcpyDeviceToHost, stream_);
+        cudaFreeAsync(d_occ, stream_);
+        cuda_check(e, "snapshot bins");
+    }
+    if (nc) cuda_check(cudaMemcpyAsync(nc, s.snap_nc, n * 8, cudaMemcpyDeviceToHost, stream_), "copy snapshots");
+    if (pi) cuda_check(cudaMemcpyAsync(pi, s.snap_pi, n * 16, cudaMemcpyDeviceToHost, stream_), "copy snapshots");
+    cuda_check(cudaStreamSynchronize(stream_), "snapshot sync");
+    return s.nshots;
+}
+
 void Engine::harmonics(int id, double w0, int hmax, double *band_power)
 {
     Solve &s = get(id);
@@ -593,6 +633,8 @@ void Engine::remove(int id)
     cudaFreeAsync(s.partial, stream_);
     cudaFreeAsync(s.jout, stream_);
     cudaFreeAsync(s.constpart, stream_);
+    if (s.snap_nc) cudaFreeAsync(s.snap_nc, stream_);
+    if (s.snap_pi) cudaFreeAsync(s.snap_pi, stream_);
     if (s.fetched) cudaEventSynchronize(s.ev);
     pinned_.put(s.h_jout, (size_t)s.Nt * NSLOT * 8);
     pinned_.put(s.h_const, (size_t)s.ntiles * NSLOT * 8);

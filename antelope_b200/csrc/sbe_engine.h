@@ -33,6 +33,7 @@ struct EngineOptions {
     int steps_per_launch = 0;  // S (0: default)
     bool allow_tuning = true;  // false: a cached tuned shape or the heuristic, never a tuning run
     int k_begin = 0, k_end = 0;  // k-slice [k_begin, k_end) of the grid (0, 0: all of it)
+    bool snapshots = true;       // take the problem's density snapshots (calc.shotNumber)
 };
 
 // Pinned staging for host->device uploads: copies are issued from a pinned
@@ -119,6 +120,11 @@ public:
     // fetched solve (waits for the copy); assemble_outputs() turns them into
     // the output arrays.
     void raw_outputs(int id, std::vector<double> &jout, double cp[NSLOT]);
+    // Density snapshots of a finished solve (waits for the stream):
+    // occ1d[nshots][N0] (the 1-D integrated conduction occupation, summed over
+    // this solve's k-points), nc[nshots][nk], pi[nshots][nk][2]; any may be
+    // null.  Returns the number of snapshots (0: none were taken).
+    int snapshots(int id, double *occ1d, double *nc, double *pi);
     // harmonic band powers h = 1..hmax of a finished solve, from its
     // device-resident sums (sbe_spectrum.h); synchronises the stream
     void harmonics(int id, double w0, int hmax, double *band_power);

@@ -75,6 +75,26 @@ template <> struct Tableau<5> {  // Fehlberg tableau with its 5th-order weights
     __device__ static constexpr int ti(int i) { return i; }
 };
 
+// ------------------------------------------------------ density snapshots
+// Snapshots follow the steps s = 0, F, 2F, ... (antelope.cpp:340-342); the
+// first one at or after a launch's first step s0.
+__device__ __forceinline__ int first_shot(int s0, int F)
+{
+    return F > 0 ? ((s0 + F - 1) / F) * F : 0x7fffffff;
+}
+
+// Velocity gauge: rho_11 = rho0_11 + db = rho0_11 - da and rho_10 = conj(z)
+// in the band basis, the elements the reference reads at index Nval*N + Nval
+// and Nval*N + Nval - 1 (antelope.cpp:391-398).
+__device__ __forceinline__ void vg_snapshot(const SolveDev &sd, int s, int k, double r11, double da, double zr,
+                                            double zi)
+{
+    const size_t i = (size_t)(s / sd.shot_every) * sd.nk + k;
+    sd.snap_nc[i] = r11 - da;
+    sd.snap_pi[2 * i] = zr;
+    sd.snap_pi[2 * i + 1] = -zi;
+}
+
 // ---------------------------------------------- packed FP32 (f32x2) math
 // Two k-points per thread share every instruction: .x belongs to the first,
 // .y to the second (PTX f32x2 arithmetic, sm_100+).
@@ -282,6 +302,7 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 #pragma unroll
         for (int j = 0; j < KPT; ++j) hstart[j] = vg_field<Real>(c[j], A0);
     }
+    int next_shot = first_shot(s0, sd.shot_every);
 
     for (int s = s0; s < s1; ++s) {
         Real y0[KPT][D_N];
@@ -344,6 +365,14 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
             }
 #pragma unroll
             for (int q = 0; q < D_N; ++q) y64[j][q] = F64 ? double(acc[q]) : y64[j][q] + double(acc[q]);
+        }
+        if (s == next_shot) {   // density snapshot of the state after step s
+#pragma unroll
+            for (int j = 0; j < KPT; ++j)
+                if (ok[j])
+                    vg_snapshot(sd, s, kidx[j], double(kc[(size_t)VG_R11 * nkp + kidx[j]]), y64[j][D_DA],
+                                y64[j][D_ZR], y64[j][D_ZI]);
+            next_shot += sd.shot_every;
         }
         // the staged sums reach the partial buffer after the step's arithmetic,
         // so the warp reduction above can overlap it
@@ -456,19 +485,24 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
     for (int i = 1; i < TB::NT; ++i) An[i] = __ldg(arow + i);
     // The FP64 state is y64 = (rounded to FP32: yhi) and the FP32 sum `acc` of
     // the increments since the last fold (each step's b_i k_i are added onto
-    // it directly); every XSTEP steps acc is added to y64 in FP64.  The stage input yhi + acc is rounded once, as float(y64)
+    // it directly); after every step s with (s + 1) % XSTEP == 0 acc is added
+    // to y64 in FP64.  An unfolded acc is kept in the state rows VG_ACC.. at
+    // the end of a launch, so splitting the time loop changes no bit.  The stage input yhi + acc is rounded once, as float(y64)
     // would be, and acc holds only a few increments, so the state keeps its
     // FP64 accumulation while the f64<->f32 conversions drop XSTEP-fold.
     float2 yhi[D_N], acc[D_N];
 #pragma unroll
     for (int q = 0; q < D_N; ++q) {
         yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
-        acc[q] = make_float2(0.f, 0.f);
+        acc[q] = make_float2(ok0 ? float(st[(size_t)(VG_ACC + q) * nkp + k0]) : 0.f,
+                             ok1 ? float(st[(size_t)(VG_ACC + q) * nkp + k1]) : 0.f);
     }
     TileReducer red(red_s);
     // warp-stage reduction role of this lane (see above)
     const int xrow = (lane & 15) >> 1, xgrp = lane & 1;
     const float4 *const xsrc = xst + (lane & 15) * XROW + (lane >> 4) * 16;
+
+    int next_shot = first_shot(s0, sd.shot_every);
 
     // one time step s, staged in row j of the warp stage
     auto step = [&](int j, int s) {
@@ -516,26 +550,40 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
             for (int q = 0; q < D_N; ++q)
                 if (TB::b(i) != 0.0) acc[q] = fma2(bc2(sg[q] * float(TB::b(i))), kk[i][q], acc[q]);
         }
+        if (s == next_shot) {   // density snapshot: the FP64 state after step s
+            // is y64 plus the increments not yet folded into it
+            if (ok0)
+                vg_snapshot(sd, s, k0, double(kc[(size_t)VG_R11 * nkp + k0]), y64[0][D_DA] + double(acc[D_DA].x),
+                            y64[0][D_ZR] + double(acc[D_ZR].x), y64[0][D_ZI] + double(acc[D_ZI].x));
+            if (ok1)
+                vg_snapshot(sd, s, k1, double(kc[(size_t)VG_R11 * nkp + k1]), y64[1][D_DA] + double(acc[D_DA].y),
+                            y64[1][D_ZR] + double(acc[D_ZR].y), y64[1][D_ZI] + double(acc[D_ZI].y));
+            next_shot += sd.shot_every;
+        }
     };
 
-    for (int sb = s0; sb < s1; sb += SUB) {
-        const int nb = min(SUB, s1 - sb);
-        for (int r8 = 0; r8 < nb; r8 += XSTEP) {
-            const int m = min(XSTEP, nb - r8);
+    // blocks of SUB steps (block stage) and XSTEP steps (warp stage, fold),
+    // both aligned to absolute step multiples
+    for (int b0 = s0; b0 < s1;) {
+        const int b1 = min(s1, (b0 / SUB + 1) * SUB);
+        for (int e0 = b0; e0 < b1;) {
+            const int e1 = min(b1, (e0 / XSTEP + 1) * XSTEP), m = e1 - e0;
             if (m == XSTEP) {
 #pragma unroll
-                for (int j = 0; j < XSTEP; ++j) step(j, sb + r8 + j);
+                for (int j = 0; j < XSTEP; ++j) step(j, e0 + j);
             } else {
 #pragma unroll 1
-                for (int j = 0; j < m; ++j) step(j, sb + r8 + j);
+                for (int j = 0; j < m; ++j) step(j, e0 + j);
             }
-            // fold the FP32 increments into the FP64 state
+            if (e1 % XSTEP == 0) {
+                // fold the FP32 increments into the FP64 state
 #pragma unroll
-            for (int q = 0; q < D_N; ++q) {
-                y64[0][q] += double(acc[q].x);
-                y64[1][q] += double(acc[q].y);
-                yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
-                acc[q] = make_float2(0.f, 0.f);
+                for (int q = 0; q < D_N; ++q) {
+                    y64[0][q] += double(acc[q].x);
+                    y64[1][q] += double(acc[q].y);
+                    yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+                    acc[q] = make_float2(0.f, 0.f);
+                }
             }
             // warp sums of the m staged rows
             __syncwarp();
@@ -553,7 +601,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
             a.w += __shfl_xor_sync(0xffffffffu, a.w, 16);
             __syncwarp();
             if (lane < 16 && xrow < m) {
-                double *dst = red.red[red.half][r8 + xrow][warp];
+                double *dst = red.red[red.half][(e0 - b0) + xrow][warp];
                 if (xgrp == 0) {
                     dst[0] = double(a.x); dst[1] = double(a.y); dst[2] = double(a.z); dst[3] = double(a.w);
                 } else {
@@ -561,16 +609,52 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
                     dst[6] = double(a.y); dst[7] = double(a.z);
                 }
             }
+            e0 = e1;
         }
-        red.flush(nb, sb - s0, ntiles, tl.tile, partial);
+        red.flush(b1 - b0, b0 - s0, ntiles, tl.tile, partial);
+        b0 = b1;
     }
 #pragma unroll
     for (int q = 0; q < D_N; ++q) {
-        if (ok0) st[(size_t)slot[q] * nkp + k0] = y64[0][q];
-        if (ok1) st[(size_t)slot[q] * nkp + k1] = y64[1][q];
+        if (ok0) {
+            st[(size_t)slot[q] * nkp + k0] = y64[0][q];
+            st[(size_t)(VG_ACC + q) * nkp + k0] = double(acc[q].x);
+        }
+        if (ok1) {
+            st[(size_t)slot[q] * nkp + k1] = y64[1][q];
+            st[(size_t)(VG_ACC + q) * nkp + k1] = double(acc[q].y);
+        }
     }
     if (ok0) st[(size_t)VG_DB * nkp + k0] = -y64[0][D_DA];
     if (ok1) st[(size_t)VG_DB * nkp + k1] = -y64[1][D_DA];
+}
+
+// Closed-form eigenvectors of n.sigma for unit n: |+> (eigenvalue +1) and
+// |-> (eigenvalue -1), choosing the chart that avoids 1 +/- nz -> 0.
+__device__ __forceinline__ void spinors(double nx, double ny, double nz, double2 (&up)[2], double2 (&dn)[2])
+{
+    if (nz >= 0.0) {
+        const double r = 1.0 / sqrt(2.0 * (1.0 + nz));
+        up[0] = make_double2((1.0 + nz) * r, 0.0);
+        up[1] = make_double2(nx * r, ny * r);
+        dn[0] = make_double2(-nx * r, ny * r);
+        dn[1] = make_double2((1.0 + nz) * r, 0.0);
+    } else {
+        const double r = 1.0 / sqrt(2.0 * (1.0 - nz));
+        up[0] = make_double2(nx * r, -ny * r);
+        up[1] = make_double2((1.0 - nz) * r, 0.0);
+        dn[0] = make_double2((1.0 - nz) * r, 0.0);
+        dn[1] = make_double2(-nx * r, -ny * r);
+    }
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconjmul(double2 a, double2 b)  // conj(a) * b
+{
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
 }
 
 // -------------------------------------------------------- length gauge
@@ -647,9 +731,11 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
     for (int q = 0; q < 4; ++q) y64[q] = ok ? st[(size_t)q * nkp + kidx] : 0.0;
     if (!ok) c[LW_CA0] = c[LW_CB0] = Real(1);  // padding lanes: a harmless k = 0 point, weight 0
     TileReducer red(red_s);
+    int next_shot = first_shot(s0, sd.shot_every);
 
     for (int s = s0; s < s1; ++s) {
         const Real *row = tab + (size_t)s * TB::NT * LW_NPHASE;
+        double Bt[3];   // B of H0(k + A(t_s)), kept for a snapshot after the step
         Real y0[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) y0[q] = Real(y64[q]);
@@ -668,6 +754,9 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
             const double B1 = double(t1dt) * (double(ca[0]) + double(ca[1]) + double(ca[2]));
             const double B2 = double(t1dt) * (double(sa[0]) + double(sa[1]) + double(sa[2]));
             const double B3 = double(Mdt) - double(t2sdt) * (double(sb[0]) + double(sb[1]) + double(sb[2]));
+            Bt[0] = B1;
+            Bt[1] = B2;
+            Bt[2] = B3;
             const double al = y64[LW_AL], sx = y64[LW_SX], sy = y64[LW_SY], sz = y64[LW_SZ];
             const double bb = B1 * B1 + B2 * B2 + B3 * B3;
             const double sB = sx * B1 + sy * B2 + sz * B3;
@@ -707,6 +796,30 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) y64[q] = F64 ? double(acc[q]) : y64[q] + double(acc[q]);
+        if (s == next_shot) {
+            // density snapshot: rho after the step in the eigenbasis of
+            // H0(k + A(t_s)) (SBEs::WannierToHamiltonian at the step's start
+            // time, as antelope.cpp:358 calls it); conduction = |+>, valence = |->
+            if (ok) {
+                const double bn = sqrt(Bt[0] * Bt[0] + Bt[1] * Bt[1] + Bt[2] * Bt[2]);
+                double nx = 0.0, ny = 0.0, nz = 1.0;
+                if (bn > 0.0) { nx = Bt[0] / bn; ny = Bt[1] / bn; nz = Bt[2] / bn; }
+                const double al = y64[LW_AL], sx = y64[LW_SX], sy = y64[LW_SY], sz = y64[LW_SZ];
+                double2 up[2], dn[2];
+                spinors(nx, ny, nz, up, dn);
+                // rho |-> with rho = [[al + sz, sx - i sy], [sx + i sy, al - sz]]
+                const double2 r0 = make_double2((al + sz) * dn[0].x + sx * dn[1].x + sy * dn[1].y,
+                                                (al + sz) * dn[0].y + sx * dn[1].y - sy * dn[1].x);
+                const double2 r1 = make_double2(sx * dn[0].x - sy * dn[0].y + (al - sz) * dn[1].x,
+                                                sx * dn[0].y + sy * dn[0].x + (al - sz) * dn[1].y);
+                const double2 q0 = cconjmul(up[0], r0), q1 = cconjmul(up[1], r1);
+                const size_t i = (size_t)(s / sd.shot_every) * sd.nk + kidx;
+                sd.snap_nc[i] = al + sx * nx + sy * ny + sz * nz;
+                sd.snap_pi[2 * i] = q0.x + q1.x;
+                sd.snap_pi[2 * i + 1] = q0.y + q1.y;
+            }
+            next_shot += sd.shot_every;
+        }
         const int r = (s - s0) % SUB;
         if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, sd.partial);
     }
@@ -748,34 +861,6 @@ __global__ void __launch_bounds__(256) reduce_tiles(const SolveDev *__restrict__
 }
 
 // ------------------------------------------------------------ set-up
-// Closed-form eigenvectors of n.sigma for unit n: |+> (eigenvalue +1) and
-// |-> (eigenvalue -1), choosing the chart that avoids 1 +/- nz -> 0.
-__device__ __forceinline__ void spinors(double nx, double ny, double nz, double2 (&up)[2], double2 (&dn)[2])
-{
-    if (nz >= 0.0) {
-        const double r = 1.0 / sqrt(2.0 * (1.0 + nz));
-        up[0] = make_double2((1.0 + nz) * r, 0.0);
-        up[1] = make_double2(nx * r, ny * r);
-        dn[0] = make_double2(-nx * r, ny * r);
-        dn[1] = make_double2((1.0 + nz) * r, 0.0);
-    } else {
-        const double r = 1.0 / sqrt(2.0 * (1.0 - nz));
-        up[0] = make_double2(nx * r, -ny * r);
-        up[1] = make_double2((1.0 - nz) * r, 0.0);
-        dn[0] = make_double2((1.0 - nz) * r, 0.0);
-        dn[1] = make_double2(-nx * r, -ny * r);
-    }
-}
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b)
-{
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cconjmul(double2 a, double2 b)  // conj(a) * b
-{
-    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
-}
-
 template <class Real>
 __global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restrict__ kc, double *__restrict__ st,
                                                     double *__restrict__ constpart)
@@ -869,6 +954,7 @@ __global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restric
                 w};
 #pragma unroll
             for (int q = 0; q < VG_NCONST; ++q) kc[q * P + k] = Real(cv[q]);
+            kc[VG_R11 * P + k] = Real(f1);
 #pragma unroll
             for (int q = 0; q < VG_NSTATE; ++q) st[q * P + k] = 0.0;
             cp[0] += w * (f0 * P00[0] + f1 * P11[0]);
@@ -906,6 +992,34 @@ __global__ void __launch_bounds__(256) init_haldane(InitArgs ia, Real *__restric
 }
 
 // ------------------------------------------------- FMA peak microbench
+// 1-D integrated conduction occupation of the snapshots (antelope.cpp:343-
+// 370): for every snapshot and first grid index m, the weighted sum of the
+// per-k values over the solve's k-points with that index, divided by N1.  One
+// CTA per (m, snapshot), fixed summation order.
+__global__ void __launch_bounds__(256) snapshot_bins(const double *__restrict__ nc, int nk, int k_offset, int N0,
+                                                     int N1, int N2, double *__restrict__ occ1d)
+{
+    __shared__ double red[256];
+    const int m = blockIdx.x, shot = blockIdx.y, blk = N1 * N2;
+    const int g0 = max(m * blk, k_offset), g1 = min((m + 1) * blk, k_offset + nk);
+    const double wi = (N0 != 1 && (m == 0 || m == N0 - 1)) ? 0.5 : 1.0;
+    double acc = 0.0;
+    for (int g = g0 + (int)threadIdx.x; g < g1; g += blockDim.x) {
+        const int j = (g / N2) % N1, l = g % N2;
+        double w = wi;   // trapezoid weight (momaxis.h:147-186)
+        if (N1 != 1 && (j == 0 || j == N1 - 1)) w *= 0.5;
+        if (N2 != 1 && (l == 0 || l == N2 - 1)) w *= 0.5;
+        acc += w * nc[(size_t)shot * nk + (g - k_offset)];
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) occ1d[(size_t)shot * N0 + m] = red[0] / (double)N1;
+}
+
 // Independent FMA chains (8 per thread) to measure the FP64 / FP32 vector
 // pipe peaks that the roofline fractions are quoted against.
 template <class Real>
@@ -1048,6 +1162,15 @@ cudaError_t launch_init_haldane(const InitArgs &ia, int precision, void *kc, voi
     else
         init_haldane<float><<<ntiles, 256, 0, stream>>>(ia, static_cast<float *>(kc), static_cast<double *>(st),
                                                         constpart);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_snapshot_bins(const double *nc, int nk, int k_offset, const int N[3], int nshots, double *occ1d,
+                                 cudaStream_t stream)
+{
+    if (nshots <= 0 || nk <= 0) return cudaSuccess;
+    dim3 grid(N[0], nshots);
+    snapshot_bins<<<grid, 256, 0, stream>>>(nc, nk, k_offset, N[0], N[1], N[2], occ1d);
     return cudaGetLastError();
 }
 

@@ -32,6 +32,10 @@ cudaError_t launch_reduce(const SolveDev *solves, const int *solve_ids, int nsol
                           cudaStream_t stream);
 cudaError_t launch_init_haldane(const InitArgs &ia, int precision, void *kc, void *st, double *constpart,
                                 cudaStream_t stream);
+// occ1d[nshots][N0] from the per-k snapshot values nc[nshots][nk] of a solve
+// whose k-points are the flat grid indices [k_offset, k_offset + nk)
+cudaError_t launch_snapshot_bins(const double *nc, int nk, int k_offset, const int N[3], int nshots, double *occ1d,
+                                 cudaStream_t stream);
 cudaError_t launch_fma_peak(int which, int blocks, int iters, void *out, cudaStream_t stream);
 
 }  // namespace sbe

@@ -107,13 +107,14 @@ extern "C" sbe_status sbe_solve_noalloc(const sbe_problem *problem, const sbe_op
     const double *cfr = p.rk == 4 ? c4 : c5;
     const int nts = p.rk == 4 ? 3 : 6;
     const int ncols = vg ? 2 : LW_NPHASE;
-    const size_t nconst = vg ? (size_t)VG_NCONST : (size_t)LW_NCONST;
+    const size_t nconst = vg ? (size_t)VG_NCONST_ALL : (size_t)LW_NCONST;   // as the init kernel writes
 
     // carve the scratch array
     Layout L{};
     size_t off = 0;
     L.kc = off;      off += round256(nconst * nk_pad * real);
-    L.st = off;      off += round256(4 * nk_pad * 8);
+    const size_t nstate = vg ? (size_t)VG_NSTATE_ALL : (size_t)LW_NSTATE;
+    L.st = off;      off += round256(nstate * nk_pad * 8);
     L.tab = off;     off += round256((size_t)Nt * nts * ncols * real);
     L.jout = off;    off += round256((size_t)Nt * NSLOT * 8);
     L.cp = off;      off += round256((size_t)ntiles * NSLOT * 8);
@@ -252,7 +253,7 @@ extern "C" sbe_status sbe_solve_noalloc(const sbe_problem *problem, const sbe_op
     ia.Ef = p.Ef;
     ia.dt = p.dt;
     if (!cu(cudaMemsetAsync(base + L.kc, 0, nconst * nk_pad * real, st), "clear constants") ||
-        !cu(cudaMemsetAsync(base + L.st, 0, 4 * nk_pad * 8, st), "clear state") ||
+        !cu(cudaMemsetAsync(base + L.st, 0, nstate * nk_pad * 8, st), "clear state") ||
         !cu(launch_init_haldane(ia, precision, base + L.kc, base + L.st, reinterpret_cast<double *>(base + L.cp), st),
             "init kernel"))
         return SBE_CUDA_ERROR;

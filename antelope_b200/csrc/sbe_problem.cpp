@@ -373,6 +373,20 @@ void Problem::derive_grid()
     total_weight = tw;
 }
 
+// shotFrequency of antelope.cpp:274-278, from the first pulse's period
+// (laser.h:75); snapshots follow the steps n = 0, F, 2F, ... < Nt
+int Problem::shot_every() const
+{
+    if (shot_number <= 0 || laser.pulses.empty()) return 0;
+    return (int)(laser.pulses[0].period0 / shot_number / laser.dt);
+}
+
+int Problem::nshots() const
+{
+    const int F = shot_every();
+    return F > 0 ? (laser.Nt - 1) / F + 1 : 0;
+}
+
 Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
 {
     Problem p;
@@ -590,7 +604,10 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
     p.derive_grid();
 
     if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) unsup("gauge LengthHamiltonian is not implemented in the reference either");
-    if (p.shot_number > 0) unsup("density snapshots (calc.shotNumber > 0) are not built");
+    if (p.shot_number > 0 && p.shot_every() <= 0)   // the reference would take ktime % 0
+        throw CfgError("calc.shotNumber gives a snapshot interval of 0 steps (period / shotNumber < dt)");
+    if (p.shot_number > 0 && p.model != MODEL_HALDANE)
+        unsup("density snapshots (calc.shotNumber > 0) are built for the Haldane model");
     if (p.rk == 45 && p.model == MODEL_HALDANE)
         unsup("adaptive Cash-Karp steps are built for the N-band (table) models only");
     return p;

@@ -100,6 +100,11 @@ struct Problem {
     std::vector<double> w_j;          // [nR][2][N][N] complex current-operator tables (empty:
                                       // J_a = -dH/dk_a + i[D_a, H], BaseMaterial.h:62-68)
 
+    // density snapshots: steps between them (shotFrequency,
+    // antelope.cpp:274-278) and how many the run takes; 0 when off
+    int shot_every() const;
+    int nshots() const;
+
     // derived grid quantities (momaxis.h:192-240)
     int ntotal() const { return Nk[0] * Nk[1] * Nk[2]; }
     double volume = 0.0, dV = 0.0, total_weight = 0.0;

@@ -128,6 +128,7 @@ Shape autotune_shape(int device, const Problem &p, int precision)
             eo.precision = precision;
             eo.tile_k = c.tile_k;
             eo.kpt = c.kpt;
+            eo.snapshots = false;
             e.add(q, eo);
             e.step();  // warm-up launch (also builds the lists)
             cuda_check(cudaEventRecord(a, st), "event");

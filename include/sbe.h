@@ -112,6 +112,12 @@ typedef struct sbe_model {
     double *vec, *h, *d, *j, *bz;
 } sbe_model;
 sbe_status sbe_problem_model(const sbe_problem *p, sbe_model *m);
+/* Density snapshots (calc.shotNumber > 0; antelope.cpp:267-422): every
+ * `interval` = int(period0 / shotNumber / dt) steps (period0 of the first pulse,
+ * antelope.cpp:274-278), after the step n with n % interval == 0, `nshots` in
+ * all; n0 = Npoints[0].  interval = nshots = 0 when snapshots are off.
+ * Host-only. */
+sbe_status sbe_problem_snapshots(const sbe_problem *p, int *interval, int *nshots, int *n0);
 void sbe_problem_destroy(sbe_problem *p);
 
 /* One solve (replaces SBEs + the driver loop of antelope.cpp:297-548). */
@@ -133,6 +139,26 @@ sbe_status sbe_solver_steps(const sbe_solver *s, long long *steps, long long *at
 sbe_status sbe_solver_kernel_times(sbe_solver *s, double *propagate_ms, int *propagate_launches,
                                    double *reduce_ms, int *reduce_launches);
 void sbe_solver_destroy(sbe_solver *s);
+
+/* Density snapshots of a finished solve (Haldane model, both gauges), the
+ * data of the reference's snapshot files (antelope.cpp:340-422); any array
+ * may be NULL:
+ *   occ1d[nshots*n0]       occupation_1d_integration.dat: Re sum_k w_k rho'_cc
+ *                          over the k-points with first grid index i, / Npoints[1];
+ *   nc[nshots*ntotal]      fisrt_conduction.dat: rho'_cc of every k-point;
+ *   pi[nshots*ntotal*2]    fisrt_coherence.dat: rho'[Nval][Nval-1] (re, im);
+ * rho' is rho in the band basis (velocity gauge) or in the eigenbasis of
+ * H0(k + A(t_n)) (length gauge, SBEs::WannierToHamiltonian, SBEs.h:927-940).
+ * The reference's own loop fills nc / pi through a stale k index
+ * (antelope.cpp:384-400); here each k-point gets its own value.  For a k-slice
+ * solver, the arrays cover the slice and occ1d holds its part of the sums. */
+sbe_status sbe_solver_snapshots(sbe_solver *s, double *occ1d, double *nc, double *pi);
+/* Write occupation_1d_integration.dat ("%16e    " per value, one row per
+ * snapshot), fisrt_conduction.dat and fisrt_coherence.dat (raw doubles) and
+ * the empty snapshot_log.dat into `dir`, as antelope.cpp:288-292, 365-368,
+ * 416-421 do; sbe_run_cfg writes them when the cfg asks for snapshots. */
+sbe_status sbe_write_snapshots(const sbe_problem *p, const double *occ1d, const double *nc, const double *pi,
+                               const char *dir);
 
 /* Harmonic band powers of a finished solve, computed on the GPU from its
  * device-resident results, in the convention of the reference's analysis
@@ -173,6 +199,8 @@ sbe_status sbe_batch_create(const sbe_problem *const *problems, int n, const sbe
 sbe_status sbe_batch_run(sbe_batch *b, void *stream);
 sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *out);
 int sbe_batch_launches(const sbe_batch *b);
+/* Density snapshots of solve `index` of a finished batch (as sbe_solver_snapshots). */
+sbe_status sbe_batch_snapshots(sbe_batch *b, int index, double *occ1d, double *nc, double *pi);
 sbe_status sbe_batch_harmonics(sbe_batch *b, int i, double w0, int hmax, double *band_power);
 sbe_status sbe_batch_kernel_times(sbe_batch *b, double *propagate_ms, int *propagate_launches,
                                   double *reduce_ms, int *reduce_launches);
@@ -180,7 +208,8 @@ void sbe_batch_destroy(sbe_batch *b);
 
 /* Continuous-batching server: a worker thread admits submitted solves while
  * device memory allows, advances all resident solves together, and retires
- * them as they finish.  Thread-safe. */
+ * them as they finish.  Thread-safe.  Requests return the output arrays of
+ * sbe_outputs; density snapshots are taken by sbe_solver_* and sbe_batch_*. */
 typedef struct sbe_server_opts {
     int device;
     int precision;

@@ -12,7 +12,7 @@ import pytest
 from antelope_b200 import Problem, SbeError, capi
 from antelope_b200.api import Outputs, write_outputs
 from antelope_b200 import cfgtext
-from cases import BASE, GOLDEN_CASES, MATERIAL_CASES, TEXT_CASE, variant
+from cases import BASE, GOLDEN_CASES, MATERIAL_CASES, MATERIALS, SNAPSHOT_CASES, TEXT_CASE, variant
 from oracle import pyoracle
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -87,7 +87,9 @@ def _err(case_or_text):
     (lambda c: (c.__setitem__("target", "Haldane2L"),
                 c.__setitem__("Haldane2L", dict(c["Haldane"], t11=0.01, polytype="ABC"))),
      "SBE_BAD_CONFIG", "Undefined polytype"),
-    (lambda c: c["calc"].__setitem__("shotNumber", 4), "SBE_UNSUPPORTED", "snapshots"),
+    (lambda c: c["calc"].__setitem__("shotNumber", 1000), "SBE_BAD_CONFIG", "snapshot interval of 0 steps"),
+    (lambda c: (c.__setitem__("target", "KaneMele"), c.__setitem__("KaneMele", dict(MATERIALS["KaneMele"])),
+                c["calc"].__setitem__("shotNumber", 2)), "SBE_UNSUPPORTED", "snapshots"),
     (lambda c: c.__setitem__("gauge", "Hamiltonian"), "SBE_UNSUPPORTED", "LengthHamiltonian"),
 ])
 def test_diagnostics(mutate, status, msg):
@@ -178,3 +180,32 @@ def test_haldane_has_no_tables():
     with pytest.raises(SbeError) as e:
         Problem.from_dict(BASE).model_tables()
     assert e.value.name == "SBE_INVALID_ARGUMENT"
+
+
+@pytest.mark.parametrize("name", sorted(SNAPSHOT_CASES))
+def test_snapshot_dims_match_oracle(name):
+    """shotFrequency = int(period0 / shotNumber / dt) and the number of
+    snapshot steps n = 0, F, 2F, ... < Nt (antelope.cpp:274-278, 342)."""
+    case = SNAPSHOT_CASES[name]
+    sd = Problem.from_dict(case).snapshot_dims()
+    F, ns = pyoracle.shot_dims(case)
+    assert (sd["interval"], sd["nshots"], sd["n0"]) == (F, ns, case["calc"]["Npoints"][0])
+    assert Problem.from_dict(variant()).snapshot_dims()["nshots"] == 0
+
+
+def test_snapshot_writer_formats(tmp_path):
+    """sbe_write_snapshots: occupation_1d_integration.dat rows of "%16e    "
+    (antelope.cpp:365-368), raw doubles in fisrt_conduction.dat and complex
+    doubles in fisrt_coherence.dat (416-421), an empty snapshot_log.dat."""
+    from antelope_b200.api import write_snapshots
+    case = SNAPSHOT_CASES["vg_shots"]
+    p = Problem.from_dict(case)
+    ref = np.load(os.path.join(GOLDEN, "golden_vg_shots.npz"))
+    ns, nt = ref["occ1d"].shape[0], p.ntotal
+    snaps = {"occ1d": ref["occ1d"], "nc": ref["nc"].reshape(ns, nt), "pi": ref["pi"].reshape(ns, nt)}
+    write_snapshots(p, snaps, str(tmp_path))
+    text = (tmp_path / "occupation_1d_integration.dat").read_text()
+    assert text == "".join("".join(f"{v:16e}    " for v in row) + "\n" for row in ref["occ1d"])
+    assert np.array_equal(np.fromfile(tmp_path / "fisrt_conduction.dat"), ref["nc"])
+    assert np.array_equal(np.fromfile(tmp_path / "fisrt_coherence.dat", dtype=np.complex128), ref["pi"])
+    assert (tmp_path / "snapshot_log.dat").read_bytes() == b""
