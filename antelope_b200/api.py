@@ -325,10 +325,15 @@ class Server:
         return rid.value
 
     def wait(self, rid: int, timeout: float = -1.0):
+        """Outputs and latency of a request.  Its final state is returned once
+        (the server then forgets the request); a timeout leaves it waitable."""
         prob = self._problems[rid]
         out = Outputs.empty(prob.dims)
         lat = C.c_double(0.0)
-        _check(lib.sbe_server_wait(self._h, rid, float(timeout), C.byref(out.c()), C.byref(lat)))
+        st = lib.sbe_server_wait(self._h, rid, float(timeout), C.byref(out.c()), C.byref(lat))
+        if STATUS.get(st) != "SBE_TIMEOUT":
+            self._problems.pop(rid, None)
+        _check(st)
         return out, lat.value
 
     def cancel(self, rid: int):

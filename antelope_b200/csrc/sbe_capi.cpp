@@ -186,13 +186,8 @@ extern "C" sbe_status sbe_problem_dims(const sbe_problem *p, sbe_dims *d)
 extern "C" sbe_status sbe_problem_laser(const sbe_problem *p, double *laser)
 {
     if (!p || !laser) return fail(SBE_INVALID_ARGUMENT, "null argument");
-    const Laser &L = p->p.laser;
-    for (int n = 0; n < L.Nt; ++n) {
-        const double t = L.atmin + L.dt * n;  // antelope.cpp:215
-        double *row = laser + (size_t)n * 7;
-        row[0] = t;
-        L.eval(t, row + 4, row + 1);
-    }
+    const std::vector<double> rows = laser_rows(p->p);
+    std::copy(rows.begin(), rows.end(), laser);
     return SBE_OK;
 }
 
@@ -646,13 +641,17 @@ using Clock = std::chrono::steady_clock;
 struct Request {
     long long id = 0;
     Problem prob;
-    std::vector<double> atab;     // built by the submitting thread
+    std::vector<double> atab;     // field table, built by the submitting thread
+    std::vector<double> laser;    // laser columns of the outputs, built by the submitting thread
     std::vector<double> jout;     // raw per-step sums, assembled by the waiting thread
     double cp[NSLOT] = {0};
     Clock::time_point t_submit, t_done;
-    enum State { QUEUED, RESIDENT, DONE, FAILED, CANCELLED } state = QUEUED;
-    int solve = -1;
+    // ADMITTING: taken off the queue, being set up by the worker outside the lock
+    enum State { QUEUED, ADMITTING, RESIDENT, DONE, FAILED, CANCELLED } state = QUEUED;
+    int solve = -1;               // engine solve id while the engine holds it
     bool fetching = false;
+    bool cancel_asked = false;    // cancelled while ADMITTING
+    bool delivered = false;       // a wait returned its final state: the worker may erase it
     SolveOutputs out;
     std::string err;
 };
@@ -686,57 +685,82 @@ void sbe_server::loop()
     eo.kpt = opts.k_per_thread;
     eo.allow_tuning = false;  // never stall the serving loop on a tuning run
     eo.snapshots = false;     // requests return the file outputs only (sbe_server_wait)
+    // admissions set up between two tick issues: a burst of arrivals is
+    // admitted in slices while the GPU keeps working on the queued ticks
+    constexpr size_t kAdmitPerTurn = 16;
     std::vector<cudaEvent_t> pool;
+    std::vector<Request *> batch;
     for (;;) {
-        std::unique_lock<std::mutex> lk(mu);
-        // admission: FIFO while memory and slots allow
-        while (!queue.empty()) {
-            Request &r = *reqs[queue.front()];
-            if (r.state != Request::QUEUED) { queue.pop_front(); continue; }
-            size_t need = 0;
-            try {
-                need = eng->bytes_needed(r.prob, eo);
-            } catch (const std::exception &e) {
-                r.state = Request::FAILED;
-                r.err = e.what();
-                ++n_failed;
-                queue.pop_front();
-                cv_done.notify_all();
-                continue;
-            }
-            const bool slots_ok = opts.max_resident <= 0 || eng->nresident() < opts.max_resident;
-            if (!slots_ok || (double)(eng->bytes_in_use() + need) > budget) {
-                if (eng->nresident() == 0) {  // can never fit
+        batch.clear();
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            // admission: FIFO while memory and slots allow
+            size_t planned = 0;
+            while (!queue.empty() && batch.size() < kAdmitPerTurn) {
+                auto it = reqs.find(queue.front());
+                if (it == reqs.end() || it->second->state != Request::QUEUED) {
+                    queue.pop_front();
+                    continue;
+                }
+                Request &r = *it->second;
+                size_t need = 0;
+                try {
+                    need = eng->bytes_needed(r.prob, eo);
+                } catch (const std::exception &e) {
                     r.state = Request::FAILED;
-                    r.err = "admission refused: request needs more device memory than the budget";
+                    r.err = e.what();
                     ++n_failed;
                     queue.pop_front();
                     cv_done.notify_all();
                     continue;
                 }
-                break;
+                const int resident = eng->nresident() + (int)batch.size();
+                const bool slots_ok = opts.max_resident <= 0 || resident < opts.max_resident;
+                if (!slots_ok || (double)(eng->bytes_in_use() + planned + need) > budget) {
+                    if (resident == 0) {  // can never fit
+                        r.state = Request::FAILED;
+                        r.err = "admission refused: request needs more device memory than the budget";
+                        ++n_failed;
+                        queue.pop_front();
+                        cv_done.notify_all();
+                        continue;
+                    }
+                    break;
+                }
+                r.state = Request::ADMITTING;
+                planned += need;
+                batch.push_back(&r);
+                queue.pop_front();
             }
+            if (batch.empty() && eng->nresident() == 0) {
+                if (stop) break;
+                cv_work.wait_for(lk, std::chrono::milliseconds(50));
+                continue;
+            }
+        }
+        // set the admitted solves up outside the lock, so that submitting
+        // and waiting threads are not held up by it
+        for (Request *r : batch) {
             try {
-                r.solve = eng->add(r.prob, eo, &r.atab);
-                r.state = Request::RESIDENT;
-                std::vector<double>().swap(r.atab);
+                r->solve = eng->add(r->prob, eo, &r->atab);
             } catch (const std::exception &e) {
-                r.state = Request::FAILED;
-                r.err = e.what();
-                ++n_failed;
-                cv_done.notify_all();
+                r->solve = -1;
+                r->err = e.what();
             }
-            queue.pop_front();
         }
-        bool active = false;
-        for (auto &kv : reqs)
-            if (kv.second->state == Request::RESIDENT) { active = true; break; }
-        if (!active) {
-            if (stop) break;
-            cv_work.wait_for(lk, std::chrono::milliseconds(50));
-            continue;
+        if (!batch.empty()) {
+            std::lock_guard<std::mutex> g(mu);
+            for (Request *r : batch) {
+                std::vector<double>().swap(r->atab);
+                if (r->solve < 0) {
+                    r->state = Request::FAILED;
+                    ++n_failed;
+                } else {
+                    r->state = r->cancel_asked ? Request::CANCELLED : Request::RESIDENT;
+                }
+            }
+            cv_done.notify_all();
         }
-        lk.unlock();
         try {
             // bounded run-ahead: at most two ticks queued on the GPU, so new
             // arrivals join after a short wait
@@ -764,37 +788,45 @@ void sbe_server::loop()
             cv_done.notify_all();
             break;
         }
-        lk.lock();
+        std::lock_guard<std::mutex> g(mu);
         n_launches += eng->last_launches();
-        // retire finished and cancelled solves
-        for (auto &kv : reqs) {
-            Request &r = *kv.second;
+        // retire finished and cancelled solves; forget requests whose final
+        // state a wait has returned
+        for (auto it = reqs.begin(); it != reqs.end();) {
+            Request &r = *it->second;
             if (r.state == Request::CANCELLED && r.solve >= 0) {
                 try {
                     eng->remove(r.solve);
                 } catch (...) {
                 }
                 r.solve = -1;
+            }
+            const bool final_state = r.state == Request::DONE || r.state == Request::FAILED ||
+                                     r.state == Request::CANCELLED;
+            if (final_state && r.delivered && r.solve < 0) {
+                it = reqs.erase(it);
                 continue;
             }
-            if (r.state != Request::RESIDENT) continue;
-            if (!eng->finished(r.solve)) continue;
-            try {
-                if (!r.fetching) { eng->fetch_async(r.solve); r.fetching = true; }
-                if (eng->ready(r.solve)) {
-                    eng->raw_outputs(r.solve, r.jout, r.cp);
-                    eng->remove(r.solve);
-                    r.t_done = Clock::now();
-                    r.state = Request::DONE;
-                    ++n_completed;
+            if (r.state == Request::RESIDENT && eng->finished(r.solve)) {
+                try {
+                    if (!r.fetching) { eng->fetch_async(r.solve); r.fetching = true; }
+                    if (eng->ready(r.solve)) {
+                        eng->raw_outputs(r.solve, r.jout, r.cp);
+                        eng->remove(r.solve);
+                        r.solve = -1;
+                        r.t_done = Clock::now();
+                        r.state = Request::DONE;
+                        ++n_completed;
+                        cv_done.notify_all();
+                    }
+                } catch (const std::exception &e) {
+                    r.state = Request::FAILED;
+                    r.err = e.what();
+                    ++n_failed;
                     cv_done.notify_all();
                 }
-            } catch (const std::exception &e) {
-                r.state = Request::FAILED;
-                r.err = e.what();
-                ++n_failed;
-                cv_done.notify_all();
             }
+            ++it;
         }
     }
     for (auto ev : inflight) cudaEventDestroy(ev);
@@ -834,7 +866,9 @@ extern "C" sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, lon
     r->t_submit = Clock::now();
     r->prob = p->p;
     try {
-        r->atab = a_table(r->prob);  // host FP64 field table, built on the caller's thread
+        // host FP64 field table and the laser output columns, built on the caller's thread
+        r->atab = a_table(r->prob);
+        r->laser = laser_rows(r->prob);
     } catch (const std::exception &e) {
         return fail(SBE_INVALID_ARGUMENT, e.what());
     }
@@ -857,10 +891,13 @@ extern "C" sbe_status sbe_server_wait(sbe_server *s, long long id, double timeou
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return fail(SBE_INVALID_ARGUMENT, "unknown request id");
     Request &r = *it->second;
-    auto pending = [&]() { return r.state == Request::QUEUED || r.state == Request::RESIDENT; };
+    auto pending = [&]() {
+        return r.state == Request::QUEUED || r.state == Request::ADMITTING || r.state == Request::RESIDENT;
+    };
     if (timeout_s < 0) s->cv_done.wait(lk, [&]() { return !pending(); });
     else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&]() { return !pending(); }))
         return fail(SBE_TIMEOUT, "request not finished within the timeout");
+    r.delivered = true;   // the worker forgets the request from now on
     if (r.state == Request::CANCELLED) return fail(SBE_CANCELLED, "request was cancelled");
     if (r.state == Request::FAILED) {
         const bool oom = r.err.find("memory") != std::string::npos;
@@ -869,14 +906,14 @@ extern "C" sbe_status sbe_server_wait(sbe_server *s, long long id, double timeou
     if (latency_s) *latency_s = std::chrono::duration<double>(r.t_done - r.t_submit).count();
     if (out) {
         // assemble on the waiting thread, outside the lock
-        std::vector<double> j = r.jout;
+        std::vector<double> j = std::move(r.jout), laser = std::move(r.laser);
         double cp[NSLOT];
         for (int q = 0; q < NSLOT; ++q) cp[q] = r.cp[q];
         Problem prob = r.prob;
         lk.unlock();
         return guard([&]() -> sbe_status {
             SolveOutputs o;
-            assemble_outputs(prob, j, cp, o);
+            assemble_outputs(prob, j, cp, o, &laser);
             copy_out(o, out);
             return SBE_OK;
         });
@@ -893,6 +930,8 @@ extern "C" sbe_status sbe_server_cancel(sbe_server *s, long long id)
     Request &r = *it->second;
     if (r.state == Request::QUEUED) {
         r.state = Request::CANCELLED;
+    } else if (r.state == Request::ADMITTING) {
+        r.cancel_asked = true;   // the worker cancels it once its set-up returns
     } else if (r.state == Request::RESIDENT) {
         r.state = Request::CANCELLED;  // the worker, which owns the engine, drops the solve
         s->cv_work.notify_all();

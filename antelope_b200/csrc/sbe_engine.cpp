@@ -149,10 +149,39 @@ struct Engine::Group {
     int cap = 0;
 };
 
+namespace {
+// Device memory of resident solves comes from one pool per device that keeps
+// what it has (no release to the driver) and never makes an allocation wait
+// for another stream's pending work: a block freed on the compute stream is
+// reused by the copy stream only once that free has completed.
+cudaMemPool_t engine_pool(int device)
+{
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool;
+    cuda_check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attribute");
+    int no = 0;
+    cuda_check(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no), "pool attribute");
+    pools[device] = pool;
+    return pool;
+}
+}  // namespace
+
 Engine::Engine(int device, cudaStream_t stream, int steps_per_launch)
     : device_(device), stream_(stream), S_(steps_per_launch > 0 ? steps_per_launch : 512)
 {
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&up_, cudaStreamNonBlocking), "stream create");
+    pool_ = engine_pool(device_);
     capacity_ = 4096;
     cuda_check(cudaMalloc(&d_solves_, sizeof(SolveDev) * capacity_), "cudaMalloc(solves)");
     h_solves_ = new SolveDev[capacity_];
@@ -168,6 +197,7 @@ Engine::Engine(int device, cudaStream_t stream, int steps_per_launch)
 
 Engine::~Engine()
 {
+    cudaStreamSynchronize(up_);
     cudaStreamSynchronize(stream_);
     for (auto &kv : live_) {
         Solve &s = *kv.second;
@@ -190,9 +220,21 @@ Engine::~Engine()
     for (auto &e : prop_ev_) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     for (auto &e : red_ev_) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     cudaStreamSynchronize(stream_);
+    for (auto ev : pending_) cudaEventDestroy(ev);
+    for (auto ev : spare_ev_) cudaEventDestroy(ev);
+    cudaStreamDestroy(up_);
     cudaFree(d_solves_);
     delete[] h_solves_;
     cudaFree(d_ids_);
+}
+
+void Engine::drain_pending()
+{
+    for (cudaEvent_t ev : pending_) {
+        cuda_check(cudaStreamWaitEvent(stream_, ev, 0), "stream wait");
+        spare_ev_.push_back(ev);
+    }
+    pending_.clear();
 }
 
 Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
@@ -273,15 +315,11 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     const size_t cp_b = (size_t)s->ntiles * NSLOT * 8;
 
     auto alloc = [&](void **ptr, size_t b, const char *what) {
-        cudaError_t e = cudaMallocAsync(ptr, b, stream_);
+        cudaError_t e = cudaMallocFromPoolAsync(ptr, b, pool_, up_);
         if (e != cudaSuccess) {
-            cudaFreeAsync(s->kc, stream_);
-            cudaFreeAsync(s->st, stream_);
-            cudaFreeAsync(s->tab, stream_);
-            cudaFreeAsync(s->partial, stream_);
-            cudaFreeAsync(s->jout, stream_);
-            cudaFreeAsync(s->constpart, stream_);
-            if (s->snap_nc) cudaFreeAsync(s->snap_nc, stream_);
+            for (void *q : {s->kc, s->st, s->tab, (void *)s->partial, (void *)s->jout, (void *)s->constpart,
+                            (void *)s->snap_nc})
+                if (q) cudaFreeAsync(q, up_);
             cuda_check(e, what);
         }
     };
@@ -296,8 +334,6 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
         alloc((void **)&s->snap_pi, snap_n * 16, "alloc snapshots");
     }
     s->bytes = kc_b + st_b + tab_n * real + part_b + jout_b + cp_b + snap_n * 24;
-    s->h_jout = static_cast<double *>(pinned_.get(jout_b));
-    s->h_const = static_cast<double *>(pinned_.get(cp_b));
     cuda_check(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate");
 
     // field tables (host FP64, rounded once to the kernel's Real)
@@ -308,10 +344,10 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     if (!vg) tabd_own = phase_table(p, atab);
     const std::vector<double> &tabd = vg ? atab : tabd_own;
     if (s->precision == PREC_FP64) {
-        ring_.upload(s->tab, tabd.data(), tab_n * 8, stream_);
+        ring_.upload(s->tab, tabd.data(), tab_n * 8, up_);
     } else {
         std::vector<float> tf(tabd.begin(), tabd.end());
-        ring_.upload(s->tab, tf.data(), tab_n * 4, stream_);
+        ring_.upload(s->tab, tf.data(), tab_n * 4, up_);
     }
     InitArgs ia{};
     ia.nk = s->nk;
@@ -332,9 +368,14 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
         for (int j = 0; j < 2; ++j) { ia.va[i][j] = p.hal_va[i][j]; ia.vb[i][j] = p.hal_vb[i][j]; }
     ia.Ef = p.Ef;
     ia.dt = p.dt;
-    cuda_check(cudaMemsetAsync(s->kc, 0, kc_b, stream_), "memset constants");
-    cuda_check(cudaMemsetAsync(s->st, 0, st_b, stream_), "memset state");
-    cuda_check(launch_init_haldane(ia, s->precision, s->kc, s->st, s->constpart, stream_), "init kernel");
+    cuda_check(cudaMemsetAsync(s->kc, 0, kc_b, up_), "memset constants");
+    cuda_check(cudaMemsetAsync(s->st, 0, st_b, up_), "memset state");
+    cuda_check(launch_init_haldane(ia, s->precision, s->kc, s->st, s->constpart, up_), "init kernel");
+    cudaEvent_t ready;
+    if (spare_ev_.empty()) cuda_check(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event create");
+    else { ready = spare_ev_.back(); spare_ev_.pop_back(); }
+    cuda_check(cudaEventRecord(ready, up_), "event record");
+    pending_.push_back(ready);
 
     s->slot = free_slots_.back();
     free_slots_.pop_back();
@@ -446,6 +487,7 @@ void Engine::rebuild_lists()
 
 void Engine::step()
 {
+    drain_pending();
     // a solve that finished at the previous tick leaves the launch lists
     for (auto &kv : live_)
         if (kv.second->admit_tick + kv.second->nticks == tick_) dirty_ = true;
@@ -529,7 +571,12 @@ void Engine::kernel_times(double *prop_ms, int *prop_n, double *red_ms, int *red
 
 void Engine::fetch_async(int id)
 {
+    drain_pending();
     Solve &s = get(id);
+    // pinned result buffers are taken when a solve finishes, not when it is
+    // admitted (a burst of admissions would otherwise wait on page locking)
+    if (!s.h_jout) s.h_jout = static_cast<double *>(pinned_.get((size_t)s.Nt * NSLOT * 8));
+    if (!s.h_const) s.h_const = static_cast<double *>(pinned_.get((size_t)s.ntiles * NSLOT * 8));
     cuda_check(cudaMemcpyAsync(s.h_jout, s.jout, (size_t)s.Nt * NSLOT * 8, cudaMemcpyDeviceToHost, stream_),
                "copy outputs");
     cuda_check(cudaMemcpyAsync(s.h_const, s.constpart, (size_t)s.ntiles * NSLOT * 8, cudaMemcpyDeviceToHost, stream_),
@@ -561,6 +608,7 @@ void Engine::raw_outputs(int id, std::vector<double> &jout, double cp[NSLOT])
 
 int Engine::snapshots(int id, double *occ1d, double *nc, double *pi)
 {
+    drain_pending();
     Solve &s = get(id);
     if (s.nshots == 0) return 0;
     const Problem &p = s.prob;
@@ -582,6 +630,7 @@ int Engine::snapshots(int id, double *occ1d, double *nc, double *pi)
 
 void Engine::harmonics(int id, double w0, int hmax, double *band_power)
 {
+    drain_pending();
     Solve &s = get(id);
     const Problem &p = s.prob;
     HarmonicsInput in;
@@ -626,6 +675,7 @@ void Engine::remove(int id)
 {
     auto it = live_.find(id);
     if (it == live_.end()) return;
+    drain_pending();   // the frees below follow the solve's set-up on the copy stream
     Solve &s = *it->second;
     cudaFreeAsync(s.kc, stream_);
     cudaFreeAsync(s.st, stream_);
@@ -646,7 +696,8 @@ void Engine::remove(int id)
 }
 
 // ================================================================ outputs
-void assemble_outputs(const Problem &p, const std::vector<double> &jout, const double cp[NSLOT], SolveOutputs &o)
+void assemble_outputs(const Problem &p, const std::vector<double> &jout, const double cp[NSLOT], SolveOutputs &o,
+                      const std::vector<double> *laser)
 {
     const int Nt = p.laser.Nt, N = p.nband;
     o.Nt = Nt;
@@ -655,18 +706,14 @@ void assemble_outputs(const Problem &p, const std::vector<double> &jout, const d
     o.intra.assign((size_t)Nt * 3, 0.0);
     o.occ.assign((size_t)Nt * (N + 1), 0.0);
     o.coh.assign((size_t)Nt * 2, 0.0);
-    o.laser.assign((size_t)Nt * 7, 0.0);
+    if (laser && laser->size() == (size_t)Nt * 7) o.laser = *laser;
+    else o.laser = laser_rows(p);
     const bool vg = p.gauge == GAUGE_VELOCITY;
     const double W = p.total_weight, dV = p.dV, Ntot = (double)p.ntotal();
     std::vector<double> occ00((size_t)Nt), occ01r((size_t)Nt), occ01i((size_t)Nt);
     for (int n = 0; n < Nt; ++n) {
         const double *j = &jout[(size_t)n * NSLOT];
-        const double t = p.laser.atmin + p.laser.dt * n;
-        double A[3], E[3];
-        p.laser.eval(t, A, E);
-        double *L = &o.laser[(size_t)n * 7];
-        L[0] = t;
-        for (int d = 0; d < 3; ++d) { L[1 + d] = E[d]; L[4 + d] = A[d]; }
+        const double *A = &o.laser[(size_t)n * 7 + 4];
         double inter[3] = {j[0], j[1], 0.0};
         double intra[3] = {j[2], j[3], 0.0};
         if (vg) {

@@ -150,8 +150,15 @@ private:
     Solve &get(int id);
     const Solve &get(int id) const;
 
+    // Admission work (allocations, uploads, per-k set-up) runs on its own
+    // copy stream `up_` so it never waits behind queued ticks; the compute
+    // stream waits on the events in `pending_` before it next touches solves.
+    void drain_pending();
     int device_;
     cudaStream_t stream_;
+    cudaStream_t up_ = nullptr;
+    cudaMemPool_t pool_ = nullptr;
+    std::vector<cudaEvent_t> pending_, spare_ev_;
     int S_;
     int tick_ = 0;
     int next_id_ = 0;
@@ -181,9 +188,10 @@ Shape autotune_shape(int device, const Problem &p, int precision);
 // Cached tuned shape only (no tuning run); false when none is cached.
 bool autotune_lookup(int device, const Problem &p, int precision, Shape *out);
 
-// Assemble the reference's output quantities from the per-step slot sums.
+// Assemble the reference's output quantities from the per-step slot sums;
+// `laser` may hold the problem's laser_rows() already built by the caller.
 void assemble_outputs(const Problem &p, const std::vector<double> &jout, const double constpart[NSLOT],
-                      SolveOutputs &out);
+                      SolveOutputs &out, const std::vector<double> *laser = nullptr);
 
 // Write the reference's output files into `dir` (antelope.cpp:176-184,
 // 208-235, 514-548), byte-for-byte in its formats.

@@ -637,6 +637,18 @@ std::vector<double> a_table(const Problem &p)
     return tab;
 }
 
+std::vector<double> laser_rows(const Problem &p)
+{
+    const Laser &L = p.laser;
+    std::vector<double> rows((size_t)L.Nt * 7);
+    for (int n = 0; n < L.Nt; ++n) {
+        double *r = &rows[(size_t)n * 7];
+        r[0] = L.atmin + L.dt * n;  // antelope.cpp:215
+        L.eval(r[0], r + 4, r + 1);
+    }
+    return rows;
+}
+
 std::vector<double> phase_table(const Problem &p, const std::vector<double> &atab)
 {
     const size_t rows = atab.size() / 2;

@@ -133,6 +133,9 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported);
 std::vector<double> stage_fractions(int rk);
 // A(t) table [Nt][nts][2] (x, y) at t = (atmin + dt n) + c dt, FP64.
 std::vector<double> a_table(const Problem &p);
+// The columns of outlaserdata.dat, [Nt][7]: t_n, E(t_n), A(t_n)
+// (antelope.cpp:208-235; laser.h:301-322).
+std::vector<double> laser_rows(const Problem &p);
 // Haldane length gauge: [Nt][nts][12] cos/sin of A.a_i and A.b_i.
 std::vector<double> phase_table(const Problem &p, const std::vector<double> &atab);
 

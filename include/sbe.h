@@ -223,7 +223,8 @@ typedef struct sbe_server_opts {
 sbe_status sbe_server_create(const sbe_server_opts *opts, sbe_server **out);
 sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, long long *request_id);
 /* Wait up to timeout_s (< 0: forever) for a request; fill its outputs and
- * its latency (submit -> result available, seconds). */
+ * its latency (submit -> result available, seconds).  A request's final state
+ * is returned once: afterwards the server forgets it (unknown request id). */
 sbe_status sbe_server_wait(sbe_server *s, long long request_id, double timeout_s, const sbe_outputs *out,
                            double *latency_s);
 sbe_status sbe_server_cancel(sbe_server *s, long long request_id);

@@ -154,6 +154,37 @@ def test_server_alone_equals_in_mix():
     srv.close()
 
 
+def test_server_cancel_and_single_delivery():
+    """Requests cancelled in any state end CANCELLED and free their solve;
+    the others complete with the same bits as alone; a request's final state
+    is returned once, after which the server has forgotten it."""
+    cases = [variant(calc__Npoints=[12 + i, 9], pulse__cep=15.0 * i) for i in range(20)]
+    probs = [ab.Problem.from_dict(c) for c in cases]
+    shape = dict(tile_k=64, k_per_thread=1)   # the server never tunes: fix the shape on both sides
+    srv = ab.Server(precision="fp64", steps_per_launch=64, **shape)
+    ids = [srv.submit(p) for p in probs]
+    cancelled = set(ids[1::3])
+    for rid in cancelled:
+        srv.cancel(rid)
+    for i, rid in enumerate(ids):
+        if rid in cancelled:
+            try:
+                srv.wait(rid, timeout=120)   # may have finished before the cancel arrived
+            except ab.SbeError as e:
+                assert e.name == "SBE_CANCELLED"
+        else:
+            o, _ = srv.wait(rid, timeout=120)
+            ref = ab.solve(probs[i], precision="fp64", steps_per_launch=64, **shape)
+            assert np.array_equal(o.inter, ref.inter) and np.array_equal(o.occ, ref.occ)
+    srv._problems[ids[0]] = probs[0]   # ask again for a delivered request
+    with pytest.raises(ab.SbeError) as e:
+        srv.wait(ids[0], timeout=1)
+    assert "unknown request id" in str(e.value)
+    st = srv.stats()
+    assert st["failed"] == 0 and st["resident"] == 0
+    srv.close()
+
+
 def test_cli_drop_in(tmp_path):
     """sbe_run in a directory holding inputParam.cfg writes the reference's
     six files with the reference's values."""
