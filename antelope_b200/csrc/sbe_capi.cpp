@@ -684,6 +684,7 @@ void sbe_server::loop()
     eo.tile_k = opts.tile_k;
     eo.kpt = opts.k_per_thread;
     eo.allow_tuning = false;  // never stall the serving loop on a tuning run
+    eo.throughput_shape = true;  // resident solves share the GPU: full CTAs unless a tuned shape is cached
     eo.snapshots = false;     // requests return the file outputs only (sbe_server_wait)
     // admissions set up between two tick issues: a burst of arrivals is
     // admitted in slices while the GPU keeps working on the queued ticks

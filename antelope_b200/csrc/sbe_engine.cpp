@@ -250,6 +250,9 @@ Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
     } else if (o.kpt <= 0 && autotune_enabled() &&
                (o.allow_tuning || autotune_lookup(device_, p, prec, &s))) {
         return o.allow_tuning ? autotune_shape(device_, p, prec) : s;
+    } else if (o.throughput_shape) {
+        // solves that share the GPU with many others: full CTAs
+        s.tile_k = 256 * s.kpt;
     } else {
         // largest CTA (<= 128 threads) that still gives >= 2 CTAs per SM
         int sms = 148;

@@ -32,6 +32,7 @@ struct EngineOptions {
     int kpt = 0;             // k-points per thread (0: tuned default)
     int steps_per_launch = 0;  // S (0: default)
     bool allow_tuning = true;  // false: a cached tuned shape or the heuristic, never a tuning run
+    bool throughput_shape = false;  // heuristic: full 256-thread CTAs (many solves share the GPU)
     int k_begin = 0, k_end = 0;  // k-slice [k_begin, k_end) of the grid (0, 0: all of it)
     bool snapshots = true;       // take the problem's density snapshots (calc.shotNumber)
 };
