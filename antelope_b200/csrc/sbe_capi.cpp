@@ -404,9 +404,9 @@ extern "C" sbe_status sbe_solver_snapshots(sbe_solver *s, double *occ1d, double 
     if (!s) return fail(SBE_INVALID_ARGUMENT, "null solver");
     if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
     return guard([&]() -> sbe_status {
-        if (!s->eng) return fail(SBE_UNSUPPORTED, "density snapshots are built for the Haldane model");
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
-        if (s->eng->snapshots(s->id, occ1d, nc, pi) == 0)
+        const int n = s->wan ? s->wan->snapshots(occ1d, nc, pi) : s->eng->snapshots(s->id, occ1d, nc, pi);
+        if (n == 0)
             return fail(SBE_INVALID_ARGUMENT, "the problem takes no snapshots (calc.shotNumber <= 0)");
         return SBE_OK;
     });

@@ -606,8 +606,6 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
     if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) unsup("gauge LengthHamiltonian is not implemented in the reference either");
     if (p.shot_number > 0 && p.shot_every() <= 0)   // the reference would take ktime % 0
         throw CfgError("calc.shotNumber gives a snapshot interval of 0 steps (period / shotNumber < dt)");
-    if (p.shot_number > 0 && p.model != MODEL_HALDANE)
-        unsup("density snapshots (calc.shotNumber > 0) are built for the Haldane model");
     if (p.rk == 45 && p.model == MODEL_HALDANE)
         unsup("adaptive Cash-Karp steps are built for the N-band (table) models only");
     return p;

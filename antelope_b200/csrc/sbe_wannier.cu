@@ -1170,6 +1170,7 @@ __device__ void control_decide(const WanDev &P, WanCtl *ctl, double emax)
 {
     ctl->attempts++;
     ctl->need_current = 0;
+    ctl->shot = -1;
     ctl->emax = emax;
     const double dt = P.dt, tend = P.atmin + dt * (ctl->n + 1);
     bool accept = true;
@@ -1196,6 +1197,9 @@ __device__ void control_decide(const WanDev &P, WanCtl *ctl, double emax)
         ctl->steps++;
         if (ctl->last) {
             ctl->tc = tend;
+            // the state is now past interval n: its snapshot (after step n,
+            // antelope.cpp:342) is due when n is a multiple of the interval
+            if (P.shot_every > 0 && ctl->n % P.shot_every == 0) ctl->shot = ctl->n;
             ctl->n++;
             if (ctl->n >= P.Nt) {
                 ctl->done = 1;
@@ -1222,7 +1226,10 @@ template <class RF> __global__ void __launch_bounds__(1024) wan_control(const Wa
     __shared__ double cs[WAN_NSLOT][64];
     const WanDev &P = *Pp;
     WanCtl *ctl = P.ctl;
-    if (ctl->done) return;
+    if (ctl->done) {
+        if (threadIdx.x == 0) ctl->shot = -1;   // a snapshot is taken once
+        return;
+    }
     const int t = threadIdx.x, nt = P.ntiles;
     double m = 0.0;
     for (int i = t; i < nt; i += blockDim.x) m = fmax(m, P.tile_err[i]);
@@ -1251,6 +1258,85 @@ template <class RF> __global__ void __launch_bounds__(1024) wan_control(const Wa
     if (!c.done) prepare_stages<RF>(P, c);
 }
 
+// ============================================================= snapshots
+// Density snapshot of the output step ctl->shot, taken after the controller
+// accepted the end of that interval (the committed state is at t_{shot+1}).
+// Velocity gauge: rho is in the band basis and its elements [Nval][Nval] and
+// [Nval][Nval-1] are read directly (antelope.cpp:391-398).  Length gauge:
+// rho' = U^dag rho U with U the eigenvectors of H0(k + A(t_shot)) --
+// SBEs::WannierToHamiltonian at the step's start time (SBEs.h:927-940,
+// antelope.cpp:358) -- from the same Fourier sums as the attempt kernel and
+// Jacobi sweeps from the identity, eigenvectors ranked by ascending
+// eigenvalue as zheevr orders them.  One warp per k-point.
+template <class RF>
+__global__ void __launch_bounds__(32 * WAN_WARPS) wan_snapshot(const WanDev *__restrict__ Pp)
+{
+    const WanDev &P = *Pp;
+    const int shot = P.ctl->shot;
+    if (shot < 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const WanSmem L = wan_smem(P.N, P.nR, sizeof(RF));
+    RF *Rc = reinterpret_cast<RF *>(smem_raw + L.Rc);
+    BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    if (!P.vg) {
+        load_lattice<RF>(P, Rc);
+        fill_tables(bh, P.N);
+    }
+    __syncthreads();
+    const int k = blockIdx.x * WAN_WARPS + wi;
+    if (k >= P.nk) return;
+    const int N = P.N, NN = N * N, nv = P.nval;
+    const double2 *rho = P.rho[P.ctl->buf] + (size_t)k * NN;
+    const size_t o = (size_t)(shot / P.shot_every) * P.nk + k;
+    if (P.vg) {
+        if (lane == 0) {
+            P.snap_nc[o] = rho[nv * N + nv].x;
+            P.snap_pi[2 * o] = rho[nv * N + nv - 1].x;
+            P.snap_pi[2 * o + 1] = rho[nv * N + nv - 1].y;
+        }
+        return;
+    }
+    const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, P.N, P.nR);
+    double kv[3], wt, A[3], E[3];
+    kpoint(P, k, kv, wt);
+    laser_eval(P.laser, P.atmin + P.dt * shot, A, E);   // antelope.cpp:299
+    for (int d = 0; d < 3; ++d) kv[d] += A[d];
+    kphases<RF>(P, kv, w.ph, lane);
+    for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
+    __syncwarp();
+    fourier<RF>(w, bh.ut, P, false, Rc, lane);
+    for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
+    __syncwarp();
+    jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
+    if (lane == 0) {
+        int c = 0, v = 0;   // eigenvector columns of ascending rank nv and nv - 1
+        for (int j = 0; j < N; ++j) {
+            const double ej = w.B[j * N + j].x;
+            int rank = 0;
+            for (int i = 0; i < N; ++i) {
+                const double ei = w.B[i * N + i].x;
+                rank += (ei < ej) || (ei == ej && i < j);
+            }
+            if (rank == nv) c = j;
+            if (rank == nv - 1) v = j;
+        }
+        double2 cc = make_double2(0, 0), cv = make_double2(0, 0);
+        for (int i = 0; i < N; ++i) {
+            double2 rc = make_double2(0, 0), rv = make_double2(0, 0);   // (rho U)_{ic}, (rho U)_{iv}
+            for (int j = 0; j < N; ++j) {
+                cfma(rc, rho[i * N + j], w.U[j * N + c]);
+                cfma(rv, rho[i * N + j], w.U[j * N + v]);
+            }
+            cfmac(cc, w.U[i * N + c], rc);
+            cfmac(cv, w.U[i * N + c], rv);
+        }
+        P.snap_nc[o] = cc.x;
+        P.snap_pi[2 * o] = cv.x;
+        P.snap_pi[2 * o + 1] = cv.y;
+    }
+}
+
 // ============================================================= launchers
 template <class RF> static cudaError_t allow_smem()
 {
@@ -1264,6 +1350,8 @@ template <class RF> static cudaError_t allow_smem()
         e = cudaFuncSetAttribute(wan_vg_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(wan_vg_attempt<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(wan_snapshot<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     done = e == cudaSuccess;
     return e;
 }
@@ -1311,6 +1399,18 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
         if (precision == 0) wan_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
         else wan_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wan_snapshot(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st)
+{
+    if (w.shot_every <= 0) return cudaSuccess;
+    const int grid = (w.nk + WAN_WARPS - 1) / WAN_WARPS;
+    cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
+    if (e != cudaSuccess) return e;
+    const size_t sm = wan_smem_bytes(w.N, w.nR, precision);
+    if (precision == 0) wan_snapshot<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    else wan_snapshot<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
     return cudaGetLastError();
 }
 

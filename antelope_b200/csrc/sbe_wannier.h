@@ -39,6 +39,7 @@ struct WanCtl {
     int need_current;   // the next attempt records the currents at tc = t_n first
     int done;
     int error;          // 1: step-size underflow / too many rejections
+    int shot;           // output step whose density snapshot is due (the interval just completed), or -1
     long long steps, attempts, rejects;
 };
 
@@ -67,6 +68,13 @@ struct WanDev {
     double2 *vg_P;          // velocity gauge: [nk][2][N*N] P_a = U^dag J_a U
     double *stage_AE;       // [6][6] A and E at the stage times of the next attempt
     void *stage_cA;         // [6][nR] e^{i A(t_s) R} of the next attempt (Fourier precision)
+    // density snapshots (antelope.cpp:340-422): every shot_every output steps
+    // (0: none), per k the conduction occupation and coherence of rho after
+    // the step, in the band basis (velocity gauge) or in the eigenbasis of
+    // H0(k + A(t_n)) (length gauge); [nshots][nk] and [nshots][nk][2]
+    int shot_every;
+    double *snap_nc;
+    double *snap_pi;
 };
 
 size_t wan_smem_bytes(int N, int nR, int precision);
@@ -74,5 +82,7 @@ cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st);
 cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st);
 cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st);
 cudaError_t launch_wan_control(const WanDev *dw, int precision, cudaStream_t st);
+// the snapshot of the interval the last control step completed, if one is due
+cudaError_t launch_wan_snapshot(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st);
 
 }  // namespace sbe

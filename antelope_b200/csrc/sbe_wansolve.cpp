@@ -3,6 +3,7 @@
 // reference's output quantities for N bands (antelope.cpp:514-548).
 #include "sbe_wansolve.h"
 
+#include "sbe_kernels.h"
 #include "sbe_spectrum.h"
 
 #include <algorithm>
@@ -88,6 +89,12 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     dalloc(&w_.ctl, sizeof(WanCtl), st, "alloc control");
     dalloc(&w_.stage_AE, sizeof(double) * 36, st, "alloc stage fields");
     dalloc(&w_.stage_cA, cplx * 6 * (size_t)w_.nR, st, "alloc stage phases");
+    nshots_ = p.nshots();
+    if (nshots_ > 0) {   // density snapshots (antelope.cpp:267-422)
+        w_.shot_every = p.shot_every();
+        dalloc(&w_.snap_nc, sizeof(double) * nshots_ * nk, st, "alloc snapshots");
+        dalloc(&w_.snap_pi, sizeof(double) * 2 * nshots_ * nk, st, "alloc snapshots");
+    }
     dalloc(&d_w_, sizeof(WanDev), st, "alloc descriptor");
     w_.V = V;
     w_.h = h;
@@ -114,6 +121,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     c.n = 0;
     c.buf = 0;
     c.need_current = 1;
+    c.shot = -1;
     const double tend = w_.atmin + w_.dt;
     c.hs = c.h;
     c.last = 0;
@@ -150,6 +158,8 @@ WannierSolve::~WannierSolve()
     cudaFreeAsync(w_.stage_AE, stream_);
     cudaFreeAsync(w_.stage_cA, stream_);
     cudaFreeAsync(d_w_, stream_);
+    if (w_.snap_nc) cudaFreeAsync(w_.snap_nc, stream_);
+    if (w_.snap_pi) cudaFreeAsync(w_.snap_pi, stream_);
     cudaStreamSynchronize(stream_);
     if (h_ctl_) cudaFreeHost(h_ctl_);
 }
@@ -166,6 +176,7 @@ void WannierSolve::run(cudaStream_t st)
         for (int c = 0; c < chunk; ++c) {
             cuda_check(launch_wan_attempt(w_, d_w_, precision_, st), "Wannier attempt kernel");
             cuda_check(launch_wan_control(d_w_, precision_, st), "Wannier control kernel");
+            cuda_check(launch_wan_snapshot(w_, d_w_, precision_, st), "Wannier snapshot kernel");
         }
         launched += chunk;
         cuda_check(cudaMemcpyAsync(h_ctl_, w_.ctl, sizeof(WanCtl), cudaMemcpyDeviceToHost, st), "copy control");
@@ -174,7 +185,7 @@ void WannierSolve::run(cudaStream_t st)
         if (launched > max_attempts) throw CudaError("Wannier solve made no progress (step-size controller)");
     }
     if (h_ctl_->error) throw CudaError("Cash-Karp step size underflow: tolerance unreachable");
-    launches_ = (int)(2 * launched);
+    launches_ = (int)((w_.shot_every > 0 ? 3 : 2) * launched);   // attempt, control (, snapshot)
 }
 
 void WannierSolve::harmonics(double w0, int hmax, double *band_power)
@@ -202,6 +213,25 @@ void WannierSolve::harmonics(double w0, int hmax, double *band_power)
     }
     harmonics_on_device(in, w0, hmax, band_power, stream_);
     if (A) cudaFreeAsync(A, stream_);
+}
+
+int WannierSolve::snapshots(double *occ1d, double *nc, double *pi)
+{
+    if (nshots_ == 0) return 0;
+    const size_t n = (size_t)nshots_ * w_.nk;
+    if (occ1d) {
+        double *d_occ = nullptr;
+        const size_t b = (size_t)nshots_ * prob_.Nk[0] * 8;
+        dalloc(&d_occ, b, stream_, "alloc snapshot bins");
+        cudaError_t e = launch_snapshot_bins(w_.snap_nc, w_.nk, w_.k_offset, prob_.Nk, nshots_, d_occ, stream_);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(occ1d, d_occ, b, cudaMemcpyDeviceToHost, stream_);
+        cudaFreeAsync(d_occ, stream_);
+        cuda_check(e, "snapshot bins");
+    }
+    if (nc) cuda_check(cudaMemcpyAsync(nc, w_.snap_nc, n * 8, cudaMemcpyDeviceToHost, stream_), "copy snapshots");
+    if (pi) cuda_check(cudaMemcpyAsync(pi, w_.snap_pi, n * 16, cudaMemcpyDeviceToHost, stream_), "copy snapshots");
+    cuda_check(cudaStreamSynchronize(stream_), "snapshot sync");
+    return nshots_;
 }
 
 std::vector<double> WannierSolve::sums()

@@ -22,12 +22,14 @@ public:
     std::vector<double> sums();
     // harmonic band powers h = 1..hmax from the device-resident sums
     void harmonics(double w0, int hmax, double *band_power);
+    // density snapshots (as Engine::snapshots); returns their number
+    int snapshots(double *occ1d, double *nc, double *pi);
     int launches() const { return launches_; }
     const WanCtl &control() const { return *h_ctl_; }
 
 private:
     Problem prob_;
-    int precision_, device_;
+    int precision_, device_, nshots_ = 0;
     cudaStream_t stream_;
     WanDev w_{};
     WanDev *d_w_ = nullptr;

@@ -140,7 +140,7 @@ sbe_status sbe_solver_kernel_times(sbe_solver *s, double *propagate_ms, int *pro
                                    double *reduce_ms, int *reduce_launches);
 void sbe_solver_destroy(sbe_solver *s);
 
-/* Density snapshots of a finished solve (Haldane model, both gauges), the
+/* Density snapshots of a finished solve (every model, both gauges), the
  * data of the reference's snapshot files (antelope.cpp:340-422); any array
  * may be NULL:
  *   occ1d[nshots*n0]       occupation_1d_integration.dat: Re sum_k w_k rho'_cc

@@ -127,6 +127,7 @@ SNAPSHOT_CASES = {
     "lw_shots": variant(top__gauge="Wannier", calc__shotNumber=3, calc__Npoints=[7, 6]),
     "vg_shots_fermi_t1": variant(Haldane__Ef=0.0, calc__T1=150.0, calc__shotNumber=5, pulse__ellip=0.3),
     "kanemele_w_shots": _km_shots,
+    "tmdcs_v_shots": material("TMDCs", "Velocity", calc__shotNumber=3),
 }
 
 # A one-cycle case whose output files are kept verbatim (byte format pin).

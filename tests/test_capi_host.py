@@ -12,7 +12,7 @@ import pytest
 from antelope_b200 import Problem, SbeError, capi
 from antelope_b200.api import Outputs, write_outputs
 from antelope_b200 import cfgtext
-from cases import BASE, GOLDEN_CASES, MATERIAL_CASES, MATERIALS, SNAPSHOT_CASES, TEXT_CASE, variant
+from cases import BASE, GOLDEN_CASES, MATERIAL_CASES, SNAPSHOT_CASES, TEXT_CASE, variant
 from oracle import pyoracle
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -88,8 +88,6 @@ def _err(case_or_text):
                 c.__setitem__("Haldane2L", dict(c["Haldane"], t11=0.01, polytype="ABC"))),
      "SBE_BAD_CONFIG", "Undefined polytype"),
     (lambda c: c["calc"].__setitem__("shotNumber", 1000), "SBE_BAD_CONFIG", "snapshot interval of 0 steps"),
-    (lambda c: (c.__setitem__("target", "KaneMele"), c.__setitem__("KaneMele", dict(MATERIALS["KaneMele"])),
-                c["calc"].__setitem__("shotNumber", 2)), "SBE_UNSUPPORTED", "snapshots"),
     (lambda c: c.__setitem__("gauge", "Hamiltonian"), "SBE_UNSUPPORTED", "LengthHamiltonian"),
 ])
 def test_diagnostics(mutate, status, msg):

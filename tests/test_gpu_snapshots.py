@@ -25,6 +25,7 @@ from oracle import pyoracle
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 HALDANE_SHOTS = ["vg_shots", "lw_shots", "vg_shots_fermi_t1"]
+TABLE_SHOTS = ["kanemele_w_shots", "tmdcs_v_shots"]   # N-band kernels, both gauges
 
 
 def _run(case, **opts):
@@ -39,7 +40,7 @@ def _close(a, b, tol):
     return np.abs(a - b).max() <= tol * np.abs(b).max()
 
 
-@pytest.mark.parametrize("name", HALDANE_SHOTS)
+@pytest.mark.parametrize("name", HALDANE_SHOTS + TABLE_SHOTS)
 def test_fp64_snapshots_match_oracle_and_reference(name):
     case = SNAPSHOT_CASES[name]
     _, snaps = _run(case, precision="fp64")
@@ -59,7 +60,7 @@ def test_fp64_snapshots_match_oracle_and_reference(name):
     assert np.abs(np.abs(snaps["pi"][:, -1]) - np.abs(rp[:, -1])).max() <= 1e-10 * np.abs(rp[:, -1]).max()
 
 
-@pytest.mark.parametrize("name", HALDANE_SHOTS)
+@pytest.mark.parametrize("name", HALDANE_SHOTS + TABLE_SHOTS)
 def test_mixed_snapshots_near_fp64(name):
     case = SNAPSHOT_CASES[name]
     _, a = _run(case, precision="fp64")
@@ -127,3 +128,20 @@ def test_solver_without_snapshots_refuses_to_return_them():
         s.snapshots()
     s.close()
     assert "no snapshots" in str(e.value)
+
+
+def test_adaptive_table_model_snapshots_match_oracle():
+    """Cash-Karp 4(5) steps (one step size per solve, steps landing on the
+    output times): the snapshot of output step n is taken once the accepted
+    steps reach t_{n+1}."""
+    from antelope_b200 import wannier
+    case = wannier.wannier_case(seed=3, n=9, ncycles=0.05, rk="cashkarp45", tol=1e-9)
+    case["calc"]["shotNumber"] = 100
+    _, snaps = _run(case, precision="fp64")
+    ref = pyoracle.run(case)
+    assert snaps["nc"].shape == ref["nc"].shape and snaps["nc"].shape[0] > 2
+    # adaptive steps: the step sequence is the oracle's to rounding, the
+    # values to the controller's tolerance
+    assert _close(snaps["occ1d"], ref["occ1d"], 1e-7)
+    assert _close(snaps["nc"], ref["nc"], 1e-7)
+    assert _close(np.abs(snaps["pi"]), np.abs(ref["pi"]), 1e-7)
