@@ -379,6 +379,100 @@ void square_sband(const CfgValue *mat, Problem &p)
     set_bz(p, PI / a0, PI / a0);
 }
 
+// ------------------------------------------------------------ Bi2Se3surf
+// Bi2Se3surf.h (surface states, PRA 103, 023101): two bands, parameters
+// hard-coded in the constructor (the cfg group is not read), triangular
+// vectors a_i and b_i (SetBasis).  With A = sum over i of cos / sin (k.a_i),
+// B likewise, and w = -2 pi / 3 (GenBcomp):
+//   h0 = 2 A0 cosA + 2 B0 cosB,   h5 = 2 A1 cosA + 2 B1 cosB + m11,
+//   h1 = -2 A3 sin(w) (sin a_1 - sin a_2) + 2 B3 (sin b_0 + cos(w) (sin b_1 - sin b_2)),
+//   h2 = -2 B3 sin(w) (sin b_1 - sin b_2) - 2 A3 (sin a_0 + cos(w) (sin a_1 + sin a_2)),
+//   h3 = 2 A2 sinA;
+//   B0 = h0 + (B0/B1)(h5(Gamma) - h5), B_{1,2,3} = sqrt(1 - B0^2/B1^2) h_{1,2,3},
+//   H = [[B0 + B3, B1 - i B2], [B1 + i B2, B0 - B3]].
+// GenJMatrix writes J = -(dB/dk) term by term: its derivative of the B3 part
+// of h1 carries (b_1 + b_2) where h1 has (b_1 - b_2) -- transcribed as
+// written; B3 = 0 in the hard-coded set, so the term vanishes.
+void bi2se3_surface(Problem &p)
+{
+    const double AU_EV = 27.211386245988;  // constant.h:35
+    const double Ac[4] = {-0.0255 / AU_EV, 0.1937 / AU_EV, 0.2240 / AU_EV, 0.0551 / AU_EV};
+    const double Bc[4] = {0.0164 / AU_EV, 0.1203 / AU_EV, 0.3264 / AU_EV, 0.0 / AU_EV};
+    const double m11 = -1.6978 / AU_EV, a0 = 4.14 / AU_ANGSTROM, r3 = std::sqrt(3.);
+    const double va[3][2] = {{a0, 0.}, {-a0 / 2, r3 / 2 * a0}, {-a0 / 2, -r3 / 2 * a0}};
+    const double vb[3][2] = {{0., r3 * a0 / 3}, {-a0 / 2, -r3 / 6 * a0}, {a0 / 2, -r3 / 6 * a0}};
+    const double w = -2. * PI / 3., sw = std::sin(w), cw = std::cos(w);
+    const double rb = Bc[0] / Bc[1], bco = std::sqrt(1. - Bc[0] * Bc[0] / (Bc[1] * Bc[1]));
+    const double h5g = 6. * Ac[1] + 6. * Bc[1] + m11;
+    TBBuilder tb(2);
+    // B0 on both diagonal entries; B3 = +/- on them
+    auto diag = [&](int a, int sign, auto add) {
+        add(a, 0, 0, 1.0);
+        add(a, 1, 1, sign);
+    };
+    for (int i = 0; i < 3; ++i) {
+        // B0 = h0 - rb h5 + rb h5(Gamma)
+        diag(-1, 1, [&](int a, int m, int n, double sg) {
+            tb.cos_(a, m, n, va[i][0], va[i][1], sg * (2. * Ac[0] - rb * 2. * Ac[1]));
+            tb.cos_(a, m, n, vb[i][0], vb[i][1], sg * (2. * Bc[0] - rb * 2. * Bc[1]));
+        });
+        // B3 = bco 2 A2 sinA: +H00, -H11
+        diag(-1, -1, [&](int a, int m, int n, double sg) {
+            tb.sin_(a, m, n, va[i][0], va[i][1], sg * bco * 2. * Ac[2]);
+        });
+    }
+    diag(-1, 1, [&](int a, int m, int n, double sg) { tb.const_(a, m, n, sg * rb * (h5g - m11)); });
+    // B1 -/+ i B2 off the diagonal: (0,1) gets B1 - i B2, (1,0) B1 + i B2
+    auto offd = [&](int a, double vx, double vy, bool is_cos, double c1, double c2) {
+        // c1 f(k.v) into B1 and c2 f(k.v) into B2
+        for (int m = 0; m < 2; ++m) {
+            const cplx c = c1 + (m == 0 ? -1.0 : 1.0) * I1 * c2;
+            if (is_cos) tb.cos_(a, m, 1 - m, vx, vy, c);
+            else tb.sin_(a, m, 1 - m, vx, vy, c);
+        }
+    };
+    // h1 = -2 A3 sw (sin a1 - sin a2) + 2 B3 (sin b0 + cw (sin b1 - sin b2))
+    offd(-1, va[1][0], va[1][1], false, bco * (-2. * Ac[3] * sw), 0.);
+    offd(-1, va[2][0], va[2][1], false, bco * (2. * Ac[3] * sw), 0.);
+    offd(-1, vb[0][0], vb[0][1], false, bco * (2. * Bc[3]), 0.);
+    offd(-1, vb[1][0], vb[1][1], false, bco * (2. * Bc[3] * cw), 0.);
+    offd(-1, vb[2][0], vb[2][1], false, bco * (-2. * Bc[3] * cw), 0.);
+    // h2 = -2 B3 sw (sin b1 - sin b2) - 2 A3 (sin a0 + cw (sin a1 + sin a2))
+    offd(-1, vb[1][0], vb[1][1], false, 0., bco * (-2. * Bc[3] * sw));
+    offd(-1, vb[2][0], vb[2][1], false, 0., bco * (2. * Bc[3] * sw));
+    offd(-1, va[0][0], va[0][1], false, 0., bco * (-2. * Ac[3]));
+    offd(-1, va[1][0], va[1][1], false, 0., bco * (-2. * Ac[3] * cw));
+    offd(-1, va[2][0], va[2][1], false, 0., bco * (-2. * Ac[3] * cw));
+    // J_a = -(dB/dk_a), GenJMatrix term by term
+    for (int a = 0; a < 2; ++a) {
+        for (int i = 0; i < 3; ++i) {
+            // d/dk_a cos(k.v) = -v_a sin(k.v); J gets the minus sign of -(dB0 +/- dB3)
+            diag(a, 1, [&](int aa, int m, int n, double sg) {
+                tb.sin_(aa, m, n, va[i][0], va[i][1], -sg * -va[i][a] * (2. * Ac[0] - rb * 2. * Ac[1]));
+                tb.sin_(aa, m, n, vb[i][0], vb[i][1], -sg * -vb[i][a] * (2. * Bc[0] - rb * 2. * Bc[1]));
+            });
+            diag(a, -1, [&](int aa, int m, int n, double sg) {
+                tb.cos_(aa, m, n, va[i][0], va[i][1], -sg * va[i][a] * bco * 2. * Ac[2]);
+            });
+        }
+        // dh1 = -2 A3 sw (a1 cos a1 - a2 cos a2) + 2 B3 (b0 cos b0 + cw (b1 cos b1 + b2 cos b2))
+        offd(a, va[1][0], va[1][1], true, -bco * (-2. * Ac[3] * sw * va[1][a]), 0.);
+        offd(a, va[2][0], va[2][1], true, -bco * (2. * Ac[3] * sw * va[2][a]), 0.);
+        offd(a, vb[0][0], vb[0][1], true, -bco * (2. * Bc[3] * vb[0][a]), 0.);
+        offd(a, vb[1][0], vb[1][1], true, -bco * (2. * Bc[3] * cw * vb[1][a]), 0.);
+        offd(a, vb[2][0], vb[2][1], true, -bco * (2. * Bc[3] * cw * vb[2][a]), 0.);
+        // dh2 = -2 B3 sw (b1 cos b1 - b2 cos b2) - 2 A3 (a0 cos a0 + cw (a1 cos a1 + a2 cos a2))
+        offd(a, vb[1][0], vb[1][1], true, 0., -bco * (-2. * Bc[3] * sw * vb[1][a]));
+        offd(a, vb[2][0], vb[2][1], true, 0., -bco * (2. * Bc[3] * sw * vb[2][a]));
+        offd(a, va[0][0], va[0][1], true, 0., -bco * (-2. * Ac[3] * va[0][a]));
+        offd(a, va[1][0], va[1][1], true, 0., -bco * (-2. * Ac[3] * cw * va[1][a]));
+        offd(a, va[2][0], va[2][1], true, 0., -bco * (-2. * Ac[3] * cw * va[2][a]));
+    }
+    tb.to_problem(p);
+    p.nval = 1;
+    set_bz(p, PI / a0, 2. * PI / r3 / a0);
+}
+
 // ------------------------------------------------------------ TMDCs
 // TMDCs.h: the three-band (d_z2, d_xy, d_x2-y2) tight-binding model of
 // monolayer MX2 with up to third-neighbour hoppings (G.-B. Liu et al.,
@@ -595,6 +689,7 @@ bool build_material(const std::string &target, const CfgValue *mat, Problem &p)
     else if (target == "XYHlattice") xyh_lattice(mat, p);
     else if (target == "TMDCs") tmdcs(mat, p);
     else if (target == "SquareSBand") square_sband(mat, p);
+    else if (target == "Bi2Se3surf") bi2se3_surface(p);   // SBEs.h:183-186; no parameters read
     else return false;
     p.model = MODEL_TB;
     return true;

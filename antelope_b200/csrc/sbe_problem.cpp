@@ -584,8 +584,7 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
     } else if (build_material(p.target, mat, p)) {
         if (custom)
             throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
-    } else if (p.target == "Bi2Se3surf" ||
-               p.target == "WDSM_TaAs" || p.target == "MultiWSM") {
+    } else if (p.target == "WDSM_TaAs" || p.target == "MultiWSM") {
         unsup("material '" + p.target + "' is not built on the GPU path");
         return p;
     } else {

@@ -99,7 +99,7 @@ sbe_status sbe_problem_laser(const sbe_problem *p, double *laser);
 
 /* The tight-binding tables a table model runs on: the SyntheticWannier cfg
  * group, or an analytic material of the reference (KaneMele, Haldane2L,
- * WilsonMass, XYHlattice, TMDCs, SquareSBand) restated as H(k) = sum_v h_v e^{ik.v} and its
+ * WilsonMass, XYHlattice, TMDCs, SquareSBand, Bi2Se3surf) restated as H(k) = sum_v h_v e^{ik.v} and its
  * GenJMatrix as J_a(k) = sum_v j_{a,v} e^{ik.v}.  Call once with the array
  * pointers NULL to read the sizes, then with caller-owned arrays:
  *   vec[nvec*2] Cartesian vectors (bohr), h[nvec*N*N*2], d and j

@@ -86,7 +86,7 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-MATERIAL_TABLES = ("KaneMele", "Haldane2L", "WilsonMass", "XYHlattice", "TMDCs", "SquareSBand")
+MATERIAL_TABLES = ("KaneMele", "Haldane2L", "WilsonMass", "XYHlattice", "TMDCs", "SquareSBand", "Bi2Se3surf")
 
 
 def to_problem(case: dict, nthreads: int = 1):
