@@ -242,16 +242,21 @@ __device__ __forceinline__ VgField<Real> vg_field(const Real (&c)[VG_NCONST], ty
             fma(A.y, c[VG_PYI], A.x * c[VG_PXI])};
 }
 
+// The factor 2 of 2 Im(w z*) and of (rho_11 - rho_00) w is folded into the
+// constants: the kernel doubles the P01 coefficients (so h.wr, h.wi hold
+// 2 dt w) and halves c0.  Scaling by 2 is exact and commutes with rounding,
+// so every result is bit for bit that of the unscaled arithmetic, one
+// multiplication per right-hand side cheaper.
 template <class Real, bool G1>
-__device__ __forceinline__ void vg_rhs(const VgField<Real> &h, Real c0, const Real (&y)[D_N], Real g1, Real g2,
+__device__ __forceinline__ void vg_rhs(const VgField<Real> &h, Real hc0, const Real (&y)[D_N], Real g1, Real g2,
                                        Real (&k)[D_N])
 {
-    const Real im2 = Real(2) * fma(h.wi, y[D_ZR], -(h.wr * y[D_ZI]));  // 2 Im(w z*)
+    const Real im2 = fma(h.wi, y[D_ZR], -(h.wr * y[D_ZI]));   // 2 Im(w z*)
     k[D_DA] = G1 ? fma(-g1, y[D_DA], im2) : im2;
-    const Real bma = fma(Real(-2), y[D_DA], c0);                       // rho_11 - rho_00 = c0 + db - da
-    const Real xr = fma(bma, h.wr, h.d * y[D_ZR]);
-    const Real xi = fma(bma, h.wi, h.d * y[D_ZI]);
-    k[D_ZR] = fma(-g2, y[D_ZR], xi);                                   // -i X - g2 z
+    const Real hbma = hc0 - y[D_DA];                         // (rho_11 - rho_00) / 2 = (c0 + db - da) / 2
+    const Real xr = fma(hbma, h.wr, h.d * y[D_ZR]);
+    const Real xi = fma(hbma, h.wi, h.d * y[D_ZI]);
+    k[D_ZR] = fma(-g2, y[D_ZR], xi);                           // -i X - g2 z
     k[D_ZI] = fma(-g2, y[D_ZI], -xr);
 }
 
@@ -292,6 +297,9 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
 #pragma unroll
         for (int q = 0; q < VG_NCONST; ++q) c[j][q] = ok[j] ? kc[(size_t)q * nkp + kidx[j]] : Real(0);
 #pragma unroll
+        for (int q = VG_PXR; q <= VG_PYI; ++q) c[j][q] = c[j][q] + c[j][q];   // see vg_rhs
+        c[j][VG_C0] = c[j][VG_C0] * Real(0.5);
+#pragma unroll
         for (int q = 0; q < D_N; ++q) y64[j][q] = ok[j] ? st[(size_t)slot[q] * nkp + kidx[j]] : 0.0;
     }
     TileReducer red(red_s);
@@ -331,41 +339,50 @@ __global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ 
         const int r = (s - s0) % SUB;
         red.push(v, r);
 
-        // one RK step
+        // one RK step of the thread's k-points, stage by stage so that their
+        // independent dependency chains interleave
         T2 A[TB::NT];
 #pragma unroll
         for (int i = 1; i < TB::NT; ++i) A[i] = __ldg(tab + (size_t)s * TB::NT + i);
+        VgField<Real> h[KPT][TB::NT];
 #pragma unroll
         for (int j = 0; j < KPT; ++j) {
-            VgField<Real> h[TB::NT];
-            h[0] = hstart[j];
+            h[j][0] = hstart[j];
 #pragma unroll
-            for (int i = 1; i < TB::NT; ++i) h[i] = vg_field<Real>(c[j], A[i]);
-            hstart[j] = h[TB::END];
-            // FP64: acc = rho + sum_i dt b_i k_i in the reference's order
-            // (SBEs.h:614-623); mixed: the sum is formed in FP32 first
-            Real kk[TB::S][D_N], y[D_N], acc[D_N];
+            for (int i = 1; i < TB::NT; ++i) h[j][i] = vg_field<Real>(c[j], A[i]);
+            hstart[j] = h[j][TB::END];
+        }
+        // FP64: acc = rho + sum_i dt b_i k_i in the reference's order
+        // (SBEs.h:614-623); mixed: the sum is formed in FP32 first
+        Real kk[KPT][TB::S][D_N], acc[KPT][D_N];
 #pragma unroll
-            for (int q = 0; q < D_N; ++q) acc[q] = F64 ? y0[j][q] : Real(0);
+        for (int j = 0; j < KPT; ++j)
 #pragma unroll
-            for (int i = 0; i < TB::S; ++i) {
+            for (int q = 0; q < D_N; ++q) acc[j][q] = F64 ? y0[j][q] : Real(0);
+#pragma unroll
+        for (int i = 0; i < TB::S; ++i) {
+#pragma unroll
+            for (int j = 0; j < KPT; ++j) {
+                Real y[D_N];
 #pragma unroll
                 for (int q = 0; q < D_N; ++q) {
                     Real t = y0[j][q];
 #pragma unroll
                     for (int m = 0; m < i; ++m)
-                        if (TB::a(i, m) != 0.0) t = fma(Real(TB::a(i, m)), kk[m][q], t);
+                        if (TB::a(i, m) != 0.0) t = fma(Real(TB::a(i, m)), kk[j][m][q], t);
                     y[q] = t;
                 }
-                vg_rhs<Real, G1>(h[TB::ti(i)], c[j][VG_C0], y, g1, g2, kk[i]);
+                vg_rhs<Real, G1>(h[j][TB::ti(i)], c[j][VG_C0], y, g1, g2, kk[j][i]);
                 if (TB::b(i) != 0.0) {
 #pragma unroll
-                    for (int q = 0; q < D_N; ++q) acc[q] = fma(Real(TB::b(i)), kk[i][q], acc[q]);
+                    for (int q = 0; q < D_N; ++q) acc[j][q] = fma(Real(TB::b(i)), kk[j][i][q], acc[j][q]);
                 }
             }
-#pragma unroll
-            for (int q = 0; q < D_N; ++q) y64[j][q] = F64 ? double(acc[q]) : y64[j][q] + double(acc[q]);
         }
+#pragma unroll
+        for (int j = 0; j < KPT; ++j)
+#pragma unroll
+            for (int q = 0; q < D_N; ++q) y64[j][q] = F64 ? double(acc[j][q]) : y64[j][q] + double(acc[j][q]);
         if (s == next_shot) {   // density snapshot of the state after step s
 #pragma unroll
             for (int j = 0; j < KPT; ++j)
