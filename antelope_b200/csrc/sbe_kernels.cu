@@ -260,8 +260,10 @@ __device__ __forceinline__ void vg_rhs(const VgField<Real> &h, Real hc0, const R
     k[D_ZI] = fma(-g2, y[D_ZI], -xr);
 }
 
+// RK4 fits in 128 registers without spilling (4 CTAs of 128 threads per SM
+// instead of 3 at the compiler's unbounded choice); Fehlberg-5 would spill.
 template <class Real, int RK, int KPT, bool G1>
-__global__ void __launch_bounds__(256) propagate_vg(const TileDev *__restrict__ tiles,
+__global__ void __launch_bounds__(256, RK == 4 ? 2 : 1) propagate_vg(const TileDev *__restrict__ tiles,
                                                     const SolveDev *__restrict__ solves, int tick, int S)
 {
     using T2 = typename V2<Real>::T;
