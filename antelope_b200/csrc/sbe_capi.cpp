@@ -222,6 +222,8 @@ extern "C" void sbe_problem_destroy(sbe_problem *p) { delete p; }
 
 // ================================================================= solver
 struct sbe_solver {
+    Problem prob;
+    std::vector<double> laser;          // output laser columns, built while the GPU runs
     std::unique_ptr<Engine> eng;
     std::unique_ptr<WannierSolve> wan;  // N-band Wannier problems
     cudaStream_t own = nullptr;
@@ -242,6 +244,7 @@ sbe_status create_solver(const sbe_problem *p, const sbe_opts *opts, int kb, int
     *out = nullptr;
     return guard([&]() -> sbe_status {
         auto s = std::make_unique<sbe_solver>();
+        s->prob = p->p;
         s->device = opts ? opts->device : 0;
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking), "stream create");
@@ -345,6 +348,8 @@ extern "C" sbe_status sbe_solver_run(sbe_solver *s, void *stream)
         run_engine(*s->eng, s->use_graph, &s->launches);
         s->eng->fetch_async(s->id);
         s->ran = true;
+        // host work of sbe_solver_get done while the GPU propagates
+        s->laser = laser_rows(s->prob);
         return SBE_OK;
     });
 }
@@ -355,7 +360,7 @@ extern "C" sbe_status sbe_solver_get(sbe_solver *s, const sbe_outputs *out)
     if (!s->ran) return fail(SBE_NOT_READY, "sbe_solver_run has not been called");
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(s->device), "cudaSetDevice");
-        SolveOutputs o = s->wan ? s->wan->outputs() : s->eng->outputs(s->id);
+        SolveOutputs o = s->wan ? s->wan->outputs() : s->eng->outputs(s->id, &s->laser);
         copy_out(o, out);
         return SBE_OK;
     });
@@ -641,7 +646,6 @@ using Clock = std::chrono::steady_clock;
 struct Request {
     long long id = 0;
     Problem prob;
-    std::vector<double> atab;     // field table, built by the submitting thread
     std::vector<double> laser;    // laser columns of the outputs, built by the submitting thread
     std::vector<double> jout;     // raw per-step sums, assembled by the waiting thread
     double cp[NSLOT] = {0};
@@ -743,7 +747,7 @@ void sbe_server::loop()
         // and waiting threads are not held up by it
         for (Request *r : batch) {
             try {
-                r->solve = eng->add(r->prob, eo, &r->atab);
+                r->solve = eng->add(r->prob, eo);
             } catch (const std::exception &e) {
                 r->solve = -1;
                 r->err = e.what();
@@ -752,7 +756,6 @@ void sbe_server::loop()
         if (!batch.empty()) {
             std::lock_guard<std::mutex> g(mu);
             for (Request *r : batch) {
-                std::vector<double>().swap(r->atab);
                 if (r->solve < 0) {
                     r->state = Request::FAILED;
                     ++n_failed;
@@ -867,8 +870,7 @@ extern "C" sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, lon
     r->t_submit = Clock::now();
     r->prob = p->p;
     try {
-        // host FP64 field table and the laser output columns, built on the caller's thread
-        r->atab = a_table(r->prob);
+        // the laser output columns, built on the caller's thread
         r->laser = laser_rows(r->prob);
     } catch (const std::exception &e) {
         return fail(SBE_INVALID_ARGUMENT, e.what());

@@ -10,6 +10,7 @@
 #include <map>
 
 #include "sbe_kernels.h"
+#include "sbe_wannier.h"
 
 namespace sbe {
 
@@ -284,7 +285,7 @@ size_t Engine::bytes_needed(const Problem &p, const EngineOptions &o) const
            (size_t)ntiles * NSLOT * 8 + snap;
 }
 
-int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<double> *atab_in)
+int Engine::add(const Problem &p, const EngineOptions &o)
 {
     if (p.model != MODEL_HALDANE) throw CfgError("only the Haldane model is built on this path");
     if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) throw CfgError("gauge LengthHamiltonian is not implemented");
@@ -339,18 +340,13 @@ int Engine::add(const Problem &p, const EngineOptions &o, const std::vector<doub
     s->bytes = kc_b + st_b + tab_n * real + part_b + jout_b + cp_b + snap_n * 24;
     cuda_check(cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming), "cudaEventCreate");
 
-    // field tables (host FP64, rounded once to the kernel's Real)
-    std::vector<double> atab_own;
-    if (!atab_in) atab_own = a_table(p);
-    const std::vector<double> &atab = atab_in ? *atab_in : atab_own;
-    std::vector<double> tabd_own;
-    if (!vg) tabd_own = phase_table(p, atab);
-    const std::vector<double> &tabd = vg ? atab : tabd_own;
-    if (s->precision == PREC_FP64) {
-        ring_.upload(s->tab, tabd.data(), tab_n * 8, up_);
-    } else {
-        std::vector<float> tf(tabd.begin(), tabd.end());
-        ring_.upload(s->tab, tf.data(), tab_n * 4, up_);
+    // field table on the device: the laser evaluated at every stage time in
+    // FP64 (rounded once to the kernel's Real)
+    {
+        const LaserDev ld = laser_dev(p.laser);
+        cuda_check(launch_field_table(ld, p.laser.atmin, p.laser.dt, s->Nt, s->nts, cfr.data(), vg, p.hal_va,
+                                      p.hal_vb, s->tab, s->precision != PREC_FP64, up_),
+                   "field table kernel");
     }
     InitArgs ia{};
     ia.nk = s->nk;
@@ -664,13 +660,13 @@ void Engine::harmonics(int id, double w0, int hmax, double *band_power)
     if (A) cudaFreeAsync(A, stream_);
 }
 
-SolveOutputs Engine::outputs(int id)
+SolveOutputs Engine::outputs(int id, const std::vector<double> *laser)
 {
     std::vector<double> j;
     double cp[NSLOT];
     raw_outputs(id, j, cp);
     SolveOutputs o;
-    assemble_outputs(get(id).prob, j, cp, o);
+    assemble_outputs(get(id).prob, j, cp, o, laser);
     return o;
 }
 

@@ -97,9 +97,9 @@ public:
 
     // Device bytes a solve of this problem needs (admission control).
     size_t bytes_needed(const Problem &p, const EngineOptions &o) const;
-    // Set up a solve on the stream; it starts advancing at the next step().
-    // `atab` may hold the problem's a_table() already built by the caller.
-    int add(const Problem &p, const EngineOptions &o, const std::vector<double> *atab = nullptr);
+    // Set up a solve (on the engine's copy stream); it starts advancing at the
+    // next step().  Its field table is computed on the device.
+    int add(const Problem &p, const EngineOptions &o);
     // Advance every resident solve by up to S steps (one propagate launch per
     // launch class, then the tile reduction).
     void step();
@@ -116,7 +116,8 @@ public:
     // memory and record an event; ready() polls it, outputs() assembles.
     void fetch_async(int id);
     bool ready(int id);
-    SolveOutputs outputs(int id);
+    // `laser` may hold the problem's laser_rows() already built by the caller
+    SolveOutputs outputs(int id, const std::vector<double> *laser = nullptr);
     // The raw per-step sums [Nt][NSLOT] and the summed constant parts of a
     // fetched solve (waits for the copy); assemble_outputs() turns them into
     // the output arrays.

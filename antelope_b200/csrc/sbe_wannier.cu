@@ -31,6 +31,7 @@
 
 #include <type_traits>
 
+#include "sbe_problem.h"
 #include "sbe_wannier.h"
 
 namespace sbe {
@@ -1335,6 +1336,73 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_snapshot(const WanDev *__r
         P.snap_pi[2 * o] = cv.x;
         P.snap_pi[2 * o + 1] = cv.y;
     }
+}
+
+// ============================================================= field tables
+struct FieldTabArgs {
+    double c[6], va[3][2], vb[3][2];
+};
+
+// One thread per (step, stage time): the stage time is formed as the host and
+// the reference form it (SBEs.h:612, antelope.cpp:299).
+__global__ void __launch_bounds__(256) field_table(LaserDev L, double atmin, double dt, int Nt, int nts,
+                                                   FieldTabArgs fa, bool vg, void *out, bool f32)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Nt * nts) return;
+    const int n = i / nts, j = i % nts;
+    const double t = atmin + dt * n;
+    double A[3], E[3];
+    laser_eval(L, j == 0 ? t : t + fa.c[j] * dt, A, E);
+    double v[12];
+    int nv = 2;
+    if (vg) {
+        v[0] = A[0];
+        v[1] = A[1];
+    } else {
+        nv = 12;
+        for (int r = 0; r < 3; ++r) {
+            const double aa = A[0] * fa.va[r][0] + A[1] * fa.va[r][1];
+            const double ab = A[0] * fa.vb[r][0] + A[1] * fa.vb[r][1];
+            sincos(aa, &v[3 + r], &v[r]);
+            sincos(ab, &v[9 + r], &v[6 + r]);
+        }
+    }
+    for (int q = 0; q < nv; ++q) {
+        if (f32) static_cast<float *>(out)[(size_t)i * nv + q] = float(v[q]);
+        else static_cast<double *>(out)[(size_t)i * nv + q] = v[q];
+    }
+}
+
+LaserDev laser_dev(const Laser &las)
+{
+    LaserDev L{};
+    L.npulses = (int)las.pulses.size();
+    if (L.npulses > 8) throw CfgError("at most 8 pulses");
+    for (int i = 0; i < L.npulses; ++i) {
+        const Pulse &q = las.pulses[i];
+        PulseDev &d = L.p[i];
+        d.E0x = q.E0x; d.E0y = q.E0y; d.A0x = q.A0x; d.A0y = q.A0y; d.w0 = q.w0; d.cep = q.cep; d.t0 = q.t0;
+        d.twidth = q.twidth; d.twidth_clipped = q.twidth_clipped; d.envfactor = q.envfactor; d.env = q.env;
+        for (int j = 0; j < 3; ++j) { d.xdir[j] = q.xdir[j]; d.ydir[j] = q.ydir[j]; }
+    }
+    for (int j = 0; j < 3; ++j) { L.init_A[j] = las.init_A[j]; L.init_E[j] = las.init_E[j]; }
+    return L;
+}
+
+cudaError_t launch_field_table(const LaserDev &L, double atmin, double dt, int Nt, int nts, const double *c,
+                               bool vg, const double (*va)[2], const double (*vb)[2], void *out, bool f32,
+                               cudaStream_t st)
+{
+    if (nts < 1 || nts > 6 || Nt <= 0) return cudaErrorInvalidValue;
+    FieldTabArgs fa{};
+    for (int j = 0; j < nts; ++j) fa.c[j] = c[j];
+    if (!vg)
+        for (int r = 0; r < 3; ++r)
+            for (int x = 0; x < 2; ++x) { fa.va[r][x] = va[r][x]; fa.vb[r][x] = vb[r][x]; }
+    const int n = Nt * nts;
+    field_table<<<(n + 255) / 256, 256, 0, st>>>(L, atmin, dt, Nt, nts, fa, vg, out, f32);
+    return cudaGetLastError();
 }
 
 // ============================================================= launchers

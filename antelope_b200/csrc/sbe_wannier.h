@@ -77,6 +77,19 @@ struct WanDev {
     double *snap_pi;
 };
 
+struct Laser;
+// The laser of a problem in the device layout (throws CfgError beyond 8 pulses).
+LaserDev laser_dev(const Laser &L);
+
+// Field tables of the two-band kernels, computed on the device with the same
+// laser evaluation as the N-band path: at t = (atmin + dt n) + c_j dt for the
+// nts stage-time fractions c (c_0 = 0), either A_x, A_y ([Nt][nts][2], VG) or
+// cos / sin of A.a_i and A.b_i ([Nt][nts][12], Haldane length gauge; a, b:
+// the [3][2] vectors).  out: doubles (f32 = 0) or floats (f32 = 1).
+cudaError_t launch_field_table(const LaserDev &L, double atmin, double dt, int Nt, int nts, const double *c,
+                               bool vg, const double (*va)[2], const double (*vb)[2], void *out, bool f32,
+                               cudaStream_t st);
+
 size_t wan_smem_bytes(int N, int nR, int precision);
 cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st);
 cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st);

@@ -53,17 +53,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     for (int i = 0; i < 3; ++i) w_.Ngrid[i] = p.Nk[i];
     for (int i = 0; i < 9; ++i) w_.axes[i] = p.bzaxes[i];
     for (int i = 0; i < 3; ++i) w_.origin[i] = p.bzorigin[i];
-    LaserDev &L = w_.laser;
-    L.npulses = (int)p.laser.pulses.size();
-    if (L.npulses > 8) throw CfgError("at most 8 pulses");
-    for (int i = 0; i < L.npulses; ++i) {
-        const Pulse &q = p.laser.pulses[i];
-        PulseDev &d = L.p[i];
-        d.E0x = q.E0x; d.E0y = q.E0y; d.A0x = q.A0x; d.A0y = q.A0y; d.w0 = q.w0; d.cep = q.cep; d.t0 = q.t0;
-        d.twidth = q.twidth; d.twidth_clipped = q.twidth_clipped; d.envfactor = q.envfactor; d.env = q.env;
-        for (int j = 0; j < 3; ++j) { d.xdir[j] = q.xdir[j]; d.ydir[j] = q.ydir[j]; }
-    }
-    for (int j = 0; j < 3; ++j) { L.init_A[j] = p.laser.init_A[j]; L.init_E[j] = p.laser.init_E[j]; }
+    w_.laser = laser_dev(p.laser);
 
     const size_t real = precision_ == 0 ? 8 : 4, cplx = 2 * real;
     const size_t nk = (size_t)w_.nk;
