@@ -644,15 +644,12 @@ void Engine::harmonics(int id, double w0, int hmax, double *band_power)
         in.ntiles = s.ntiles;
         in.cp_stride = NSLOT;
         in.cp_slot = 2;
-        std::vector<double> a(2 * (size_t)s.Nt);
-        for (int n = 0; n < s.Nt; ++n) {
-            double A3[3], E3[3];
-            p.laser.eval(p.laser.atmin + p.laser.dt * n, A3, E3);
-            a[2 * (size_t)n] = A3[0];
-            a[2 * (size_t)n + 1] = A3[1];
-        }
-        cuda_check(cudaMallocAsync(reinterpret_cast<void **>(&A), a.size() * 8, stream_), "alloc A table");
-        UploadRing::shared().upload(A, a.data(), a.size() * 8, stream_);
+        // A(t_n) in FP64 on the device (the stage-time table with the single fraction 0)
+        const double c0 = 0.0;
+        cuda_check(cudaMallocAsync(reinterpret_cast<void **>(&A), 16 * (size_t)s.Nt, stream_), "alloc A table");
+        cuda_check(launch_field_table(laser_dev(p.laser), p.laser.atmin, p.laser.dt, s.Nt, 1, &c0, true, nullptr,
+                                      nullptr, A, false, stream_),
+                   "A table kernel");
         in.A = A;
         in.nvw = p.nval * p.total_weight;
     }

@@ -4,6 +4,7 @@
 #include "sbe_wansolve.h"
 
 #include "sbe_kernels.h"
+#include "sbe_wannier.h"
 #include "sbe_spectrum.h"
 
 #include <algorithm>
@@ -189,15 +190,12 @@ void WannierSolve::harmonics(double w0, int hmax, double *band_power)
     in.dV = p.dV;
     double *A = nullptr;
     if (w_.vg) {  // intra += Nval A(t_n) sum_k w_k
-        std::vector<double> a(2 * (size_t)w_.Nt);
-        for (int n = 0; n < w_.Nt; ++n) {
-            double A3[3], E3[3];
-            p.laser.eval(p.laser.atmin + p.laser.dt * n, A3, E3);
-            a[2 * (size_t)n] = A3[0];
-            a[2 * (size_t)n + 1] = A3[1];
-        }
-        cuda_check(cudaMallocAsync(reinterpret_cast<void **>(&A), a.size() * 8, stream_), "alloc A table");
-        UploadRing::shared().upload(A, a.data(), a.size() * 8, stream_);
+        // A(t_n) in FP64 on the device (the stage-time table with the single fraction 0)
+        const double c0 = 0.0;
+        cuda_check(cudaMallocAsync(reinterpret_cast<void **>(&A), 16 * (size_t)w_.Nt, stream_), "alloc A table");
+        cuda_check(launch_field_table(laser_dev(p.laser), p.laser.atmin, p.laser.dt, w_.Nt, 1, &c0, true, nullptr,
+                                      nullptr, A, false, stream_),
+                   "A table kernel");
         in.A = A;
         in.nvw = p.nval * p.total_weight;
     }
