@@ -602,6 +602,7 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
             p.bzorigin[i] = elem_double(*bo, i, "Type exception in calc group");
     p.derive_grid();
 
+    if (p.laser.pulses.size() > 16) unsup("more than 16 laser pulses");
     if (p.gauge == GAUGE_LENGTH_HAMILTONIAN) unsup("gauge LengthHamiltonian is not implemented in the reference either");
     if (p.shot_number > 0 && p.shot_every() <= 0)   // the reference would take ktime % 0
         throw CfgError("calc.shotNumber gives a snapshot interval of 0 steps (period / shotNumber < dt)");

@@ -1378,7 +1378,7 @@ LaserDev laser_dev(const Laser &las)
 {
     LaserDev L{};
     L.npulses = (int)las.pulses.size();
-    if (L.npulses > 8) throw CfgError("at most 8 pulses");
+    if (L.npulses > MAX_PULSES) throw CfgError("at most 16 laser pulses");
     for (int i = 0; i < L.npulses; ++i) {
         const Pulse &q = las.pulses[i];
         PulseDev &d = L.p[i];

@@ -22,9 +22,11 @@ struct PulseDev {
     int env;
 };
 
+constexpr int MAX_PULSES = 16;   // laser pulses a problem may have (device layout)
+
 struct LaserDev {
     int npulses;
-    PulseDev p[8];
+    PulseDev p[MAX_PULSES];
     double init_A[3], init_E[3];
 };
 

@@ -89,6 +89,7 @@ def _err(case_or_text):
      "SBE_BAD_CONFIG", "Undefined polytype"),
     (lambda c: c["calc"].__setitem__("shotNumber", 1000), "SBE_BAD_CONFIG", "snapshot interval of 0 steps"),
     (lambda c: c.__setitem__("gauge", "Hamiltonian"), "SBE_UNSUPPORTED", "LengthHamiltonian"),
+    (lambda c: c["laser"].__setitem__("pulses", c["laser"]["pulses"] * 17), "SBE_UNSUPPORTED", "16 laser pulses"),
 ])
 def test_diagnostics(mutate, status, msg):
     c = copy.deepcopy(BASE)

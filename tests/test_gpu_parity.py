@@ -185,6 +185,27 @@ def test_server_cancel_and_single_delivery():
     srv.close()
 
 
+def test_many_pulses_device_table_matches_host_table():
+    """Ten pulses of every envelope kind: the field table the solver builds
+    on the device agrees with the host-built one of sbe_solve_noalloc to the
+    FP64 parity bar (the two evaluations of A(t) differ by about an ulp)."""
+    from antelope_b200.api import solve_noalloc
+    c = variant(calc__Npoints=[9, 8], calc__RKorder=5)
+    envs = ["cos4", "gauss", "sin2", "cos4_clipped", "gauss_clipped"]
+    c["laser"]["pulses"] = [{"E0": 0.001 + 0.0003 * i, "w0": 0.05 + 0.01 * i, "ncycles": 1.0 + 0.2 * i,
+                             "ellip": 0.1 * (i % 3), "cep": 30.0 * i, "t0": 10.0 * i, "phix": 5.0 * i,
+                             "env_name": envs[i % 5], "ncycles_clipped": 0.5} for i in range(10)]
+    p = ab.Problem.from_dict(c)
+    for prec, tol in (("fp64", FP64_TOL), ("mixed", 1e-6)):
+        a = ab.solve(p, precision=prec, tile_k=64, k_per_thread=1)
+        b = solve_noalloc(p, precision=prec, tile_k=64, k_per_thread=1)
+        scale = max(np.abs(b.inter).max(), np.abs(b.intra).max())
+        for key in ("inter", "intra"):
+            for ax in range(2):
+                assert rel_series(getattr(a, key)[:, ax], getattr(b, key)[:, ax], scale) < tol, (prec, key, ax)
+        assert np.array_equal(a.laser, b.laser)
+
+
 def test_cli_drop_in(tmp_path):
     """sbe_run in a directory holding inputParam.cfg writes the reference's
     six files with the reference's values."""
