@@ -789,8 +789,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
             // in the mixed method, to 1e-10 with a first-order finish once the
             // rotations left are below 1e-5 (an O(1e-10) error against the
             // ~1e-7 of its FP32 Fourier sums)
-            if (F32) jacobi_track<RF>(w, bh, N, 6, 1e-20, 1e-5, lane);
-            else jacobi_sweeps<RF>(w, bh, N, 6, 1e-30, lane);
+            jacobi_track<RF>(w, bh, N, 6, F32 ? 1e-20 : 1e-30, F32 ? 1e-5 : 1e-7, lane);
             // the eigenbasis at t + h (c = 1) warm-starts the next attempt,
             // whose first stage is at that time once this step is accepted
             if (tab.c[s] == 1.0) {
