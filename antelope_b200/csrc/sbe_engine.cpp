@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <map>
 
@@ -330,6 +331,8 @@ int Engine::add(const Problem &p, const EngineOptions &o)
     alloc(&s->kc, kc_b, "alloc constants");
     alloc(&s->st, st_b, "alloc state");
     alloc(&s->tab, tab_n * real, "alloc field table");
+    if (reinterpret_cast<uintptr_t>(s->tab) % 16 != 0)   // the kernels read its entries in 16-byte loads
+        throw std::runtime_error("field table not 16-byte aligned");
     alloc((void **)&s->partial, part_b, "alloc partials");
     alloc((void **)&s->jout, jout_b, "alloc outputs");
     alloc((void **)&s->constpart, cp_b, "alloc constant parts");

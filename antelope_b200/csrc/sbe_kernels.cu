@@ -145,25 +145,26 @@ template <> struct V2<float> { using T = float2; };
 // each lane with one partially summed value (index lane>>2 for lanes that are
 // multiples of 4), two more exchanges finish it: 9 shuffles instead of 40.
 // The pattern is fixed, so the result is deterministic.
-__device__ __forceinline__ double warp_sum8(const double (&v)[8], int lane)
+template <class T>
+__device__ __forceinline__ T warp_sum8(const T (&v)[8], int lane)
 {
     const bool h4 = lane & 16, h2 = lane & 8, h1 = lane & 4;
-    double u[4];
+    T u[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        double send = h4 ? v[i] : v[i + 4];
-        double keep = h4 ? v[i + 4] : v[i];
+        T send = h4 ? v[i] : v[i + 4];
+        T keep = h4 ? v[i + 4] : v[i];
         u[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
     }
-    double x[2];
+    T x[2];
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-        double send = h2 ? u[i] : u[i + 2];
-        double keep = h2 ? u[i + 2] : u[i];
+        T send = h2 ? u[i] : u[i + 2];
+        T keep = h2 ? u[i + 2] : u[i];
         x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
     }
-    double send = h1 ? x[0] : x[1];
-    double y = (h1 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    T send = h1 ? x[0] : x[1];
+    T y = (h1 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
     y += __shfl_xor_sync(0xffffffffu, y, 2);
     y += __shfl_xor_sync(0xffffffffu, y, 1);
     return y;  // lanes 4*i hold the sum of v[i]
@@ -190,7 +191,7 @@ struct TileReducer {
     }
     __device__ __forceinline__ void push(const double (&v)[8], int r)
     {
-        put(warp_sum8(v, threadIdx.x & 31), r);
+        put(warp_sum8<double>(v, threadIdx.x & 31), r);
     }
     __device__ __forceinline__ void flush(int nrows, int row0, int ntiles, int tile, double *partial)
     {
@@ -684,37 +685,142 @@ template <class Real>
 __device__ __forceinline__ void lw_field(const Real (&c)[LW_NCONST], const Real *ph, Real (&ca)[3], Real (&sa)[3],
                                          Real (&cb)[3], Real (&sb)[3])
 {
+    // one table entry, 48 or 96 bytes at a 16-byte boundary, in 16-byte loads
+    Real p[LW_NPHASE];
+    constexpr int PER = 16 / sizeof(Real);
+#pragma unroll
+    for (int i = 0; i < LW_NPHASE / PER; ++i) {
+        if constexpr (sizeof(Real) == 4) {
+            const float4 u = __ldg(reinterpret_cast<const float4 *>(ph) + i);
+            p[4 * i] = u.x; p[4 * i + 1] = u.y; p[4 * i + 2] = u.z; p[4 * i + 3] = u.w;
+        } else {
+            const double2 u = __ldg(reinterpret_cast<const double2 *>(ph) + i);
+            p[2 * i] = u.x; p[2 * i + 1] = u.y;
+        }
+    }
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         // cos/sin(k.v + A.v) from the per-k and per-stage-time factors
-        ca[i] = fma(c[LW_CA0 + i], ph[i], -(c[LW_SA0 + i] * ph[3 + i]));
-        sa[i] = fma(c[LW_SA0 + i], ph[i], c[LW_CA0 + i] * ph[3 + i]);
-        cb[i] = fma(c[LW_CB0 + i], ph[6 + i], -(c[LW_SB0 + i] * ph[9 + i]));
-        sb[i] = fma(c[LW_SB0 + i], ph[6 + i], c[LW_CB0 + i] * ph[9 + i]);
+        ca[i] = fma(c[LW_CA0 + i], p[i], -(c[LW_SA0 + i] * p[3 + i]));
+        sa[i] = fma(c[LW_SA0 + i], p[i], c[LW_CA0 + i] * p[3 + i]);
+        cb[i] = fma(c[LW_CB0 + i], p[6 + i], -(c[LW_SB0 + i] * p[9 + i]));
+        sb[i] = fma(c[LW_SB0 + i], p[6 + i], c[LW_CB0 + i] * p[9 + i]);
     }
 }
 
+// cos / sin of k.v + A(t).v for the three a and three b vectors at one
+// stage time.
+template <class Real> struct LwTrig {
+    Real ca[3], sa[3], cb[3], sb[3];
+};
+
+// Field terms of H0(k + A) at one stage time: B = (B1, B2, B3) (dt-scaled),
+// ib = 1 / |B|^2 and q = (g2 - g1) ib, the dephasing's weight of (s.B) B, so
+// that neither the right-hand side nor the currents divide.
+template <class Real> struct LwField {
+    Real B1, B2, B3, q, ib;
+};
+
+template <class Real> __device__ __forceinline__ Real lw_recip(Real x);
+template <> __device__ __forceinline__ double lw_recip<double>(double x) { return 1.0 / x; }
+// the FP32 stages of the mixed method take the fast reciprocal (2 ulp)
+template <> __device__ __forceinline__ float lw_recip<float>(float x) { return __fdividef(1.0f, x); }
+
+template <class Real>
+__device__ __forceinline__ LwField<Real> lw_field_terms(const LwTrig<Real> &T, Real t1dt, Real t2sdt, Real Mdt,
+                                                        Real gd)
+{
+    LwField<Real> F;
+    F.B1 = t1dt * (T.ca[0] + T.ca[1] + T.ca[2]);
+    F.B2 = t1dt * (T.sa[0] + T.sa[1] + T.sa[2]);
+    F.B3 = fma(-t2sdt, T.sb[0] + T.sb[1] + T.sb[2], Mdt);
+    const Real bb = fma(F.B1, F.B1, fma(F.B2, F.B2, F.B3 * F.B3));
+    F.ib = bb > Real(0) ? lw_recip<Real>(bb) : Real(0);
+    F.q = gd * F.ib;
+    return F;
+}
+
+template <class Real>
+__device__ __forceinline__ LwField<Real> lw_field_terms(const Real (&c)[LW_NCONST], const Real *ph, Real t1dt,
+                                                        Real t2sdt, Real Mdt, Real gd)
+{
+    LwTrig<Real> T;
+    lw_field<Real>(c, ph, T.ca, T.sa, T.cb, T.sb);
+    return lw_field_terms<Real>(T, t1dt, t2sdt, Mdt, gd);
+}
+
 template <class Real, bool G1>
-__device__ __forceinline__ void lw_rhs(const Real (&c)[LW_NCONST], const Real *ph, const Real (&y)[4], Real t1dt,
-                                       Real t2sdt, Real Mdt, Real g1, Real g2, Real (&k)[4])
+__device__ __forceinline__ void lw_rhs(const LwField<Real> &F, const Real (&y)[4], Real g1, Real g2, Real (&k)[4])
+{
+    const Real sx = y[LW_SX], sy = y[LW_SY], sz = y[LW_SZ];
+    const Real sB = fma(sx, F.B1, fma(sy, F.B2, sz * F.B3));
+    const Real f = sB * F.q;  // (g2-g1) (s.n)/|B|
+    k[LW_AL] = G1 ? -g1 * y[LW_AL] : Real(0);
+    k[LW_SX] = fma(Real(2), fma(F.B2, sz, -(F.B3 * sy)), fma(f, F.B1, -g2 * sx));
+    k[LW_SY] = fma(Real(2), fma(F.B3, sx, -(F.B1 * sz)), fma(f, F.B2, -g2 * sy));
+    k[LW_SZ] = fma(Real(2), fma(F.B1, sy, -(F.B2 * sx)), fma(f, F.B3, -g2 * sz));
+}
+
+template <class Real> struct LwCurrentConsts {
+    Real t1, t2c, t2s;
+    Real va[3][2], vb[3][2];
+};
+
+// Currents and density-matrix sums at k + A(t) (SBEs.h:694-760) from that
+// time's trig factors T and field terms F and the state y at t, in the stage
+// arithmetic (the per-k terms of the mixed method in FP32, like the velocity
+// gauge's), summed over the warp: lanes 4i return slot i.  The tile and
+// k-sums above the warp are FP64 in both methods.
+template <class Real>
+__device__ __forceinline__ double lw_current_sum(const LwCurrentConsts<Real> &K, const LwTrig<Real> &T,
+                                                 const LwField<Real> &F, const Real (&y)[4], Real w)
+{
+    Real j0[2], j1[2], j2[2], j3[2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        j0[a] = K.t2c * fma(K.vb[0][a], T.sb[0], fma(K.vb[1][a], T.sb[1], K.vb[2][a] * T.sb[2]));
+        j1[a] = K.t1 * fma(K.va[0][a], T.sa[0], fma(K.va[1][a], T.sa[1], K.va[2][a] * T.sa[2]));
+        j2[a] = -K.t1 * fma(K.va[0][a], T.ca[0], fma(K.va[1][a], T.ca[1], K.va[2][a] * T.ca[2]));
+        j3[a] = K.t2s * fma(K.vb[0][a], T.cb[0], fma(K.vb[1][a], T.cb[1], K.vb[2][a] * T.cb[2]));
+    }
+    const Real al = y[LW_AL], sx = y[LW_SX], sy = y[LW_SY], sz = y[LW_SZ];
+    const Real sBi = fma(sx, F.B1, fma(sy, F.B2, sz * F.B3)) * F.ib;   // (s.B) / |B|^2
+    const Real w2 = w + w;
+    Real v[8];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const Real sj = fma(sx, j1[a], fma(sy, j2[a], sz * j3[a]));
+        const Real par = sBi * fma(j1[a], F.B1, fma(j2[a], F.B2, j3[a] * F.B3));
+        v[a] = w2 * (sj - par);                // interband
+        v[2 + a] = w2 * fma(al, j0[a], par);   // intraband
+    }
+    v[4] = w * (al + sz);
+    v[5] = w * (al - sz);
+    v[6] = w * sx;
+    v[7] = -w * sy;
+    return double(warp_sum8<Real>(v, threadIdx.x & 31));
+}
+
+// B of H0(k + A(t)) in FP64 from the field-table entry ph of time t (the
+// eigenbasis of a density snapshot).
+template <class Real>
+__device__ __forceinline__ void lw_B64(const Real (&c)[LW_NCONST], const Real *ph, double t1dt, double t2sdt,
+                                       double Mdt, double (&Bt)[3])
 {
     Real ca[3], sa[3], cb[3], sb[3];
     lw_field<Real>(c, ph, ca, sa, cb, sb);
-    const Real B1 = t1dt * (ca[0] + ca[1] + ca[2]);
-    const Real B2 = t1dt * (sa[0] + sa[1] + sa[2]);
-    const Real B3 = fma(-t2sdt, sb[0] + sb[1] + sb[2], Mdt);
-    const Real sx = y[LW_SX], sy = y[LW_SY], sz = y[LW_SZ];
-    const Real bb = fma(B1, B1, fma(B2, B2, B3 * B3));
-    const Real sB = fma(sx, B1, fma(sy, B2, sz * B3));
-    const Real f = bb > Real(0) ? (g2 - g1) * sB / bb : Real(0);  // (g2-g1) (s.n)/|B|
-    k[LW_AL] = G1 ? -g1 * y[LW_AL] : Real(0);
-    k[LW_SX] = fma(Real(2), fma(B2, sz, -(B3 * sy)), fma(f, B1, -g2 * sx));
-    k[LW_SY] = fma(Real(2), fma(B3, sx, -(B1 * sz)), fma(f, B2, -g2 * sy));
-    k[LW_SZ] = fma(Real(2), fma(B1, sy, -(B2 * sx)), fma(f, B3, -g2 * sz));
+    Bt[0] = t1dt * (double(ca[0]) + double(ca[1]) + double(ca[2]));
+    Bt[1] = t1dt * (double(sa[0]) + double(sa[1]) + double(sa[2]));
+    Bt[2] = Mdt - t2sdt * (double(sb[0]) + double(sb[1]) + double(sb[2]));
 }
 
+// One k-point per thread.  Field terms once per distinct stage time (RK4:
+// t, t + dt/2 for stages 2 and 3, t + dt), the t + dt terms carried into the
+// next step (a launch beginning at s loads the entry of step s-1 at its end,
+// see vg_start_row); the currents of step s+1 are formed at the end of step s
+// from that entry's trig factors and the new state.
 template <class Real, int RK, bool G1>
-__global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ tiles,
+__global__ void __launch_bounds__(256, 2) propagate_lw(const TileDev *__restrict__ tiles,
                                                     const SolveDev *__restrict__ solves, int tick, int S)
 {
     using TB = Tableau<RK>;
@@ -730,96 +836,84 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
     const Real *__restrict__ kc = static_cast<const Real *>(sd.kc);
     double *__restrict__ st = static_cast<double *>(sd.st);
     const Real *__restrict__ tab = static_cast<const Real *>(sd.tab);
-    const Real g1 = Real(sd.g1), g2 = Real(sd.g2);
+    const Real g1 = Real(sd.g1), g2 = Real(sd.g2), gd = Real(sd.g2 - sd.g1);
     const Real t1dt = Real(sd.t1dt), t2sdt = Real(sd.t2sdt), Mdt = Real(sd.Mdt);
-    const double t1 = sd.t1, t2c = sd.t2c, t2s = sd.t2s;
-    double va[3][2], vb[3][2];
+    LwCurrentConsts<Real> K;
+    K.t1 = Real(sd.t1);
+    K.t2c = Real(sd.t2c);
+    K.t2s = Real(sd.t2s);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int a = 0; a < 2; ++a) { va[i][a] = sd.va[i][a]; vb[i][a] = sd.vb[i][a]; }
+        for (int a = 0; a < 2; ++a) { K.va[i][a] = Real(sd.va[i][a]); K.vb[i][a] = Real(sd.vb[i][a]); }
 
     const int local = threadIdx.x;
     const bool ok = local < tl.kcount;
     const int kidx = tl.k0 + local;
     Real c[LW_NCONST];
     double y64[4];
+    Real yr[4];   // the state rounded to the stage arithmetic
 #pragma unroll
     for (int q = 0; q < LW_NCONST; ++q) c[q] = ok ? kc[(size_t)q * nkp + kidx] : Real(0);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) y64[q] = ok ? st[(size_t)q * nkp + kidx] : 0.0;
+    for (int q = 0; q < 4; ++q) {
+        y64[q] = ok ? st[(size_t)q * nkp + kidx] : 0.0;
+        yr[q] = Real(y64[q]);
+    }
     if (!ok) c[LW_CA0] = c[LW_CB0] = Real(1);  // padding lanes: a harmless k = 0 point, weight 0
+    const Real w = c[LW_W];
     TileReducer red(red_s);
     int next_shot = first_shot(s0, sd.shot_every);
 
+    // field and currents at the launch's first step
+    LwTrig<Real> Te;   // trig factors at the end of the step (t + dt)
+    lw_field<Real>(c, tab + vg_start_row<TB>(s0) * LW_NPHASE, Te.ca, Te.sa, Te.cb, Te.sb);
+    LwField<Real> F0 = lw_field_terms<Real>(Te, t1dt, t2sdt, Mdt, gd);
+    red.put(lw_current_sum<Real>(K, Te, F0, yr, w), 0);
+
     for (int s = s0; s < s1; ++s) {
         const Real *row = tab + (size_t)s * TB::NT * LW_NPHASE;
-        double Bt[3];   // B of H0(k + A(t_s)), kept for a snapshot after the step
-        Real y0[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) y0[q] = Real(y64[q]);
-        // currents at k + A(t_s) (SBEs.h:694-760), computed in FP64
-        {
-            Real ca[3], sa[3], cb[3], sb[3];
-            lw_field<Real>(c, row, ca, sa, cb, sb);
-            double j0[2], j1[2], j2[2], j3[2];
-#pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                j0[a] = t2c * (vb[0][a] * double(sb[0]) + vb[1][a] * double(sb[1]) + vb[2][a] * double(sb[2]));
-                j1[a] = t1 * (va[0][a] * double(sa[0]) + va[1][a] * double(sa[1]) + va[2][a] * double(sa[2]));
-                j2[a] = -t1 * (va[0][a] * double(ca[0]) + va[1][a] * double(ca[1]) + va[2][a] * double(ca[2]));
-                j3[a] = t2s * (vb[0][a] * double(cb[0]) + vb[1][a] * double(cb[1]) + vb[2][a] * double(cb[2]));
-            }
-            const double B1 = double(t1dt) * (double(ca[0]) + double(ca[1]) + double(ca[2]));
-            const double B2 = double(t1dt) * (double(sa[0]) + double(sa[1]) + double(sa[2]));
-            const double B3 = double(Mdt) - double(t2sdt) * (double(sb[0]) + double(sb[1]) + double(sb[2]));
-            Bt[0] = B1;
-            Bt[1] = B2;
-            Bt[2] = B3;
-            const double al = y64[LW_AL], sx = y64[LW_SX], sy = y64[LW_SY], sz = y64[LW_SZ];
-            const double bb = B1 * B1 + B2 * B2 + B3 * B3;
-            const double sB = sx * B1 + sy * B2 + sz * B3;
-            const double w = c[LW_W];
-            double v[8];
-#pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                const double sj = sx * j1[a] + sy * j2[a] + sz * j3[a];
-                const double par = bb > 0.0 ? sB * (j1[a] * B1 + j2[a] * B2 + j3[a] * B3) / bb : 0.0;
-                v[a] = 2.0 * w * (sj - par);               // interband
-                v[2 + a] = 2.0 * w * (al * j0[a] + par);   // intraband
-            }
-            v[4] = w * (al + sz);
-            v[5] = w * (al - sz);
-            v[6] = w * sx;
-            v[7] = -w * sy;
-            red.push(v, (s - s0) % SUB);
-        }
+        LwField<Real> Fc = F0;   // field at the current stage's time; a new time evaluates it once
         Real kk[TB::S][4], y[4], acc[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = F64 ? y0[q] : Real(0);
+        for (int q = 0; q < 4; ++q) acc[q] = F64 ? yr[q] : Real(0);
 #pragma unroll
         for (int i = 0; i < TB::S; ++i) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                Real t = y0[q];
+                Real t = yr[q];
 #pragma unroll
                 for (int m = 0; m < i; ++m)
                     if (TB::a(i, m) != 0.0) t = fma(Real(TB::a(i, m)), kk[m][q], t);
                 y[q] = t;
             }
-            lw_rhs<Real, G1>(c, row + TB::ti(i) * LW_NPHASE, y, t1dt, t2sdt, Mdt, g1, g2, kk[i]);
+            if (TB::ti(i) == TB::END) {   // its trig factors also give the next step's currents
+                lw_field<Real>(c, row + TB::END * LW_NPHASE, Te.ca, Te.sa, Te.cb, Te.sb);
+                Fc = F0 = lw_field_terms<Real>(Te, t1dt, t2sdt, Mdt, gd);
+            } else if (i > 0 && TB::ti(i) != TB::ti(i - 1)) {
+                Fc = lw_field_terms<Real>(c, row + TB::ti(i) * LW_NPHASE, t1dt, t2sdt, Mdt, gd);
+            }
+            lw_rhs<Real, G1>(Fc, y, g1, g2, kk[i]);
             if (TB::b(i) != 0.0) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) acc[q] = fma(Real(TB::b(i)), kk[i][q], acc[q]);
             }
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) y64[q] = F64 ? double(acc[q]) : y64[q] + double(acc[q]);
+        for (int q = 0; q < 4; ++q) {
+            y64[q] = F64 ? double(acc[q]) : y64[q] + double(acc[q]);
+            yr[q] = Real(y64[q]);
+        }
+        // currents of step s+1 at k + A(t_{s+1}) with the state after step s,
+        // summed over the warp now and staged after this step's flush
+        const double jsum = s + 1 < s1 ? lw_current_sum<Real>(K, Te, F0, yr, w) : 0.0;
         if (s == next_shot) {
             // density snapshot: rho after the step in the eigenbasis of
             // H0(k + A(t_s)) (SBEs::WannierToHamiltonian at the step's start
             // time, as antelope.cpp:358 calls it); conduction = |+>, valence = |->
             if (ok) {
+                double Bt[3];
+                lw_B64<Real>(c, tab + vg_start_row<TB>(s) * LW_NPHASE, sd.t1dt, sd.t2sdt, sd.Mdt, Bt);
                 const double bn = sqrt(Bt[0] * Bt[0] + Bt[1] * Bt[1] + Bt[2] * Bt[2]);
                 double nx = 0.0, ny = 0.0, nz = 1.0;
                 if (bn > 0.0) { nx = Bt[0] / bn; ny = Bt[1] / bn; nz = Bt[2] / bn; }
@@ -841,6 +935,7 @@ __global__ void __launch_bounds__(256) propagate_lw(const TileDev *__restrict__ 
         }
         const int r = (s - s0) % SUB;
         if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, sd.partial);
+        if (s + 1 < s1) red.put(jsum, (s + 1 - s0) % SUB);
     }
     if (ok)
 #pragma unroll

@@ -80,8 +80,11 @@ def test_launch_shape_only_reorders_the_k_sum(opts):
     assert rel(out.intra, base.intra) < 1e-13
 
 
-def test_steps_per_launch_and_graph_are_bitwise_neutral():
-    case = variant(calc__Npoints=[16, 16], calc__RKorder=5)
+@pytest.mark.parametrize("gauge,rk", [("Velocity", 5), ("Wannier", 4), ("Wannier", 5)])
+def test_steps_per_launch_and_graph_are_bitwise_neutral(gauge, rk):
+    """Both gauges carry the field at a step's end into the next step; a
+    launch that starts at step s reads the same table entry."""
+    case = variant(top__gauge=gauge, calc__Npoints=[16, 16], calc__RKorder=rk)
     a = ab.solve(case, precision="fp64", steps_per_launch=1024)
     b = ab.solve(case, precision="fp64", steps_per_launch=37)
     c = ab.solve(case, precision="fp64", steps_per_launch=100, use_graph=True)

@@ -70,11 +70,13 @@ def test_mixed_snapshots_near_fp64(name):
     assert _close(np.abs(b["pi"]), np.abs(a["pi"]), 1e-5)
 
 
-@pytest.mark.parametrize("prec,kpt", [("fp64", 1), ("fp64", 2), ("mixed", 2)])
-def test_snapshots_independent_of_launch_split_graphs_and_batching(prec, kpt):
+@pytest.mark.parametrize("name,prec,kpt", [("vg_shots", "fp64", 1), ("vg_shots", "fp64", 2),
+                                           ("vg_shots", "mixed", 2), ("lw_shots", "fp64", 1),
+                                           ("lw_shots", "mixed", 1)])
+def test_snapshots_independent_of_launch_split_graphs_and_batching(name, prec, kpt):
     """Steps per launch, CUDA graphs and batching leave the snapshots bitwise
     unchanged (same tiling); the snapshot steps need not align with launches."""
-    case = SNAPSHOT_CASES["vg_shots"]
+    case = SNAPSHOT_CASES[name]
     shape = dict(precision=prec, tile_k=64 * kpt, k_per_thread=kpt)
     _, a = _run(case, steps_per_launch=1024, **shape)
     _, b = _run(case, steps_per_launch=37, use_graph=True, **shape)
