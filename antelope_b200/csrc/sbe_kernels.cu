@@ -177,17 +177,27 @@ constexpr int MAX_WARPS = 8;
 // block sums over warps and writes one row of the partial buffer per step.
 // The staging area has two halves used in turn, so one barrier per flush
 // suffices: a warp writes a half again only after the next flush's barrier,
-// which every thread reaches after finishing its reads of that half.
+// which every thread reaches after finishing its reads of that half.  A
+// kernel sizes the area by its own warp count in dynamic shared memory
+// (red_stage_bytes), so that small tiles leave the SM's L1 to the table
+// reads, or declares the fixed 8-warp RedStage.
 using RedStage = double[2][SUB][MAX_WARPS][NSLOT];
 
+constexpr int red_stage_bytes(int threads) { return 2 * SUB * (threads / 32) * NSLOT * (int)sizeof(double); }
+
 struct TileReducer {
-    double (*red)[SUB][MAX_WARPS][NSLOT];
-    int half;
-    __device__ __forceinline__ explicit TileReducer(RedStage &s) : red(s), half(0) {}
+    double *red;
+    int nw, half;   // warp stride of the area, half in use
+    __device__ __forceinline__ explicit TileReducer(RedStage &s) : red(&s[0][0][0][0]), nw(MAX_WARPS), half(0) {}
+    __device__ __forceinline__ TileReducer(double *s, int nwarps) : red(s), nw(nwarps), half(0) {}
+    __device__ __forceinline__ double &at(int h, int r, int w, int slot)
+    {
+        return red[((h * SUB + r) * nw + w) * NSLOT + slot];
+    }
     __device__ __forceinline__ void put(double y, int r)
     {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        if ((lane & 3) == 0) red[half][r][warp][lane >> 2] = y;
+        if ((lane & 3) == 0) at(half, r, warp, lane >> 2) = y;
     }
     __device__ __forceinline__ void push(const double (&v)[8], int r)
     {
@@ -200,7 +210,7 @@ struct TileReducer {
         for (int idx = threadIdx.x; idx < nrows * NSLOT; idx += blockDim.x) {
             const int row = idx / NSLOT, slot = idx % NSLOT;
             double acc = 0.0;
-            for (int w = 0; w < nwarp; ++w) acc += red[half][row][w][slot];
+            for (int w = 0; w < nwarp; ++w) acc += at(half, row, w, slot);
             partial[((size_t)(row0 + row) * ntiles + tile) * NSLOT + slot] = acc;
         }
         half ^= 1;
@@ -270,7 +280,7 @@ __global__ void __launch_bounds__(256, RK == 4 ? 2 : 1) propagate_vg(const TileD
     using T2 = typename V2<Real>::T;
     using TB = Tableau<RK>;
     constexpr bool F64 = std::is_same<Real, double>::value;
-    __shared__ RedStage red_s;
+    extern __shared__ double red_dyn[];   // red_stage_bytes(blockDim.x)
     const TileDev tl = tiles[blockIdx.x];
     const SolveDev &sd = solves[tl.solve];
     const int s0 = (tick - sd.admit_tick) * S;
@@ -305,7 +315,7 @@ __global__ void __launch_bounds__(256, RK == 4 ? 2 : 1) propagate_vg(const TileD
 #pragma unroll
         for (int q = 0; q < D_N; ++q) y64[j][q] = ok[j] ? st[(size_t)slot[q] * nkp + kidx[j]] : 0.0;
     }
-    TileReducer red(red_s);
+    TileReducer red(red_dyn, blockDim.x >> 5);
     // field terms at the start of the launch's first step (see vg_start_row)
     VgField<Real> hstart[KPT];
     {
@@ -621,7 +631,7 @@ __global__ void __launch_bounds__(256) propagate_vg_x2(const TileDev *__restrict
             a.w += __shfl_xor_sync(0xffffffffu, a.w, 16);
             __syncwarp();
             if (lane < 16 && xrow < m) {
-                double *dst = red.red[red.half][(e0 - b0) + xrow][warp];
+                double *dst = &red.at(red.half, (e0 - b0) + xrow, warp, 0);
                 if (xgrp == 0) {
                     dst[0] = double(a.x); dst[1] = double(a.y); dst[2] = double(a.z); dst[3] = double(a.w);
                 } else {
@@ -824,7 +834,7 @@ __global__ void __launch_bounds__(256, 2) propagate_lw(const TileDev *__restrict
                                                     const SolveDev *__restrict__ solves, int tick, int S)
 {
     using TB = Tableau<RK>;
-    __shared__ RedStage red_s;
+    extern __shared__ double red_dyn[];   // red_stage_bytes(blockDim.x)
     const TileDev tl = tiles[blockIdx.x];
     const SolveDev &sd = solves[tl.solve];
     const int s0 = (tick - sd.admit_tick) * S;
@@ -862,7 +872,7 @@ __global__ void __launch_bounds__(256, 2) propagate_lw(const TileDev *__restrict
     }
     if (!ok) c[LW_CA0] = c[LW_CB0] = Real(1);  // padding lanes: a harmless k = 0 point, weight 0
     const Real w = c[LW_W];
-    TileReducer red(red_s);
+    TileReducer red(red_dyn, blockDim.x >> 5);
     int next_shot = first_shot(s0, sd.shot_every);
 
     // field and currents at the launch's first step
@@ -1176,9 +1186,9 @@ template <class Real, int RK, int KPT>
 static cudaError_t launch_vg_t(const LaunchArgs &la, bool g1)
 {
     if (g1)
-        propagate_vg<Real, RK, KPT, true><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+        propagate_vg<Real, RK, KPT, true><<<la.ntiles, la.threads, red_stage_bytes(la.threads), la.stream>>>(la.tiles, la.solves, la.tick, la.S);
     else
-        propagate_vg<Real, RK, KPT, false><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+        propagate_vg<Real, RK, KPT, false><<<la.ntiles, la.threads, red_stage_bytes(la.threads), la.stream>>>(la.tiles, la.solves, la.tick, la.S);
     SBE_CHECK_LAUNCH();
 }
 
@@ -1215,9 +1225,9 @@ template <class Real, int RK>
 static cudaError_t launch_lw_t(const LaunchArgs &la, bool g1)
 {
     if (g1)
-        propagate_lw<Real, RK, true><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+        propagate_lw<Real, RK, true><<<la.ntiles, la.threads, red_stage_bytes(la.threads), la.stream>>>(la.tiles, la.solves, la.tick, la.S);
     else
-        propagate_lw<Real, RK, false><<<la.ntiles, la.threads, 0, la.stream>>>(la.tiles, la.solves, la.tick, la.S);
+        propagate_lw<Real, RK, false><<<la.ntiles, la.threads, red_stage_bytes(la.threads), la.stream>>>(la.tiles, la.solves, la.tick, la.S);
     SBE_CHECK_LAUNCH();
 }
 
