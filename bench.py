@@ -45,6 +45,17 @@ def wannier_flops_per_rhs(N: int, nR: int) -> float:
     (3 nR N^2 8/2), the commutator (16 N^3) and the eigenbasis dephasing
     rotations (4 x 8 N^3).  The eigensolver is not counted."""
     return 3 * nR * N * N * 8 / 2 + 16 * N ** 3 + 4 * 8 * N ** 3
+# Algorithmic flops per k-point step of the 2-band Haldane length gauge
+# (FMA = 2): field terms of H0(k+A) at one stage time 44 (angle additions 27,
+# B 10, |B|^2 5, 1/|B|^2 and (g2-g1)/|B|^2 2); right-hand side 30 (s.B 5,
+# f 1, three components of 2 B x s + f B - g2 s at 8 each); currents and
+# occupations 100 (cos of the b-vector angles 9, four j sums per axis 48,
+# (s.B)/|B|^2 6, per axis interband and intraband 30, weights 1,
+# occupations 6).  RK4: 4 RHS + 2 new stage times + 3 stage inputs and the
+# final combination over 4 components (24 + 32) + currents = 364; Fehlberg
+# RK5: 6 RHS + 5 new stage times + 15 stage-input and 5 final terms over 4
+# components (120 + 40) + currents = 660.
+LW_FLOPS_PER_KSTEP = {4: 364.0, 5: 660.0}
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -251,6 +262,8 @@ def run_ours(args):
         "gpu_launches": int(launches) * 2,   # propagate + reduce per launch tick, timed steps only
         "clocks": clocks,
     }
+    if args.lw_grid > 0 and world == 1:
+        line["length_gauge"] = run_length_gauge(args, stream, fp64_tf, fp32_tf)
     if args.wannier_grid > 0 and world == 1:
         line["wannier"] = run_wannier(args, stream, fp64_tf)
     if args.scan_solves > 0:
@@ -263,6 +276,58 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_length_gauge(args, stream, fp64_tf, fp32_tf):
+    """The Haldane configuration (same model, pulse, dt, RK4, T2) in the
+    length gauge, the reference's H0(k + A) form with eigenbasis dephasing,
+    on its --lw-grid k-grid: plain FP64 and mixed, one solve each after a
+    warm-up solve (launch shapes from the autotuner)."""
+    import torch
+
+    import antelope_b200 as ab
+    from antelope_b200 import workloads
+    from antelope_b200.api import Solver
+    from antelope_b200.spectrum import per_harmonic_error
+
+    n = args.lw_grid
+    res, outs = {}, {}
+    for prec in ("fp64", "mixed"):
+        p = ab.Problem.from_dict(workloads.haldane_case(n=n, precision=prec, ncycles=args.ncycles,
+                                                        gauge="Wannier"))
+        kst = float(p.dims.ntotal) * p.dims.Nt
+        ms = []
+        for rep in range(2):   # the first solve is the warm-up
+            s = Solver(p, precision=prec, profile=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            s.run(stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            kt = s.kernel_times()
+            outs[prec] = s.get()
+            s.close()
+        t = ms[-1]
+        tf = LW_FLOPS_PER_KSTEP[4] * kst / (kt["propagate_ms"] * 1e-3) / 1e12
+        peak = fp64_tf if prec == "fp64" else fp32_tf
+        res[prec] = {"ms_per_solve": t, "k_steps_per_s": kst / (t * 1e-3), "propagate_ms": kt["propagate_ms"],
+                     "reduce_ms": kt["reduce_ms"], "achieved_tflops": tf, "roofline_frac": tf / peak,
+                     "roofline_peak": "fp64 FMA pipe" if prec == "fp64" else "fp32 FMA pipe"}
+    a, b = outs["fp64"], outs["mixed"]
+    w0 = workloads.haldane_case(n=n)["laser"]["pulses"][0]["w0"]
+    err = {}
+    for floor in (1e-6, 1e-8):
+        _, e, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra}, {"inter": a.inter, "intra": a.intra},
+                                     0.1, w0, floor=floor)
+        err[f"max_floor_{floor:g}"] = float(e.max())
+    return {"workload": f"Haldane {n}x{n} length gauge (H0(k+A), eigenbasis dephasing), 3.2um "
+                        f"{args.ncycles:g}-cycle sin2, dt=0.1, RK4, T2=220",
+            "fp64": res["fp64"], "mixed": res["mixed"],
+            "mixed_over_fp64": res["fp64"]["ms_per_solve"] / res["mixed"]["ms_per_solve"],
+            "flops_per_kstep": LW_FLOPS_PER_KSTEP[4],
+            "spectral_error": dict(err, vs="fp64 run")}
 
 
 def run_wannier(args, stream, fp64_tf):
@@ -600,6 +665,7 @@ def main():
     ap.add_argument("--scan-solves", dest="scan_solves", type=int, default=256)
     ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=600)
     ap.add_argument("--serve-rate", dest="serve_rate", type=float, default=40.0)
+    ap.add_argument("--lw-grid", dest="lw_grid", type=int, default=600)
     ap.add_argument("--wannier-grid", dest="wannier_grid", type=int, default=300)
     ap.add_argument("--wannier-cycles", dest="wannier_cycles", type=float, default=0.5)
     args = ap.parse_args()
