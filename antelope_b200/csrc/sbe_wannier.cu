@@ -249,7 +249,7 @@ template <class RF> struct WarpView {
 };
 
 // C = op(A) * B over the full matrices, lanes stride over the elements.
-__device__ void mat_mul(double2 *C, const double2 *A, const double2 *B, int N, bool conjA, int lane)
+__device__ __forceinline__ void mat_mul(double2 *C, const double2 *A, const double2 *B, int N, bool conjA, int lane)
 {
     for (int e = lane; e < N * N; e += 32) {
         const int m = e / N, n = e % N;
@@ -332,7 +332,7 @@ __device__ __forceinline__ void jcol(const WarpView<RF> &w, const signed char *m
 // B <- J^dag B J and U <- U J are applied element by element in one pass
 // (inputs read, then written).
 template <class RF>
-__device__ void jacobi_round(const WarpView<RF> &w, const BlockHead &bh, int N, int r, int lane)
+__device__ __forceinline__ void jacobi_round(const WarpView<RF> &w, const BlockHead &bh, int N, int r, int lane)
 {
     const unsigned char(*ut)[2] = bh.ut;
     const signed char *mt = bh.mate[r];
@@ -446,7 +446,7 @@ __device__ void jacobi_sweeps(const WarpView<RF> &w, const BlockHead &bh, int N,
 // max |X| <= xmax, so that this error stays far below what a further sweep
 // would remove; returns false (nothing changed) otherwise.  B is left stale.
 template <class RF>
-__device__ bool jacobi_first_order(const WarpView<RF> &w, const BlockHead &bh, int N, double xmax, int lane)
+__device__ __forceinline__ bool jacobi_first_order(const WarpView<RF> &w, const BlockHead &bh, int N, double xmax, int lane)
 {
     const int NU = N * (N + 1) / 2, NN = N * N;
     double xm = 0.0;
@@ -481,7 +481,7 @@ __device__ bool jacobi_first_order(const WarpView<RF> &w, const BlockHead &bh, i
 // diagonal to tol2 (as jacobi_sweeps), except that once the off-diagonal part
 // is below 1e-5 of the diagonal a first-order step finishes when it can.
 template <class RF>
-__device__ void jacobi_track(const WarpView<RF> &w, const BlockHead &bh, int N, int max_sweeps, double tol2,
+__device__ __forceinline__ void jacobi_track(const WarpView<RF> &w, const BlockHead &bh, int N, int max_sweeps, double tol2,
                              double xmax, int lane)
 {
     const int P = N + (N & 1);
@@ -505,11 +505,11 @@ __device__ void jacobi_track(const WarpView<RF> &w, const BlockHead &bh, int N, 
 // Fourier sums at the phases w.ph: H0, D0, D1 and (optionally) S_a = sum R_a
 // h_R e^{i(k+A)R}, one (quantity, upper element) sum per lane task.
 template <class RF>
-__device__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], const WanDev &P, bool with_S,
-                        const RF *Rc, int lane)
+__device__ __forceinline__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], const WanDev &P, bool with_S,
+                                        const RF *Rc, int N, int lane)
 {
     using TF = typename Cx<RF>::T;
-    const int N = P.N, NN = N * N, nR = P.nR, NU = N * (N + 1) / 2;
+    const int NN = N * N, nR = P.nR, NU = N * (N + 1) / 2;
     const bool jt = with_S && P.has_jtab;  // current operator from its own tables
     const bool sS = with_S && !P.has_jtab;  // current operator from S_a = sum R_a h_R e^{iKR}
     const int nh = (P.has_dip ? 3 : 1) * NU, nt = nh + (jt ? 2 * NN : 0);
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
     kphases<RF>(P, kv, w.ph, lane);
     for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
     __syncwarp();
-    fourier<RF>(w, ut, P, false, Rc, lane);
+    fourier<RF>(w, ut, P, false, Rc, P.N, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
     jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
@@ -691,7 +691,9 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
 // ============================================================= attempt
 // Stage fields and e^{iA(t_s)R} of the attempt come precomputed (wan_control
 // / wan_prepare); each warp advances one k-point through all stages.
-template <class RF>
+// NC: the band count as a compile-time constant (0: read at run time), so
+// that index arithmetic and the loops over N fold at the common sizes.
+template <class RF, int NC>
 __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *__restrict__ Pp)
 {
     using TF = typename Cx<RF>::T;
@@ -701,14 +703,14 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
     const WanDev &P = *Pp;
     const WanCtl ctl = *P.ctl;
     if (ctl.done) return;
-    const WanSmem L = wan_smem(P.N, P.nR, sizeof(RF));
+    const int N = NC > 0 ? NC : P.N, NN = N * N, NU = N * (N + 1) / 2, nR = P.nR;
+    const WanSmem L = wan_smem(N, nR, sizeof(RF));
     BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
     TF *cA = reinterpret_cast<TF *>(smem_raw + L.cA);
     RF *Rc = reinterpret_cast<RF *>(smem_raw + L.Rc);
     double(*AE)[6] = bh.AE;
     WTab &tab = bh.tab;
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-    const int N = P.N, NN = N * N, NU = N * (N + 1) / 2, nR = P.nR;
     const double h = ctl.hs;
     const int buf = ctl.buf;
     const bool cur = ctl.need_current;
@@ -767,7 +769,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
             for (int r = lane; r < nR; r += 32) w.ph[r] = cmul(w.pk[r], cA[s * nR + r]);
             __syncwarp();
             const bool with_cur = cur && s == 0;
-            fourier<RF>(w, ut, P, with_cur, Rc, lane);
+            fourier<RF>(w, ut, P, with_cur, Rc, N, lane);
             // H = H0 + E.D (SBEs.h:770-783)
             const double Ex = AE[s][3], Ey = AE[s][4];
             for (int e = lane; e < NN; e += 32) {
@@ -957,7 +959,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
     kphases<RF>(P, kv, w.ph, lane);
     for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
     __syncwarp();
-    fourier<RF>(w, bh.ut, P, true, Rc, lane);
+    fourier<RF>(w, bh.ut, P, true, Rc, P.N, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
     jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
@@ -1372,7 +1374,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_snapshot(const WanDev *__r
     kphases<RF>(P, kv, w.ph, lane);
     for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
     __syncwarp();
-    fourier<RF>(w, bh.ut, P, false, Rc, lane);
+    fourier<RF>(w, bh.ut, P, false, Rc, P.N, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
     jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
@@ -1479,7 +1481,9 @@ template <class RF> static cudaError_t allow_smem()
     const int bytes = (int)wan_smem(WAN_MAXN, WAN_MAXR, sizeof(RF)).total;
     cudaError_t e = cudaFuncSetAttribute(wan_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(wan_attempt<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = cudaFuncSetAttribute(wan_attempt<RF, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(wan_attempt<RF, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(wan_vg_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
@@ -1530,8 +1534,14 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
         if (precision == 0) wan_vg_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
         else wan_vg_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
     } else {
-        if (precision == 0) wan_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-        else wan_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+        const bool n6 = w.N == 6;   // an instance with N folded in (the N = 6 Wannier configuration)
+        if (precision == 0) {
+            if (n6) wan_attempt<double, 6><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+            else wan_attempt<double, 0><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+        } else {
+            if (n6) wan_attempt<float, 6><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+            else wan_attempt<float, 0><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+        }
     }
     return cudaGetLastError();
 }
