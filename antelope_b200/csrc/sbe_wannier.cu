@@ -1028,7 +1028,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
     }
 }
 
-template <class RF>
+template <class RF, int NC>   // NC: as in wan_attempt
 __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev *__restrict__ Pp)
 {
     using T = double2;
@@ -1036,12 +1036,12 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev
     const WanDev &P = *Pp;
     const WanCtl ctl = *P.ctl;
     if (ctl.done) return;
-    const WanSmem L = wan_smem(P.N, P.nR, sizeof(RF));
+    const int N = NC > 0 ? NC : P.N, NN = N * N, NU = N * (N + 1) / 2;
+    const WanSmem L = wan_smem(N, P.nR, sizeof(RF));
     BlockHead &bh = *reinterpret_cast<BlockHead *>(smem_raw);
     double(*AE)[6] = bh.AE;
     WTab &tab = bh.tab;
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-    const int N = P.N, NN = N * N, NU = N * (N + 1) / 2;
     const double h = ctl.hs;
     const int buf = ctl.buf;
     const bool cur = ctl.need_current;
@@ -1474,20 +1474,30 @@ cudaError_t launch_field_table(const LaserDev &L, double atmin, double dt, int N
 }
 
 // ============================================================= launchers
+using WanKernel = void (*)(const WanDev *);
+template <class RF> static WanKernel wan_attempt_n(int N, bool vg)
+{
+    switch (N) {
+    case 2: return vg ? wan_vg_attempt<RF, 2> : wan_attempt<RF, 2>;
+    case 3: return vg ? wan_vg_attempt<RF, 3> : wan_attempt<RF, 3>;
+    case 4: return vg ? wan_vg_attempt<RF, 4> : wan_attempt<RF, 4>;
+    case 6: return vg ? wan_vg_attempt<RF, 6> : wan_attempt<RF, 6>;
+    default: return vg ? wan_vg_attempt<RF, 0> : wan_attempt<RF, 0>;
+    }
+}
+
 template <class RF> static cudaError_t allow_smem()
 {
     static bool done = false;  // per process; the attribute applies to every device
     if (done) return cudaSuccess;
     const int bytes = (int)wan_smem(WAN_MAXN, WAN_MAXR, sizeof(RF)).total;
     cudaError_t e = cudaFuncSetAttribute(wan_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(wan_attempt<RF, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(wan_attempt<RF, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    for (int n : {0, 2, 3, 4, 6})
+        for (bool vg : {false, true})
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(wan_attempt_n<RF>(n, vg), cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(wan_vg_init<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(wan_vg_attempt<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(wan_snapshot<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     done = e == cudaSuccess;
@@ -1528,21 +1538,12 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
     const size_t sm = wan_smem_bytes(w.N, w.nR, precision);
-    if (w.vg) {
-        // the stage arithmetic is FP64 in both methods (no per-stage Fourier
-        // sums); the instantiation must match the layout `sm` was sized for
-        if (precision == 0) wan_vg_attempt<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-        else wan_vg_attempt<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-    } else {
-        const bool n6 = w.N == 6;   // an instance with N folded in (the N = 6 Wannier configuration)
-        if (precision == 0) {
-            if (n6) wan_attempt<double, 6><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-            else wan_attempt<double, 0><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-        } else {
-            if (n6) wan_attempt<float, 6><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-            else wan_attempt<float, 0><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-        }
-    }
+    // instances with N folded in for the band counts of the materials and the
+    // N = 6 Wannier configuration, other N read at run time; the velocity
+    // gauge's stage arithmetic is FP64 in both methods (no per-stage Fourier
+    // sums), its RF instance only matches the layout `sm` was sized for
+    if (precision == 0) wan_attempt_n<double>(w.N, w.vg)<<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    else wan_attempt_n<float>(w.N, w.vg)<<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
     return cudaGetLastError();
 }
 
