@@ -52,6 +52,7 @@ class OrcProblem(C.Structure):
         ("w_h", C.POINTER(C.c_double)), ("w_d", C.POINTER(C.c_double)),
         ("w_vec", C.POINTER(C.c_double)), ("w_j", C.POINTER(C.c_double)), ("w_bz", C.c_double * 9),
         ("nthreads", C.c_int),
+        ("mw_n", C.c_double), ("mw_v", C.c_double), ("mw_alphan", C.c_double), ("mw_a0_ang", C.c_double),
     ]
 
 
@@ -138,6 +139,10 @@ def to_problem(case: dict, nthreads: int = 1):
         p.model = 0
         p.hal_a0_ang, p.hal_t1, p.hal_t2, p.hal_phi0 = mat["a0"], mat["t1"], mat["t2"], mat["phi0"]
         p.hal_M0 = mat["M0"] if "M0" in mat else mat["Mt2"] * mat["t2"]
+    elif target == "MultiWSM":
+        # the continuum two-band model (Materials/MultiWSM.h), restated in C
+        p.model = 2
+        p.mw_n, p.mw_v, p.mw_alphan, p.mw_a0_ang = mat["n"], mat["v"], mat["alphan"], mat["a0"]
     elif target == "SyntheticWannier":
         # explicit tight-binding tables of the cfg group (Nband, Nval, lattice,
         # R pairs, h_re/h_im [nR][N][N], optional d_re/d_im [nR][2][N][N])

@@ -175,6 +175,8 @@ typedef struct {
     int kind, N, nval, dipole;
     /* Haldane (Materials/Haldane.h:46-84, 134-143) */
     double t1, t2, M0, phi0, a0, va[3][2], vb[3][2];
+    /* MultiWSM (Materials/MultiWSM.h:45-70) */
+    double mw_n, mw_v, mw_alphan;
     /* Wannier */
     int nR;
     double (*Rc)[2];        /* Cartesian R vectors */
@@ -200,6 +202,15 @@ static int model_build(model_t *m, const orc_problem *p)
         m->vb[2][0] = -sqrt(3.) / 2 * a0; m->vb[2][1] = -3. / 2. * a0;
         double kxMax = PI / sqrt(3.) / a0, kyMax = 2. * PI / 3. / a0;   /* Haldane.h:77-81 */
         m->bzaxes[0] = 2 * kxMax; m->bzaxes[4] = 2 * kyMax;
+        return 0;
+    }
+    if (p->model == ORC_MODEL_MULTIWSM) {   /* MultiWSM.h:45-70 */
+        if (!(p->mw_a0_ang > 0)) return -1;
+        m->N = 2; m->nval = 1; m->dipole = 0;
+        m->mw_n = p->mw_n; m->mw_v = p->mw_v; m->mw_alphan = p->mw_alphan;
+        m->a0 = p->mw_a0_ang / AU_ANGSTROM;
+        double kmax = PI / m->a0;
+        m->bzaxes[0] = 2 * kmax; m->bzaxes[4] = 2 * kmax; m->bzaxes[8] = 2 * kmax;
         return 0;
     }
     if (p->model == ORC_MODEL_WANNIER) {
@@ -323,14 +334,51 @@ static void wannier_HDJ(const model_t *m, const double *k, cplx *H, cplx *D, cpl
     }
 }
 
+/* MultiWSM::GenBcomp + GenHamiltonian (MultiWSM.h:76-82, 186-200) */
+static void multiwsm_H(const model_t *m, const double *k, cplx *H)
+{
+    const double n = m->mw_n, al = m->mw_alphan;
+    double B[4];
+    B[0] = 0.;
+    B[1] = al * pow(k[0] * k[0] + k[1] * k[1], n / 2.) * cos(n * atan2(k[1], k[0]));
+    B[2] = al * pow(k[0] * k[0] + k[1] * k[1], n / 2.) * sin(n * atan2(k[1], k[0]));
+    B[3] = m->mw_v * k[2];
+    H[0] = B[0] + B[3]; H[1] = B[1] - I * B[2];
+    H[2] = B[1] + I * B[2]; H[3] = B[0] - B[3];
+}
+
+/* MultiWSM::GenJMatrix (MultiWSM.h:84-147), the derivative of B as written
+ * there (it is undefined on the k_x = k_y = 0 line) */
+static void multiwsm_J(const model_t *m, const double *k, cplx *J /* [3][4] */)
+{
+    const double n = m->mw_n, al = m->mw_alphan;
+    const double phip = atan2(k[1], k[0]);
+    const double psq = k[0] * k[0] + k[1] * k[1];
+    double xd[4] = {0, 0, 0, 0}, yd[4] = {0, 0, 0, 0}, zd[4] = {0, 0, 0, 0};
+    xd[1] = n * al * k[0] * cos(n * phip) * pow(psq, n / 2. - 1) + n * al * sin(n * phip) * pow(psq, n / 2.) * k[1] / psq;
+    yd[1] = n * al * k[1] * cos(n * phip) * pow(psq, n / 2. - 1) - n * al * sin(n * phip) * pow(psq, n / 2.) * k[0] / psq;
+    xd[2] = +n * al * k[0] * sin(n * phip) * pow(psq, n / 2. - 1) - n * al * k[1] * cos(n * phip) * pow(psq, n / 2.) / psq;
+    yd[2] = +n * al * k[1] * sin(n * phip) * pow(psq, n / 2. - 1) + n * al * k[0] * cos(n * phip) * pow(psq, n / 2.) / psq;
+    zd[3] = m->mw_v;
+    const double *d[3] = {xd, yd, zd};
+    for (int a = 0; a < 3; ++a) {
+        J[4 * a + 0] = -(d[a][0] + d[a][3]);
+        J[4 * a + 1] = -(d[a][1] - I * d[a][2]);
+        J[4 * a + 2] = -(d[a][1] + I * d[a][2]);
+        J[4 * a + 3] = -(d[a][0] - d[a][3]);
+    }
+}
+
 static void model_H(const model_t *m, const double *k, cplx *H)
 {
     if (m->kind == ORC_MODEL_HALDANE) haldane_H(m, k, H);
+    else if (m->kind == ORC_MODEL_MULTIWSM) multiwsm_H(m, k, H);
     else wannier_HDJ(m, k, H, NULL, NULL);
 }
 static void model_J(const model_t *m, const double *k, cplx *J)
 {
     if (m->kind == ORC_MODEL_HALDANE) { haldane_J(m, k, J); return; }
+    if (m->kind == ORC_MODEL_MULTIWSM) { multiwsm_J(m, k, J); return; }
     cplx H[ORC_MAX_BANDS * ORC_MAX_BANDS], D[3 * ORC_MAX_BANDS * ORC_MAX_BANDS];
     wannier_HDJ(m, k, H, D, J);
 }

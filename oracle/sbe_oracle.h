@@ -22,7 +22,7 @@ extern "C" {
 enum { ORC_ENV_GAUSS = 0, ORC_ENV_GAUSS_CLIPPED = 1, ORC_ENV_COS4 = 2, ORC_ENV_COS4_CLIPPED = 3,
        ORC_ENV_SIN2 = 4 };
 enum { ORC_GAUGE_LENGTH_WANNIER = 0, ORC_GAUGE_LENGTH_HAMILTONIAN = 1, ORC_GAUGE_VELOCITY = 2 };
-enum { ORC_MODEL_HALDANE = 0, ORC_MODEL_WANNIER = 1 };
+enum { ORC_MODEL_HALDANE = 0, ORC_MODEL_WANNIER = 1, ORC_MODEL_MULTIWSM = 2 };
 enum { ORC_RK4 = 4, ORC_RK5_FEHLBERG = 5, ORC_RK45_CASHKARP = 45 };
 
 #define ORC_MAX_PULSES 8
@@ -71,6 +71,10 @@ typedef struct {
     const double *w_j;   /* [nR][2][N][N] complex, interleaved re/im, or NULL */
     double w_bz[9];      /* used when w_vec != NULL */
     int nthreads;        /* k-range split as ParaRange (utility.h:104-115); 1 = sequential */
+    /* MultiWSM (Materials/MultiWSM.h): the continuum two-band model with
+     * B = (alphan |k_p|^n cos(n phi_k), alphan |k_p|^n sin(n phi_k), v k_z);
+     * a0 in Angstrom (sets the Brillouin zone). */
+    double mw_n, mw_v, mw_alphan, mw_a0_ang;
 } orc_problem;
 
 typedef struct {

@@ -91,6 +91,25 @@ def material(name, gauge, **kw):
 
 
 MATERIAL_CASES = {f"{m.lower()}_{g[0].lower()}": material(m, g) for m in MATERIALS for g in ("Velocity", "Wannier")}
+
+
+# MultiWSM (Materials/MultiWSM.h): the continuum two-band model on a 3-D grid
+# around k = 0, the parameters of the reference's InputParams/MultiWSM.cfg.
+# Its GenJMatrix divides 0 by 0 on the k_x = k_y = 0 line, so the k_x and
+# k_y point counts are even (no grid point there).
+def multiwsm(gauge, n=1.0, Npoints=(6, 6, 4), **kw):
+    c = variant(top__gauge=gauge, calc__Npoints=list(Npoints), pulse__ellip=0.3, **kw)
+    del c["Haldane"]
+    c["target"] = "MultiWSM"
+    c["MultiWSM"] = {"n": float(n), "v": 0.2, "alphan": 0.1, "phi0": 0.1, "a0": 1.0}
+    return c
+
+
+MULTIWSM_CASES = {
+    "multiwsm_v": multiwsm("Velocity"),
+    "multiwsm_w": multiwsm("Wannier"),
+    "multiwsm_w_n2_tilted": multiwsm("Wannier", n=2.0, Npoints=(4, 4, 4), pulse__thetaz=30.0, pulse__phiz=20.0),
+}
 # Bi2Se3surf's bands meet where every sin(k.a_i) vanishes, e.g. at
 # (pi/a0, pi/(sqrt(3) a0)), a grid point whenever Npoints[1] - 1 is a multiple
 # of 4; per-band quantities there depend on the eigensolver's basis, so its

@@ -2,7 +2,8 @@
 
 Runs the unmodified reference (oracle/_ref/exec_hhg_ref, built by
 ``make -C oracle ref`` from the reference sources with the stand-in headers of
-oracle/refshim) on every case of cases.GOLDEN_CASES, cases.MATERIAL_CASES and
+oracle/refshim) on every case of cases.GOLDEN_CASES, cases.MATERIAL_CASES,
+cases.MULTIWSM_CASES and
 cases.SNAPSHOT_CASES and stores its output files (snapshot files included) as
 arrays in golden_<name>.npz; TEXT_CASE's files
 are also kept verbatim in text_case/.
@@ -20,7 +21,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from cases import GOLDEN_CASES, MATERIAL_CASES, SNAPSHOT_CASES, TEXT_CASE  # noqa: E402
+from cases import GOLDEN_CASES, MATERIAL_CASES, MULTIWSM_CASES, SNAPSHOT_CASES, TEXT_CASE  # noqa: E402
 from oracle import pyoracle  # noqa: E402
 from antelope_b200 import cfgtext  # noqa: E402
 
@@ -29,7 +30,7 @@ FILES = ["interband_dipole_full_evol.dat", "intraband_current_full_evol.dat",
 
 
 def main(names):
-    cases = {**GOLDEN_CASES, **MATERIAL_CASES, **SNAPSHOT_CASES}
+    cases = {**GOLDEN_CASES, **MATERIAL_CASES, **MULTIWSM_CASES, **SNAPSHOT_CASES}
     for name in names or cases:
         with tempfile.TemporaryDirectory() as d:
             out = pyoracle.run_reference(cases[name], d)

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from cases import BAND_GROUPS, GOLDEN_CASES, MATERIAL_CASES, SNAPSHOT_CASES
+from cases import BAND_GROUPS, GOLDEN_CASES, MATERIAL_CASES, MULTIWSM_CASES, SNAPSHOT_CASES
 from oracle import pyoracle
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -18,9 +18,9 @@ def _rel(a, b):
     return np.abs(a - b).max() / (m if m > 0 else 1.0)
 
 
-@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES) + sorted(MULTIWSM_CASES))
 def test_oracle_matches_reference_outputs(name):
-    case = GOLDEN_CASES[name]
+    case = {**GOLDEN_CASES, **MULTIWSM_CASES}[name]
     ref = np.load(os.path.join(GOLDEN, f"golden_{name}.npz"))
     out = pyoracle.run(case)
     N = out["dims"]["nband"]
