@@ -196,6 +196,7 @@ extern "C" sbe_status sbe_problem_model(const sbe_problem *p, sbe_model *m)
     if (!p || !m) return fail(SBE_INVALID_ARGUMENT, "null argument");
     const Problem &q = p->p;
     if (q.model == MODEL_HALDANE) return fail(SBE_INVALID_ARGUMENT, "the Haldane model has no tables");
+    if (q.model == MODEL_MULTIWSM) return fail(SBE_INVALID_ARGUMENT, "MultiWSM is a continuum model with no tables");
     m->nband = q.nband;
     m->nval = q.nval;
     m->nvec = q.w_nR;

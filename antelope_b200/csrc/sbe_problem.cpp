@@ -584,7 +584,25 @@ Problem problem_from_cfg(const CfgValue &root, std::string *unsupported)
     } else if (build_material(p.target, mat, p)) {
         if (custom)
             throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
-    } else if (p.target == "WDSM_TaAs" || p.target == "MultiWSM") {
+    } else if (p.target == "MultiWSM") {
+        // MultiWSM.h:45-70: strict double lookups (an integer value is missing
+        // to libconfig's lookupValue(double&)), a0 in Angstrom, the zone the
+        // cube [-pi/a0, pi/a0]^3
+        p.model = MODEL_MULTIWSM;
+        p.nband = 2;
+        p.nval = 1;
+        if (!(mat && get_double(mat, "n", p.mw_n) && get_double(mat, "v", p.mw_v) &&
+              get_double(mat, "alphan", p.mw_alphan) && get_double(mat, "phi0", p.mw_phi0) &&
+              get_double(mat, "a0", p.mw_a0)))
+            throw CfgError("Some MultiWSM paramters are missing");
+        p.mw_a0 /= AU_ANGSTROM;
+        const double kmax = PI / p.mw_a0;
+        const double axes[9] = {2 * kmax, 0, 0, 0, 2 * kmax, 0, 0, 0, 2 * kmax};
+        for (int i = 0; i < 9; ++i) p.bzaxes[i] = axes[i];
+        for (int i = 0; i < 3; ++i) p.bzorigin[i] = 0.0;
+        if (custom)
+            throw CfgError("Error: Try to using custom inital value without implementing GenInitialValue.");
+    } else if (p.target == "WDSM_TaAs") {
         unsup("material '" + p.target + "' is not built on the GPU path");
         return p;
     } else {

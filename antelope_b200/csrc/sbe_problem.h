@@ -65,6 +65,7 @@ enum Model {
     MODEL_HALDANE = 0,
     MODEL_SYNTHETIC_WANNIER = 1,  // tight-binding tables given in the cfg
     MODEL_TB = 2,                 // an analytic material restated as tables (sbe_materials.cpp)
+    MODEL_MULTIWSM = 3,           // the continuum two-band model of Materials/MultiWSM.h
 };
 
 struct Problem {
@@ -89,6 +90,10 @@ struct Problem {
     // Haldane (Materials/Haldane.h:46-84): a0 in bohr
     double hal_t1 = 0, hal_t2 = 0, hal_M0 = 0, hal_phi0 = 0, hal_a0 = 0;
     double hal_va[3][2] = {{0}}, hal_vb[3][2] = {{0}};
+    // MultiWSM (Materials/MultiWSM.h:45-70): B = (alphan |k_p|^n cos(n phi),
+    // alphan |k_p|^n sin(n phi), v k_z); a0 in bohr (sets the zone); phi0 is
+    // read, as the reference reads it, and unused by its formulas
+    double mw_n = 0, mw_v = 0, mw_alphan = 0, mw_phi0 = 0, mw_a0 = 0;
     // Synthetic Wannier model (N <= 8 bands): H(k) = sum_R h_R e^{ik.R},
     // D_a(k) = sum_R d_{a,R} e^{ik.R}, R = n1 a1 + n2 a2
     int w_nR = 0;

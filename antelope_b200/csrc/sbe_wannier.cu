@@ -502,13 +502,58 @@ __device__ __forceinline__ void jacobi_track(const WarpView<RF> &w, const BlockH
     }
 }
 
+// MultiWSM::GenBcomp, GenHamiltonian and GenJMatrix (MultiWSM.h:76-147,
+// 186-200) at the point K, by lane 0: H0 and, when J0 is given, the x and y
+// components of the model's current operator (its formulas, undefined on
+// K_x = K_y = 0 as the reference's).  The z component is diag(-v, v)
+// everywhere (mwsm_jz).
+__device__ void mwsm_hj(const WanDev &P, const double *K, double2 *H, double2 *J0, double2 *J1)
+{
+    const double n = P.mw_n, al = P.mw_alphan;
+    const double psq = K[0] * K[0] + K[1] * K[1];
+    const double phip = atan2(K[1], K[0]);
+    const double B1 = al * pow(psq, n / 2.) * cos(n * phip);
+    const double B2 = al * pow(psq, n / 2.) * sin(n * phip);
+    const double B3 = P.mw_v * K[2];
+    H[0] = make_double2(B3, 0.0);
+    H[1] = make_double2(B1, -B2);
+    H[2] = make_double2(B1, B2);
+    H[3] = make_double2(-B3, 0.0);
+    if (!J0) return;
+    const double c = cos(n * phip), s = sin(n * phip);
+    const double xd1 = n * al * K[0] * c * pow(psq, n / 2. - 1) + n * al * s * pow(psq, n / 2.) * K[1] / psq;
+    const double yd1 = n * al * K[1] * c * pow(psq, n / 2. - 1) - n * al * s * pow(psq, n / 2.) * K[0] / psq;
+    const double xd2 = +n * al * K[0] * s * pow(psq, n / 2. - 1) - n * al * K[1] * c * pow(psq, n / 2.) / psq;
+    const double yd2 = +n * al * K[1] * s * pow(psq, n / 2. - 1) + n * al * K[0] * c * pow(psq, n / 2.) / psq;
+    // J_a = [[-(d0 + d3), -(d1 - i d2)], [-(d1 + i d2), -(d0 - d3)]] with d0 = d3 = 0 in x and y
+    J0[0] = make_double2(0.0, 0.0);
+    J0[1] = make_double2(-xd1, xd2);
+    J0[2] = make_double2(-xd1, -xd2);
+    J0[3] = make_double2(0.0, 0.0);
+    J1[0] = make_double2(0.0, 0.0);
+    J1[1] = make_double2(-yd1, yd2);
+    J1[2] = make_double2(-yd1, -yd2);
+    J1[3] = make_double2(0.0, 0.0);
+}
+
+// element e of MultiWSM's z current operator, -d(B3 sigma_z)/dk_z
+__device__ __forceinline__ double2 mwsm_jz(const WanDev &P, int e)
+{
+    return make_double2(e == 0 ? -P.mw_v : (e == 3 ? P.mw_v : 0.0), 0.0);
+}
+
 // Fourier sums at the phases w.ph: H0, D0, D1 and (optionally) S_a = sum R_a
 // h_R e^{i(k+A)R}, one (quantity, upper element) sum per lane task.
 template <class RF>
 __device__ __forceinline__ void fourier(const WarpView<RF> &w, const unsigned char (*ut)[2], const WanDev &P, bool with_S,
-                                        const RF *Rc, int N, int lane)
+                                        const RF *Rc, int N, const double *K, int lane)
 {
     using TF = typename Cx<RF>::T;
+    if (P.cont) {   // the continuum model at the point K (k + A)
+        if (lane == 0) mwsm_hj(P, K, w.H0, with_S ? w.S0 : nullptr, with_S ? w.S1 : nullptr);
+        __syncwarp();
+        return;
+    }
     const int NN = N * N, nR = P.nR, NU = N * (N + 1) / 2;
     const bool jt = with_S && P.has_jtab;  // current operator from its own tables
     const bool sS = with_S && !P.has_jtab;  // current operator from S_a = sum R_a h_R e^{iKR}
@@ -649,7 +694,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
     kphases<RF>(P, kv, w.ph, lane);
     for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
     __syncwarp();
-    fourier<RF>(w, ut, P, false, Rc, P.N, lane);
+    fourier<RF>(w, ut, P, false, Rc, P.N, kv, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
     jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
@@ -769,7 +814,8 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
             for (int r = lane; r < nR; r += 32) w.ph[r] = cmul(w.pk[r], cA[s * nR + r]);
             __syncwarp();
             const bool with_cur = cur && s == 0;
-            fourier<RF>(w, ut, P, with_cur, Rc, N, lane);
+            const double Ks[3] = {kv[0] + AE[s][0], kv[1] + AE[s][1], kv[2] + AE[s][2]};   // k + A (continuum)
+            fourier<RF>(w, ut, P, with_cur, Rc, N, Ks, lane);
             // H = H0 + E.D (SBEs.h:770-783)
             const double Ex = AE[s][3], Ey = AE[s][4];
             for (int e = lane; e < NN; e += 32) {
@@ -811,11 +857,15 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
                 // currents at k + A(t_n) (SBEs.h:694-760): J_a = -i S_a + i[D_a, H0];
                 // lane 0 records this k's weighted values in its warp's slot row
                 double *val = bh.part[wi];
-                for (int a = 0; a < 2; ++a) {
+                for (int a = 0; a < (P.cont ? 3 : 2); ++a) {   // z: the continuum model only
                     T *Da = a == 0 ? w.D0 : w.D1;
                     T *Sa = a == 0 ? w.S0 : w.S1;
                     // J_a into B (B is free after the rounds above), then total = Re Tr(Y J_a)
                     for (int e = lane; e < NN; e += 32) {
+                        if (a == 2) {
+                            w.B[e] = mwsm_jz(P, e);
+                            continue;
+                        }
                         if (P.has_jtab) {  // the model's own current operator at k + A
                             w.B[e] = Sa[e];
                             continue;
@@ -850,8 +900,8 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
                     }
                     intra = warp_sum(intra);
                     if (lane == 0) {
-                        val[a] = wk * (tot - intra);
-                        val[2 + a] = wk * intra;
+                        val[a < 2 ? a : WAN_SLOT_INTER_Z] = wk * (tot - intra);
+                        val[a < 2 ? 2 + a : WAN_SLOT_INTRA_Z] = wk * intra;
                     }
                     __syncwarp();
                 }
@@ -959,7 +1009,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
     kphases<RF>(P, kv, w.ph, lane);
     for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
     __syncwarp();
-    fourier<RF>(w, bh.ut, P, true, Rc, P.N, lane);
+    fourier<RF>(w, bh.ut, P, true, Rc, P.N, kv, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
     jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);
@@ -994,11 +1044,16 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
         P.vg_eps[(size_t)k * N + lane] = w.dv[lane].x;
         P.vg_f[(size_t)k * N + lane] = w.dv[lane].y;
     }
-    // P_a = U^dag J_a U (SBEs.h:366-372)
-    for (int a = 0; a < 2; ++a) {
+    // P_a = U^dag J_a U (SBEs.h:366-372); a z component for the continuum model
+    const int na = P.cont ? 3 : 2;
+    for (int a = 0; a < na; ++a) {
         T *Sa = a == 0 ? w.S0 : w.S1;
         T *Da = a == 0 ? w.D0 : w.D1;
         for (int e = lane; e < NN; e += 32) {
+            if (a == 2) {
+                w.B[e] = mwsm_jz(P, e);
+                continue;
+            }
             if (P.has_jtab) {
                 w.B[e] = Sa[e];
                 continue;
@@ -1018,7 +1073,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
         __syncwarp();
         mat_mul(w.B, w.U, w.Tm, N, true, lane);
         __syncwarp();
-        for (int e = lane; e < NN; e += 32) P.vg_P[((size_t)k * 2 + a) * NN + e] = w.B[e];
+        for (int e = lane; e < NN; e += 32) P.vg_P[((size_t)k * na + a) * NN + e] = w.B[e];
         __syncwarp();
     }
     // rho = rho0 = diag(f) in the band basis
@@ -1058,9 +1113,11 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev
         const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, N, P.nR);
         double kv[3], wk;
         kpoint(P, k, kv, wk);
+        const int na = P.cont ? 3 : 2;   // P_z (in S0) for the continuum model
         for (int e = lane; e < NN; e += 32) {
-            w.D0[e] = P.vg_P[((size_t)k * 2 + 0) * NN + e];
-            w.D1[e] = P.vg_P[((size_t)k * 2 + 1) * NN + e];
+            w.D0[e] = P.vg_P[((size_t)k * na + 0) * NN + e];
+            w.D1[e] = P.vg_P[((size_t)k * na + 1) * NN + e];
+            if (na == 3) w.S0[e] = P.vg_P[((size_t)k * na + 2) * NN + e];
         }
         if (lane < N) w.dv[lane] = make_double2(P.vg_eps[(size_t)k * N + lane], P.vg_f[(size_t)k * N + lane]);
         const double2 *rho = P.rho[buf] + (size_t)k * NN;
@@ -1094,11 +1151,15 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev
                 w.Y[n * N + m] = cconj(y);
             }
             // H = diag(eps) + A.P (SBEs.h:787-805)
-            const double Ax = AE[s][0], Ay = AE[s][1];
+            const double Ax = AE[s][0], Ay = AE[s][1], Az = AE[s][2];
             for (int e = lane; e < NN; e += 32) {
                 T v;
                 v.x = fma(Ax, w.D0[e].x, Ay * w.D1[e].x);
                 v.y = fma(Ax, w.D0[e].y, Ay * w.D1[e].y);
+                if (na == 3) {
+                    v.x = fma(Az, w.S0[e].x, v.x);
+                    v.y = fma(Az, w.S0[e].y, v.y);
+                }
                 if (e / N == e % N) v.x += w.dv[e / N].x;
                 w.HT[e] = v;
             }
@@ -1106,8 +1167,8 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev
             if (cur && s == 0) {
                 // currents at k (SBEs.h:694-760): Re sum_ij rho_ij P_a,ji, diagonal -> intra
                 double *val = bh.part[wi];
-                for (int a = 0; a < 2; ++a) {
-                    const T *Pa = a == 0 ? w.D0 : w.D1;
+                for (int a = 0; a < na; ++a) {
+                    const T *Pa = a == 0 ? w.D0 : (a == 1 ? w.D1 : w.S0);
                     double tot = 0.0, intra = 0.0;
                     for (int e = lane; e < NN; e += 32) {
                         const int m = e / N, n = e % N;
@@ -1119,8 +1180,8 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev
                     tot = warp_sum(tot);
                     intra = warp_sum(intra);
                     if (lane == 0) {
-                        val[a] = wk * (tot - intra);
-                        val[2 + a] = wk * intra;
+                        val[a < 2 ? a : WAN_SLOT_INTER_Z] = wk * (tot - intra);
+                        val[a < 2 ? 2 + a : WAN_SLOT_INTRA_Z] = wk * intra;
                     }
                 }
                 if (lane < N) val[4 + lane] = wk * w.Y[lane * N + lane].x;
@@ -1374,7 +1435,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_snapshot(const WanDev *__r
     kphases<RF>(P, kv, w.ph, lane);
     for (int e = lane; e < NN; e += 32) w.U[e] = make_double2((e / N) == (e % N) ? 1 : 0, 0);
     __syncwarp();
-    fourier<RF>(w, bh.ut, P, false, Rc, P.N, lane);
+    fourier<RF>(w, bh.ut, P, false, Rc, P.N, kv, lane);
     for (int e = lane; e < NN; e += 32) w.B[e] = w.H0[e];
     __syncwarp();
     jacobi_sweeps<RF>(w, bh, N, 16, 1e-30, lane);

@@ -13,7 +13,8 @@ namespace sbe {
 
 constexpr int WAN_MAXN = 8;
 constexpr int WAN_MAXR = 64;       // lattice vectors
-constexpr int WAN_NSLOT = 16;      // inter x,y; intra x,y; occupations (N); coherence re, im
+constexpr int WAN_NSLOT = 16;      // inter x,y; intra x,y; occupations (N); coherence re, im; ...
+constexpr int WAN_SLOT_INTER_Z = 14, WAN_SLOT_INTRA_Z = 15;   // ... z currents (N <= 8: past the others)
 constexpr int WAN_WARPS = 4;       // warps (k-points) per CTA
 
 struct PulseDev {
@@ -48,6 +49,11 @@ struct WanCtl {
 struct WanDev {
     int N, nval, nR, nk, Nt, ntiles, rk, inter_intra, use_fermi, has_dip, has_jtab;
     int vg;                 // 1: velocity gauge (band basis), 0: length gauge (Wannier basis)
+    // 1: the continuum MultiWSM model (Materials/MultiWSM.h): H and the
+    // current operator from formulas at k + A instead of Fourier tables (nR = 0),
+    // a z current; its parameters n, v, alphan
+    int cont;
+    double mw_n, mw_v, mw_alphan;
     int k_offset;           // flat grid index of local k-point 0 (a k-slice of the grid)
     double Ef, dt, atmin, tol, g1, g2;  // g1 = 1/T1, g2 = 1/T2 (0 when disabled)
     int Ngrid[3];
@@ -67,7 +73,7 @@ struct WanDev {
     WanCtl *ctl;
     double *vg_eps;         // velocity gauge: [nk][N] band energies (ascending)
     double *vg_f;           // velocity gauge: [nk][N] initial occupations
-    double2 *vg_P;          // velocity gauge: [nk][2][N*N] P_a = U^dag J_a U
+    double2 *vg_P;          // velocity gauge: [nk][2 or 3 (cont)][N*N] P_a = U^dag J_a U
     double *stage_AE;       // [6][6] A and E at the stage times of the next attempt
     void *stage_cA;         // [6][nR] e^{i A(t_s) R} of the next attempt (Fourier precision)
     // density snapshots (antelope.cpp:340-422): every shot_every output steps

@@ -16,14 +16,16 @@ namespace sbe {
 namespace {
 template <class T> void dalloc(T **p, size_t bytes, cudaStream_t st, const char *what)
 {
-    cuda_check(cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st), what);
+    // a continuum model has no tables: its table buffers get a token size
+    cuda_check(cudaMallocAsync(reinterpret_cast<void **>(p), std::max<size_t>(bytes, 16), st), what);
 }
 }  // namespace
 
 WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStream_t st, int k_begin, int k_end)
     : prob_(p), precision_(precision), device_(device), stream_(st)
 {
-    if (p.model != MODEL_SYNTHETIC_WANNIER && p.model != MODEL_TB) throw CfgError("not a tight-binding problem");
+    if (p.model != MODEL_SYNTHETIC_WANNIER && p.model != MODEL_TB && p.model != MODEL_MULTIWSM)
+        throw CfgError("not a tight-binding problem");
     if (p.gauge != GAUGE_LENGTH_WANNIER && p.gauge != GAUGE_VELOCITY)
         throw CfgError("tight-binding models run in the LengthWannier or Velocity gauge");
     if (p.w_nR > WAN_MAXR) throw CfgError("tight-binding model: at most 64 hopping vectors");
@@ -45,6 +47,13 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     w_.has_dip = p.w_d.empty() ? 0 : 1;
     w_.has_jtab = p.w_j.empty() ? 0 : 1;
     w_.vg = p.gauge == GAUGE_VELOCITY ? 1 : 0;
+    if (p.model == MODEL_MULTIWSM) {   // formulas in place of tables; its own current operator
+        w_.cont = 1;
+        w_.has_jtab = 1;
+        w_.mw_n = p.mw_n;
+        w_.mw_v = p.mw_v;
+        w_.mw_alphan = p.mw_alphan;
+    }
     w_.Ef = p.Ef;
     w_.dt = p.dt;
     w_.atmin = p.laser.atmin;
@@ -63,7 +72,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     dalloc(&V, sizeof(double) * p.w_vec.size(), st, "alloc hopping vectors");
     dalloc(&h, cplx * p.w_h.size() / 2, st, "alloc h");
     if (w_.has_dip) dalloc(&d, cplx * p.w_d.size() / 2, st, "alloc d");
-    if (w_.has_jtab) dalloc(&j, cplx * p.w_j.size() / 2, st, "alloc current tables");
+    if (w_.has_jtab && !w_.cont) dalloc(&j, cplx * p.w_j.size() / 2, st, "alloc current tables");
     for (int b = 0; b < 2; ++b) {
         dalloc(&w_.rho[b], sizeof(double2) * nk * NN, st, "alloc rho");
         dalloc(&w_.U[b], sizeof(double2) * nk * NN, st, "alloc U");
@@ -72,7 +81,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     if (w_.vg) {
         dalloc(&w_.vg_eps, sizeof(double) * nk * N, st, "alloc band energies");
         dalloc(&w_.vg_f, sizeof(double) * nk * N, st, "alloc occupations");
-        dalloc(&w_.vg_P, sizeof(double2) * nk * 2 * NN, st, "alloc momentum matrices");
+        dalloc(&w_.vg_P, sizeof(double2) * nk * (w_.cont ? 3 : 2) * NN, st, "alloc momentum matrices");
     }
     dalloc(&w_.tile_err, sizeof(double) * w_.ntiles, st, "alloc tile errors");
     dalloc(&w_.cur_part, sizeof(double) * w_.ntiles * WAN_NSLOT, st, "alloc current partials");
@@ -92,7 +101,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     w_.d = d;
     w_.jt = j;
     UploadRing &ring = UploadRing::shared();
-    ring.upload(V, p.w_vec.data(), sizeof(double) * p.w_vec.size(), st);
+    if (!p.w_vec.empty()) ring.upload(V, p.w_vec.data(), sizeof(double) * p.w_vec.size(), st);
     auto up_real = [&](void *dst, const std::vector<double> &src) {
         if (precision_ == 0) {
             ring.upload(dst, src.data(), src.size() * 8, st);
@@ -101,9 +110,9 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
             ring.upload(dst, f.data(), f.size() * 4, st);
         }
     };
-    up_real(h, p.w_h);
+    if (!p.w_h.empty()) up_real(h, p.w_h);
     if (w_.has_dip) up_real(d, p.w_d);
-    if (w_.has_jtab) up_real(j, p.w_j);
+    if (w_.has_jtab && !w_.cont) up_real(j, p.w_j);
     cuda_check(cudaMemsetAsync(w_.jout, 0, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st), "clear outputs");
     // initial controller state: t = t_min, h = dt, currents first
     WanCtl c{};
@@ -260,8 +269,9 @@ void assemble_table_outputs(const Problem &p, const std::vector<double> &j, Solv
         double *L = &o.laser[(size_t)n * 7];
         L[0] = t;
         for (int d = 0; d < 3; ++d) { L[1 + d] = E[d]; L[4 + d] = A[d]; }
-        for (int a = 0; a < 3; ++a) {  // in-plane models: no z current besides Nval A_z
-            const double ie = a < 2 ? r[a] : 0.0, ia = (a < 2 ? r[2 + a] : 0.0) + nvw * A[a];
+        for (int a = 0; a < 3; ++a) {  // z: the continuum model's slots (zero for the in-plane models)
+            const double ie = a < 2 ? r[a] : r[WAN_SLOT_INTER_Z];
+            const double ia = (a < 2 ? r[2 + a] : r[WAN_SLOT_INTRA_Z]) + nvw * A[a];
             if (p.inter_intra) {
                 o.inter[(size_t)n * 3 + a] = ie * dV;
                 o.intra[(size_t)n * 3 + a] = ia * dV;

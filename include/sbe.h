@@ -105,7 +105,8 @@ sbe_status sbe_problem_laser(const sbe_problem *p, double *laser);
  *   vec[nvec*2] Cartesian vectors (bohr), h[nvec*N*N*2], d and j
  *   [nvec*2*N*N*2] (complex interleaved; d / j only when the flags say so),
  *   bz[9] Brillouin-zone axes before ksfactor / BZaxes overrides.
- * The Haldane model has closed-form kernels and no tables:
+ * The Haldane model (closed-form kernels) and MultiWSM (a continuum model
+ * evaluated from its formulas) have no tables:
  * SBE_INVALID_ARGUMENT. */
 typedef struct sbe_model {
     int nband, nval, nvec, has_dipoles, has_current_tables;

@@ -80,7 +80,11 @@ def _err(case_or_text):
     (lambda c: c["Haldane"].pop("t1"), "SBE_BAD_CONFIG", "Some Haldane paramters are missing"),
     (lambda c: c["Haldane"].pop("Mt2"), "SBE_BAD_CONFIG", "M0 param missing"),
     (lambda c: c.__setitem__("target", "Graphene"), "SBE_BAD_CONFIG", "Undefined Material"),
-    (lambda c: c.__setitem__("target", "MultiWSM"), "SBE_UNSUPPORTED", "not built"),
+    (lambda c: c.__setitem__("target", "WDSM_TaAs"), "SBE_UNSUPPORTED", "not built"),
+    (lambda c: c.__setitem__("target", "MultiWSM"), "SBE_BAD_CONFIG", "Some MultiWSM paramters are missing"),
+    (lambda c: (c.__setitem__("target", "MultiWSM"),   # libconfig: an integer is not a double
+                c.__setitem__("MultiWSM", {"n": 1, "v": 0.2, "alphan": 0.1, "phi0": 0.1, "a0": 1.0})),
+     "SBE_BAD_CONFIG", "Some MultiWSM paramters are missing"),
     (lambda c: c.__setitem__("target", "TMDCs"), "SBE_BAD_CONFIG", "Unknowm material: "),
     (lambda c: c.__setitem__("target", "KaneMele"), "SBE_BAD_CONFIG", "Some KaneMele paramters are missing"),
     (lambda c: c.__setitem__("target", "WilsonMass"), "SBE_BAD_CONFIG", "Some Haldane paramters are missing"),

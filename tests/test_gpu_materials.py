@@ -1,5 +1,6 @@
 """The reference's analytic materials (KaneMele, Haldane2L, WilsonMass,
-XYHlattice) on the GPU as Fourier tables of H(k) and GenJMatrix, both gauges,
+XYHlattice, ...) on the GPU as Fourier tables of H(k) and GenJMatrix, and the
+continuum MultiWSM model from its formulas, both gauges,
 against the reference's own outputs on the same cfgs (golden fixtures made by
 tests/golden/make_golden.py).  FP64 bar: 1e-10 of max_t |J| per current
 series; occupations 1e-12."""
@@ -9,7 +10,7 @@ import numpy as np
 import pytest
 
 import antelope_b200 as ab
-from cases import BAND_GROUPS, MATERIAL_CASES
+from cases import BAND_GROUPS, MATERIAL_CASES, MULTIWSM_CASES
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -42,6 +43,31 @@ def test_material_fp64_matches_reference(name):
     # in the length gauge (Wannier basis) only
     if case["gauge"] != "Velocity":
         assert np.abs(out.coh - ref["coh_file"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("name", sorted(MULTIWSM_CASES))
+def test_multiwsm_fp64_matches_reference(name):
+    """The continuum MultiWSM model (formulas at k + A in place of Fourier
+    tables) on a 3-D grid, with its z current, against the reference's files.
+    Every series to 1e-10 of the largest current; the z series, 1e-3 to 1e-2
+    of the in-plane ones here and residuals of O(v) terms that cancel over
+    the grid, also to 1e-8 of their own maximum (measured: up to 1.2e-9; the
+    device's pow and atan2 round differently from the host's, an ulp in H)."""
+    case = MULTIWSM_CASES[name]
+    ref = np.load(os.path.join(GOLDEN, f"golden_{name}.npz"))
+    out = ab.solve(case, precision="fp64")
+    scale = max(np.abs(ref["inter"]).max(), np.abs(ref["intra"]).max())
+    for key in ("inter", "intra"):
+        for a in range(3):
+            d = np.abs(getattr(out, key)[:, a] - ref[key][:, a]).max()
+            assert d < 1e-10 * scale, (key, a, d / scale)
+            assert d < 1e-8 * max(np.abs(ref[key][:, a]).max(), 1e-3 * scale), (key, a)
+    assert np.abs(out.occ[:, :2] - ref["occ_file"][:, :2]).max() < 1e-12
+    if case["gauge"] != "Velocity":
+        assert np.abs(out.coh - ref["coh_file"]).max() < 1e-12
+    mix = ab.solve(case, precision="mixed")
+    for key in ("inter", "intra"):
+        assert np.abs(getattr(mix, key) - getattr(out, key)).max() < 1e-5 * scale, key
 
 
 @pytest.mark.parametrize("name", ["kanemele_w", "haldane2l_v", "xyhlattice_w"])
