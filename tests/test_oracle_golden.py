@@ -2,6 +2,7 @@
 itself (golden fixtures made by tests/golden/make_golden.py from the
 unmodified reference sources).  This pins the oracle before the GPU kernels are
 compared with it."""
+import copy
 import os
 
 import numpy as np
@@ -84,6 +85,35 @@ def test_oracle_haldane_j_is_minus_dh_dk():
         Hm, _ = pyoracle.model_hj(case, k - dk)
         assert np.allclose(J[a], -(Hp - Hm) / (2 * h), atol=1e-8)
     assert np.all(J[2] == 0)
+
+
+@pytest.mark.parametrize("n", [1.0, 2.0, 1.5])
+def test_oracle_multiwsm_j_is_minus_dh_dk(n):
+    """MultiWSM's GenJMatrix formulas (MultiWSM.h:84-147) are -dH/dk of its
+    GenBcomp (MultiWSM.h:186-200) away from the k_x = k_y = 0 line, z included."""
+    case = copy.deepcopy(MULTIWSM_CASES["multiwsm_w"])
+    case["MultiWSM"]["n"] = n
+    k = np.array([0.31, -0.17, 0.4])
+    _, J = pyoracle.model_hj(case, k)
+    h = 1e-6
+    for a in range(3):
+        dk = np.zeros(3)
+        dk[a] = h
+        Hp, _ = pyoracle.model_hj(case, k + dk)
+        Hm, _ = pyoracle.model_hj(case, k - dk)
+        assert np.allclose(J[a], -(Hp - Hm) / (2 * h), atol=1e-8), a
+    assert np.allclose(J[2], np.diag([-0.2, 0.2]))
+
+
+def test_multiwsm_problem_matches_oracle_grid():
+    """The cfg front end's MultiWSM problem: the oracle's 3-D grid and zone
+    (the cube [-pi/a0, pi/a0]^3, a0 in Angstrom)."""
+    from antelope_b200 import Problem
+
+    for name, case in MULTIWSM_CASES.items():
+        d, od = Problem.from_dict(case).dims, pyoracle.dims(case)
+        assert (d.ntotal, d.Nt, d.nband, d.nval) == (od["ntotal"], od["Nt"], od["nband"], od["nval"]), name
+        assert d.dV == od["dV"], name
 
 
 @pytest.mark.skipif(not os.path.exists(pyoracle.REF_EXE), reason="reference build absent")
