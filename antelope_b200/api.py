@@ -289,6 +289,12 @@ class Batch:
         _check(lib.sbe_batch_harmonics(self._h, i, C.c_double(w0), hmax, out.ctypes.data))
         return out
 
+    def steps(self, i: int) -> dict:
+        """Accepted steps, attempts and rejected attempts of solve i."""
+        v = [C.c_longlong() for _ in range(3)]
+        _check(lib.sbe_batch_steps(self._h, i, *[C.byref(x) for x in v]))
+        return {"steps": v[0].value, "attempts": v[1].value, "rejects": v[2].value}
+
     @property
     def launches(self) -> int:
         return lib.sbe_batch_launches(self._h)

@@ -89,6 +89,8 @@ def _load():
         "sbe_batch_run": (C.c_int, [P, C.c_void_p]),
         "sbe_batch_get": (C.c_int, [P, C.c_int, C.POINTER(COutputs)]),
         "sbe_batch_launches": (C.c_int, [P]),
+        "sbe_batch_steps": (C.c_int, [P, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                      C.POINTER(C.c_longlong)]),
         "sbe_batch_destroy": (None, [P]),
         "sbe_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(P)]),
         "sbe_server_submit": (C.c_int, [P, P, C.POINTER(C.c_longlong)]),

@@ -521,11 +521,18 @@ extern "C" sbe_status sbe_run_cfg(const char *cfg_path, const char *out_dir, con
 }
 
 // ================================================================= batch
+// Two-band Haldane problems go to the engine (closed-form kernels, one launch
+// per launch class per step chunk); table and continuum models to a
+// WannierBatch (N-band kernels, one attempt and one control launch per launch
+// class per iteration).  A batch may hold both; they run one after the other
+// on the batch's stream.
 struct sbe_batch {
     std::unique_ptr<Engine> eng;
+    std::unique_ptr<WannierBatch> wan;
     cudaStream_t own = nullptr;
     cudaEvent_t ready = nullptr;
-    std::vector<int> ids;
+    std::vector<int> ids;        // engine solve id, or -1 - (index in the Wannier batch)
+    std::vector<long long> nt;   // output steps of each solve
     bool use_graph = false, ran = false;
     int launches = 0, device = 0;
 };
@@ -535,31 +542,40 @@ extern "C" sbe_status sbe_batch_create(const sbe_problem *const *problems, int n
 {
     if (!problems || n <= 0 || !out) return fail(SBE_INVALID_ARGUMENT, "need at least one problem");
     *out = nullptr;
-    for (int i = 0; i < n; ++i) {
+    for (int i = 0; i < n; ++i)
         if (sbe_status st = check_problem(problems[i])) return st;
-        if (problems[i]->p.model != MODEL_HALDANE)
-            return fail(SBE_UNSUPPORTED, "Wannier models run through sbe_solver_* (one solve at a time)");
-    }
     return guard([&]() -> sbe_status {
         auto b = std::make_unique<sbe_batch>();
         b->device = opts ? opts->device : 0;
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
         cuda_check(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking), "stream create");
         cuda_check(cudaEventCreateWithFlags(&b->ready, cudaEventDisableTiming), "event create");
-        b->eng = std::make_unique<Engine>(b->device, b->own, default_steps(opts));
-        // longest solves first: their tiles lead every launch's tile list
-        std::vector<int> order(n);
-        for (int i = 0; i < n; ++i) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-            return (double)problems[a]->p.laser.Nt * problems[a]->p.ntotal() >
-                   (double)problems[c]->p.laser.Nt * problems[c]->p.ntotal();
-        });
         b->ids.assign(n, -1);
-        EngineOptions eo = to_engine_opts(opts);
-        for (int i : order) b->ids[i] = b->eng->add(problems[i]->p, eo);
+        for (int i = 0; i < n; ++i) b->nt.push_back(problems[i]->p.laser.Nt);
+        std::vector<int> order, wan_order;
+        for (int i = 0; i < n; ++i) (problems[i]->p.model == MODEL_HALDANE ? order : wan_order).push_back(i);
+        if (!order.empty()) {
+            b->eng = std::make_unique<Engine>(b->device, b->own, default_steps(opts));
+            // longest solves first: their tiles lead every launch's tile list
+            std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+                return (double)problems[a]->p.laser.Nt * problems[a]->p.ntotal() >
+                       (double)problems[c]->p.laser.Nt * problems[c]->p.ntotal();
+            });
+            EngineOptions eo = to_engine_opts(opts);
+            for (int i : order) b->ids[i] = b->eng->add(problems[i]->p, eo);
+            b->eng->set_profile(opts && opts->profile);
+        }
+        if (!wan_order.empty()) {
+            std::vector<const Problem *> probs;
+            for (int j = 0; j < (int)wan_order.size(); ++j) {
+                probs.push_back(&problems[wan_order[j]]->p);
+                b->ids[wan_order[j]] = -1 - j;
+            }
+            const int prec = opts ? opts->precision : -1;
+            b->wan = std::make_unique<WannierBatch>(probs, prec, b->device, b->own);
+        }
         cuda_check(cudaEventRecord(b->ready, b->own), "event record");
         b->use_graph = opts && opts->use_graph && !opts->profile;
-        b->eng->set_profile(opts && opts->profile);
         *out = b.release();
         return SBE_OK;
     });
@@ -573,9 +589,17 @@ extern "C" sbe_status sbe_batch_run(sbe_batch *b, void *stream)
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->own;
         cuda_check(cudaStreamWaitEvent(st, b->ready, 0), "stream wait");
-        b->eng->set_stream(st);
-        run_engine(*b->eng, b->use_graph, &b->launches);
-        for (int id : b->ids) b->eng->fetch_async(id);
+        b->launches = 0;
+        if (b->eng) {
+            b->eng->set_stream(st);
+            run_engine(*b->eng, b->use_graph, &b->launches);
+            for (int id : b->ids)
+                if (id >= 0) b->eng->fetch_async(id);
+        }
+        if (b->wan) {
+            b->wan->run(st, b->use_graph);
+            b->launches += b->wan->launches();
+        }
         b->ran = true;
         return SBE_OK;
     });
@@ -587,9 +611,31 @@ extern "C" sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *
     if (!b->ran) return fail(SBE_NOT_READY, "sbe_batch_run has not been called");
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
-        copy_out(b->eng->outputs(b->ids[index]), out);
+        const int id = b->ids[index];
+        copy_out(id >= 0 ? b->eng->outputs(id) : b->wan->solve(-1 - id).outputs(), out);
         return SBE_OK;
     });
+}
+
+extern "C" sbe_status sbe_batch_steps(sbe_batch *b, int index, long long *steps, long long *attempts,
+                                      long long *rejects)
+{
+    if (!b || index < 0 || index >= (int)b->ids.size()) return fail(SBE_INVALID_ARGUMENT, "bad batch index");
+    if (!b->ran) return fail(SBE_NOT_READY, "sbe_batch_run has not been called");
+    const int id = b->ids[index];
+    long long st = 0, at = 0, rj = 0;
+    if (id < 0) {
+        const WanCtl &c = b->wan->solve(-1 - id).control();
+        st = c.steps;
+        at = c.attempts;
+        rj = c.rejects;
+    } else {
+        st = at = b->nt[index];   // fixed step: one step per output time
+    }
+    if (steps) *steps = st;
+    if (attempts) *attempts = at;
+    if (rejects) *rejects = rj;
+    return SBE_OK;
 }
 
 extern "C" sbe_status sbe_batch_harmonics(sbe_batch *b, int index, double w0, int hmax, double *band_power)
@@ -599,7 +645,9 @@ extern "C" sbe_status sbe_batch_harmonics(sbe_batch *b, int index, double w0, in
     if (!b->ran) return fail(SBE_NOT_READY, "sbe_batch_run has not been called");
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
-        b->eng->harmonics(b->ids[index], w0, hmax, band_power);
+        const int id = b->ids[index];
+        if (id >= 0) b->eng->harmonics(id, w0, hmax, band_power);
+        else b->wan->solve(-1 - id).harmonics(w0, hmax, band_power);
         return SBE_OK;
     });
 }
@@ -610,7 +658,9 @@ extern "C" sbe_status sbe_batch_snapshots(sbe_batch *b, int index, double *occ1d
     if (!b->ran) return fail(SBE_NOT_READY, "sbe_batch_run has not been called");
     return guard([&]() -> sbe_status {
         cuda_check(cudaSetDevice(b->device), "cudaSetDevice");
-        if (b->eng->snapshots(b->ids[index], occ1d, nc, pi) == 0)
+        const int id = b->ids[index];
+        const int n = id >= 0 ? b->eng->snapshots(id, occ1d, nc, pi) : b->wan->solve(-1 - id).snapshots(occ1d, nc, pi);
+        if (n == 0)
             return fail(SBE_INVALID_ARGUMENT, "the problem takes no snapshots (calc.shotNumber <= 0)");
         return SBE_OK;
     });
@@ -622,7 +672,11 @@ extern "C" sbe_status sbe_batch_kernel_times(sbe_batch *b, double *pms, int *pn,
 {
     if (!b) return fail(SBE_INVALID_ARGUMENT, "null batch");
     return guard([&]() -> sbe_status {
-        b->eng->kernel_times(pms, pn, rms, rn);
+        if (pms) *pms = 0;
+        if (pn) *pn = 0;
+        if (rms) *rms = 0;
+        if (rn) *rn = 0;
+        if (b->eng) b->eng->kernel_times(pms, pn, rms, rn);
         return SBE_OK;
     });
 }
@@ -632,6 +686,7 @@ extern "C" void sbe_batch_destroy(sbe_batch *b)
     if (!b) return;
     cudaSetDevice(b->device);
     b->eng.reset();
+    b->wan.reset();
     if (b->ready) cudaEventDestroy(b->ready);
     if (b->own) {
         cudaStreamSynchronize(b->own);

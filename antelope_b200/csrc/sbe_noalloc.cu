@@ -27,6 +27,13 @@
 //    partials into what is left.
 //  - No cudaMalloc, cudaFree, cudaMallocHost or other allocating routine is
 //    called; host-side staging uses a fixed static buffer.
+//  - The caller's current device is restored before returning, and every
+//    return -- error paths included -- comes after the GPU work this call
+//    queued has finished, so the next call never races on the array.
+//  - Default launch shape: the engine's heuristic without the autotuner (two
+//    k-points per thread for the mixed velocity gauge, the largest CTA of at
+//    most 128 threads that still gives two CTAs per SM); with the same tile_k
+//    and k_per_thread the results equal sbe_solver_*'s bit for bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -91,12 +98,23 @@ extern "C" sbe_status sbe_solve_noalloc(const sbe_problem *problem, const sbe_op
                                                  "sbe_solver_* (velocity or length gauge, RKorder 4 or 5)");
     const int device = opts ? opts->device : 0;
     const int precision = (opts && opts->precision >= 0) ? opts->precision : p.precision;
-    const int kpt = (opts && opts->k_per_thread > 0 && p.gauge == GAUGE_VELOCITY) ? opts->k_per_thread : 1;
-    const int tile_k = (opts && opts->tile_k > 0) ? opts->tile_k : 128 * kpt;
+    const bool is_vg = p.gauge == GAUGE_VELOCITY;
+    // launch shape: the engine's defaults (Engine::shape_for) without the autotuner
+    int kpt = (opts && opts->k_per_thread > 0) ? opts->k_per_thread : ((is_vg && precision == PREC_MIXED) ? 2 : 1);
+    if (!is_vg) kpt = 1;
+    if (kpt != 1 && kpt != 2) return sbe_noalloc_fail(SBE_INVALID_ARGUMENT, "k_per_thread must be 1 or 2");
+    int tile_k = (opts && opts->tile_k > 0) ? opts->tile_k : 0;
+    if (tile_k == 0) {
+        int sms = 148;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) sms = 148;
+        int th = 128;
+        while (th > 32 && (long long)p.ntotal() < 2LL * sms * th * kpt) th /= 2;
+        tile_k = th * kpt;
+    }
     const int threads = tile_k / kpt;
     if (threads < 32 || threads > 256 || threads % 32 || tile_k % kpt)
         return sbe_noalloc_fail(SBE_INVALID_ARGUMENT, "tile_k / k_per_thread must be a multiple of 32 in [32, 256]");
-    const bool vg = p.gauge == GAUGE_VELOCITY;
+    const bool vg = is_vg;
     const int variant = vg ? VAR_HALDANE_VG : VAR_HALDANE_LW;
     const size_t real = precision == PREC_FP64 ? 8 : 4;
     const int nk = p.ntotal(), Nt = p.laser.Nt;
@@ -141,6 +159,20 @@ extern "C" sbe_status sbe_solve_noalloc(const sbe_problem *problem, const sbe_op
         return false;
     };
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // on every return: wait for what this call queued (so an early error
+    // cannot leave work running on the shared array after the lock is
+    // released), then give the caller back its current device
+    struct Leave {
+        int prev = -1;
+        cudaStream_t st = nullptr;
+        ~Leave()
+        {
+            cudaStreamSynchronize(st);
+            if (prev >= 0) cudaSetDevice(prev);
+        }
+    } leave;
+    leave.st = st;
+    if (!cu(cudaGetDevice(&leave.prev), "cudaGetDevice")) return SBE_CUDA_ERROR;
     unsigned char *base = nullptr;
     if (!cu(cudaSetDevice(device), "cudaSetDevice")) return SBE_CUDA_ERROR;
     if (!cu(scratch_address(device, &base), "cudaGetSymbolAddress(scratch)")) return SBE_CUDA_ERROR;

@@ -739,13 +739,17 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_init(WanDev P)
 // NC: the band count as a compile-time constant (0: read at run time), so
 // that index arithmetic and the loops over N fold at the common sizes.
 template <class RF, int NC>
-__global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *__restrict__ Pp)
+__global__ void __launch_bounds__(32 * WAN_WARPS, 5)
+    wan_attempt(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs,
+                const WanTileRef *__restrict__ tiles)
 {
     using TF = typename Cx<RF>::T;
     using T = double2;
     constexpr bool F32 = std::is_same<RF, float>::value;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const WanDev &P = *Pp;
+    // a single solve (tiles == nullptr: block = tile) or a tile of a batch
+    const int tile = tiles ? tiles[blockIdx.x].tile : (int)blockIdx.x;
+    const WanDev &P = tiles ? *descs[tiles[blockIdx.x].solve] : *Pp;
     const WanCtl ctl = *P.ctl;
     if (ctl.done) return;
     const int N = NC > 0 ? NC : P.N, NN = N * N, NU = N * (N + 1) / 2, nR = P.nR;
@@ -771,7 +775,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
     __syncthreads();
     const int S = tab.S;
 
-    const int k = blockIdx.x * WAN_WARPS + wi;
+    const int k = tile * WAN_WARPS + wi;
     double emax = 0.0;
     if (k < P.nk) {
         const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, N, nR);
@@ -972,12 +976,12 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_attempt(const WanDev *_
     if (threadIdx.x == 0) {
         double m = 0.0;
         for (int i = 0; i < WAN_WARPS; ++i) m = fmax(m, bh.errw[i]);
-        P.tile_err[blockIdx.x] = m;
+        P.tile_err[tile] = m;
     }
     if (cur && threadIdx.x < WAN_NSLOT) {
         double s = 0.0;
         for (int i = 0; i < WAN_WARPS; ++i) s += bh.part[i][threadIdx.x];
-        P.cur_part[(size_t)blockIdx.x * WAN_NSLOT + threadIdx.x] = s;
+        P.cur_part[(size_t)tile * WAN_NSLOT + threadIdx.x] = s;
     }
 }
 
@@ -1084,11 +1088,14 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
 }
 
 template <class RF, int NC>   // NC: as in wan_attempt
-__global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev *__restrict__ Pp)
+__global__ void __launch_bounds__(32 * WAN_WARPS, 5)
+    wan_vg_attempt(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs,
+                   const WanTileRef *__restrict__ tiles)
 {
     using T = double2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const WanDev &P = *Pp;
+    const int tile = tiles ? tiles[blockIdx.x].tile : (int)blockIdx.x;
+    const WanDev &P = tiles ? *descs[tiles[blockIdx.x].solve] : *Pp;
     const WanCtl ctl = *P.ctl;
     if (ctl.done) return;
     const int N = NC > 0 ? NC : P.N, NN = N * N, NU = N * (N + 1) / 2;
@@ -1107,7 +1114,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev
     if (threadIdx.x < WAN_WARPS) bh.errw[threadIdx.x] = 0.0;
     __syncthreads();
     const int S = tab.S;
-    const int k = blockIdx.x * WAN_WARPS + wi;
+    const int k = tile * WAN_WARPS + wi;
     double emax = 0.0;
     if (k < P.nk) {
         const WarpView<RF> w(smem_raw + L.warp0 + wi * L.warp_bytes, N, P.nR);
@@ -1246,12 +1253,12 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5) wan_vg_attempt(const WanDev
     if (threadIdx.x == 0) {
         double m = 0.0;
         for (int i = 0; i < WAN_WARPS; ++i) m = fmax(m, bh.errw[i]);
-        P.tile_err[blockIdx.x] = m;
+        P.tile_err[tile] = m;
     }
     if (cur && threadIdx.x < WAN_NSLOT) {
         double s = 0.0;
         for (int i = 0; i < WAN_WARPS; ++i) s += bh.part[i][threadIdx.x];
-        P.cur_part[(size_t)blockIdx.x * WAN_NSLOT + threadIdx.x] = s;
+        P.cur_part[(size_t)tile * WAN_NSLOT + threadIdx.x] = s;
     }
 }
 
@@ -1350,11 +1357,12 @@ __device__ void control_decide(const WanDev &P, WanCtl *ctl, double emax)
     }
 }
 
-template <class RF> __global__ void __launch_bounds__(1024) wan_control(const WanDev *__restrict__ Pp)
+template <class RF>
+__global__ void __launch_bounds__(1024) wan_control(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs)
 {
     __shared__ double red[1024];
     __shared__ double cs[WAN_NSLOT][64];
-    const WanDev &P = *Pp;
+    const WanDev &P = descs ? *descs[blockIdx.x] : *Pp;   // batches: one block per solve
     WanCtl *ctl = P.ctl;
     if (ctl->done) {
         if (threadIdx.x == 0) ctl->shot = -1;   // a snapshot is taken once
@@ -1399,9 +1407,13 @@ template <class RF> __global__ void __launch_bounds__(1024) wan_control(const Wa
 // Jacobi sweeps from the identity, eigenvectors ranked by ascending
 // eigenvalue as zheevr orders them.  One warp per k-point.
 template <class RF>
-__global__ void __launch_bounds__(32 * WAN_WARPS) wan_snapshot(const WanDev *__restrict__ Pp)
+__global__ void __launch_bounds__(32 * WAN_WARPS)
+    wan_snapshot(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs,
+                 const WanTileRef *__restrict__ tiles)
 {
-    const WanDev &P = *Pp;
+    const int tile = tiles ? tiles[blockIdx.x].tile : (int)blockIdx.x;
+    const WanDev &P = tiles ? *descs[tiles[blockIdx.x].solve] : *Pp;
+    if (P.shot_every <= 0) return;
     const int shot = P.ctl->shot;
     if (shot < 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1414,7 +1426,7 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_snapshot(const WanDev *__r
         fill_tables(bh, P.N);
     }
     __syncthreads();
-    const int k = blockIdx.x * WAN_WARPS + wi;
+    const int k = tile * WAN_WARPS + wi;
     if (k >= P.nk) return;
     const int N = P.N, NN = N * N, nv = P.nval;
     const double2 *rho = P.rho[P.ctl->buf] + (size_t)k * NN;
@@ -1535,7 +1547,7 @@ cudaError_t launch_field_table(const LaserDev &L, double atmin, double dt, int N
 }
 
 // ============================================================= launchers
-using WanKernel = void (*)(const WanDev *);
+using WanKernel = void (*)(const WanDev *, const WanDev *const *, const WanTileRef *);
 template <class RF> static WanKernel wan_attempt_n(int N, bool vg)
 {
     switch (N) {
@@ -1603,8 +1615,20 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
     // N = 6 Wannier configuration, other N read at run time; the velocity
     // gauge's stage arithmetic is FP64 in both methods (no per-stage Fourier
     // sums), its RF instance only matches the layout `sm` was sized for
-    if (precision == 0) wan_attempt_n<double>(w.N, w.vg)<<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-    else wan_attempt_n<float>(w.N, w.vg)<<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    if (precision == 0) wan_attempt_n<double>(w.N, w.vg)<<<grid, 32 * WAN_WARPS, sm, st>>>(dw, nullptr, nullptr);
+    else wan_attempt_n<float>(w.N, w.vg)<<<grid, 32 * WAN_WARPS, sm, st>>>(dw, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wan_attempt_batch(int N, int nR_max, bool vg, const WanDev *const *descs, const WanTileRef *tiles,
+                                     int ntiles, int precision, cudaStream_t st)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
+    if (e != cudaSuccess) return e;
+    const size_t sm = wan_smem_bytes(N, nR_max, precision);
+    if (precision == 0) wan_attempt_n<double>(N, vg)<<<ntiles, 32 * WAN_WARPS, sm, st>>>(nullptr, descs, tiles);
+    else wan_attempt_n<float>(N, vg)<<<ntiles, 32 * WAN_WARPS, sm, st>>>(nullptr, descs, tiles);
     return cudaGetLastError();
 }
 
@@ -1615,15 +1639,35 @@ cudaError_t launch_wan_snapshot(const WanDev &w, const WanDev *dw, int precision
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
     const size_t sm = wan_smem_bytes(w.N, w.nR, precision);
-    if (precision == 0) wan_snapshot<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
-    else wan_snapshot<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw);
+    if (precision == 0) wan_snapshot<double><<<grid, 32 * WAN_WARPS, sm, st>>>(dw, nullptr, nullptr);
+    else wan_snapshot<float><<<grid, 32 * WAN_WARPS, sm, st>>>(dw, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wan_snapshot_batch(int N, int nR_max, const WanDev *const *descs, const WanTileRef *tiles,
+                                      int ntiles, int precision, cudaStream_t st)
+{
+    if (ntiles <= 0) return cudaSuccess;
+    cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
+    if (e != cudaSuccess) return e;
+    const size_t sm = wan_smem_bytes(N, nR_max, precision);
+    if (precision == 0) wan_snapshot<double><<<ntiles, 32 * WAN_WARPS, sm, st>>>(nullptr, descs, tiles);
+    else wan_snapshot<float><<<ntiles, 32 * WAN_WARPS, sm, st>>>(nullptr, descs, tiles);
     return cudaGetLastError();
 }
 
 cudaError_t launch_wan_control(const WanDev *dw, int precision, cudaStream_t st)
 {
-    if (precision == 0) wan_control<double><<<1, 1024, 0, st>>>(dw);
-    else wan_control<float><<<1, 1024, 0, st>>>(dw);
+    if (precision == 0) wan_control<double><<<1, 1024, 0, st>>>(dw, nullptr);
+    else wan_control<float><<<1, 1024, 0, st>>>(dw, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wan_control_batch(const WanDev *const *descs, int nsolves, int precision, cudaStream_t st)
+{
+    if (nsolves <= 0) return cudaSuccess;
+    if (precision == 0) wan_control<double><<<nsolves, 1024, 0, st>>>(nullptr, descs);
+    else wan_control<float><<<nsolves, 1024, 0, st>>>(nullptr, descs);
     return cudaGetLastError();
 }
 

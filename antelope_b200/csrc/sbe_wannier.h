@@ -85,6 +85,15 @@ struct WanDev {
     double *snap_pi;
 };
 
+// A tile of a batched launch: tile `tile` (WAN_WARPS k-points) of solve
+// `solve` of the launch's descriptor array.  Batches of N-band solves advance
+// every solve of a launch class (same N, gauge and precision) with one
+// attempt launch over all their tiles and one control launch with one block
+// per solve, each solve keeping its own step-size controller.
+struct WanTileRef {
+    int solve, tile;
+};
+
 struct Laser;
 // The laser of a problem in the device layout (throws CfgError beyond 8 pulses).
 LaserDev laser_dev(const Laser &L);
@@ -105,5 +114,14 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
 cudaError_t launch_wan_control(const WanDev *dw, int precision, cudaStream_t st);
 // the snapshot of the interval the last control step completed, if one is due
 cudaError_t launch_wan_snapshot(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st);
+// Batched forms: `descs` [nsolves] device pointers to the solves' descriptors,
+// `tiles` [ntiles] the tiles of all of them (device memory); N, nR_max and
+// the gauge (vg) of the launch class size the shared memory and pick the
+// instance.  Control: one block per solve.
+cudaError_t launch_wan_attempt_batch(int N, int nR_max, bool vg, const WanDev *const *descs, const WanTileRef *tiles,
+                                     int ntiles, int precision, cudaStream_t st);
+cudaError_t launch_wan_control_batch(const WanDev *const *descs, int nsolves, int precision, cudaStream_t st);
+cudaError_t launch_wan_snapshot_batch(int N, int nR_max, const WanDev *const *descs, const WanTileRef *tiles,
+                                      int ntiles, int precision, cudaStream_t st);
 
 }  // namespace sbe

@@ -188,6 +188,136 @@ void WannierSolve::run(cudaStream_t st)
     launches_ = (int)((w_.shot_every > 0 ? 3 : 2) * launched);   // attempt, control (, snapshot)
 }
 
+void WannierSolve::finish_batched(const WanCtl &c, int launches)
+{
+    *h_ctl_ = c;
+    launches_ = launches;
+    if (c.error) throw CudaError("Cash-Karp step size underflow: tolerance unreachable");
+}
+
+// ============================================================= batches
+WannierBatch::WannierBatch(const std::vector<const Problem *> &probs, int precision, int device, cudaStream_t st)
+    : device_(device), stream_(st)
+{
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    for (const Problem *p : probs) {
+        const int prec = precision >= 0 ? precision : p->precision;
+        solves_.push_back(std::make_unique<WannierSolve>(*p, prec, device_, st));
+    }
+    // launch classes; within a class the solves with the most k-point steps
+    // lead the tile list, so their blocks are scheduled first
+    for (int i = 0; i < (int)solves_.size(); ++i) {
+        const WanDev &w = solves_[i]->dev();
+        Class *c = nullptr;
+        for (Class &x : classes_)
+            if (x.N == w.N && x.vg == (w.vg != 0) && x.precision == solves_[i]->precision()) c = &x;
+        if (!c) {
+            classes_.emplace_back();
+            c = &classes_.back();
+            c->N = w.N;
+            c->vg = w.vg != 0;
+            c->precision = solves_[i]->precision();
+        }
+        c->members.push_back(i);
+        c->nR = std::max(c->nR, w.nR);
+        c->shots = c->shots || w.shot_every > 0;
+    }
+    UploadRing &ring = UploadRing::shared();
+    for (Class &c : classes_) {
+        std::stable_sort(c.members.begin(), c.members.end(), [&](int a, int b) {
+            const WanDev &x = solves_[a]->dev(), &y = solves_[b]->dev();
+            return (double)x.nk * x.Nt > (double)y.nk * y.Nt;
+        });
+        std::vector<const WanDev *> descs;
+        std::vector<WanTileRef> tiles;
+        for (int j = 0; j < (int)c.members.size(); ++j) {
+            const WannierSolve &s = *solves_[c.members[j]];
+            descs.push_back(s.dev_ptr());
+        }
+        // interleave the solves' tiles round-robin (longest first), so that
+        // the blocks of one launch spread every solve over the whole GPU
+        int maxt = 0;
+        for (int m : c.members) maxt = std::max(maxt, solves_[m]->dev().ntiles);
+        for (int t = 0; t < maxt; ++t)
+            for (int j = 0; j < (int)c.members.size(); ++j)
+                if (t < solves_[c.members[j]]->dev().ntiles) tiles.push_back(WanTileRef{j, t});
+        c.ntiles = (int)tiles.size();
+        dalloc(&c.d_descs, sizeof(WanDev *) * descs.size(), st, "alloc batch descriptors");
+        dalloc(&c.d_tiles, sizeof(WanTileRef) * tiles.size(), st, "alloc batch tiles");
+        ring.upload(c.d_descs, descs.data(), sizeof(WanDev *) * descs.size(), st);
+        ring.upload(c.d_tiles, tiles.data(), sizeof(WanTileRef) * tiles.size(), st);
+        per_iter_ += c.shots ? 3 : 2;
+    }
+    cuda_check(cudaMallocHost(&h_ctls_, sizeof(WanCtl) * std::max<size_t>(1, solves_.size())),
+               "cudaMallocHost(batch control)");
+}
+
+WannierBatch::~WannierBatch()
+{
+    cudaStreamSynchronize(stream_);
+    for (Class &c : classes_) {
+        if (c.d_descs) cudaFreeAsync(c.d_descs, stream_);
+        if (c.d_tiles) cudaFreeAsync(c.d_tiles, stream_);
+    }
+    cudaStreamSynchronize(stream_);
+    solves_.clear();
+    if (h_ctls_) cudaFreeHost(h_ctls_);
+}
+
+void WannierBatch::enqueue_chunk(cudaStream_t st, int iters)
+{
+    for (int it = 0; it < iters; ++it)
+        for (const Class &c : classes_) {
+            cuda_check(launch_wan_attempt_batch(c.N, c.nR, c.vg, c.d_descs, c.d_tiles, c.ntiles, c.precision, st),
+                       "Wannier attempt kernel (batch)");
+            cuda_check(launch_wan_control_batch(c.d_descs, (int)c.members.size(), c.precision, st),
+                       "Wannier control kernel (batch)");
+            if (c.shots)
+                cuda_check(launch_wan_snapshot_batch(c.N, c.nR, c.d_descs, c.d_tiles, c.ntiles, c.precision, st),
+                           "Wannier snapshot kernel (batch)");
+        }
+}
+
+void WannierBatch::run(cudaStream_t st, bool use_graph)
+{
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    stream_ = st;
+    for (auto &s : solves_) s->set_stream(st);
+    const int chunk = 64;
+    long long max_nt = 0;
+    for (auto &s : solves_) max_nt = std::max<long long>(max_nt, s->dev().Nt);
+    const long long max_iters = 64LL * max_nt + 1000;
+    cudaGraphExec_t ge = nullptr;
+    if (use_graph) {
+        cudaGraph_t g;
+        cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+        enqueue_chunk(st, chunk);
+        cuda_check(cudaStreamEndCapture(st, &g), "end capture");
+        cuda_check(cudaGraphInstantiate(&ge, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+    }
+    long long iters = 0;
+    bool all_done = false;
+    while (!all_done) {
+        if (ge) cuda_check(cudaGraphLaunch(ge, st), "graph launch");
+        else enqueue_chunk(st, chunk);
+        iters += chunk;
+        for (int i = 0; i < (int)solves_.size(); ++i)
+            cuda_check(cudaMemcpyAsync(&h_ctls_[i], solves_[i]->dev().ctl, sizeof(WanCtl), cudaMemcpyDeviceToHost, st),
+                       "copy control");
+        cuda_check(cudaStreamSynchronize(st), "sync");
+        all_done = true;
+        for (int i = 0; i < (int)solves_.size(); ++i) all_done = all_done && h_ctls_[i].done;
+        if (!all_done && iters > max_iters) {
+            if (ge) cudaGraphExecDestroy(ge);
+            throw CudaError("Wannier batch made no progress (step-size controller)");
+        }
+    }
+    if (ge) cudaGraphExecDestroy(ge);
+    launches_ = (int)(per_iter_ * iters);
+    for (int i = 0; i < (int)solves_.size(); ++i) solves_[i]->finish_batched(h_ctls_[i], launches_);
+}
+
 void WannierSolve::harmonics(double w0, int hmax, double *band_power)
 {
     const Problem &p = prob_;

@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
+#include <vector>
+
 #include "sbe_engine.h"
 #include "sbe_wannier.h"
 
@@ -27,6 +30,14 @@ public:
     int launches() const { return launches_; }
     const WanCtl &control() const { return *h_ctl_; }
 
+    // used by WannierBatch, which launches this solve's kernels itself
+    const WanDev &dev() const { return w_; }
+    const WanDev *dev_ptr() const { return d_w_; }
+    int precision() const { return precision_; }
+    void set_stream(cudaStream_t st) { stream_ = st; }
+    // the controller state after a batched run (copied in by the batch)
+    void finish_batched(const WanCtl &c, int launches);
+
 private:
     Problem prob_;
     int precision_, device_, nshots_ = 0;
@@ -35,6 +46,42 @@ private:
     WanDev *d_w_ = nullptr;
     WanCtl *h_ctl_ = nullptr;
     int launches_ = 0;
+};
+
+// Many N-band solves advanced together: solves of the same launch class
+// (band count, gauge, precision) share one attempt launch over all their
+// tiles and one control launch with one block per solve per iteration; each
+// solve keeps its own controller (its own Cash-Karp step size, or the fixed
+// step), so results equal the solves run alone bit for bit.  Solves that are
+// done leave their blocks idle until the longest one finishes.  The host
+// launches chunks of iterations and checks the controllers once per chunk;
+// with use_graph a chunk is captured once as a CUDA graph and replayed.
+class WannierBatch {
+public:
+    WannierBatch(const std::vector<const Problem *> &probs, int precision, int device, cudaStream_t st);
+    ~WannierBatch();
+    WannierBatch(const WannierBatch &) = delete;
+    WannierBatch &operator=(const WannierBatch &) = delete;
+    void run(cudaStream_t st, bool use_graph);
+    WannierSolve &solve(int i) { return *solves_[i]; }
+    int size() const { return (int)solves_.size(); }
+    int launches() const { return launches_; }
+
+private:
+    struct Class {
+        int N = 0, nR = 0, precision = 0;
+        bool vg = false, shots = false;
+        std::vector<int> members;
+        const WanDev **d_descs = nullptr;
+        WanTileRef *d_tiles = nullptr;
+        int ntiles = 0;
+    };
+    void enqueue_chunk(cudaStream_t st, int iters);
+    std::vector<std::unique_ptr<WannierSolve>> solves_;
+    std::vector<Class> classes_;
+    int device_ = 0, launches_ = 0, per_iter_ = 0;
+    cudaStream_t stream_ = nullptr;
+    WanCtl *h_ctls_ = nullptr;
 };
 
 // The reference's output arrays of a table model from its per-step sums

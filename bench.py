@@ -109,6 +109,15 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- GPU arm
+def bench_config(n: int, Nt: int, ncycles: float, env: str) -> dict:
+    """The workload of one bench step, identical in both arms."""
+    return {"workload": f"Haldane {n}x{n} velocity gauge, 3.2um {ncycles:g}-cycle {env} pulse (E0=0.0045), "
+                        f"dt=0.1 ({Nt} steps), RK4, T2=220; one whole solve per step",
+            "k_points": n * n, "time_steps": Nt, "precision": "fp64",
+            "l2": "flushed (512 MiB write) between timed GPU steps; per-k state 69 MB > L2 per solve",
+            "parallelism": "independent whole solves per device (weak scaling)"}
+
+
 def run_ours(args):
     import torch
 
@@ -118,7 +127,7 @@ def run_ours(args):
 
     import antelope_b200 as ab
     from antelope_b200 import cfgtext, workloads
-    from antelope_b200.api import Outputs, Solver
+    from antelope_b200.api import Solver
     from antelope_b200.spectrum import per_harmonic_error
 
     rank, world, local = dist_env()
@@ -132,9 +141,10 @@ def run_ours(args):
     stream = torch.cuda.Stream(device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     n = args.grid
-    case = {p: workloads.haldane_case(n=n, precision=p, ncycles=args.ncycles) for p in ("mixed", "fp64")}
+    case = {p: workloads.haldane_case(n=n, precision=p, ncycles=args.ncycles, env=args.env)
+            for p in ("mixed", "fp64")}
     probs = {p: ab.Problem.from_dict(c) for p, c in case.items()}
-    dims = probs["mixed"].dims
+    dims = probs["fp64"].dims
     kst = float(dims.ntotal) * dims.Nt
 
     def timed(prec, k, w, profile):
@@ -172,92 +182,96 @@ def run_ours(args):
             s.close()
         return ms, launches, ktimes, out
 
-    with ClockSampler(local) as clk:
-        ms_mixed, launches, kt_mixed, out_mixed = timed("mixed", args.steps, args.warmup, True)
-        ms_fp64, launches64, kt_fp64, out_fp64 = timed("fp64", max(2, args.steps // 3), 1, True)
-    clocks = clk.summary()
-
     from antelope_b200.dist import max_over_ranks
 
-    total_ms = max_over_ranks(sum(ms_mixed), dev)   # whole-job device time: max over ranks
+    # headline: the plain FP64 kernel, the reference's precision, on the
+    # reference arm's workload; the mixed method follows as an extra section
+    with ClockSampler(local) as clk:
+        ms_fp64, launches, kt_fp64, out_fp64 = timed("fp64", args.steps, args.warmup, True)
+        total_ms = max_over_ranks(sum(ms_fp64), dev)   # whole-job device time: max over ranks
+        ms_mixed, launches_mixed, kt_mixed, out_mixed = timed("mixed", max(3, args.steps // 2), 2, True)
+    clocks = clk.summary()
     value = world * args.steps * kst / (total_ms * 1e-3)
-    fp64_value = kst / (statistics.mean(ms_fp64) * 1e-3)
+    mixed_value = kst / (statistics.mean(ms_mixed) * 1e-3)
 
     # per-harmonic spectral error of the mixed run against the FP64 run
-    orders, err, _ = per_harmonic_error({"inter": out_mixed.inter, "intra": out_mixed.intra},
-                                        {"inter": out_fp64.inter, "intra": out_fp64.intra}, dims.dt, 0.014238)
+    w0 = case["fp64"]["laser"]["pulses"][0]["w0"]
+    spectral = {}
+    for floor in (1e-6, 1e-8):
+        orders, err, _ = per_harmonic_error({"inter": out_mixed.inter, "intra": out_mixed.intra},
+                                            {"inter": out_fp64.inter, "intra": out_fp64.intra}, dims.dt, w0,
+                                            floor=floor)
+        spectral[f"max_floor_{floor:g}"] = float(err.max())
+        spectral[f"harmonics_floor_{floor:g}"] = int(len(orders))
 
-    # e2e through the C ABI from host inputs to host outputs
+    # e2e through the C ABI from host inputs to host outputs, plain FP64
     e2e_s, phases = [], []
-    text = cfgtext.dumps(case["mixed"])
-    h2d = d2h = 0
+    text = cfgtext.dumps(case["fp64"])
     for i in range(max(3, args.steps // 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         p = ab.Problem.from_text(text)
         t1 = time.perf_counter()
-        s = Solver(p, precision="mixed")
+        s = Solver(p, precision="fp64")
         t2 = time.perf_counter()
         s.run(0)
-        o = s.get()
+        s.get()
         t3 = time.perf_counter()
         s.close()
         t4 = time.perf_counter()
         e2e_s.append(t4 - t0)
         phases.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
     shapes_now = read_tune_cache()
-    tile_k = args.tile_k or next((v["tile_k"] for k, v in shapes_now.items() if k.startswith("vg-mixed")), 512)
+    tile_k = args.tile_k or next((v["tile_k"] for k, v in shapes_now.items() if k.startswith("vg-fp64")), 128)
     ntiles = -(-dims.ntotal // tile_k)
     # the field table and per-k set-up are computed on the device from the
     # problem; what crosses to the device is the solve descriptor (with the
     # laser parameters) and the tile list, and back the per-step sums
     h2d = 512 + ntiles * 16
     d2h = dims.Nt * 8 * 8 + ntiles * 8 * 8       # per-step sums + per-tile constants
-    # median over the samples: one host-side hiccup would dominate a mean of five
+    # median over the samples: one host-side hiccup would dominate a mean
     e2e_value = kst / statistics.median(e2e_s)
 
-    # roofline of the propagate kernel from its own launch events
-    prop_ms = sum(k["propagate_ms"] for k in kt_mixed)
-    prop_n = sum(k["propagate_launches"] for k in kt_mixed)
-    red_ms = sum(k["reduce_ms"] for k in kt_mixed)
+    # roofline of the propagate kernels from their own launch events
     fp64_tf, fp32_tf, fp32x2_tf = ab.measure_fma_peaks(local)
-    flops = FLOPS_PER_KSTEP[4] * kst * args.steps
-    achieved = flops / (prop_ms * 1e-3) / 1e12
     prop64 = sum(k["propagate_ms"] for k in kt_fp64)
-    ach64 = FLOPS_PER_KSTEP[4] * kst * len(kt_fp64) / (prop64 * 1e-3) / 1e12
-    traffic = read_traffic()
+    red64 = sum(k["reduce_ms"] for k in kt_fp64)
+    achieved = FLOPS_PER_KSTEP[4] * kst * len(kt_fp64) / (prop64 * 1e-3) / 1e12
+    propm = sum(k["propagate_ms"] for k in kt_mixed)
+    redm = sum(k["reduce_ms"] for k in kt_mixed)
+    ach_m = FLOPS_PER_KSTEP[4] * kst * len(kt_mixed) / (propm * 1e-3) / 1e12
     shapes = read_tune_cache()
     kpt_mixed = args.kpt or next((v["k_per_thread"] for k, v in shapes.items() if k.startswith("vg-mixed")), 2)
-    kernel_name = "propagate_vg_x2<4> (2 k-points per thread, packed f32x2)" if kpt_mixed == 2 \
+    mixed_kernel = "propagate_vg_x2<4> (2 k-points per thread, packed f32x2)" if kpt_mixed == 2 \
         else "propagate_vg<float,4,1>"
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 stages / f64 sums", "data": "synthetic",
-        "config": {"workload": f"Haldane {n}x{n} velocity gauge, 3.2um 8-cycle sin2, dt=0.1 "
-                               f"({dims.Nt} steps), RK4, T2=220; mixed precision",
-                   "k_points": dims.ntotal, "time_steps": dims.Nt, "precision": "mixed",
-                   "l2": "flushed (512 MiB write) between timed steps",
-                   "parallelism": f"independent solves per GPU x{world}"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": bench_config(n, dims.Nt, args.ncycles, args.env),
         "solves_per_hour": value / kst * 3600.0,
-        "fp64": {"value": fp64_value, "unit": UNIT, "solves_per_hour": fp64_value / kst * 3600.0,
-                 "ms_per_solve": statistics.mean(ms_fp64), "roofline_frac": ach64 / fp64_tf,
-                 "achieved_tflops": ach64},
-        "mixed_over_fp64": value / world / fp64_value,
-        "spectral_error": {"max_per_harmonic": float(err.max()), "harmonics": int(len(orders)),
-                           "floor": "band power >= 1e-8 of the strongest", "vs": "fp64 run"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "seconds_per_solve": statistics.median(e2e_s), "statistic": f"median of {len(e2e_s)} solves",
                 "seconds_min_max": [min(e2e_s), max(e2e_s)],
                 "phase_seconds": dict(zip(("parse", "create", "run_and_get", "destroy"),
                                           [statistics.mean(x) for x in zip(*phases)])),
-                "path": "sbe_problem_from_string -> sbe_solver_create -> run -> sbe_solver_get"},
-        "roofline": {"bound": "fp32 FMA pipe", "achieved": achieved, "peak": fp32_tf, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_tf, "traffic": traffic,
-                     "peak_source": "measured FMA-chain microbenchmark (MEASURED_PEAKS.json has no FP32/FP64)",
-                     "flops_per_kstep": FLOPS_PER_KSTEP[4], "kernel": kernel_name,
-                     "kernel_share": prop_ms / (prop_ms + red_ms)},
+                "path": "sbe_problem_from_string -> sbe_solver_create -> run -> sbe_solver_get (fp64)"},
+        "roofline": {"bound": "fp64 FMA pipe", "achieved": achieved, "peak": fp64_tf, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_tf, "traffic": read_traffic("fp64"),
+                     "peak_source": "measured FMA-chain microbenchmark on this GPU in this run "
+                                    "(MEASURED_PEAKS.json has no FP64/FP32 figure)",
+                     "flops_per_kstep": FLOPS_PER_KSTEP[4], "kernel": "propagate_vg<double,4,1>",
+                     "kernel_share": prop64 / (prop64 + red64)},
+        "mixed": {"value": mixed_value, "unit": UNIT, "dtype": "f32 stages / f64 state and sums",
+                  "ms_per_solve": statistics.mean(ms_mixed), "solves_per_hour": mixed_value / kst * 3600.0,
+                  "over_fp64": mixed_value / (value / world),
+                  "spectral_error_vs_fp64": dict(spectral, floor="band power >= floor x the strongest"),
+                  "roofline": {"bound": "fp32 FMA pipe", "achieved": ach_m, "peak": fp32_tf, "unit": "TFLOP/s",
+                               "frac": ach_m / fp32_tf, "traffic": read_traffic("mixed"),
+                               "kernel": mixed_kernel, "kernel_share": propm / (propm + redm)},
+                  "launches": int(launches_mixed)},
+        "fma_peaks_tflops": {"fp64": fp64_tf, "fp32": fp32_tf, "fp32x2": fp32x2_tf},
         "launch_shapes": shapes,
         "gpu_launches": int(launches) * 2,   # propagate + reduce per launch tick, timed steps only
         "clocks": clocks,
@@ -271,7 +285,7 @@ def run_ours(args):
     if args.serve_requests > 0 and world == 1:
         line["serving"] = run_serve(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(n, dims.Nt, budget_s=args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(n, budget_s=args.cpu_seconds, ncycles=args.ncycles)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -333,11 +347,15 @@ def run_length_gauge(args, stream, fp64_tf, fp32_tf):
 def run_wannier(args, stream, fp64_tf):
     """The N = 6 Wannier configuration (triangular lattice, 37 lattice
     vectors, 3 valence bands, T2 = 220, 3.2 um sin2 pulse, Cash-Karp 4(5) at
-    tol 1e-8 with one step size per solve) on its full k-grid, with a pulse of
-    --wannier-cycles cycles in place of 10 so that the run stays bounded (the
-    same work per step over fewer steps; the spectrum is that of the shorter
-    pulse), plain FP64 and mixed.  k.steps count accepted steps; the roofline
-    counts attempted ones."""
+    tol 1e-8 with one step size per solve) on its full k-grid: --wannier-seeds
+    seeded models in one mixed-precision batch (sbe_batch_*: one attempt
+    launch over all their k-points per iteration, each solve with its own
+    controller, launches captured as CUDA graphs) against plain FP64 solves
+    of the same models one at a time.  The pulse has --wannier-cycles cycles
+    in place of 10 so that the run stays bounded: the work per step is the
+    configuration's and the step count scales with the pulse length, so the
+    10-cycle figures follow by the ratio of output steps (stated in the
+    line).  k.steps count accepted steps; the roofline counts attempted ones."""
     import torch
 
     import antelope_b200 as ab
@@ -345,43 +363,83 @@ def run_wannier(args, stream, fp64_tf):
     from antelope_b200.api import Solver
     from antelope_b200.spectrum import per_harmonic_error
 
-    n = args.wannier_grid
-    case = wannier.wannier_case(seed=1, n=n, ncycles=args.wannier_cycles, rk="cashkarp45", tol=1e-8)
-    group = case["SyntheticWannier"]
+    n, nseeds = args.wannier_grid, args.wannier_seeds
+    seeds = list(range(1, nseeds + 1))
+    cases = [wannier.wannier_case(seed=s, n=n, ncycles=args.wannier_cycles, rk="cashkarp45", tol=1e-8)
+             for s in seeds]
+    group = cases[0]["SyntheticWannier"]
     N, nR = int(group["Nband"]), len(group["R"]) // 2
-    res, outs = {}, {}
-    for prec in ("fp64", "mixed"):
-        p = ab.Problem.from_dict(dict(case, calc=dict(case["calc"], precision=prec)))
-        s = Solver(p, precision=prec)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    probs = {prec: [ab.Problem.from_dict(dict(c, calc=dict(c["calc"], precision=prec))) for c in cases]
+             for prec in ("fp64", "mixed")}
+    nk = probs["fp64"][0].dims.ntotal
+    Nt = probs["fp64"][0].dims.Nt
+    full_steps = wannier.wannier_case(seed=1, n=4, ncycles=10.0)
+    Nt_full = ab.Problem.from_dict(full_steps).dims.Nt
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    # plain FP64, one solve at a time (the first --wannier-fp64-seeds models)
+    fp64_ms, fp64_out, fp64_st = [], [], []
+    for p in probs["fp64"][:args.wannier_fp64_seeds]:
+        s = Solver(p, precision="fp64")
+        e0, e1 = ev(), ev()
         torch.cuda.synchronize()
         e0.record(stream)
         s.run(stream.cuda_stream)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        st = s.steps()
-        outs[prec] = s.get()
+        fp64_ms.append(e0.elapsed_time(e1))
+        fp64_st.append(s.steps())
+        fp64_out.append(s.get())
         s.close()
-        nk = p.dims.ntotal
-        flops = wannier_flops_per_rhs(N, nR) * 6 * nk * st["attempts"]
-        res[prec] = {"ms": ms, "k_steps_per_s": nk * st["steps"] / (ms * 1e-3), **st,
-                     "achieved_tflops": flops / (ms * 1e-3) / 1e12}
-        res[prec]["roofline_frac_fp64"] = res[prec]["achieved_tflops"] / fp64_tf
-    a, b = outs["fp64"], outs["mixed"]
-    w0 = case["laser"]["pulses"][0]["w0"]
-    o6, e6, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra}, {"inter": a.inter, "intra": a.intra},
-                                   0.1, w0, floor=1e-6)
-    o8, e8, _ = per_harmonic_error({"inter": b.inter, "intra": b.intra}, {"inter": a.inter, "intra": a.intra},
-                                   0.1, w0, floor=1e-8)
-    out = {"workload": f"SyntheticWannier N={N}, {nR} R, {n}x{n} k, length gauge, Cash-Karp tol 1e-8, "
-                        f"3.2um sin2 pulse of {args.wannier_cycles:g} cycles in place of the configuration's 10 "
-                        f"(its per-step work over a bounded number of steps; the spectrum is this pulse's)",
-            "k_points": n * n, "output_steps": int(a.inter.shape[0]), "fp64": res["fp64"], "mixed": res["mixed"],
-            "mixed_over_fp64": res["mixed"]["k_steps_per_s"] / res["fp64"]["k_steps_per_s"],
-            "flops_per_rhs": wannier_flops_per_rhs(N, nR), "rhs_per_attempt": 6,
-            "spectral_error": {"max_floor_1e-6": float(e6.max()), "max_floor_1e-8": float(e8.max()),
-                               "vs": "fp64 run"}}
+    # mixed, all seeds in one batch
+    b = ab.Batch(probs["mixed"], precision="mixed", use_graph=True)
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.run(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+    mst = [b.steps(i) for i in range(nseeds)]
+    errs6, errs8 = [], []
+    w0 = cases[0]["laser"]["pulses"][0]["w0"]
+    for i, a in enumerate(fp64_out):
+        o = b.get(i)
+        _, e6, _ = per_harmonic_error({"inter": o.inter, "intra": o.intra}, {"inter": a.inter, "intra": a.intra},
+                                      0.1, w0, floor=1e-6)
+        _, e8, _ = per_harmonic_error({"inter": o.inter, "intra": o.intra}, {"inter": a.inter, "intra": a.intra},
+                                      0.1, w0, floor=1e-8)
+        errs6.append(float(e6.max()))
+        errs8.append(float(e8.max()))
+    launches = b.launches
+    b.close()
+    rhs_flops = wannier_flops_per_rhs(N, nR) * 6 * nk
+    fp64_att = sum(x["attempts"] for x in fp64_st)
+    fp64_tflops = rhs_flops * fp64_att / (sum(fp64_ms) * 1e-3) / 1e12
+    mixed_att = sum(x["attempts"] for x in mst)
+    mixed_tflops = rhs_flops * mixed_att / (batch_ms * 1e-3) / 1e12
+    sph_fp64 = len(fp64_ms) / (sum(fp64_ms) * 1e-3) * 3600.0
+    sph_mixed = nseeds / (batch_ms * 1e-3) * 3600.0
+    scale = Nt / Nt_full   # solves/hour of the 10-cycle pulse: step counts scale with its length
+    out = {"workload": f"SyntheticWannier N={N}, {nR} R, {n}x{n} k, length gauge, Cash-Karp tol 1e-8, 3.2um sin2 "
+                       f"pulse of {args.wannier_cycles:g} cycles ({Nt} output steps) in place of the "
+                       f"configuration's 10 ({Nt_full} steps); {nseeds} seeds",
+           "k_points": nk, "output_steps": Nt, "output_steps_10_cycles": Nt_full,
+           "fp64": {"solves": len(fp64_ms), "ms_per_solve": statistics.mean(fp64_ms),
+                    "k_steps_per_s": nk * sum(x["steps"] for x in fp64_st) / (sum(fp64_ms) * 1e-3),
+                    "steps": fp64_st[0]["steps"], "attempts": fp64_st[0]["attempts"],
+                    "solves_per_hour": sph_fp64, "solves_per_hour_10_cycles": sph_fp64 * scale,
+                    "achieved_tflops": fp64_tflops, "roofline_frac_fp64": fp64_tflops / fp64_tf},
+           "mixed_batch": {"solves": nseeds, "ms": batch_ms, "launches": launches, "graph": True,
+                           "k_steps_per_s": nk * sum(x["steps"] for x in mst) / (batch_ms * 1e-3),
+                           "solves_per_hour": sph_mixed, "solves_per_hour_10_cycles": sph_mixed * scale,
+                           "achieved_tflops": mixed_tflops, "roofline_frac_fp64": mixed_tflops / fp64_tf},
+           "batched_mixed_over_sequential_fp64": sph_mixed / sph_fp64,
+           "flops_per_rhs": wannier_flops_per_rhs(N, nR), "rhs_per_attempt": 6,
+           "spectral_error": {"max_floor_1e-6": max(errs6), "max_floor_1e-8": max(errs8),
+                              "vs": f"fp64 solves of the first {len(fp64_out)} seeds"}}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = wannier_cpu_baseline(args.wannier_cycles, budget_s=args.cpu_seconds / 2)
     return out
@@ -559,12 +617,13 @@ def read_tune_cache():
     return out
 
 
-def read_traffic():
-    """DRAM bytes per propagate launch from the committed ncu summary, if any."""
+def read_traffic(kind: str):
+    """DRAM bytes per propagate launch of the `kind` kernel (fp64 or mixed)
+    from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "propagate_vg_dram_bytes.txt")
     try:
         for line in open(path):
-            if line.startswith("bytes_per_launch_bench_workload"):
+            if line.startswith(f"bytes_per_launch_{kind} "):
                 return float(line.split()[1])
     except OSError:
         pass
@@ -572,21 +631,32 @@ def read_traffic():
 
 
 # ---------------------------------------------------------------- CPU arms
-def cpu_baseline(n: int, Nt: int, budget_s: float = 15.0, samples: int = 1):
+def reference_case(n: int, ncycles: float) -> dict:
+    """The bench workload as the unmodified reference reads it: its cos4
+    envelope, no precision key."""
+    from antelope_b200 import workloads
+
+    case = workloads.haldane_case(n=n, env="cos4", ncycles=ncycles)
+    del case["calc"]["precision"]
+    return case
+
+
+def cpu_baseline(n: int, budget_s: float = 15.0, samples: int = 1, ncycles: float = 8.0):
     """Time the reference on the host cores on a bounded k-slice of the
     n x n workload (each process = one emulated MPI rank of a large rank
-    count; ParaRange, utility.h:104-115, gives it ~budget_s of work)."""
-    from antelope_b200 import cfgtext, workloads
+    count; ParaRange, utility.h:104-115, gives it ~budget_s of work).  Nt is
+    read from the reference's own outlaserdata.dat (rank 0 writes it), so this
+    arm loads nothing of the product."""
+    from antelope_b200 import cfgtext
     from oracle import pyoracle
 
     cores = os.cpu_count() or 1
-    per_kstep = 2.4e-6   # single-core seconds per k.step measured for this path
-    kper = max(4, int(budget_s / (Nt * per_kstep)))
+    per_kstep = 2.4e-6                       # single-core seconds per k.step measured for this path
+    Nt_est = int(35303 * ncycles / 8.0)
+    kper = max(4, int(budget_s / (Nt_est * per_kstep)))
     ntot = n * n
     size = max(cores, ntot // kper)
-    # the unmodified reference has no sin2 envelope: cos4 has the same duration N*T
-    case = workloads.haldane_case(n=n, env="cos4")
-    del case["calc"]["precision"]
+    case = reference_case(n, ncycles)
     if os.path.exists(pyoracle.REF_EXE):
         kind, vals = "reference", []
         for _ in range(samples):
@@ -599,52 +669,50 @@ def cpu_baseline(n: int, Nt: int, budget_s: float = 15.0, samples: int = 1):
                          for r in range(cores)]
                 rc = [p.wait() for p in procs]
                 wall = time.perf_counter() - t0
+                with open(os.path.join(d, "outlaserdata.dat")) as f:
+                    Nt = sum(1 for line in f if line.strip())
             if any(rc):
                 raise RuntimeError(f"reference run failed: {rc}")
             kdone = sum(ntot // size + (1 if ntot % size > r else 0) for r in range(cores))
             vals.append(kdone * Nt / wall)
         sample = (f"{cores} processes x 1 emulated rank of {size} (ParaRange slices of the {n}x{n} grid, "
-                  f"{kdone} k-points) x {Nt} steps, cos4 twin of the sin2 pulse")
+                  f"{kdone} k-points) x {Nt} steps")
     else:
         kind = "port"
         g = max(2, int(np.sqrt(cores * kper)))
-        c2 = workloads.haldane_case(n=g, env="cos4")
+        c2 = reference_case(g, ncycles)
         vals = []
         for _ in range(samples):
             t0 = time.perf_counter()
-            pyoracle.run(c2, nthreads=cores)
+            r = pyoracle.run(c2, nthreads=cores)
             wall = time.perf_counter() - t0
+            Nt = r["dims"]["Nt"]
             vals.append(g * g * Nt / wall)
         sample = f"C oracle on a {g}x{g} grid x {Nt} steps, {cores} threads"
-    return {"value": float(statistics.median(vals)), "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": sample, "solves_per_hour": float(statistics.median(vals)) / (ntot * Nt) * 3600.0}
+    v = float(statistics.median(vals))
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+            "solves_per_hour": v / (ntot * Nt) * 3600.0, "time_steps": Nt}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU code on this host's cores
+    (the unmodified sources built in oracle/_ref), on the same workload and
+    metric as the GPU arm.  Under torchrun only rank 0 runs."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from antelope_b200 import workloads
-
-    Nt = 35302
-    try:
-        import antelope_b200 as ab
-        Nt = ab.Problem.from_dict(workloads.haldane_case(n=args.grid, ncycles=args.ncycles)).dims.Nt
-    except Exception:
-        pass
     for _ in range(args.warmup):
-        cpu_baseline(args.grid, Nt, budget_s=args.ref_seconds)
-    vals = [cpu_baseline(args.grid, Nt, budget_s=args.ref_seconds) for _ in range(args.steps)]
+        cpu_baseline(args.grid, budget_s=args.ref_seconds, ncycles=args.ncycles)
+    vals = [cpu_baseline(args.grid, budget_s=args.ref_seconds, ncycles=args.ncycles) for _ in range(args.steps)]
     v = statistics.median([x["value"] for x in vals])
     cb = dict(vals[-1])
     cb["value"] = v
+    Nt = cb["time_steps"]
     ntot = args.grid * args.grid
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"Haldane {args.grid}x{args.grid} velocity gauge, 3.2um 8-cycle "
-                                   f"(cos4 twin), dt=0.1 ({Nt} steps), RK4, T2=220",
-                       "k_points": ntot, "time_steps": Nt},
+            "config": bench_config(args.grid, Nt, args.ncycles, "cos4"),
             "solves_per_hour": v / (ntot * Nt) * 3600.0,
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -659,6 +727,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--grid", type=int, default=600)
     ap.add_argument("--ncycles", type=float, default=8.0)
+    ap.add_argument("--env", default="cos4", choices=["cos4", "sin2"],
+                    help="pulse envelope; cos4 is the twin the unmodified reference can run (same duration)")
     ap.add_argument("--tile-k", dest="tile_k", type=int, default=0)
     ap.add_argument("--kpt", type=int, default=0)
     ap.add_argument("--steps-per-launch", dest="steps_per_launch", type=int, default=0)
@@ -666,11 +736,13 @@ def main():
     ap.add_argument("--ref-seconds", dest="ref_seconds", type=float, default=6.0)
     ap.add_argument("--no-cpu-baseline", dest="no_cpu_baseline", action="store_true")
     ap.add_argument("--scan-solves", dest="scan_solves", type=int, default=256)
-    ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=600)
+    ap.add_argument("--serve-requests", dest="serve_requests", type=int, default=2000)
     ap.add_argument("--serve-rate", dest="serve_rate", type=float, default=40.0)
     ap.add_argument("--lw-grid", dest="lw_grid", type=int, default=600)
     ap.add_argument("--wannier-grid", dest="wannier_grid", type=int, default=300)
-    ap.add_argument("--wannier-cycles", dest="wannier_cycles", type=float, default=0.5)
+    ap.add_argument("--wannier-cycles", dest="wannier_cycles", type=float, default=0.25)
+    ap.add_argument("--wannier-seeds", dest="wannier_seeds", type=int, default=16)
+    ap.add_argument("--wannier-fp64-seeds", dest="wannier_fp64_seeds", type=int, default=2)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

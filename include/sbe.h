@@ -194,11 +194,21 @@ sbe_status sbe_write_outputs(const sbe_problem *p, const sbe_outputs *o, const c
 sbe_status sbe_run_cfg(const char *cfg_path, const char *out_dir, const sbe_opts *opts);
 
 /* Many solves with their own grids, pulses and model parameters advanced
- * together (one launch per launch class per step chunk).  The problems must
+ * together: the reference runs one such parameter point per job
+ * (src/_SH/SLURM/loop__run__jobs__mt2.sh).  Two-band Haldane problems share
+ * one launch per launch class per step chunk; N-band table and continuum
+ * models (the SyntheticWannier group, the analytic materials, MultiWSM) share
+ * one attempt launch over all their k-points and one control launch per
+ * iteration, each solve keeping its own step-size controller (Cash-Karp or
+ * fixed step), so every result equals its solve run alone bit for bit.
+ * opts.use_graph captures the launches as CUDA graphs.  The problems must
  * stay alive until sbe_batch_destroy. */
 sbe_status sbe_batch_create(const sbe_problem *const *problems, int n, const sbe_opts *opts, sbe_batch **out);
 sbe_status sbe_batch_run(sbe_batch *b, void *stream);
 sbe_status sbe_batch_get(sbe_batch *b, int index, const sbe_outputs *out);
+/* Time-stepping statistics of solve `index` of a finished batch (as
+ * sbe_solver_steps). */
+sbe_status sbe_batch_steps(sbe_batch *b, int index, long long *steps, long long *attempts, long long *rejects);
 int sbe_batch_launches(const sbe_batch *b);
 /* Density snapshots of solve `index` of a finished batch (as sbe_solver_snapshots). */
 sbe_status sbe_batch_snapshots(sbe_batch *b, int index, double *occ1d, double *nc, double *pi);

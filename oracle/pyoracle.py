@@ -21,6 +21,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle_sbe.so")
 REF_EXE = os.path.join(HERE, "_ref", "exec_hhg_ref")
+# the reference build with the harness additions of make_harness.py (the sin2
+# envelope and the SyntheticWannier material with dipoles)
+HARNESS_EXE = os.path.join(HERE, "_ref", "exec_hhg_harness")
 
 ENV = {"gauss": 0, "gauss_clipped": 1, "cos4": 2, "cos4_clipped": 3, "sin2": 4}
 GAUGE = {"Wannier": 0, "LengthWannier": 0, "Hamiltonian": 1, "LengthHamiltonian": 1,
@@ -80,6 +83,7 @@ def lib():
         _lib.orc_kgrid.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p]
         _lib.orc_model_hj.argtypes = [C.POINTER(OrcProblem), C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_eigh.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_tableau.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     return _lib
 
 
@@ -276,22 +280,52 @@ def eigh(a):
     return w, v
 
 
-def run_reference(case: dict, workdir: str, env: dict | None = None, timeout: float = 3600):
-    """Run the unmodified reference build (oracle/_ref) on a case in
-    ``workdir``; returns the parsed output files."""
+def tableau(rk: int):
+    """(c, a, b, bstar) of the oracle's integrator for rk = 4, 5 or 45."""
+    c, b, bs = np.zeros(7), np.zeros(7), np.zeros(7)
+    a = np.zeros((7, 7))
+    s = lib().orc_tableau(int(rk), _ptr(c), _ptr(a), _ptr(b), _ptr(bs))
+    if s < 0:
+        raise ValueError(f"no tableau for rk={rk}")
+    return c[:s], a[:s, :s], b[:s], bs[:s]
+
+
+def run_reference(case: dict, workdir: str, env: dict | None = None, timeout: float = 3600,
+                  harness: bool = False, read: bool = True):
+    """Run the unmodified reference build (oracle/_ref/exec_hhg_ref) -- or,
+    with ``harness``, the harness build with the sin2 envelope and the
+    SyntheticWannier material -- on a case in ``workdir``; returns the parsed
+    output files (``read``)."""
     from antelope_b200 import cfgtext
 
-    if not os.path.exists(REF_EXE):
-        raise FileNotFoundError("oracle/_ref/exec_hhg_ref not built (needs the reference sources)")
+    exe = HARNESS_EXE if harness else REF_EXE
+    if not os.path.exists(exe):
+        raise FileNotFoundError(f"{exe} not built (needs the reference sources)")
     os.makedirs(workdir, exist_ok=True)
     with open(os.path.join(workdir, "inputParam.cfg"), "w") as f:
         f.write(cfgtext.dumps(case))
     e = dict(os.environ)
     if env:
         e.update(env)
-    subprocess.run([REF_EXE], cwd=workdir, env=e, check=True, timeout=timeout,
+    subprocess.run([exe], cwd=workdir, env=e, check=True, timeout=timeout,
                    stdout=subprocess.DEVNULL)
-    return read_outputs(workdir)
+    return read_outputs(workdir) if read else None
+
+
+def read_reduce_dumps(prefix: str, Nt: int, N: int) -> dict:
+    """The partial k-sums one emulated rank dumped at the reference's final
+    reduce (REF_DUMP, oracle/refshim/mpi.h; antelope.cpp:482-512): inter and
+    intra [Nt, 3] (weighted, before the factor dV) and the weighted density
+    matrix ``dmi`` [Nt, N, N].  Snapshot reduces, if any, come first."""
+    import glob
+
+    files = sorted(glob.glob(prefix + ".*.bin"), key=lambda f: int(f.rsplit(".", 2)[1]))
+    tail = files[-7:]
+    arr = [np.fromfile(f, dtype=np.complex128) for f in tail]
+    inter = np.stack([arr[0], arr[2], arr[4]], axis=1).real
+    intra = np.stack([arr[1], arr[3], arr[5]], axis=1).real
+    dmi = arr[6].reshape(Nt, N, N)
+    return {"inter": inter, "intra": intra, "dmi": dmi}
 
 
 def read_outputs(workdir: str) -> dict:

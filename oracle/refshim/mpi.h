@@ -11,10 +11,20 @@
  *  - Reductions and gathers are no-ops: in the reference every one of them is
  *    either in place on the master (antelope.cpp:366,435,487,496,506) or feeds
  *    only stdout, so a single rank already holds the full result.
+ *  - With REF_DUMP set to a path prefix, every MPI_Reduce also writes the
+ *    calling rank's buffer (the receive buffer for MPI_IN_PLACE) as raw bytes
+ *    to <prefix>.<call number>.bin, call numbers counting from 0 in call
+ *    order.  At the final reduce (antelope.cpp:482-512) these are the rank's
+ *    partial k-sums -- inter and intra current per axis (Nt complex each, in
+ *    the order x inter, x intra, y inter, ...), then the weighted density
+ *    matrix (Nt x N^2 complex) -- so the k-slice that ParaRange gives one
+ *    emulated rank can be compared with another implementation's slice, and
+ *    the slices of all ranks summed in rank order give the whole grid.
  */
 #ifndef ORACLE_REFSHIM_MPI_H
 #define ORACLE_REFSHIM_MPI_H
 
+#include <stdio.h>
 #include <stdlib.h>
 
 typedef int MPI_Comm;
@@ -52,8 +62,22 @@ static inline int MPI_Op_create(MPI_User_function *, int, MPI_Op *op)
     *op = 0;
     return MPI_SUCCESS;
 }
-static inline int MPI_Reduce(const void *, void *, int, MPI_Datatype, MPI_Op, int, MPI_Comm)
+static inline int MPI_Reduce(const void *send, void *recv, int count, MPI_Datatype type, MPI_Op, int, MPI_Comm)
 {
+    static int calls = 0;
+    const char *prefix = getenv("REF_DUMP");
+    const int call = calls++;
+    if (!prefix) return MPI_SUCCESS;
+    const void *buf = send == MPI_IN_PLACE ? recv : send;
+    const size_t elem = type == MPI_DOUBLE_COMPLEX ? 16 : 8;
+    char path[4096];
+    snprintf(path, sizeof(path), "%s.%d.bin", prefix, call);
+    FILE *f = fopen(path, "wb");
+    if (!f || fwrite(buf, elem, (size_t)count, f) != (size_t)count) {
+        fprintf(stderr, "refshim: cannot write %s\n", path);
+        exit(EXIT_FAILURE);
+    }
+    fclose(f);
     return MPI_SUCCESS;
 }
 static inline int MPI_Gatherv(const void *, int, MPI_Datatype, void *, const int *, const int *,

@@ -1072,3 +1072,16 @@ int orc_eigh(int n, const double *a, double *w, double *v)
     for (int i = 0; i < n * n; ++i) { v[2 * i] = creal(U[i]); v[2 * i + 1] = cimag(U[i]); }
     return 0;
 }
+
+int orc_tableau(int rk, double *c, double *a, double *b, double *bstar)
+{
+    tableau_t T;
+    if (tableau_build(&T, rk)) return -1;
+    for (int i = 0; i < 7; ++i) {
+        c[i] = T.c[i];
+        b[i] = T.b[i];
+        bstar[i] = T.bstar[i];
+        for (int j = 0; j < 7; ++j) a[i * 7 + j] = T.a[i][j];
+    }
+    return T.stages;
+}

@@ -113,6 +113,11 @@ void orc_laser_eval(const orc_problem *p, double t, double *A3, double *E3);
 int orc_kgrid(const orc_problem *p, double *k3, double *w);
 int orc_model_hj(const orc_problem *p, const double *k3, double *H, double *J3);
 int orc_eigh(int n, const double *a, double *w, double *v);
+/* The Butcher tableau the propagator uses for `rk` (ORC_RK4, ORC_RK5_FEHLBERG,
+ * ORC_RK45_CASHKARP): c[7], a[7*7] (row-major), b[7] (the weights that
+ * advance the state) and bstar[7] (the embedded weights; zeros when the method
+ * has none).  Returns the number of stages, or -1 for an unknown rk. */
+int orc_tableau(int rk, double *c, double *a, double *b, double *bstar);
 
 #ifdef __cplusplus
 }

@@ -158,3 +158,41 @@ SNAPSHOT_CASES = {
 
 # A one-cycle case whose output files are kept verbatim (byte format pin).
 TEXT_CASE = variant(pulse__ncycles=1.0, pulse__w0=0.114, calc__Npoints=[5, 6])
+
+# Cases the harness build of the reference runs (oracle/make_harness.py: its
+# SBEs.h and laser.h with the sin2 envelope and the SyntheticWannier material
+# of oracle/refharness/SyntheticWannier.h, which has dipole matrices).  They pin
+# what the unmodified reference cannot run: the sin2 pulse of the
+# configurations, the length gauge's E(t).D(k+A) term (SBEs.h:771-782) and the
+# current operator -dH/dk + i[D, H] (BaseMaterial.h:62-68) of an N-band model.
+def synthetic(gauge, rk=4, seed=4, nband=6, nval=3, npoints=(5, 4), w0=0.057, dipoles=True, **kw):
+    from antelope_b200 import wannier
+
+    c = variant(top__gauge=gauge, calc__Npoints=list(npoints), calc__RKorder=rk, pulse__w0=w0,
+                pulse__ncycles=0.5, pulse__env_name="sin2", **kw)
+    del c["Haldane"]
+    c["target"] = "SyntheticWannier"
+    g = wannier.generate(seed, nband=nband, nval=nval)
+    if not dipoles:
+        del g["d_re"], g["d_im"]
+    c["SyntheticWannier"] = g
+    return c
+
+
+HARNESS_CASES = {
+    "sin2_vg_rk4": variant(pulse__env_name="sin2"),
+    "sin2_lw_rk5_elliptic": variant(top__gauge="Wannier", pulse__env_name="sin2", calc__RKorder=5,
+                                    pulse__ellip=0.3, pulse__cep=25.0),
+    "synw6_w_rk4": synthetic("Wannier", 4),
+    "synw6_w_rk5": synthetic("Wannier", 5),
+    "synw6_v_rk4": synthetic("Velocity", 4),
+    "synw6_v_rk5": synthetic("Velocity", 5),
+    "synw6_w_rk4_no_dipoles": synthetic("Wannier", 4, dipoles=False),
+    "synw4_w_t1_elliptic": synthetic("Wannier", 4, seed=9, nband=4, nval=2, npoints=(6, 5),
+                                     calc__T1=300.0, pulse__ellip=0.5, pulse__phix=20.0),
+}
+# The N = 6 length-gauge case with the reference's fixed-step Fehlberg-5 at
+# dt = 0.025: a fine solution of the same equations by the reference's own
+# integrator, against which the adaptive Cash-Karp extension (no counterpart
+# in the reference) is shown to converge.
+HARNESS_CASES["synw6_w_rk5_fine"] = synthetic("Wannier", 5, calc__dt=0.025)

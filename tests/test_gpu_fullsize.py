@@ -1,0 +1,78 @@
+"""Parity at the configurations' own size (golden fixtures full_*.npz made by
+tests/golden/make_golden_full.py from the reference itself): the Haldane model
+on 150 x 150 k-points with the 3.2 um 8-cycle pulse over all 35 303 steps of
+dt = 0.1, RK4, T2 = 220 -- velocity and length gauge with the cos4 envelope
+(the unmodified reference) and velocity gauge with the configuration's sin2
+envelope (the harness build) -- and two ParaRange blocks of the 600 x 600
+grid (rank 0 and rank 117 of 160 emulated MPI ranks, 2 250 k-points each)
+against the reference's partial sums of the same blocks at its final reduce.
+FP64 bar: 1e-10 of max_t |J| per current series, occupations 1e-12, so
+rounding that builds up over the 35k steps would show."""
+import os
+
+import numpy as np
+import pytest
+
+import antelope_b200 as ab
+from antelope_b200 import workloads
+from antelope_b200.api import Solver
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+FP64_TOL = 1e-10
+
+
+def case(n, gauge, env):
+    c = workloads.haldane_case(n=n, env=env, gauge=gauge)
+    del c["calc"]["precision"]
+    return c
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("name,gauge,env", [("c1_vg_cos4", "Velocity", "cos4"), ("c1_lw_cos4", "Wannier", "cos4"),
+                                            ("c1_vg_sin2", "Velocity", "sin2")])
+def test_full_configuration_fp64_matches_reference(name, gauge, env):
+    ref = np.load(os.path.join(GOLDEN, f"full_{name}.npz"))
+    out = ab.solve(case(150, gauge, env), precision="fp64")
+    assert out.inter.shape[0] == int(ref["Nt"]) == 35303
+    for key in ("inter", "intra"):
+        for a in range(2):
+            assert rel(getattr(out, key)[:, a], ref[key][:, a]) < FP64_TOL, (key, a)
+        assert np.all(getattr(out, key)[:, 2] == 0)
+    assert np.abs(out.occ - ref["occ_file"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("rank", [0, 117])
+def test_c2_block_matches_reference_rank(rank):
+    """The k-slice solver on the block ParaRange gives one MPI rank
+    (utility.h:104-115) against that rank's partial sums in the reference:
+    Sum_k w_k J(k, t_n) before the factor dV, and Sum_k w_k rho(k, t_n)."""
+    ref = np.load(os.path.join(GOLDEN, f"full_c2_slice_{rank}.npz"))
+    c = case(600, "Velocity", "cos4")
+    p = ab.Problem.from_dict(c)
+    kb, ke = int(ref["k_begin"]), int(ref["k_end"])
+    s = Solver(p, k_slice=(kb, ke), precision="fp64")
+    s.run()
+    sums = s.sums()
+    s.close()
+    Nt = p.dims.Nt
+    j, cp = sums[:Nt], sums[Nt]
+    # the velocity gauge's intraband current carries + Nval A(t) per k-point
+    # (SBEs.h:750-757), added once for the slice's total weight
+    from oracle import pyoracle
+
+    _, w = pyoracle.kgrid(c)
+    wslice = w[kb:ke].sum()
+    A = p.laser()[:, 4:6]
+    inter = j[:, 0:2]
+    intra = j[:, 2:4] + cp[2:4] + p.dims.nval * A * wslice
+    for a in range(2):
+        assert rel(inter[:, a], ref["inter"][:, a]) < FP64_TOL, ("inter", a)
+        assert rel(intra[:, a], ref["intra"][:, a]) < FP64_TOL, ("intra", a)
+    assert np.abs(j[:, 4] + cp[4] - ref["rho00"]).max() < 1e-12 * wslice
+    assert np.abs(j[:, 5] + cp[5] - ref["rho11"]).max() < 1e-12 * wslice
+    rho01 = (j[:, 6] + cp[6]) + 1j * (j[:, 7] + cp[7])
+    assert np.abs(rho01 - ref["rho01"]).max() < 1e-12 * wslice

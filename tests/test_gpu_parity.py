@@ -188,6 +188,31 @@ def test_server_cancel_and_single_delivery():
     srv.close()
 
 
+def test_server_refuses_a_request_beyond_its_memory_budget():
+    """Admission by device memory with a fixed budget (sbe_server_opts.
+    mem_budget_bytes): a request that can never fit fails alone -- SBE_OOM with
+    its own message -- while the requests around it, admitted as memory frees
+    up, complete with the same bits as alone; failures do not leak into the
+    rest of the stream."""
+    shape = dict(tile_k=64, k_per_thread=1)
+    small = [ab.Problem.from_dict(variant(calc__Npoints=[12 + i, 9], pulse__cep=15.0 * i)) for i in range(8)]
+    big = ab.Problem.from_dict(variant(calc__Npoints=[400, 400]))
+    srv = ab.Server(precision="fp64", steps_per_launch=64, mem_budget_bytes=2.0e6, **shape)
+    ids = [srv.submit(p) for p in small[:4]]
+    big_id = srv.submit(big)
+    ids += [srv.submit(p) for p in small[4:]]
+    with pytest.raises(ab.SbeError) as e:
+        srv.wait(big_id, timeout=120)
+    assert e.value.name == "SBE_OOM" and "admission refused" in str(e.value)
+    for p, rid in zip(small, ids):
+        o, _ = srv.wait(rid, timeout=120)
+        ref = ab.solve(p, precision="fp64", steps_per_launch=64, **shape)
+        assert np.array_equal(o.inter, ref.inter) and np.array_equal(o.occ, ref.occ)
+    st = srv.stats()
+    assert st["failed"] == 1 and st["completed"] == len(small) and st["resident"] == 0
+    srv.close()
+
+
 def test_many_pulses_device_table_matches_host_table():
     """Ten pulses of every envelope kind: the field table the solver builds
     on the device agrees with the host-built one of sbe_solve_noalloc to the

@@ -111,3 +111,75 @@ def test_step_statistics():
     ref = pyoracle.run(c)
     assert st["steps"] == ref["steps"]
     assert st["attempts"] == st["steps"] + st["rejects"]
+
+
+def _same(a, b):
+    return all(np.array_equal(getattr(a, k), getattr(b, k)) for k in ("inter", "intra", "occ", "coh"))
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_of_nband_solves_equals_single_solves_bitwise(graph):
+    """N-band solves with their own models, grids, gauges and step rules
+    advanced together (one attempt launch over all their tiles and one
+    control launch per iteration, sbe_batch_*): each solve keeps its own
+    controller, so results and step counts equal the solves run alone."""
+    from cases import MATERIAL_CASES
+
+    cases = [small_case("cashkarp45", tol=1e-9, seed=4),
+             small_case("cashkarp45", tol=1e-12, n=(5, 7), seed=6),
+             small_case(None, n=(7, 4), seed=8, T1=300.0),
+             MATERIAL_CASES["kanemele_w"]]
+    cases[2]["calc"].pop("rk", None)
+    v = small_case("cashkarp45", n=(4, 6), seed=5)
+    v["gauge"] = "Velocity"
+    cases.append(v)
+    probs = [ab.Problem.from_dict(c) for c in cases]
+    alone, steps = [], []
+    for p in probs:
+        s = ab.api.Solver(p, precision="fp64")
+        s.run()
+        alone.append(s.get())
+        steps.append(s.steps())
+        s.close()
+    b = ab.Batch(probs, precision="fp64", use_graph=graph)
+    b.run()
+    for i in range(len(probs)):
+        assert _same(b.get(i), alone[i]), i
+        assert b.steps(i) == steps[i], i
+    assert b.launches > 0
+    b.close()
+
+
+def test_batch_mixes_haldane_and_nband_solves():
+    """A batch holding two-band Haldane problems (closed-form kernels) and
+    N-band problems (table kernels) runs both kinds; each equals its solve
+    alone."""
+    from cases import variant
+
+    probs = [ab.Problem.from_dict(variant(calc__Npoints=[9, 7])), ab.Problem.from_dict(small_case("rk5")),
+             ab.Problem.from_dict(variant(top__gauge="Wannier", calc__Npoints=[6, 8]))]
+    alone = [ab.solve(p, precision="fp64") for p in probs]
+    b = ab.Batch(probs, precision="fp64")
+    b.run()
+    for i, a in enumerate(alone):
+        assert _same(b.get(i), a), i
+    b.close()
+
+
+def test_batch_nband_mixed_precision_and_snapshots():
+    """Mixed-precision N-band solves in a batch equal their mixed solves alone,
+    and batch snapshots equal the single solve's."""
+    c = small_case("cashkarp45", tol=1e-8)
+    c["calc"]["shotNumber"] = 2
+    probs = [ab.Problem.from_dict(c), ab.Problem.from_dict(small_case("cashkarp45", seed=7, n=(5, 5)))]
+    s = ab.api.Solver(probs[0], precision="mixed")
+    s.run()
+    a, shots = s.get(), s.snapshots()
+    s.close()
+    b = ab.Batch(probs, precision="mixed", use_graph=True)
+    b.run()
+    assert _same(b.get(0), a)
+    got = b.snapshots(0)
+    for key in ("occ1d", "nc", "pi"):
+        assert np.array_equal(got[key], shots[key]), key
+    b.close()
