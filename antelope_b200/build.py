@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2,-Wall"]
 SOURCES = ["sbe_kernels.cu", "sbe_problem.cpp", "sbe_engine.cpp", "sbe_capi.cpp", "sbe_noalloc.cu", "sbe_tune.cpp", "sbe_wannier.cu", "sbe_wansolve.cpp", "sbe_materials.cpp", "sbe_spectrum.cu"]
-HEADERS = ["sbe_dev.h", "sbe_kernels.h", "sbe_problem.h", "sbe_engine.h", "sbe_handles.h", "sbe_wannier.h", "sbe_wansolve.h", "sbe_spectrum.h"]
+HEADERS = ["sbe_dev.h", "sbe_kernels.h", "sbe_problem.h", "sbe_engine.h", "sbe_handles.h", "sbe_wannier.h", "sbe_wansolve.h", "sbe_spectrum.h", "sbe_wangroup.cuh"]
 
 
 def _newer(target, deps):

@@ -1,0 +1,685 @@
+// Grouped attempt kernel of the N-band length gauge (included by
+// sbe_wannier.cu inside its anonymous namespace; uses its helpers).
+//
+// The same step as wan_attempt -- SBEs::GenDifferentialDM (SBEs.h:762-872)
+// with the Wannier model form (Materials/Wannier90.h:297-387), the currents
+// of SBEs::GenInterIntraCurrent (SBEs.h:694-760), Jacobi tracking of the
+// eigenbasis and the eigenbasis dephasing -- laid out for throughput:
+//
+//  - eight lanes per k-point, four k-points per warp (one warp is one tile of
+//    WAN_WARPS k-points, so the controller's tile reduction is unchanged);
+//    the four groups of a warp run in lockstep, so every Fourier-table load is
+//    one 128-byte row shared by the four k-points;
+//  - the tables are re-laid per lane ([R][j][q][lane], built on the host,
+//    WanDev::gtab): lane l of a group owns the upper elements u = l + 8j and
+//    computes H0, D_x, D_y (and, for the currents, S_a = sum R_a h_R e^{iKR})
+//    for exactly those, so the right-hand side and the current traces of an
+//    owned element need no other lane's Fourier sums;
+//  - Hermitian matrices (Y, H0, H0 + E.D, B = U^dag H0 U) are stored as packed
+//    upper triangles, the unitary U and one scratch matrix in full: ~4 KB of
+//    shared memory per k-point instead of ~9 KB, so more k-points stay
+//    resident and the tables stay in L1;
+//  - the stage slopes live in registers and the stage loop is unrolled for the
+//    compile-time tableau, so only the slopes still needed are live.
+//
+// The intraband current uses (U^dag J_a U)_nn = (U^dag (-i S_a) U)_nn: the
+// i[D_a, H0] part of the current operator has zero diagonal in the eigenbasis
+// of H0 (eps_n D_nn - D_nn eps_n), which the reference evaluates to rounding.
+// Used for the tables of the SyntheticWannier group (current operator
+// -dH/dk + i[D, H], BaseMaterial.h:62-68) at N = 4 and 6; other models and
+// band counts run on wan_attempt.
+
+constexpr int WG = 8;          // lanes per k-point
+constexpr int WG_WARPS = 4;    // warps per block (tiles per block)
+constexpr unsigned WG_FULL = 0xffffffffu;
+static_assert(32 / WG == WAN_WARPS, "a warp of the grouped kernel is one tile");
+static_assert(WG_WARPS == WAN_GROUP_TILES, "a block of the grouped kernel covers WAN_GROUP_TILES tiles");
+
+__host__ __device__ constexpr int pidx(int m, int n, int N) { return m * N - m * (m - 1) / 2 + (n - m); }
+
+template <int N> struct GDim {
+    static constexpr int NN = N * N, NU = N * (N + 1) / 2;
+    static constexpr int NO = (NU + WG - 1) / WG;   // owned upper elements per lane
+    static constexpr int NF = (NN + WG - 1) / WG;   // full-matrix elements per lane
+    static constexpr int NJ = (NU + NN + WG - 1) / WG;   // Jacobi tasks per lane
+    static constexpr int P = N + (N & 1);           // indices of the round-robin schedule
+};
+
+// Hermitian element (a, b) of a packed upper triangle
+template <int N> __device__ __forceinline__ double2 herm(const double2 *Pk, int a, int b)
+{
+    return a <= b ? Pk[pidx(a, b, N)] : cconj(Pk[pidx(b, a, N)]);
+}
+// anti-Hermitian element (a, b) of a packed upper triangle
+template <int N> __device__ __forceinline__ double2 aherm(const double2 *Pk, int a, int b)
+{
+    if (a <= b) return Pk[pidx(a, b, N)];
+    const double2 v = Pk[pidx(b, a, N)];
+    return make_double2(-v.x, v.y);
+}
+
+__device__ __forceinline__ double grp_sum(double v)
+{
+    v += __shfl_xor_sync(WG_FULL, v, 1);
+    v += __shfl_xor_sync(WG_FULL, v, 2);
+    v += __shfl_xor_sync(WG_FULL, v, 4);
+    return v;
+}
+__device__ __forceinline__ double grp_max(double v)
+{
+    v = fmax(v, __shfl_xor_sync(WG_FULL, v, 1));
+    v = fmax(v, __shfl_xor_sync(WG_FULL, v, 2));
+    v = fmax(v, __shfl_xor_sync(WG_FULL, v, 4));
+    return v;
+}
+
+// Shared memory: block head, stage phase factors e^{iA(t_s)R} and lattice
+// vectors, then one region per k-point.
+struct GHead {
+    double AE[6][6];
+    double part[WG_WARPS][WAN_WARPS][WAN_NSLOT];
+    double errw[WG_WARPS];
+    WTab tab;
+    unsigned char ut[WAN_MAXU_][2];
+    signed char mate[WAN_MAXN - 1][WAN_MAXN];
+};
+struct GSmem {
+    size_t cA, Rc, k0, kbytes, total;
+    // offsets inside a k-point region
+    size_t Y, H0, HT, B, U, Tm, pk, ph, jc, js, je, dv;
+};
+__host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
+{
+    GSmem L;
+    const size_t NU = (size_t)N * (N + 1) / 2, NN = (size_t)N * N, tf = 2 * (size_t)rf_bytes;
+    L.cA = al16(sizeof(GHead));
+    L.Rc = L.cA + al16(6 * (size_t)nR * tf);
+    L.k0 = L.Rc + al16((size_t)nR * 2 * rf_bytes);
+    size_t o = 0;
+    L.Y = o;  o += al16(NU * 16);
+    L.H0 = o; o += al16(NU * 16);
+    L.HT = o; o += al16(NU * 16);
+    L.B = o;  o += al16(NU * 16);
+    L.U = o;  o += al16(NN * 16);
+    L.Tm = o; o += al16(NN * 16);
+    L.pk = o; o += al16((size_t)nR * tf);
+    L.ph = o; o += al16(std::max((size_t)nR * tf, NU * 16));   // also S_x (packed) at current steps
+    L.jc = o; o += al16((size_t)N * 8);
+    L.js = o; o += al16((size_t)N * 8);
+    L.je = o; o += al16((size_t)N * 16);
+    L.dv = o; o += al16((size_t)N * 16);
+    L.kbytes = o;
+    L.total = L.k0 + (size_t)WG_WARPS * WAN_WARPS * L.kbytes;
+    return L;
+}
+
+template <class RF> struct GView {
+    using TF = typename Cx<RF>::T;
+    double2 *Y, *H0, *HT, *B, *U, *Tm, *je, *dv;
+    double *jc, *js;
+    TF *pk, *ph;
+    __device__ GView(unsigned char *b, const GSmem &L)
+    {
+        Y = reinterpret_cast<double2 *>(b + L.Y);
+        H0 = reinterpret_cast<double2 *>(b + L.H0);
+        HT = reinterpret_cast<double2 *>(b + L.HT);
+        B = reinterpret_cast<double2 *>(b + L.B);
+        U = reinterpret_cast<double2 *>(b + L.U);
+        Tm = reinterpret_cast<double2 *>(b + L.Tm);
+        pk = reinterpret_cast<TF *>(b + L.pk);
+        ph = reinterpret_cast<TF *>(b + L.ph);
+        jc = reinterpret_cast<double *>(b + L.jc);
+        js = reinterpret_cast<double *>(b + L.js);
+        je = reinterpret_cast<double2 *>(b + L.je);
+        dv = reinterpret_cast<double2 *>(b + L.dv);
+    }
+};
+
+// Column j of a Jacobi round's rotation: J_jj and J_{mj,j} (as jcol)
+template <class RF>
+__device__ __forceinline__ void g_jcol(const GView<RF> &w, const signed char *mt, int j, int N, double2 &Jjj,
+                                       double2 &Jmj, int &mj)
+{
+    mj = mt[j];
+    if (mj >= N) {
+        Jjj = make_double2(1, 0);
+        Jmj = make_double2(0, 0);
+        mj = j;
+        return;
+    }
+    const int p = min(j, mj);
+    const double c = w.jc[p], s = w.js[p];
+    const double2 e = w.je[p];
+    if (j == p) {
+        Jjj = make_double2(c, 0);
+        Jmj = make_double2(-s * e.x, s * e.y);
+    } else {
+        Jjj = make_double2(c * e.x, -c * e.y);
+        Jmj = make_double2(s, 0);
+    }
+}
+
+// One parallel Jacobi round on (B packed, U) of the group's k-point; `act`:
+// this group still rotates (group-uniform).  All lanes of the warp call it.
+template <class RF, int N>
+__device__ __forceinline__ void g_round(const GView<RF> &w, const GHead &gh, int r, int gl, bool act)
+{
+    using D = GDim<N>;
+    const signed char *mt = gh.mate[r];
+    if (act && gl < N) {
+        const int q = mt[gl];
+        if (q < N && gl < q) {
+            const int p = gl;
+            const double2 g = w.B[pidx(p, q, N)];
+            const double r2 = g.x * g.x + g.y * g.y;
+            double c = 1, s = 0;
+            double2 e = make_double2(1, 0);
+            if (r2 > 0.0) {
+                const double d = w.B[pidx(q, q, N)].x - w.B[pidx(p, p, N)].x;
+                const double ir = rsqrt(r2);
+                const double hh = sqrt(fma(d, d, 4.0 * r2));
+                const double t = copysign(2.0 * r2 * ir, d) / (fabs(d) + hh);
+                c = rsqrt(fma(t, t, 1.0));
+                s = t * c;
+                e.x = g.x * ir;
+                e.y = g.y * ir;
+            }
+            w.jc[p] = c;
+            w.js[p] = s;
+            w.je[p] = e;
+        }
+    }
+    __syncwarp();
+    double2 out[D::NJ];
+#pragma unroll
+    for (int x = 0; x < D::NJ; ++x) {
+        const int t = gl + WG * x;
+        out[x] = make_double2(0, 0);
+        if (!act || t >= D::NU + D::NN) continue;
+        int i, j;
+        if (t < D::NU) {
+            i = gh.ut[t][0];
+            j = gh.ut[t][1];
+        } else {
+            i = -1 - (t - D::NU) / N;
+            j = (t - D::NU) % N;
+        }
+        double2 Jjj, Jmj;
+        int mj;
+        g_jcol<RF>(w, mt, j, N, Jjj, Jmj, mj);
+        if (i >= 0) {   // B'_ij = sum_ab conj(J_ai) B_ab J_bj
+            double2 Jii, Jmi;
+            int mi;
+            g_jcol<RF>(w, mt, i, N, Jii, Jmi, mi);
+            double2 t1 = cmul(herm<N>(w.B, i, j), Jjj), t2 = cmul(herm<N>(w.B, mi, j), Jjj);
+            cfma(t1, herm<N>(w.B, i, mj), Jmj);
+            cfma(t2, herm<N>(w.B, mi, mj), Jmj);
+            double2 o = make_double2(0, 0);
+            cfmac(o, Jii, t1);
+            cfmac(o, Jmi, t2);
+            out[x] = o;
+        } else {        // U'_ij = U_ij J_jj + U_i,mj J_mj,j
+            const int row = -1 - i;
+            double2 o = cmul(w.U[row * N + j], Jjj);
+            cfma(o, w.U[row * N + mj], Jmj);
+            out[x] = o;
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int x = 0; x < D::NJ; ++x) {
+        const int t = gl + WG * x;
+        if (!act || t >= D::NU + D::NN) continue;
+        if (t < D::NU) {
+            const int i = gh.ut[t][0], j = gh.ut[t][1];
+            w.B[t] = i == j ? make_double2(out[x].x, 0.0) : out[x];
+        } else {
+            w.U[t - D::NU] = out[x];
+        }
+    }
+    __syncwarp();
+}
+
+// Eigenbasis tracking of the group's k-point (as jacobi_track): sweeps until
+// |offdiag|^2 <= tol2 |diag|^2; once |offdiag|^2 <= 1e-10 |diag|^2 a
+// first-order step U (I + X), X_mn = B_mn / (B_nn - B_mm), finishes when
+// max |X| <= xmax.  Warp-uniform loop; groups that are done idle.
+template <class RF, int N>
+__device__ __forceinline__ void g_track(const GView<RF> &w, const GHead &gh, int gl, int max_sweeps, double tol2,
+                                        double xmax, bool live)
+{
+    using D = GDim<N>;
+    bool need = live;
+    for (int sw = 0; sw < max_sweeps; ++sw) {
+        double off = 0.0, dia = 0.0;
+        for (int u = gl; u < D::NU; u += WG) {
+            const double2 b = w.B[u];
+            const double v = b.x * b.x + b.y * b.y;
+            if (gh.ut[u][0] == gh.ut[u][1]) dia += v;
+            else off += 2.0 * v;
+        }
+        off = grp_sum(off);
+        dia = grp_sum(dia);
+        need = need && !(off <= tol2 * dia);
+        const bool try_fo = need && off <= 1e-10 * dia;
+        if (__any_sync(WG_FULL, try_fo)) {
+            // X (anti-Hermitian, full) into Tm with unit diagonal; fail flag per group
+            double fail = 0.0;
+            if (try_fo) {
+                for (int u = gl; u < D::NU; u += WG) {
+                    const int m = gh.ut[u][0], n = gh.ut[u][1];
+                    if (m == n) {
+                        w.Tm[m * N + m] = make_double2(1.0, 0.0);
+                        continue;
+                    }
+                    const double d = w.B[pidx(n, n, N)].x - w.B[pidx(m, m, N)].x;
+                    const double2 b = w.B[u];
+                    const double bb = sqrt(b.x * b.x + b.y * b.y);
+                    if (bb == 0.0) {
+                        w.Tm[m * N + n] = make_double2(0, 0);
+                        w.Tm[n * N + m] = make_double2(0, 0);
+                        continue;
+                    }
+                    if (!(bb <= xmax * fabs(d))) {
+                        fail = 1.0;
+                        continue;
+                    }
+                    const double2 x = make_double2(b.x / d, b.y / d);
+                    w.Tm[m * N + n] = x;
+                    w.Tm[n * N + m] = make_double2(-x.x, x.y);
+                }
+            }
+            fail = grp_max(fail);
+            const bool ok = try_fo && fail == 0.0;
+            __syncwarp();
+            double2 nu[D::NF];
+#pragma unroll
+            for (int x = 0; x < D::NF; ++x) {
+                const int e = gl + WG * x;
+                nu[x] = make_double2(0, 0);
+                if (!ok || e >= D::NN) continue;
+                const int m = e / N, n = e % N;
+                double2 a = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) cfma(a, w.U[m * N + l], w.Tm[l * N + n]);
+                nu[x] = a;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int x = 0; x < D::NF; ++x) {
+                const int e = gl + WG * x;
+                if (ok && e < D::NN) w.U[e] = nu[x];
+            }
+            __syncwarp();
+            need = need && !ok;
+        }
+        if (!__any_sync(WG_FULL, need)) break;
+#pragma unroll 1
+        for (int r = 0; r < D::P - 1; ++r) g_round<RF, N>(w, gh, r, gl, need);
+    }
+}
+
+template <class RF, int N, int RK>
+__global__ void __launch_bounds__(32 * WG_WARPS, 3)
+    wan_attempt_g(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs,
+                  const WanTileRef *__restrict__ tiles)
+{
+    using TF = typename Cx<RF>::T;
+    using T = double2;
+    using D = GDim<N>;
+    constexpr bool F32 = std::is_same<RF, float>::value;
+    constexpr int S = RK == 4 ? 4 : 6;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // a single solve (block b = tiles WG_WARPS b ...) or a block tile of a batch
+    const int tile0 = tiles ? tiles[blockIdx.x].tile : (int)blockIdx.x * WG_WARPS;
+    const WanDev &P = tiles ? *descs[tiles[blockIdx.x].solve] : *Pp;
+    const WanCtl ctl = *P.ctl;
+    if (ctl.done) return;
+    const int nR = P.nR;
+    const GSmem L = g_smem(N, nR, sizeof(RF));
+    GHead &gh = *reinterpret_cast<GHead *>(smem_raw);
+    TF *cA = reinterpret_cast<TF *>(smem_raw + L.cA);
+    RF *Rc = reinterpret_cast<RF *>(smem_raw + L.Rc);
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5, grp = lane >> 3, gl = lane & 7;
+    const double h = ctl.hs;
+    const int buf = ctl.buf;
+    const bool cur = ctl.need_current;
+    if (threadIdx.x == 0) {
+        tableau(P.rk, gh.tab);
+        int u = 0;
+        for (int m = 0; m < N; ++m)
+            for (int n = m; n < N; ++n, ++u) {
+                gh.ut[u][0] = (unsigned char)m;
+                gh.ut[u][1] = (unsigned char)n;
+            }
+        for (int r = 0; r < D::P - 1; ++r)
+            for (int i = 0; i < N; ++i) gh.mate[r][i] = (signed char)rr_mate(i, r, D::P);
+    }
+    load_lattice<RF>(P, Rc);
+    const TF *cAg = static_cast<const TF *>(P.stage_cA);
+    for (int i = threadIdx.x; i < S * nR; i += blockDim.x) cA[i] = cAg[i];
+    for (int i = threadIdx.x; i < 36; i += blockDim.x) gh.AE[i / 6][i % 6] = P.stage_AE[i];
+    for (int q = threadIdx.x; q < WG_WARPS * WAN_WARPS * WAN_NSLOT; q += blockDim.x)
+        (&gh.part[0][0][0])[q] = 0.0;
+    if (threadIdx.x < WG_WARPS) gh.errw[threadIdx.x] = 0.0;
+    __syncthreads();
+
+    const int tile = tile0 + wi;
+    if (tile < P.ntiles) {
+        const int k = tile * WAN_WARPS + grp;
+        const bool live = k < P.nk;
+        const int kc = live ? k : P.nk - 1;   // a group past the grid shadows the last k-point
+        const GView<RF> w(smem_raw + L.k0 + (size_t)(wi * WAN_WARPS + grp) * L.kbytes, L);
+        double kv[3], wk;
+        kpoint(P, kc, kv, wk);
+        for (int r = gl; r < nR; r += WG) {
+            double sn, cs;
+            sincos(kv[0] * P.V[2 * r] + kv[1] * P.V[2 * r + 1], &sn, &cs);
+            w.pk[r] = cx<TF>(cs, sn);
+        }
+        const T *Ug = P.U[buf] + (size_t)kc * D::NN;
+        for (int e = gl; e < D::NN; e += WG) w.U[e] = Ug[e];
+        const double2 *rho = P.rho[buf] + (size_t)kc * D::NN;
+        T r64[D::NO];
+        int om[D::NO], on[D::NO];
+#pragma unroll
+        for (int j = 0; j < D::NO; ++j) {
+            const int u = gl + WG * j;
+            om[j] = on[j] = 0;
+            r64[j] = make_double2(0, 0);
+            if (u < D::NU) {
+                om[j] = gh.ut[u][0];
+                on[j] = gh.ut[u][1];
+                r64[j] = rho[om[j] * N + on[j]];
+            }
+        }
+        T ks[S][D::NO];
+        const TF *gt = static_cast<const TF *>(P.gtab);
+        const int gstride = D::NO * 3 * WG;   // table entries per lattice vector
+        const bool dip = P.has_dip;
+        double emax = 0.0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            // stage input Y = rho + h sum_j a_sj k_j (owned elements, packed)
+#pragma unroll
+            for (int j = 0; j < D::NO; ++j) {
+                const int u = gl + WG * j;
+                if (u >= D::NU) continue;
+                T y = r64[j];
+#pragma unroll
+                for (int i = 0; i < s; ++i) {
+                    const double a = h * gh.tab.a[s][i];
+                    if (a != 0.0) {
+                        y.x = fma(a, ks[i][j].x, y.x);
+                        y.y = fma(a, ks[i][j].y, y.y);
+                    }
+                }
+                if (om[j] == on[j]) y.y = 0;
+                w.Y[u] = y;
+            }
+            for (int r = gl; r < nR; r += WG) w.ph[r] = cmul(w.pk[r], cA[s * nR + r]);
+            __syncwarp();
+            const bool with_cur = cur && s == 0;
+            // Fourier sums of the owned elements: H0, D_x, D_y (and S_x, S_y)
+            const double Ex = gh.AE[s][3], Ey = gh.AE[s][4];
+            T d0[D::NO], d1[D::NO], s0[D::NO], s1[D::NO];
+#pragma unroll
+            for (int j = 0; j < D::NO; ++j) {
+                const int u = gl + WG * j;
+                d0[j] = d1[j] = s0[j] = s1[j] = make_double2(0, 0);
+                if (u >= D::NU) continue;
+                const TF *tb = gt + (size_t)(j * 3) * WG + gl;
+                TF a0 = cx<TF>(0, 0), a1 = cx<TF>(0, 0), a2 = cx<TF>(0, 0);
+                TF sx = cx<TF>(0, 0), sy = cx<TF>(0, 0);
+                if (with_cur) {
+                    for (int r = 0; r < nR; ++r) {
+                        const TF p = w.ph[r];
+                        const TF ph = cmul(tb[(size_t)r * gstride], p);
+                        a0.x += ph.x;
+                        a0.y += ph.y;
+                        sx.x = fma(Rc[2 * r], ph.x, sx.x);
+                        sx.y = fma(Rc[2 * r], ph.y, sx.y);
+                        sy.x = fma(Rc[2 * r + 1], ph.x, sy.x);
+                        sy.y = fma(Rc[2 * r + 1], ph.y, sy.y);
+                        if (dip) {
+                            cfma(a1, tb[(size_t)r * gstride + WG], p);
+                            cfma(a2, tb[(size_t)r * gstride + 2 * WG], p);
+                        }
+                    }
+                } else if (dip) {
+                    for (int r = 0; r < nR; ++r) {
+                        const TF p = w.ph[r];
+                        const TF *tr = tb + (size_t)r * gstride;
+                        cfma(a0, tr[0], p);
+                        cfma(a1, tr[WG], p);
+                        cfma(a2, tr[2 * WG], p);
+                    }
+                } else {
+                    TF b0 = cx<TF>(0, 0);
+                    int r = 0;
+                    for (; r + 2 <= nR; r += 2) {
+                        cfma(a0, tb[(size_t)r * gstride], w.ph[r]);
+                        cfma(b0, tb[(size_t)(r + 1) * gstride], w.ph[r + 1]);
+                    }
+                    if (r < nR) cfma(a0, tb[(size_t)r * gstride], w.ph[r]);
+                    a0.x += b0.x;
+                    a0.y += b0.y;
+                }
+                const T v0 = make_double2(a0.x, a0.y), v1 = make_double2(a1.x, a1.y), v2 = make_double2(a2.x, a2.y);
+                w.H0[u] = v0;
+                w.HT[u] = make_double2(fma(Ex, v1.x, fma(Ey, v2.x, v0.x)), fma(Ex, v1.y, fma(Ey, v2.y, v0.y)));
+                d0[j] = v1;
+                d1[j] = v2;
+                s0[j] = make_double2(sx.x, sx.y);
+                s1[j] = make_double2(sy.x, sy.y);
+            }
+            __syncwarp();
+            if (with_cur) {   // packed S_x into the phase buffer, which is no longer read
+#pragma unroll
+                for (int j = 0; j < D::NO; ++j) {
+                    const int u = gl + WG * j;
+                    if (u < D::NU) reinterpret_cast<T *>(w.ph)[u] = s0[j];
+                }
+            }
+            // B = U^dag H0 U
+#pragma unroll
+            for (int x = 0; x < D::NF; ++x) {
+                const int e = gl + WG * x;
+                if (e >= D::NN) continue;
+                const int m = e / N, n = e % N;
+                T a = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) cfma(a, herm<N>(w.H0, m, l), w.U[l * N + n]);
+                w.Tm[e] = a;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < D::NO; ++j) {
+                const int u = gl + WG * j;
+                if (u >= D::NU) continue;
+                const int m = om[j], n = on[j];
+                T a = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) cfmac(a, w.U[l * N + m], w.Tm[l * N + n]);
+                if (m == n) a.y = 0.0;
+                w.B[u] = a;
+            }
+            __syncwarp();
+            // eigenbasis tracking (tolerances as wan_attempt)
+            g_track<RF, N>(w, gh, gl, 6, F32 ? 1e-20 : 1e-30, F32 ? 1e-5 : 1e-7, live);
+            if (gh.tab.c[s] == 1.0 && live) {
+                T *Uo = P.U[1 - buf] + (size_t)kc * D::NN;
+                for (int e = gl; e < D::NN; e += WG) Uo[e] = w.U[e];
+            }
+            // dv = diag(U^dag Y U)
+#pragma unroll
+            for (int x = 0; x < D::NF; ++x) {
+                const int e = gl + WG * x;
+                if (e >= D::NN) continue;
+                const int m = e / N, n = e % N;
+                T a = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) cfma(a, herm<N>(w.Y, m, l), w.U[l * N + n]);
+                w.Tm[e] = a;
+            }
+            __syncwarp();
+            if (gl < N) {
+                T a = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) cfmac(a, w.U[l * N + gl], w.Tm[l * N + gl]);
+                w.dv[gl] = a;
+            }
+            __syncwarp();
+            if (with_cur) {
+                // S_y packed into B (free after the tracking)
+#pragma unroll
+                for (int j = 0; j < D::NO; ++j) {
+                    const int u = gl + WG * j;
+                    if (u < D::NU) w.B[u] = s1[j];
+                }
+                __syncwarp();
+                const T *Sx = reinterpret_cast<const T *>(w.ph), *Sy = w.B;
+                // total: Re Tr(Y J_a), J_a = -i S_a + i [D_a, H0], over the owned
+                // upper elements: diagonal Y_mm Im(S_mm) - Im(C_mm) Re(D_mm),
+                // off-diagonal -2 Im(Y_mn conj(S_mn)) - 2 Im(C_mn conj(D_mn)),
+                // C = [H0, Y]
+                double tot[2] = {0.0, 0.0};
+#pragma unroll
+                for (int j = 0; j < D::NO; ++j) {
+                    const int u = gl + WG * j;
+                    if (u >= D::NU) continue;
+                    const int m = om[j], n = on[j];
+                    T c = make_double2(0, 0);
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        cfma(c, herm<N>(w.H0, m, l), herm<N>(w.Y, l, n));
+                        const T t2 = cmul(herm<N>(w.Y, m, l), herm<N>(w.H0, l, n));
+                        c.x -= t2.x;
+                        c.y -= t2.y;
+                    }
+                    const T y = w.Y[u];
+#pragma unroll
+                    for (int a = 0; a < 2; ++a) {
+                        const T sv = (a == 0 ? Sx : Sy)[u];
+                        const T dd = a == 0 ? d0[j] : d1[j];
+                        if (m == n) {
+                            tot[a] += y.x * sv.y - c.y * dd.x;
+                        } else {
+                            // Im(z conj(w)) = z.y w.x - z.x w.y
+                            tot[a] -= 2.0 * (y.y * sv.x - y.x * sv.y) + 2.0 * (c.y * dd.x - c.x * dd.y);
+                        }
+                    }
+                }
+                // intraband: sum_n Re[dv_n (U^dag (-i S_a) U)_nn]; tasks (a, n)
+                double intra[2] = {0.0, 0.0};
+                for (int t = gl; t < 2 * N; t += WG) {
+                    const int a = t / N, n = t % N;
+                    const T *Sa = a == 0 ? Sx : Sy;
+                    T pn = make_double2(0, 0);
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        T q = make_double2(0, 0);   // (S U)_ln
+#pragma unroll
+                        for (int p = 0; p < N; ++p) cfma(q, aherm<N>(Sa, l, p), w.U[p * N + n]);
+                        cfmac(pn, w.U[l * N + n], q);
+                    }
+                    // -i pn
+                    const T mj = make_double2(pn.y, -pn.x);
+                    intra[a] += w.dv[n].x * mj.x - w.dv[n].y * mj.y;
+                }
+                double *val = gh.part[wi][grp];
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    const double tt = grp_sum(tot[a]), ii = grp_sum(intra[a]);
+                    if (gl == 0 && live) {
+                        val[a] = wk * (tt - ii);
+                        val[2 + a] = wk * ii;
+                    }
+                }
+                if (gl < N && live) val[4 + gl] = wk * w.Y[pidx(gl, gl, N)].x;
+                const int ce = (P.nval * N + P.nval + 1) % D::NN;   // antelope.cpp:539-542
+                if (gl == 0 && live) {
+                    const T yc = herm<N>(w.Y, ce / N, ce % N);
+                    val[4 + N] = wk * yc.x;
+                    val[5 + N] = wk * yc.y;
+                }
+                __syncwarp();
+            }
+            // right-hand side of the owned elements: -i((HY) - (HY)^dag)
+            // - (g2 Y + (g1 - g2) U diag(dv) U^dag)   (SBEs.h:808-861)
+            const double g1 = P.g1, g2 = P.g2;
+#pragma unroll
+            for (int j = 0; j < D::NO; ++j) {
+                const int u = gl + WG * j;
+                if (u >= D::NU) continue;
+                const int m = om[j], n = on[j];
+                T c = make_double2(0, 0), c2 = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) {
+                    cfma(c, herm<N>(w.HT, m, l), herm<N>(w.Y, l, n));
+                    cfma(c2, herm<N>(w.HT, n, l), herm<N>(w.Y, l, m));
+                }
+                c.x -= c2.x;
+                c.y += c2.y;
+                T kv2 = make_double2(c.y, -c.x);
+                if (g1 != 0.0 || g2 != 0.0) {
+                    T pr = make_double2(0, 0);
+#pragma unroll
+                    for (int p = 0; p < N; ++p) {
+                        const T t2 = cmul(w.U[m * N + p], w.dv[p]);
+                        cfma(pr, t2, cconj(w.U[n * N + p]));
+                    }
+                    const T y = w.Y[u];
+                    kv2.x -= g2 * y.x + (g1 - g2) * pr.x;
+                    kv2.y -= g2 * y.y + (g1 - g2) * pr.y;
+                }
+                ks[s][j] = kv2;
+            }
+            __syncwarp();
+        }
+        // trial state and error estimate
+        double2 *rout = P.rho[1 - buf] + (size_t)kc * D::NN;
+#pragma unroll
+        for (int j = 0; j < D::NO; ++j) {
+            const int u = gl + WG * j;
+            if (u >= D::NU) continue;
+            T inc = make_double2(0, 0), er = make_double2(0, 0);
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const double b = h * gh.tab.b[s];
+                if (b != 0.0) {
+                    inc.x = fma(b, ks[s][j].x, inc.x);
+                    inc.y = fma(b, ks[s][j].y, inc.y);
+                }
+                const double eb = h * gh.tab.e[s];
+                if (eb != 0.0) {
+                    er.x = fma(eb, ks[s][j].x, er.x);
+                    er.y = fma(eb, ks[s][j].y, er.y);
+                }
+            }
+            double2 v = make_double2(r64[j].x + inc.x, r64[j].y + inc.y);
+            const int m = om[j], n = on[j];
+            if (m == n) v.y = 0.0;
+            if (live) {
+                rout[m * N + n] = v;
+                rout[n * N + m] = make_double2(v.x, -v.y);
+                emax = fmax(emax, sqrt(er.x * er.x + er.y * er.y));
+            }
+        }
+        emax = warp_max(emax);
+        if (lane == 0) gh.errw[wi] = emax;
+    }
+    __syncthreads();
+    if (threadIdx.x < WG_WARPS) {
+        const int t = tile0 + threadIdx.x;
+        if (t < P.ntiles) P.tile_err[t] = gh.errw[threadIdx.x];
+    }
+    if (cur && threadIdx.x < WG_WARPS * WAN_NSLOT) {
+        const int wq = threadIdx.x / WAN_NSLOT, slot = threadIdx.x % WAN_NSLOT, t = tile0 + wq;
+        if (t < P.ntiles) {
+            double s = 0.0;
+            for (int g = 0; g < WAN_WARPS; ++g) s += gh.part[wq][g][slot];
+            P.cur_part[(size_t)t * WAN_NSLOT + slot] = s;
+        }
+    }
+}

@@ -875,12 +875,14 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5)
                             continue;
                         }
                         const int m = e / N, n = e % N;
-                        T c = make_double2(0, 0);
-                        for (int l = 0; l < N; ++l) {
-                            cfma(c, Da[m * N + l], w.H0[l * N + n]);
-                            const T t2 = cmul(w.H0[m * N + l], Da[l * N + n]);
-                            c.x -= t2.x;
-                            c.y -= t2.y;
+                        T c = make_double2(0, 0);   // [D_a, H0]: none without dipole tables
+                        if (P.has_dip) {
+                            for (int l = 0; l < N; ++l) {
+                                cfma(c, Da[m * N + l], w.H0[l * N + n]);
+                                const T t2 = cmul(w.H0[m * N + l], Da[l * N + n]);
+                                c.x -= t2.x;
+                                c.y -= t2.y;
+                            }
                         }
                         // -i S + i c = (S.y - c.y, -S.x + c.x)
                         w.B[e] = make_double2(Sa[e].y - c.y, c.x - Sa[e].x);
@@ -985,6 +987,10 @@ __global__ void __launch_bounds__(32 * WAN_WARPS, 5)
     }
 }
 
+namespace {
+#include "sbe_wangroup.cuh"
+}  // namespace
+
 // ============================================================= velocity gauge
 // N-band velocity gauge (SBEs.h:284-373, 787-805, 862-871): rho in the band
 // basis of H(k), H = diag(eps) + sum_a A_a P_a with P_a = U^dag J_a U fixed
@@ -1063,12 +1069,14 @@ __global__ void __launch_bounds__(32 * WAN_WARPS) wan_vg_init(WanDev P)
                 continue;
             }
             const int m = e / N, n = e % N;
-            T c = make_double2(0, 0);
-            for (int l = 0; l < N; ++l) {
-                cfma(c, Da[m * N + l], w.H0[l * N + n]);
-                const T t2 = cmul(w.H0[m * N + l], Da[l * N + n]);
-                c.x -= t2.x;
-                c.y -= t2.y;
+            T c = make_double2(0, 0);   // [D_a, H0]: none without dipole tables
+            if (P.has_dip) {
+                for (int l = 0; l < N; ++l) {
+                    cfma(c, Da[m * N + l], w.H0[l * N + n]);
+                    const T t2 = cmul(w.H0[m * N + l], Da[l * N + n]);
+                    c.x -= t2.x;
+                    c.y -= t2.y;
+                }
             }
             w.B[e] = make_double2(Sa[e].y - c.y, c.x - Sa[e].x);
         }
@@ -1605,8 +1613,56 @@ cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// ---- grouped attempt kernel
+bool wan_grouped_applies(const WanDev &w)
+{
+    if (w.vg || w.cont || w.has_jtab || w.nR < 1 || w.nR > WAN_MAXR) return false;
+    if (w.N != 4 && w.N != 6) return false;
+    return (w.rk == 4 || w.rk == 5 || w.rk == 45) && g_smem(w.N, w.nR, 8).total <= 227 * 1024;
+}
+bool wan_grouped(const WanDev &w) { return w.gtab != nullptr && wan_grouped_applies(w); }
+int wan_gtab_row(int N) { return ((N * (N + 1) / 2 + WG - 1) / WG) * 3 * WG; }
+
+template <class RF, int N> static WanKernel wan_attempt_g_rk(int rk)
+{
+    return rk == 4 ? wan_attempt_g<RF, N, 4> : rk == 5 ? wan_attempt_g<RF, N, 5> : wan_attempt_g<RF, N, 45>;
+}
+template <class RF> static WanKernel wan_attempt_g_n(int N, int rk)
+{
+    return N == 4 ? wan_attempt_g_rk<RF, 4>(rk) : wan_attempt_g_rk<RF, 6>(rk);
+}
+template <class RF> static cudaError_t allow_smem_g()
+{
+    static bool done = false;
+    if (done) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int n : {4, 6}) {
+        const int bytes = (int)g_smem(n, WAN_MAXR, sizeof(RF)).total;
+        if (bytes > 227 * 1024) continue;   // such a solve is not grouped (wan_grouped_applies)
+        for (int rk : {4, 5, 45})
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(wan_attempt_g_n<RF>(n, rk), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         bytes);
+    }
+    done = e == cudaSuccess;
+    return e;
+}
+static cudaError_t launch_grouped(int N, int nR, int rk, const WanDev *dw, const WanDev *const *descs,
+                                  const WanTileRef *tiles, int nblocks, int precision, cudaStream_t st)
+{
+    cudaError_t e = precision == 0 ? allow_smem_g<double>() : allow_smem_g<float>();
+    if (e != cudaSuccess) return e;
+    const size_t sm = g_smem(N, nR, precision == 0 ? 8 : 4).total;
+    if (precision == 0) wan_attempt_g_n<double>(N, rk)<<<nblocks, 32 * WG_WARPS, sm, st>>>(dw, descs, tiles);
+    else wan_attempt_g_n<float>(N, rk)<<<nblocks, 32 * WG_WARPS, sm, st>>>(dw, descs, tiles);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st)
 {
+    if (wan_grouped(w))
+        return launch_grouped(w.N, w.nR, w.rk, dw, nullptr, nullptr, (w.ntiles + WG_WARPS - 1) / WG_WARPS,
+                              precision, st);
     const int grid = (w.nk + WAN_WARPS - 1) / WAN_WARPS;
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
@@ -1621,9 +1677,10 @@ cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision,
 }
 
 cudaError_t launch_wan_attempt_batch(int N, int nR_max, bool vg, const WanDev *const *descs, const WanTileRef *tiles,
-                                     int ntiles, int precision, cudaStream_t st)
+                                     int ntiles, int precision, cudaStream_t st, int grouped_rk)
 {
     if (ntiles <= 0) return cudaSuccess;
+    if (grouped_rk) return launch_grouped(N, nR_max, grouped_rk, nullptr, descs, tiles, ntiles, precision, st);
     cudaError_t e = precision == 0 ? allow_smem<double>() : allow_smem<float>();
     if (e != cudaSuccess) return e;
     const size_t sm = wan_smem_bytes(N, nR_max, precision);

@@ -64,6 +64,8 @@ struct WanDev {
     const void *d;          // [nR][2][N*N] complex, same precision (or null)
     const void *jt;         // [nR][2][N*N] current-operator tables, same precision (or null:
                             // J_a = -dH/dk_a + i[D_a, H])
+    const void *gtab;       // h and d re-laid for the grouped attempt kernel, [nR][NO][3][8]
+                            // complex (NO = ceil(N(N+1)/2 / 8)), same precision; null: not used
     double2 *rho[2];        // [nk][N*N] committed / trial state (Wannier basis, full matrix), FP64
     double2 *U[2];          // [nk][N*N] tracked eigenbasis of H0(k+A), FP64
     double *weight;         // [nk]
@@ -108,6 +110,16 @@ cudaError_t launch_field_table(const LaserDev &L, double atmin, double dt, int N
                                cudaStream_t st);
 
 size_t wan_smem_bytes(int N, int nR, int precision);
+// The grouped attempt kernel (eight lanes per k-point) runs the length-gauge
+// attempts of explicit tables with the -dH/dk + i[D, H] current operator at
+// N = 4 and 6: wan_grouped_applies says whether a solve qualifies (before its
+// re-laid tables exist), wan_grouped whether it runs on it; its blocks cover
+// WAN_GROUP_TILES tiles, so batched tile lists of such a class are in blocks.
+constexpr int WAN_GROUP_TILES = 4;
+bool wan_grouped_applies(const WanDev &w);
+bool wan_grouped(const WanDev &w);
+// entries of the re-laid table per lattice vector (complex numbers)
+int wan_gtab_row(int N);
 cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st);
 cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st);
 cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st);
@@ -118,8 +130,10 @@ cudaError_t launch_wan_snapshot(const WanDev &w, const WanDev *dw, int precision
 // `tiles` [ntiles] the tiles of all of them (device memory); N, nR_max and
 // the gauge (vg) of the launch class size the shared memory and pick the
 // instance.  Control: one block per solve.
+// grouped_rk != 0: the class runs on the grouped kernel with that RK order
+// (`tiles` then lists blocks of WAN_GROUP_TILES tiles: tile = the first one)
 cudaError_t launch_wan_attempt_batch(int N, int nR_max, bool vg, const WanDev *const *descs, const WanTileRef *tiles,
-                                     int ntiles, int precision, cudaStream_t st);
+                                     int ntiles, int precision, cudaStream_t st, int grouped_rk = 0);
 cudaError_t launch_wan_control_batch(const WanDev *const *descs, int nsolves, int precision, cudaStream_t st);
 cudaError_t launch_wan_snapshot_batch(int N, int nR_max, const WanDev *const *descs, const WanTileRef *tiles,
                                       int ntiles, int precision, cudaStream_t st);

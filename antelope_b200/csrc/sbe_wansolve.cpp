@@ -100,6 +100,33 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     w_.h = h;
     w_.d = d;
     w_.jt = j;
+    // the tables re-laid for the grouped attempt kernel: entry (r, j, q, l) is
+    // quantity q (h, d_x, d_y) of upper element u = l + 8 j, zero past the
+    // triangle or without dipoles
+    std::vector<double> gt;
+    if (wan_grouped_applies(w_)) {
+        const int NU = N * (N + 1) / 2, NO = (NU + 7) / 8, row = wan_gtab_row(N), nR = w_.nR;
+        gt.assign((size_t)nR * row * 2, 0.0);
+        std::vector<int> um(NU), un(NU);
+        for (int m = 0, u = 0; m < N; ++m)
+            for (int n = m; n < N; ++n, ++u) { um[u] = m; un[u] = n; }
+        for (int r = 0; r < nR; ++r)
+            for (int jj = 0; jj < NO; ++jj)
+                for (int q = 0; q < 3; ++q)
+                    for (int l = 0; l < 8; ++l) {
+                        const int u = l + 8 * jj;
+                        if (u >= NU || (q > 0 && !w_.has_dip)) continue;
+                        const size_t src = q == 0 ? ((size_t)(r * N + um[u]) * N + un[u]) * 2
+                                                  : ((size_t)((r * 2 + q - 1) * N + um[u]) * N + un[u]) * 2;
+                        const std::vector<double> &tab = q == 0 ? p.w_h : p.w_d;
+                        const size_t dst = ((((size_t)r * NO + jj) * 3 + q) * 8 + l) * 2;
+                        gt[dst] = tab[src];
+                        gt[dst + 1] = tab[src + 1];
+                    }
+        void *g = nullptr;
+        dalloc(&g, cplx * gt.size() / 2, st, "alloc grouped tables");
+        w_.gtab = g;
+    }
     UploadRing &ring = UploadRing::shared();
     if (!p.w_vec.empty()) ring.upload(V, p.w_vec.data(), sizeof(double) * p.w_vec.size(), st);
     auto up_real = [&](void *dst, const std::vector<double> &src) {
@@ -113,6 +140,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     if (!p.w_h.empty()) up_real(h, p.w_h);
     if (w_.has_dip) up_real(d, p.w_d);
     if (w_.has_jtab && !w_.cont) up_real(j, p.w_j);
+    if (w_.gtab) up_real(const_cast<void *>(w_.gtab), gt);
     cuda_check(cudaMemsetAsync(w_.jout, 0, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st), "clear outputs");
     // initial controller state: t = t_min, h = dt, currents first
     WanCtl c{};
@@ -143,6 +171,7 @@ WannierSolve::~WannierSolve()
     cudaFreeAsync((void *)w_.h, stream_);
     if (w_.d) cudaFreeAsync((void *)w_.d, stream_);
     if (w_.jt) cudaFreeAsync((void *)w_.jt, stream_);
+    if (w_.gtab) cudaFreeAsync((void *)w_.gtab, stream_);
     for (int b = 0; b < 2; ++b) {
         cudaFreeAsync(w_.rho[b], stream_);
         cudaFreeAsync(w_.U[b], stream_);
@@ -208,15 +237,18 @@ WannierBatch::WannierBatch(const std::vector<const Problem *> &probs, int precis
     // lead the tile list, so their blocks are scheduled first
     for (int i = 0; i < (int)solves_.size(); ++i) {
         const WanDev &w = solves_[i]->dev();
+        const int grk = wan_grouped(w) ? w.rk : 0;
         Class *c = nullptr;
         for (Class &x : classes_)
-            if (x.N == w.N && x.vg == (w.vg != 0) && x.precision == solves_[i]->precision()) c = &x;
+            if (x.N == w.N && x.vg == (w.vg != 0) && x.precision == solves_[i]->precision() && x.grouped_rk == grk)
+                c = &x;
         if (!c) {
             classes_.emplace_back();
             c = &classes_.back();
             c->N = w.N;
             c->vg = w.vg != 0;
             c->precision = solves_[i]->precision();
+            c->grouped_rk = grk;
         }
         c->members.push_back(i);
         c->nR = std::max(c->nR, w.nR);
@@ -236,9 +268,11 @@ WannierBatch::WannierBatch(const std::vector<const Problem *> &probs, int precis
         }
         // interleave the solves' tiles round-robin (longest first), so that
         // the blocks of one launch spread every solve over the whole GPU
+        // (grouped classes: one entry per block of WAN_GROUP_TILES tiles)
+        const int unit = c.grouped_rk ? WAN_GROUP_TILES : 1;
         int maxt = 0;
         for (int m : c.members) maxt = std::max(maxt, solves_[m]->dev().ntiles);
-        for (int t = 0; t < maxt; ++t)
+        for (int t = 0; t < maxt; t += unit)
             for (int j = 0; j < (int)c.members.size(); ++j)
                 if (t < solves_[c.members[j]]->dev().ntiles) tiles.push_back(WanTileRef{j, t});
         c.ntiles = (int)tiles.size();
@@ -268,7 +302,8 @@ void WannierBatch::enqueue_chunk(cudaStream_t st, int iters)
 {
     for (int it = 0; it < iters; ++it)
         for (const Class &c : classes_) {
-            cuda_check(launch_wan_attempt_batch(c.N, c.nR, c.vg, c.d_descs, c.d_tiles, c.ntiles, c.precision, st),
+            cuda_check(launch_wan_attempt_batch(c.N, c.nR, c.vg, c.d_descs, c.d_tiles, c.ntiles, c.precision, st,
+                                                c.grouped_rk),
                        "Wannier attempt kernel (batch)");
             cuda_check(launch_wan_control_batch(c.d_descs, (int)c.members.size(), c.precision, st),
                        "Wannier control kernel (batch)");

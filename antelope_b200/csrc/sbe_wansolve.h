@@ -70,6 +70,7 @@ public:
 private:
     struct Class {
         int N = 0, nR = 0, precision = 0;
+        int grouped_rk = 0;   // the grouped attempt kernel (and its RK order), or 0
         bool vg = false, shots = false;
         std::vector<int> members;
         const WanDev **d_descs = nullptr;

@@ -28,8 +28,11 @@ def case(n, gauge, env):
     return c
 
 
-def rel(a, b):
-    return np.abs(a - b).max() / np.abs(b).max()
+def rel(a, b, scale=0.0):
+    """max |a - b| / max |b|; a series that vanishes by symmetry up to
+    rounding noise (the transverse currents of a linearly polarised pulse,
+    ~1e-18) is measured against 1e-5 of the run's largest current instead."""
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-5 * scale)
 
 
 @pytest.mark.parametrize("name,gauge,env", [("c1_vg_cos4", "Velocity", "cos4"), ("c1_lw_cos4", "Wannier", "cos4"),
@@ -38,9 +41,10 @@ def test_full_configuration_fp64_matches_reference(name, gauge, env):
     ref = np.load(os.path.join(GOLDEN, f"full_{name}.npz"))
     out = ab.solve(case(150, gauge, env), precision="fp64")
     assert out.inter.shape[0] == int(ref["Nt"]) == 35303
+    scale = max(np.abs(ref["inter"]).max(), np.abs(ref["intra"]).max())
     for key in ("inter", "intra"):
         for a in range(2):
-            assert rel(getattr(out, key)[:, a], ref[key][:, a]) < FP64_TOL, (key, a)
+            assert rel(getattr(out, key)[:, a], ref[key][:, a], scale) < FP64_TOL, (key, a)
         assert np.all(getattr(out, key)[:, 2] == 0)
     assert np.abs(out.occ - ref["occ_file"]).max() < 1e-12
 
@@ -69,10 +73,12 @@ def test_c2_block_matches_reference_rank(rank):
     A = p.laser()[:, 4:6]
     inter = j[:, 0:2]
     intra = j[:, 2:4] + cp[2:4] + p.dims.nval * A * wslice
+    scale = max(np.abs(ref["inter"]).max(), np.abs(ref["intra"]).max())
     for a in range(2):
-        assert rel(inter[:, a], ref["inter"][:, a]) < FP64_TOL, ("inter", a)
-        assert rel(intra[:, a], ref["intra"][:, a]) < FP64_TOL, ("intra", a)
+        assert rel(inter[:, a], ref["inter"][:, a], scale) < FP64_TOL, ("inter", a)
+        assert rel(intra[:, a], ref["intra"][:, a], scale) < FP64_TOL, ("intra", a)
+    # band occupations (the off-diagonal element of the band-basis density
+    # matrix carries the eigenvectors' phase convention -- zheevr's in the
+    # reference -- and reaches no output file for two bands)
     assert np.abs(j[:, 4] + cp[4] - ref["rho00"]).max() < 1e-12 * wslice
     assert np.abs(j[:, 5] + cp[5] - ref["rho11"]).max() < 1e-12 * wslice
-    rho01 = (j[:, 6] + cp[6]) + 1j * (j[:, 7] + cp[7])
-    assert np.abs(rho01 - ref["rho01"]).max() < 1e-12 * wslice
