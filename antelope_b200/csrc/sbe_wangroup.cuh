@@ -29,6 +29,15 @@
 // -dH/dk + i[D, H], BaseMaterial.h:62-68) at N = 4 and 6; other models and
 // band counts run on wan_attempt.
 
+// Tuning: resident blocks per SM the registers are sized for, and whether
+// the re-laid tables are staged in shared memory (one copy per block) or
+// read through L1.
+#ifndef SBE_WG_MINB
+#define SBE_WG_MINB 3
+#endif
+#ifndef SBE_WG_SMEM_TABLES
+#define SBE_WG_SMEM_TABLES 0
+#endif
 constexpr int WG = 8;          // lanes per k-point
 constexpr int WG_WARPS = 4;    // warps per block (tiles per block)
 constexpr unsigned WG_FULL = 0xffffffffu;
@@ -84,7 +93,7 @@ struct GHead {
     signed char mate[WAN_MAXN - 1][WAN_MAXN];
 };
 struct GSmem {
-    size_t cA, Rc, k0, kbytes, total;
+    size_t cA, Rc, tabs, k0, kbytes, total;
     // offsets inside a k-point region
     size_t Y, H0, HT, B, U, Tm, pk, ph, jc, js, je, dv;
 };
@@ -94,7 +103,9 @@ __host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
     const size_t NU = (size_t)N * (N + 1) / 2, NN = (size_t)N * N, tf = 2 * (size_t)rf_bytes;
     L.cA = al16(sizeof(GHead));
     L.Rc = L.cA + al16(6 * (size_t)nR * tf);
-    L.k0 = L.Rc + al16((size_t)nR * 2 * rf_bytes);
+    L.tabs = L.Rc + al16((size_t)nR * 2 * rf_bytes);
+    const size_t row = (size_t)((N * (N + 1) / 2 + WG - 1) / WG) * 3 * WG;   // table entries per vector
+    L.k0 = L.tabs + (SBE_WG_SMEM_TABLES ? al16((size_t)nR * row * tf) : 0);
     size_t o = 0;
     L.Y = o;  o += al16(NU * 16);
     L.H0 = o; o += al16(NU * 16);
@@ -320,7 +331,7 @@ __device__ __forceinline__ void g_track(const GView<RF> &w, const GHead &gh, int
 }
 
 template <class RF, int N, int RK>
-__global__ void __launch_bounds__(32 * WG_WARPS, 3)
+__global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
     wan_attempt_g(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs,
                   const WanTileRef *__restrict__ tiles)
 {
@@ -359,6 +370,14 @@ __global__ void __launch_bounds__(32 * WG_WARPS, 3)
     const TF *cAg = static_cast<const TF *>(P.stage_cA);
     for (int i = threadIdx.x; i < S * nR; i += blockDim.x) cA[i] = cAg[i];
     for (int i = threadIdx.x; i < 36; i += blockDim.x) gh.AE[i / 6][i % 6] = P.stage_AE[i];
+#if SBE_WG_SMEM_TABLES
+    {
+        TF *ts = reinterpret_cast<TF *>(smem_raw + L.tabs);
+        const TF *tg = static_cast<const TF *>(P.gtab);
+        const int n = nR * D::NO * 3 * WG;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) ts[i] = tg[i];
+    }
+#endif
     for (int q = threadIdx.x; q < WG_WARPS * WAN_WARPS * WAN_NSLOT; q += blockDim.x)
         (&gh.part[0][0][0])[q] = 0.0;
     if (threadIdx.x < WG_WARPS) gh.errw[threadIdx.x] = 0.0;
@@ -394,7 +413,11 @@ __global__ void __launch_bounds__(32 * WG_WARPS, 3)
             }
         }
         T ks[S][D::NO];
+#if SBE_WG_SMEM_TABLES
+        const TF *gt = reinterpret_cast<const TF *>(smem_raw + L.tabs);
+#else
         const TF *gt = static_cast<const TF *>(P.gtab);
+#endif
         const int gstride = D::NO * 3 * WG;   // table entries per lattice vector
         const bool dip = P.has_dip;
         double emax = 0.0;
