@@ -245,8 +245,10 @@ Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
     const bool vg = p.gauge == GAUGE_VELOCITY;
     Shape s{};
     // mixed velocity gauge: two k-points per thread in packed f32x2 registers
-    s.kpt = o.kpt > 0 ? o.kpt : ((vg && prec == PREC_MIXED) ? 2 : 1);
-    if (!vg) s.kpt = 1;
+    // mixed method: two k-points per thread in packed f32x2 registers (both
+    // gauges); the FP64 length gauge has one k-point per thread
+    s.kpt = o.kpt > 0 ? o.kpt : (prec == PREC_MIXED ? 2 : 1);
+    if (!vg && prec == PREC_FP64) s.kpt = 1;
     if (o.tile_k > 0) {
         s.tile_k = o.tile_k;
     } else if (o.kpt <= 0 && autotune_enabled() &&

@@ -952,6 +952,232 @@ __global__ void __launch_bounds__(256, 2) propagate_lw(const TileDev *__restrict
         for (int q = 0; q < 4; ++q) st[(size_t)q * nkp + kidx] = y64[q];
 }
 
+// Mixed method, length gauge, two k-points per thread in f32x2 registers (as
+// propagate_vg_x2): every field, right-hand-side and current instruction
+// advances both.  The table entry of a stage time is shared by both k-points
+// (its values broadcast); the per-k cos/sin factors, the state rounded to
+// FP32 and the stage slopes are packed.  The field terms carry 2B and -2B
+// so that each component of 2 B x s + f B - g2 s is three packed FMAs on a
+// packed product; the FP64 state takes each step's increment as
+// propagate_lw's does.
+struct LwField2 { float2 B1, B2, B3, q, ib, d1, d2, d3, n1, n2, n3; };   // d = 2B, n = -2B
+
+__device__ __forceinline__ void lw_trig2(const float2 (&c)[LW_NCONST], const float *ph, float2 (&ca)[3],
+                                         float2 (&sa)[3], float2 (&cb)[3], float2 (&sb)[3])
+{
+    float p[LW_NPHASE];
+#pragma unroll
+    for (int i = 0; i < LW_NPHASE / 4; ++i) {
+        const float4 u = __ldg(reinterpret_cast<const float4 *>(ph) + i);
+        p[4 * i] = u.x; p[4 * i + 1] = u.y; p[4 * i + 2] = u.z; p[4 * i + 3] = u.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        ca[i] = fma2(c[LW_CA0 + i], bc2(p[i]), mul2(c[LW_SA0 + i], bc2(-p[3 + i])));
+        sa[i] = fma2(c[LW_SA0 + i], bc2(p[i]), mul2(c[LW_CA0 + i], bc2(p[3 + i])));
+        cb[i] = fma2(c[LW_CB0 + i], bc2(p[6 + i]), mul2(c[LW_SB0 + i], bc2(-p[9 + i])));
+        sb[i] = fma2(c[LW_SB0 + i], bc2(p[6 + i]), mul2(c[LW_CB0 + i], bc2(p[9 + i])));
+    }
+}
+
+struct LwTrig2 { float2 ca[3], sa[3], cb[3], sb[3]; };
+
+__device__ __forceinline__ LwField2 lw_field_terms2(const LwTrig2 &T, float2 t1dt, float2 nt2sdt, float2 Mdt, float2 gd)
+{
+    LwField2 F;
+    F.B1 = mul2(t1dt, add2(add2(T.ca[0], T.ca[1]), T.ca[2]));
+    F.B2 = mul2(t1dt, add2(add2(T.sa[0], T.sa[1]), T.sa[2]));
+    F.B3 = fma2(nt2sdt, add2(add2(T.sb[0], T.sb[1]), T.sb[2]), Mdt);
+    const float2 bb = fma2(F.B1, F.B1, fma2(F.B2, F.B2, mul2(F.B3, F.B3)));
+    F.ib = make_float2(bb.x > 0.f ? __fdividef(1.0f, bb.x) : 0.f, bb.y > 0.f ? __fdividef(1.0f, bb.y) : 0.f);
+    F.q = mul2(gd, F.ib);
+    F.d1 = add2(F.B1, F.B1); F.d2 = add2(F.B2, F.B2); F.d3 = add2(F.B3, F.B3);
+    F.n1 = mul2(F.B1, bc2(-2.f)); F.n2 = mul2(F.B2, bc2(-2.f)); F.n3 = mul2(F.B3, bc2(-2.f));
+    return F;
+}
+
+template <bool G1>
+__device__ __forceinline__ void lw_rhs2(const LwField2 &F, const float2 (&y)[4], float2 ng1, float2 ng2, float2 (&k)[4])
+{
+    const float2 sx = y[LW_SX], sy = y[LW_SY], sz = y[LW_SZ];
+    const float2 f = mul2(fma2(sx, F.B1, fma2(sy, F.B2, mul2(sz, F.B3))), F.q);   // (g2-g1)(s.n)/|B|
+    k[LW_AL] = G1 ? mul2(ng1, y[LW_AL]) : make_float2(0.f, 0.f);
+    k[LW_SX] = fma2(F.d2, sz, fma2(F.n3, sy, fma2(f, F.B1, mul2(ng2, sx))));
+    k[LW_SY] = fma2(F.d3, sx, fma2(F.n1, sz, fma2(f, F.B2, mul2(ng2, sy))));
+    k[LW_SZ] = fma2(F.d1, sy, fma2(F.n2, sx, fma2(f, F.B3, mul2(ng2, sz))));
+}
+
+// j-vector constants of the currents, premultiplied: j0 = t2c vb.sin(kb),
+// j1 = t1 va.sin(ka), j2 = -t1 va.cos(ka), j3 = t2s vb.cos(kb) per axis
+struct LwCurK2 { float j0[2][3], j1[2][3], j2[2][3], j3[2][3]; };
+
+// The currents and density sums of both k-points (as lw_current_sum), added
+// over the pair in FP32 and over the warp: lanes 4i return slot i.
+__device__ __forceinline__ double lw_current_sum2(const LwCurK2 &K, const LwTrig2 &T, const LwField2 &F,
+                                                  const float2 (&y)[4], float2 w)
+{
+    float2 j0[2], j1[2], j2[2], j3[2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        j0[a] = fma2(bc2(K.j0[a][0]), T.sb[0], fma2(bc2(K.j0[a][1]), T.sb[1], mul2(bc2(K.j0[a][2]), T.sb[2])));
+        j1[a] = fma2(bc2(K.j1[a][0]), T.sa[0], fma2(bc2(K.j1[a][1]), T.sa[1], mul2(bc2(K.j1[a][2]), T.sa[2])));
+        j2[a] = fma2(bc2(K.j2[a][0]), T.ca[0], fma2(bc2(K.j2[a][1]), T.ca[1], mul2(bc2(K.j2[a][2]), T.ca[2])));
+        j3[a] = fma2(bc2(K.j3[a][0]), T.cb[0], fma2(bc2(K.j3[a][1]), T.cb[1], mul2(bc2(K.j3[a][2]), T.cb[2])));
+    }
+    const float2 al = y[LW_AL], sx = y[LW_SX], sy = y[LW_SY], sz = y[LW_SZ];
+    const float2 sBi = mul2(fma2(sx, F.B1, fma2(sy, F.B2, mul2(sz, F.B3))), F.ib);   // (s.B) / |B|^2
+    const float2 w2 = add2(w, w);
+    float v[8];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const float2 sj = fma2(sx, j1[a], fma2(sy, j2[a], mul2(sz, j3[a])));
+        const float2 par = mul2(sBi, fma2(j1[a], F.B1, fma2(j2[a], F.B2, mul2(j3[a], F.B3))));
+        const float2 ie = mul2(w2, sub2(sj, par));       // interband
+        const float2 ia = mul2(w2, fma2(al, j0[a], par)); // intraband
+        v[a] = ie.x + ie.y;
+        v[2 + a] = ia.x + ia.y;
+    }
+    const float2 o0 = mul2(w, add2(al, sz)), o1 = mul2(w, sub2(al, sz)), o2 = mul2(w, sx), o3 = mul2(w, sy);
+    v[4] = o0.x + o0.y;
+    v[5] = o1.x + o1.y;
+    v[6] = o2.x + o2.y;
+    v[7] = -(o3.x + o3.y);
+    return double(warp_sum8<float>(v, threadIdx.x & 31));
+}
+
+template <int RK, bool G1>
+__global__ void __launch_bounds__(256, 2) propagate_lw_x2(const TileDev *__restrict__ tiles,
+                                                       const SolveDev *__restrict__ solves, int tick, int S)
+{
+    using TB = Tableau<RK>;
+    extern __shared__ double red_dyn[];   // red_stage_bytes(blockDim.x)
+    const TileDev tl = tiles[blockIdx.x];
+    const SolveDev &sd = solves[tl.solve];
+    const int s0 = (tick - sd.admit_tick) * S;
+    const int Nt = sd.Nt;
+    if (s0 < 0 || s0 >= Nt) return;
+    const int s1 = min(s0 + S, Nt);
+    const int nkp = sd.nk_pad, ntiles = sd.ntiles;
+    const float *__restrict__ kc = static_cast<const float *>(sd.kc);
+    double *__restrict__ st = static_cast<double *>(sd.st);
+    const float *__restrict__ tab = static_cast<const float *>(sd.tab);
+    const float2 ng1 = bc2(-float(sd.g1)), ng2 = bc2(-float(sd.g2)), gd = bc2(float(sd.g2 - sd.g1));
+    const float2 t1dt = bc2(float(sd.t1dt)), nt2sdt = bc2(-float(sd.t2sdt)), Mdt = bc2(float(sd.Mdt));
+    LwCurK2 K;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            K.j0[a][i] = float(sd.t2c) * float(sd.vb[i][a]);
+            K.j1[a][i] = float(sd.t1) * float(sd.va[i][a]);
+            K.j2[a][i] = -float(sd.t1) * float(sd.va[i][a]);
+            K.j3[a][i] = float(sd.t2s) * float(sd.vb[i][a]);
+        }
+
+    const int l0 = threadIdx.x, l1 = threadIdx.x + blockDim.x;
+    const bool ok0 = l0 < tl.kcount, ok1 = l1 < tl.kcount;
+    const int k0 = tl.k0 + l0, k1 = tl.k0 + l1;
+    float2 c[LW_NCONST];
+#pragma unroll
+    for (int q = 0; q < LW_NCONST; ++q)
+        c[q] = make_float2(ok0 ? kc[(size_t)q * nkp + k0] : 0.f, ok1 ? kc[(size_t)q * nkp + k1] : 0.f);
+    // padding lanes: a harmless k = 0 point of weight 0
+    if (!ok0) c[LW_CA0].x = c[LW_CB0].x = 1.f;
+    if (!ok1) c[LW_CA0].y = c[LW_CB0].y = 1.f;
+    const float2 w = c[LW_W];
+    double y64[2][4];
+    float2 yr[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        y64[0][q] = ok0 ? st[(size_t)q * nkp + k0] : 0.0;
+        y64[1][q] = ok1 ? st[(size_t)q * nkp + k1] : 0.0;
+        yr[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+    }
+    TileReducer red(red_dyn, blockDim.x >> 5);
+    int next_shot = first_shot(s0, sd.shot_every);
+
+    LwTrig2 Te;   // trig factors at the end of the step (t + dt)
+    lw_trig2(c, tab + vg_start_row<TB>(s0) * LW_NPHASE, Te.ca, Te.sa, Te.cb, Te.sb);
+    LwField2 F0 = lw_field_terms2(Te, t1dt, nt2sdt, Mdt, gd);
+    red.put(lw_current_sum2(K, Te, F0, yr, w), 0);
+
+    for (int s = s0; s < s1; ++s) {
+        const float *row = tab + (size_t)s * TB::NT * LW_NPHASE;
+        LwField2 Fc = F0;
+        float2 kk[TB::S][4], y[4], acc[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < TB::S; ++i) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float2 t = yr[q];
+#pragma unroll
+                for (int m = 0; m < i; ++m)
+                    if (TB::a(i, m) != 0.0) t = fma2(bc2(float(TB::a(i, m))), kk[m][q], t);
+                y[q] = t;
+            }
+            if (TB::ti(i) == TB::END) {
+                lw_trig2(c, row + TB::END * LW_NPHASE, Te.ca, Te.sa, Te.cb, Te.sb);
+                Fc = F0 = lw_field_terms2(Te, t1dt, nt2sdt, Mdt, gd);
+            } else if (i > 0 && TB::ti(i) != TB::ti(i - 1)) {
+                LwTrig2 Tm;
+                lw_trig2(c, row + TB::ti(i) * LW_NPHASE, Tm.ca, Tm.sa, Tm.cb, Tm.sb);
+                Fc = lw_field_terms2(Tm, t1dt, nt2sdt, Mdt, gd);
+            }
+            lw_rhs2<G1>(Fc, y, ng1, ng2, kk[i]);
+            if (TB::b(i) != 0.0) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = fma2(bc2(float(TB::b(i))), kk[i][q], acc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            y64[0][q] += double(acc[q].x);
+            y64[1][q] += double(acc[q].y);
+            yr[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+        }
+        const double jsum = s + 1 < s1 ? lw_current_sum2(K, Te, F0, yr, w) : 0.0;
+        if (s == next_shot) {
+            // density snapshot of each k-point (as propagate_lw)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const bool okh = h == 0 ? ok0 : ok1;
+                if (!okh) continue;
+                float cf[LW_NCONST];
+#pragma unroll
+                for (int q = 0; q < LW_NCONST; ++q) cf[q] = h == 0 ? c[q].x : c[q].y;
+                double Bt[3];
+                lw_B64<float>(cf, tab + vg_start_row<TB>(s) * LW_NPHASE, sd.t1dt, sd.t2sdt, sd.Mdt, Bt);
+                const double bn = sqrt(Bt[0] * Bt[0] + Bt[1] * Bt[1] + Bt[2] * Bt[2]);
+                double nx = 0.0, ny = 0.0, nz = 1.0;
+                if (bn > 0.0) { nx = Bt[0] / bn; ny = Bt[1] / bn; nz = Bt[2] / bn; }
+                const double al = y64[h][LW_AL], sx = y64[h][LW_SX], sy = y64[h][LW_SY], sz = y64[h][LW_SZ];
+                double2 up[2], dn[2];
+                spinors(nx, ny, nz, up, dn);
+                const double2 r0 = make_double2((al + sz) * dn[0].x + sx * dn[1].x + sy * dn[1].y,
+                                                (al + sz) * dn[0].y + sx * dn[1].y - sy * dn[1].x);
+                const double2 r1 = make_double2(sx * dn[0].x - sy * dn[0].y + (al - sz) * dn[1].x,
+                                                sx * dn[0].y + sy * dn[0].x + (al - sz) * dn[1].y);
+                const double2 q0 = cconjmul(up[0], r0), q1 = cconjmul(up[1], r1);
+                const size_t ix = (size_t)(s / sd.shot_every) * sd.nk + (h == 0 ? k0 : k1);
+                sd.snap_nc[ix] = al + sx * nx + sy * ny + sz * nz;
+                sd.snap_pi[2 * ix] = q0.x + q1.x;
+                sd.snap_pi[2 * ix + 1] = q0.y + q1.y;
+            }
+            next_shot += sd.shot_every;
+        }
+        const int r = (s - s0) % SUB;
+        if (r == SUB - 1 || s == s1 - 1) red.flush(r + 1, s - r - s0, ntiles, tl.tile, sd.partial);
+        if (s + 1 < s1) red.put(jsum, (s + 1 - s0) % SUB);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (ok0) st[(size_t)q * nkp + k0] = y64[0][q];
+        if (ok1) st[(size_t)q * nkp + k1] = y64[1][q];
+    }
+}
+
 // ------------------------------------------------------- second pass
 // One CTA per (step, solve): its 8 warps split the tile rows into 8 fixed
 // contiguous ranges; within a warp, lanes 8g..8g+7 sum slots 0..7 over tiles
@@ -1231,6 +1457,14 @@ static cudaError_t launch_lw_t(const LaunchArgs &la, bool g1)
     SBE_CHECK_LAUNCH();
 }
 
+template <int RK, bool G1>
+static cudaError_t launch_lw_x2_t(const LaunchArgs &la)
+{
+    propagate_lw_x2<RK, G1><<<la.ntiles, la.threads, red_stage_bytes(la.threads), la.stream>>>(la.tiles, la.solves,
+                                                                                              la.tick, la.S);
+    SBE_CHECK_LAUNCH();
+}
+
 cudaError_t launch_propagate(const LaunchArgs &la)
 {
     if (la.ntiles <= 0) return cudaSuccess;
@@ -1255,6 +1489,11 @@ cudaError_t launch_propagate(const LaunchArgs &la)
         return cudaErrorInvalidValue;
     }
     if (la.variant == VAR_HALDANE_LW) {
+        if (la.kpt == 2 && la.precision != PREC_FP64) {   // the packed mixed kernel
+            if (la.rk == 4) return g1 ? launch_lw_x2_t<4, true>(la) : launch_lw_x2_t<4, false>(la);
+            if (la.rk == 5) return g1 ? launch_lw_x2_t<5, true>(la) : launch_lw_x2_t<5, false>(la);
+            return cudaErrorInvalidValue;
+        }
         if (la.kpt != 1) return cudaErrorInvalidValue;
         if (la.precision == PREC_FP64) {
             if (la.rk == 4) return launch_lw_t<double, 4>(la, g1);

@@ -31,7 +31,7 @@
 //    return -- error paths included -- comes after the GPU work this call
 //    queued has finished, so the next call never races on the array.
 //  - Default launch shape: the engine's heuristic without the autotuner (two
-//    k-points per thread for the mixed velocity gauge, the largest CTA of at
+//    k-points per thread for the mixed method, the largest CTA of at
 //    most 128 threads that still gives two CTAs per SM); with the same tile_k
 //    and k_per_thread the results equal sbe_solver_*'s bit for bit.
 #include <cuda_runtime.h>
@@ -100,8 +100,8 @@ extern "C" sbe_status sbe_solve_noalloc(const sbe_problem *problem, const sbe_op
     const int precision = (opts && opts->precision >= 0) ? opts->precision : p.precision;
     const bool is_vg = p.gauge == GAUGE_VELOCITY;
     // launch shape: the engine's defaults (Engine::shape_for) without the autotuner
-    int kpt = (opts && opts->k_per_thread > 0) ? opts->k_per_thread : ((is_vg && precision == PREC_MIXED) ? 2 : 1);
-    if (!is_vg) kpt = 1;
+    int kpt = (opts && opts->k_per_thread > 0) ? opts->k_per_thread : (precision == PREC_MIXED ? 2 : 1);
+    if (!is_vg && precision == PREC_FP64) kpt = 1;
     if (kpt != 1 && kpt != 2) return sbe_noalloc_fail(SBE_INVALID_ARGUMENT, "k_per_thread must be 1 or 2");
     int tile_k = (opts && opts->tile_k > 0) ? opts->tile_k : 0;
     if (tile_k == 0) {

@@ -108,7 +108,9 @@ Shape autotune_shape(int device, const Problem &p, int precision)
     // every CTA size in warps: the best one balances occupancy against the
     // quantisation of the tile count into waves of resident CTAs
     for (int t = 32; t <= 256; t += 32) addc(t, 1);
-    if (vg)
+    // two k-points per thread: the FP64 velocity gauge and the packed mixed
+    // kernels of both gauges
+    if (vg || precision != PREC_FP64)
         for (int t = 32; t <= 256; t += 32) addc(t, 2);
     Problem q = p;
     const int S = 128;

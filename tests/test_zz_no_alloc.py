@@ -44,7 +44,7 @@ def _check(out, ref):
     # length gauge, mixed: the twelve cos/sin columns rounded to float
     (variant(top__gauge="Wannier", calc__Npoints=[21, 17]), dict(precision="mixed", tile_k=64)),
     (variant(top__gauge="Wannier", calc__Npoints=[19, 15], calc__RKorder=5, calc__T1=300.0),
-     dict(precision="mixed", tile_k=96)),
+     dict(precision="mixed", tile_k=96, k_per_thread=1)),
 ])
 def test_noalloc_matches_regular_entry_point_twice(case, opts):
     p = ab.Problem.from_dict(case)
