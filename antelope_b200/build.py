@@ -40,14 +40,20 @@ def build(verbose_ptxas: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(os.path.dirname(CLI), exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "sbe.h")]
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
         if _newer(o, [s, __file__] + hdrs):
             extra = ["-Xptxas", "-v"] if (verbose_ptxas and src.endswith(".cu")) else []
-            _run([NVCC] + ARCH + COMMON + extra + ["-c", s, "-o", o])
+            jobs.append([NVCC] + ARCH + COMMON + extra + ["-c", s, "-o", o])
+    # the translation units are independent: compile them in parallel
+    if jobs:
+        import concurrent.futures as cf
+        with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as pool:
+            for f in [pool.submit(_run, cmd) for cmd in jobs]:
+                f.result()
     if _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
     cli_src = os.path.join(CSRC, "sbe_run.cpp")

@@ -709,6 +709,8 @@ struct Request {
     // ADMITTING: taken off the queue, being set up by the worker outside the lock
     enum State { QUEUED, ADMITTING, RESIDENT, DONE, FAILED, CANCELLED } state = QUEUED;
     int solve = -1;               // engine solve id while the engine holds it
+    bool nband = false;           // a table or continuum model: held by the N-band pool
+    int wsolve = -1;              // its pool id
     bool fetching = false;
     bool cancel_asked = false;    // cancelled while ADMITTING
     bool delivered = false;       // a wait returned its final state: the worker may erase it
@@ -720,6 +722,7 @@ struct Request {
 struct sbe_server {
     sbe_server_opts opts{};
     std::unique_ptr<Engine> eng;
+    std::unique_ptr<WannierPool> wpool;   // N-band requests
     cudaStream_t stream = nullptr;
     std::thread worker;
     std::mutex mu;
@@ -749,6 +752,9 @@ void sbe_server::loop()
     // admissions set up between two tick issues: a burst of arrivals is
     // admitted in slices while the GPU keeps working on the queued ticks
     constexpr size_t kAdmitPerTurn = 16;
+    constexpr int kPoolIters = 32;   // N-band attempted steps per tick
+    auto nband_precision = [&](const Problem &p) { return opts.precision >= 0 ? opts.precision : p.precision; };
+    wpool = std::make_unique<WannierPool>(opts.device, stream);
     std::vector<cudaEvent_t> pool;
     std::vector<Request *> batch;
     for (;;) {
@@ -766,7 +772,8 @@ void sbe_server::loop()
                 Request &r = *it->second;
                 size_t need = 0;
                 try {
-                    need = eng->bytes_needed(r.prob, eo);
+                    need = r.nband ? WannierPool::bytes_needed(r.prob, nband_precision(r.prob))
+                                   : eng->bytes_needed(r.prob, eo);
                 } catch (const std::exception &e) {
                     r.state = Request::FAILED;
                     r.err = e.what();
@@ -775,9 +782,9 @@ void sbe_server::loop()
                     cv_done.notify_all();
                     continue;
                 }
-                const int resident = eng->nresident() + (int)batch.size();
+                const int resident = eng->nresident() + wpool->nresident() + (int)batch.size();
                 const bool slots_ok = opts.max_resident <= 0 || resident < opts.max_resident;
-                if (!slots_ok || (double)(eng->bytes_in_use() + planned + need) > budget) {
+                if (!slots_ok || (double)(eng->bytes_in_use() + wpool->bytes_in_use() + planned + need) > budget) {
                     if (resident == 0) {  // can never fit
                         r.state = Request::FAILED;
                         r.err = "admission refused: request needs more device memory than the budget";
@@ -793,7 +800,7 @@ void sbe_server::loop()
                 batch.push_back(&r);
                 queue.pop_front();
             }
-            if (batch.empty() && eng->nresident() == 0) {
+            if (batch.empty() && eng->nresident() == 0 && wpool->nresident() == 0) {
                 if (stop) break;
                 cv_work.wait_for(lk, std::chrono::milliseconds(50));
                 continue;
@@ -803,16 +810,17 @@ void sbe_server::loop()
         // and waiting threads are not held up by it
         for (Request *r : batch) {
             try {
-                r->solve = eng->add(r->prob, eo);
+                if (r->nband) r->wsolve = wpool->add(r->prob, nband_precision(r->prob));
+                else r->solve = eng->add(r->prob, eo);
             } catch (const std::exception &e) {
-                r->solve = -1;
+                r->solve = r->wsolve = -1;
                 r->err = e.what();
             }
         }
         if (!batch.empty()) {
             std::lock_guard<std::mutex> g(mu);
             for (Request *r : batch) {
-                if (r->solve < 0) {
+                if ((r->nband ? r->wsolve : r->solve) < 0) {
                     r->state = Request::FAILED;
                     ++n_failed;
                 } else {
@@ -829,8 +837,11 @@ void sbe_server::loop()
                 pool.push_back(inflight.front());
                 inflight.pop_front();
             }
-            if (eng->max_remaining_ticks() > 0) {
-                eng->step();
+            const bool eng_work = eng->max_remaining_ticks() > 0, pool_work = wpool->nrunning() > 0;
+            if (eng_work) eng->step();
+            // the N-band solves advance a few attempted steps per tick
+            if (pool_work) wpool->step(kPoolIters);
+            if (eng_work || pool_work) {
                 cudaEvent_t ev;
                 if (pool.empty()) cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
                 else { ev = pool.back(); pool.pop_back(); }
@@ -848,8 +859,16 @@ void sbe_server::loop()
             cv_done.notify_all();
             break;
         }
+        try {
+            wpool->poll();
+        } catch (const std::exception &e) {
+            std::lock_guard<std::mutex> g(mu);
+            fatal = e.what();
+            cv_done.notify_all();
+            break;
+        }
         std::lock_guard<std::mutex> g(mu);
-        n_launches += eng->last_launches();
+        n_launches += eng->last_launches() + wpool->last_launches();
         // retire finished and cancelled solves; forget requests whose final
         // state a wait has returned
         for (auto it = reqs.begin(); it != reqs.end();) {
@@ -861,13 +880,41 @@ void sbe_server::loop()
                 }
                 r.solve = -1;
             }
+            if (r.state == Request::CANCELLED && r.wsolve >= 0) {
+                try {
+                    wpool->remove(r.wsolve);
+                } catch (...) {
+                }
+                r.wsolve = -1;
+            }
             const bool final_state = r.state == Request::DONE || r.state == Request::FAILED ||
                                      r.state == Request::CANCELLED;
-            if (final_state && r.delivered && r.solve < 0) {
+            if (final_state && r.delivered && r.solve < 0 && r.wsolve < 0) {
                 it = reqs.erase(it);
                 continue;
             }
-            if (r.state == Request::RESIDENT && eng->finished(r.solve)) {
+            if (r.state == Request::RESIDENT && r.nband && wpool->finished(r.wsolve)) {
+                try {
+                    if (wpool->failed(r.wsolve)) {
+                        r.state = Request::FAILED;
+                        r.err = "Cash-Karp step size underflow: tolerance unreachable";
+                        ++n_failed;
+                    } else {
+                        r.jout = wpool->sums(r.wsolve);
+                        r.t_done = Clock::now();
+                        r.state = Request::DONE;
+                        ++n_completed;
+                    }
+                    wpool->remove(r.wsolve);
+                    r.wsolve = -1;
+                } catch (const std::exception &e) {
+                    r.state = Request::FAILED;
+                    r.err = e.what();
+                    ++n_failed;
+                }
+                cv_done.notify_all();
+            }
+            if (r.state == Request::RESIDENT && !r.nband && eng->finished(r.solve)) {
                 try {
                     if (!r.fetching) { eng->fetch_async(r.solve); r.fetching = true; }
                     if (eng->ready(r.solve)) {
@@ -920,11 +967,10 @@ extern "C" sbe_status sbe_server_submit(sbe_server *s, const sbe_problem *p, lon
 {
     if (!s) return fail(SBE_INVALID_ARGUMENT, "null server");
     if (sbe_status st = check_problem(p)) return st;
-    if (p->p.model != MODEL_HALDANE)
-        return fail(SBE_UNSUPPORTED, "Wannier models run through sbe_solver_* (one solve at a time)");
     auto r = std::make_unique<Request>();
     r->t_submit = Clock::now();
     r->prob = p->p;
+    r->nband = p->p.model != MODEL_HALDANE;
     try {
         // the laser output columns, built on the caller's thread
         r->laser = laser_rows(r->prob);
@@ -969,10 +1015,12 @@ extern "C" sbe_status sbe_server_wait(sbe_server *s, long long id, double timeou
         double cp[NSLOT];
         for (int q = 0; q < NSLOT; ++q) cp[q] = r.cp[q];
         Problem prob = r.prob;
+        const bool nband = r.nband;
         lk.unlock();
         return guard([&]() -> sbe_status {
             SolveOutputs o;
-            assemble_outputs(prob, j, cp, o, &laser);
+            if (nband) assemble_table_outputs(prob, j, o);
+            else assemble_outputs(prob, j, cp, o, &laser);
             copy_out(o, out);
             return SBE_OK;
         });
@@ -1026,6 +1074,7 @@ extern "C" void sbe_server_destroy(sbe_server *s)
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->opts.device);
+    s->wpool.reset();
     s->eng.reset();
     if (s->stream) {
         cudaStreamSynchronize(s->stream);

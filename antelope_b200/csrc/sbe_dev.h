@@ -62,6 +62,9 @@ enum LwConst : int {
     LW_W, LW_NCONST
 };
 enum LwState : int { LW_AL = 0, LW_SX, LW_SY, LW_SZ, LW_NSTATE };
+// the packed mixed kernel's unfolded FP32 increments of the four components
+// (see propagate_lw_x2), kept after the state so that a launch split changes no bit
+constexpr int LW_ACC = LW_NSTATE, LW_NSTATE_ALL = LW_NSTATE + 4;
 // Phase table per stage time: cos(A.a_i) x3, sin(A.a_i) x3, cos(A.b_i) x3, sin(A.b_i) x3
 constexpr int LW_NPHASE = 12;
 

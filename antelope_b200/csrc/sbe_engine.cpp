@@ -280,7 +280,7 @@ size_t Engine::bytes_needed(const Problem &p, const EngineOptions &o) const
     const size_t nk_pad = (size_t)ntiles * sh.tile_k;
     const int nts = (int)stage_fractions(p.rk).size();
     const bool vg = p.gauge == GAUGE_VELOCITY;
-    const size_t nc = vg ? (size_t)VG_NCONST_ALL : (size_t)LW_NCONST, ns = vg ? VG_NSTATE_ALL : LW_NSTATE;
+    const size_t nc = vg ? (size_t)VG_NCONST_ALL : (size_t)LW_NCONST, ns = vg ? VG_NSTATE_ALL : LW_NSTATE_ALL;
     const size_t tab = (size_t)p.laser.Nt * nts * (vg ? 2 : LW_NPHASE) * real;
     const size_t nk = o.k_end > 0 ? (size_t)(o.k_end - o.k_begin) : (size_t)p.ntotal();
     const size_t snap = o.snapshots ? (size_t)p.nshots() * nk * 24 : 0;
@@ -312,7 +312,7 @@ int Engine::add(const Problem &p, const EngineOptions &o)
     const size_t real = s->precision == PREC_FP64 ? 8 : 4;
     const bool vg = s->variant == VAR_HALDANE_VG;
     const size_t nc = vg ? (size_t)VG_NCONST_ALL : (size_t)LW_NCONST;
-    const size_t ns = vg ? (size_t)VG_NSTATE_ALL : (size_t)LW_NSTATE;
+    const size_t ns = vg ? (size_t)VG_NSTATE_ALL : (size_t)LW_NSTATE_ALL;
     const size_t kc_b = nc * s->nk_pad * real, st_b = ns * s->nk_pad * 8;  // state is FP64 in both methods
     s->k_begin = kb;
     s->nshots = o.snapshots ? p.nshots() : 0;

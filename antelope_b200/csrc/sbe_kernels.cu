@@ -958,8 +958,8 @@ __global__ void __launch_bounds__(256, 2) propagate_lw(const TileDev *__restrict
 // (its values broadcast); the per-k cos/sin factors, the state rounded to
 // FP32 and the stage slopes are packed.  The field terms carry 2B and -2B
 // so that each component of 2 B x s + f B - g2 s is three packed FMAs on a
-// packed product; the FP64 state takes each step's increment as
-// propagate_lw's does.
+// packed product; the FP64 state receives the FP32 increments every XSTEP
+// steps (see the kernel).
 struct LwField2 { float2 B1, B2, B3, q, ib, d1, d2, d3, n1, n2, n3; };   // d = 2B, n = -2B
 
 __device__ __forceinline__ void lw_trig2(const float2 (&c)[LW_NCONST], const float *ph, float2 (&ca)[3],
@@ -1085,13 +1085,22 @@ __global__ void __launch_bounds__(256, 2) propagate_lw_x2(const TileDev *__restr
     if (!ok0) c[LW_CA0].x = c[LW_CB0].x = 1.f;
     if (!ok1) c[LW_CA0].y = c[LW_CB0].y = 1.f;
     const float2 w = c[LW_W];
+    // The FP64 state is y64 = (rounded to FP32: yhi) plus the FP32 sum `acc`
+    // of the increments since the last fold; after every step s with
+    // (s + 1) % XSTEP == 0 acc is added to y64 in FP64 (as propagate_vg_x2),
+    // and an unfolded acc is kept in the state rows LW_ACC.. at a launch's
+    // end, so splitting the time loop changes no bit.  The stage input
+    // yhi + acc is rounded once per step, as float(y64) would be.
     double y64[2][4];
-    float2 yr[4];
+    float2 yhi[4], acc[4], yr[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         y64[0][q] = ok0 ? st[(size_t)q * nkp + k0] : 0.0;
         y64[1][q] = ok1 ? st[(size_t)q * nkp + k1] : 0.0;
-        yr[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+        yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+        acc[q] = make_float2(ok0 ? float(st[(size_t)(LW_ACC + q) * nkp + k0]) : 0.f,
+                             ok1 ? float(st[(size_t)(LW_ACC + q) * nkp + k1]) : 0.f);
+        yr[q] = add2(yhi[q], acc[q]);
     }
     TileReducer red(red_dyn, blockDim.x >> 5);
     int next_shot = first_shot(s0, sd.shot_every);
@@ -1104,9 +1113,7 @@ __global__ void __launch_bounds__(256, 2) propagate_lw_x2(const TileDev *__restr
     for (int s = s0; s < s1; ++s) {
         const float *row = tab + (size_t)s * TB::NT * LW_NPHASE;
         LwField2 Fc = F0;
-        float2 kk[TB::S][4], y[4], acc[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = make_float2(0.f, 0.f);
+        float2 kk[TB::S][4], y[4];
 #pragma unroll
         for (int i = 0; i < TB::S; ++i) {
 #pragma unroll
@@ -1131,12 +1138,17 @@ __global__ void __launch_bounds__(256, 2) propagate_lw_x2(const TileDev *__restr
                 for (int q = 0; q < 4; ++q) acc[q] = fma2(bc2(float(TB::b(i))), kk[i][q], acc[q]);
             }
         }
+        if ((s + 1) % XSTEP == 0) {   // fold the FP32 increments into the FP64 state
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            y64[0][q] += double(acc[q].x);
-            y64[1][q] += double(acc[q].y);
-            yr[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+            for (int q = 0; q < 4; ++q) {
+                y64[0][q] += double(acc[q].x);
+                y64[1][q] += double(acc[q].y);
+                yhi[q] = make_float2(float(y64[0][q]), float(y64[1][q]));
+                acc[q] = make_float2(0.f, 0.f);
+            }
         }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) yr[q] = add2(yhi[q], acc[q]);
         const double jsum = s + 1 < s1 ? lw_current_sum2(K, Te, F0, yr, w) : 0.0;
         if (s == next_shot) {
             // density snapshot of each k-point (as propagate_lw)
@@ -1152,7 +1164,11 @@ __global__ void __launch_bounds__(256, 2) propagate_lw_x2(const TileDev *__restr
                 const double bn = sqrt(Bt[0] * Bt[0] + Bt[1] * Bt[1] + Bt[2] * Bt[2]);
                 double nx = 0.0, ny = 0.0, nz = 1.0;
                 if (bn > 0.0) { nx = Bt[0] / bn; ny = Bt[1] / bn; nz = Bt[2] / bn; }
-                const double al = y64[h][LW_AL], sx = y64[h][LW_SX], sy = y64[h][LW_SY], sz = y64[h][LW_SZ];
+                // the FP64 state after step s: y64 plus the increments not yet folded into it
+                const double al = y64[h][LW_AL] + double(h == 0 ? acc[LW_AL].x : acc[LW_AL].y);
+                const double sx = y64[h][LW_SX] + double(h == 0 ? acc[LW_SX].x : acc[LW_SX].y);
+                const double sy = y64[h][LW_SY] + double(h == 0 ? acc[LW_SY].x : acc[LW_SY].y);
+                const double sz = y64[h][LW_SZ] + double(h == 0 ? acc[LW_SZ].x : acc[LW_SZ].y);
                 double2 up[2], dn[2];
                 spinors(nx, ny, nz, up, dn);
                 const double2 r0 = make_double2((al + sz) * dn[0].x + sx * dn[1].x + sy * dn[1].y,
@@ -1173,8 +1189,14 @@ __global__ void __launch_bounds__(256, 2) propagate_lw_x2(const TileDev *__restr
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        if (ok0) st[(size_t)q * nkp + k0] = y64[0][q];
-        if (ok1) st[(size_t)q * nkp + k1] = y64[1][q];
+        if (ok0) {
+            st[(size_t)q * nkp + k0] = y64[0][q];
+            st[(size_t)(LW_ACC + q) * nkp + k0] = double(acc[q].x);
+        }
+        if (ok1) {
+            st[(size_t)q * nkp + k1] = y64[1][q];
+            st[(size_t)(LW_ACC + q) * nkp + k1] = double(acc[q].y);
+        }
     }
 }
 

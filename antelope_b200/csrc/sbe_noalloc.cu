@@ -131,7 +131,7 @@ extern "C" sbe_status sbe_solve_noalloc(const sbe_problem *problem, const sbe_op
     Layout L{};
     size_t off = 0;
     L.kc = off;      off += round256(nconst * nk_pad * real);
-    const size_t nstate = vg ? (size_t)VG_NSTATE_ALL : (size_t)LW_NSTATE;
+    const size_t nstate = vg ? (size_t)VG_NSTATE_ALL : (size_t)LW_NSTATE_ALL;
     L.st = off;      off += round256(nstate * nk_pad * 8);
     L.tab = off;     off += round256((size_t)Nt * nts * ncols * real);
     L.jout = off;    off += round256((size_t)Nt * NSLOT * 8);

@@ -31,7 +31,7 @@
 
 // Tuning: resident blocks per SM the registers are sized for, and whether
 // the re-laid tables are staged in shared memory (one copy per block) or
-// read through L1.
+// read through L1 (measured equal on the N = 6 configuration).
 #ifndef SBE_WG_MINB
 #define SBE_WG_MINB 3
 #endif
@@ -42,6 +42,7 @@ constexpr int WG = 8;          // lanes per k-point
 constexpr int WG_WARPS = 4;    // warps per block (tiles per block)
 constexpr unsigned WG_FULL = 0xffffffffu;
 static_assert(32 / WG == WAN_WARPS, "a warp of the grouped kernel is one tile");
+static_assert(WG_WARPS == WAN_GROUP_TILES, "a block of the grouped kernel covers WAN_GROUP_TILES tiles");
 static_assert(WG_WARPS == WAN_GROUP_TILES, "a block of the grouped kernel covers WAN_GROUP_TILES tiles");
 
 __host__ __device__ constexpr int pidx(int m, int n, int N) { return m * N - m * (m - 1) / 2 + (n - m); }
@@ -187,27 +188,10 @@ __device__ __forceinline__ void g_round(const GView<RF> &w, const GHead &gh, int
             double2 e = make_double2(1, 0);
             if (r2 > 0.0) {
                 const double d = w.B[pidx(q, q, N)].x - w.B[pidx(p, p, N)].x;
-                double ir, t;
-                if (r2 > 1e-36 && r2 < 1e36 && fabs(d) < 1e18) {
-                    // the angle need not be exact: t = tan(theta) in FP32 (a
-                    // rotation by a slightly different angle still reduces
-                    // B_pq, and convergence is judged in FP64); what must be
-                    // exact is the unitarity, so 1/|g| and c = 1/sqrt(1 + t^2)
-                    // are FP32 seeds refined by two Newton steps in FP64
-                    const float rf = (float)r2, df = (float)d;
-                    const float gf = sqrtf(rf);
-                    t = (double)(copysignf(2.0f * gf, df) / (fabsf(df) + sqrtf(fmaf(df, df, 4.0f * rf))));
-                    ir = (double)rsqrtf(rf);
-                    ir = ir * fma(-0.5 * r2, ir * ir, 1.5);
-                    ir = ir * fma(-0.5 * r2, ir * ir, 1.5);
-                } else {   // outside FP32's range
-                    ir = rsqrt(r2);
-                    t = copysign(2.0 * r2 * ir, d) / (fabs(d) + sqrt(fma(d, d, 4.0 * r2)));
-                }
-                const double x = fma(t, t, 1.0);
-                c = (double)rsqrtf((float)x);
-                c = c * fma(-0.5 * x, c * c, 1.5);
-                c = c * fma(-0.5 * x, c * c, 1.5);
+                const double ir = rsqrt(r2);
+                const double hh = sqrt(fma(d, d, 4.0 * r2));
+                const double t = copysign(2.0 * r2 * ir, d) / (fabs(d) + hh);
+                c = rsqrt(fma(t, t, 1.0));
                 s = t * c;
                 e.x = g.x * ir;
                 e.y = g.y * ir;
@@ -463,37 +447,6 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
             // Fourier sums of the owned elements: H0, D_x, D_y (and S_x, S_y)
             const double Ex = gh.AE[s][3], Ey = gh.AE[s][4];
             T d0[D::NO], d1[D::NO], s0[D::NO], s1[D::NO];
-            if (!with_cur && dip) {
-                // all owned elements at once: 3 NO independent sums per phase load
-                const int nj = (D::NU - gl + WG - 1) / WG;   // owned elements of this lane
-                TF acc[D::NO][3];
-#pragma unroll
-                for (int j = 0; j < D::NO; ++j)
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) acc[j][q] = cx<TF>(0, 0);
-                const TF *tb = gt + gl;
-#pragma unroll 2
-                for (int r = 0; r < nR; ++r) {
-                    const TF p = w.ph[r];
-                    const TF *tr = tb + (size_t)r * gstride;
-#pragma unroll
-                    for (int j = 0; j < D::NO; ++j) {
-                        if (j >= nj) break;
-#pragma unroll
-                        for (int q = 0; q < 3; ++q) cfma(acc[j][q], tr[(j * 3 + q) * WG], p);
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < D::NO; ++j) {
-                    const int u = gl + WG * j;
-                    d0[j] = d1[j] = s0[j] = s1[j] = make_double2(0, 0);
-                    if (u >= D::NU) continue;
-                    const T v0 = make_double2(acc[j][0].x, acc[j][0].y), v1 = make_double2(acc[j][1].x, acc[j][1].y),
-                            v2 = make_double2(acc[j][2].x, acc[j][2].y);
-                    w.H0[u] = v0;
-                    w.HT[u] = make_double2(fma(Ex, v1.x, fma(Ey, v2.x, v0.x)), fma(Ex, v1.y, fma(Ey, v2.y, v0.y)));
-                }
-            } else {
 #pragma unroll
             for (int j = 0; j < D::NO; ++j) {
                 const int u = gl + WG * j;
@@ -517,7 +470,15 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                             cfma(a2, tb[(size_t)r * gstride + 2 * WG], p);
                         }
                     }
-                } else {   // no dipole tables (the interleaved loop above takes the rest)
+                } else if (dip) {
+                    for (int r = 0; r < nR; ++r) {
+                        const TF p = w.ph[r];
+                        const TF *tr = tb + (size_t)r * gstride;
+                        cfma(a0, tr[0], p);
+                        cfma(a1, tr[WG], p);
+                        cfma(a2, tr[2 * WG], p);
+                    }
+                } else {
                     TF b0 = cx<TF>(0, 0);
                     int r = 0;
                     for (; r + 2 <= nR; r += 2) {
@@ -535,7 +496,6 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 d1[j] = v2;
                 s0[j] = make_double2(sx.x, sx.y);
                 s1[j] = make_double2(sy.x, sy.y);
-            }
             }
             __syncwarp();
             if (with_cur) {   // packed S_x into the phase buffer, which is no longer read

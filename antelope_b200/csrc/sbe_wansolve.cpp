@@ -353,6 +353,189 @@ void WannierBatch::run(cudaStream_t st, bool use_graph)
     for (int i = 0; i < (int)solves_.size(); ++i) solves_[i]->finish_batched(h_ctls_[i], launches_);
 }
 
+// ============================================================= server pool
+WannierPool::WannierPool(int device, cudaStream_t st) : device_(device), st_(st)
+{
+    cuda_check(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming), "event create");
+}
+
+WannierPool::~WannierPool()
+{
+    cudaStreamSynchronize(st_);
+    for (Class &c : classes_) {
+        if (c.d_descs) cudaFreeAsync(c.d_descs, st_);
+        if (c.d_tiles) cudaFreeAsync(c.d_tiles, st_);
+    }
+    solves_.clear();
+    cudaStreamSynchronize(st_);
+    if (h_ctls_) cudaFreeHost(h_ctls_);
+    if (copied_) cudaEventDestroy(copied_);
+}
+
+size_t WannierPool::bytes_needed(const Problem &p, int precision)
+{
+    const size_t N = (size_t)p.nband, NN = N * N, nk = (size_t)p.ntotal(), nR = (size_t)std::max(p.w_nR, 1);
+    const size_t real = precision == 0 ? 8 : 4, cplx = 2 * real;
+    const size_t ntiles = (nk + WAN_WARPS - 1) / WAN_WARPS;
+    size_t b = 4 * nk * NN * 16 + nk * 8;                              // rho, U (two each), weights
+    b += nR * NN * cplx * 5 + nR * 16 + nR * 72 * cplx;                // h, d, current and re-laid tables, vectors
+    b += ntiles * 8 * (1 + WAN_NSLOT) + (size_t)p.laser.Nt * WAN_NSLOT * 8;   // tile results, per-step sums
+    if (p.gauge == GAUGE_VELOCITY) b += nk * N * 16 + nk * 3 * NN * 16;  // bands, momentum matrices
+    return b + 4096;
+}
+
+int WannierPool::add(const Problem &p, int precision)
+{
+    Entry e;
+    e.s = std::make_unique<WannierSolve>(p, precision, device_, st_);
+    e.bytes = bytes_needed(p, precision);
+    bytes_ += e.bytes;
+    const int id = next_id_++;
+    solves_.emplace(id, std::move(e));
+    dirty_ = true;
+    return id;
+}
+
+void WannierPool::remove(int id)
+{
+    auto it = solves_.find(id);
+    if (it == solves_.end()) return;
+    // no launch of a later step touches it once the classes are rebuilt; the
+    // solve's destructor waits for the stream before freeing
+    bytes_ -= it->second.bytes;
+    solves_.erase(it);
+    dirty_ = true;
+}
+
+int WannierPool::nrunning() const
+{
+    int n = 0;
+    for (const auto &kv : solves_) n += kv.second.done ? 0 : 1;
+    return n;
+}
+
+bool WannierPool::finished(int id) const
+{
+    auto it = solves_.find(id);
+    return it != solves_.end() && it->second.done;
+}
+
+bool WannierPool::failed(int id) const
+{
+    auto it = solves_.find(id);
+    return it != solves_.end() && it->second.failed;
+}
+
+std::vector<double> WannierPool::sums(int id)
+{
+    auto it = solves_.find(id);
+    if (it == solves_.end()) throw CudaError("unknown pool solve");
+    return it->second.s->sums();
+}
+
+void WannierPool::rebuild()
+{
+    for (Class &c : classes_) {
+        if (c.d_descs) cudaFreeAsync(c.d_descs, st_);
+        if (c.d_tiles) cudaFreeAsync(c.d_tiles, st_);
+    }
+    classes_.clear();
+    for (auto &kv : solves_) {
+        if (kv.second.done) continue;
+        const WannierSolve &s = *kv.second.s;
+        const WanDev &w = s.dev();
+        const int grk = wan_grouped(w) ? w.rk : 0;
+        Class *c = nullptr;
+        for (Class &x : classes_)
+            if (x.N == w.N && x.vg == (w.vg != 0) && x.precision == s.precision() && x.grouped_rk == grk) c = &x;
+        if (!c) {
+            classes_.emplace_back();
+            c = &classes_.back();
+            c->N = w.N;
+            c->vg = w.vg != 0;
+            c->precision = s.precision();
+            c->grouped_rk = grk;
+        }
+        c->ids.push_back(kv.first);
+        c->nR = std::max(c->nR, w.nR);
+    }
+    UploadRing &ring = UploadRing::shared();
+    for (Class &c : classes_) {
+        std::vector<const WanDev *> descs;
+        std::vector<WanTileRef> tiles;
+        const int unit = c.grouped_rk ? WAN_GROUP_TILES : 1;
+        int maxt = 0;
+        for (int id : c.ids) {
+            descs.push_back(solves_.at(id).s->dev_ptr());
+            maxt = std::max(maxt, solves_.at(id).s->dev().ntiles);
+        }
+        for (int t = 0; t < maxt; t += unit)
+            for (int j = 0; j < (int)c.ids.size(); ++j)
+                if (t < solves_.at(c.ids[j]).s->dev().ntiles) tiles.push_back(WanTileRef{j, t});
+        c.ntiles = (int)tiles.size();
+        dalloc(&c.d_descs, sizeof(WanDev *) * descs.size(), st_, "alloc pool descriptors");
+        dalloc(&c.d_tiles, sizeof(WanTileRef) * tiles.size(), st_, "alloc pool tiles");
+        ring.upload(c.d_descs, descs.data(), sizeof(WanDev *) * descs.size(), st_);
+        ring.upload(c.d_tiles, tiles.data(), sizeof(WanTileRef) * tiles.size(), st_);
+    }
+    dirty_ = false;
+}
+
+void WannierPool::step(int iters)
+{
+    last_launches_ = 0;
+    if (pending_) poll();
+    if (dirty_) rebuild();
+    if (classes_.empty()) return;
+    for (int it = 0; it < iters; ++it)
+        for (const Class &c : classes_) {
+            cuda_check(launch_wan_attempt_batch(c.N, c.nR, c.vg, c.d_descs, c.d_tiles, c.ntiles, c.precision, st_,
+                                                c.grouped_rk),
+                       "Wannier attempt kernel (server)");
+            cuda_check(launch_wan_control_batch(c.d_descs, (int)c.ids.size(), c.precision, st_),
+                       "Wannier control kernel (server)");
+            last_launches_ += 2;
+        }
+    // controllers of the running solves, read by a later poll()
+    polled_.clear();
+    for (const Class &c : classes_)
+        for (int id : c.ids) polled_.push_back(id);
+    if ((int)polled_.size() > cap_) {
+        if (h_ctls_) {
+            cuda_check(cudaStreamSynchronize(st_), "sync");
+            cudaFreeHost(h_ctls_);
+        }
+        cap_ = std::max<int>(64, 2 * (int)polled_.size());
+        cuda_check(cudaMallocHost(&h_ctls_, sizeof(WanCtl) * cap_), "cudaMallocHost(pool control)");
+    }
+    for (int i = 0; i < (int)polled_.size(); ++i)
+        cuda_check(cudaMemcpyAsync(&h_ctls_[i], solves_.at(polled_[i]).s->dev().ctl, sizeof(WanCtl),
+                                   cudaMemcpyDeviceToHost, st_),
+                   "copy control");
+    cuda_check(cudaEventRecord(copied_, st_), "event record");
+    pending_ = true;
+}
+
+void WannierPool::poll()
+{
+    if (!pending_) return;
+    const cudaError_t q = cudaEventQuery(copied_);
+    if (q == cudaErrorNotReady) return;
+    cuda_check(q, "pool event");
+    pending_ = false;
+    for (int i = 0; i < (int)polled_.size(); ++i) {
+        auto it = solves_.find(polled_[i]);
+        if (it == solves_.end() || it->second.done) continue;
+        const WanCtl &c = h_ctls_[i];
+        if (c.done) {
+            it->second.done = true;
+            it->second.failed = c.error != 0;
+            if (!c.error) it->second.s->finish_batched(c, 0);
+            dirty_ = true;
+        }
+    }
+}
+
 void WannierSolve::harmonics(double w0, int hmax, double *band_power)
 {
     const Problem &p = prob_;

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -83,6 +84,63 @@ private:
     int device_ = 0, launches_ = 0, per_iter_ = 0;
     cudaStream_t stream_ = nullptr;
     WanCtl *h_ctls_ = nullptr;
+};
+
+// The N-band solves of the continuous-batching server: solves join and leave
+// while the others run.  step() advances every unfinished solve by a number
+// of iterations -- per launch class one attempt launch over all their tiles
+// and one control launch (as WannierBatch) -- and queues a copy of their
+// controllers; poll() reads that copy once the GPU has reached it, without
+// waiting, so finished solves are noticed one step later at most.  Every solve
+// keeps its own controller: its results equal the solve run alone bit for
+// bit.  Not thread-safe (the server's worker thread owns it).
+class WannierPool {
+public:
+    WannierPool(int device, cudaStream_t st);
+    ~WannierPool();
+    WannierPool(const WannierPool &) = delete;
+    WannierPool &operator=(const WannierPool &) = delete;
+    // device memory a solve of this problem holds
+    static size_t bytes_needed(const Problem &p, int precision);
+    int add(const Problem &p, int precision);   // returns its id
+    void remove(int id);
+    size_t bytes_in_use() const { return bytes_; }
+    int nresident() const { return (int)solves_.size(); }
+    int nrunning() const;
+    void step(int iters);
+    void poll();
+    bool finished(int id) const;
+    // a finished solve whose step-size controller gave up (tolerance unreachable)
+    bool failed(int id) const;
+    std::vector<double> sums(int id);
+    int last_launches() const { return last_launches_; }
+
+private:
+    struct Entry {
+        std::unique_ptr<WannierSolve> s;
+        size_t bytes = 0;
+        bool done = false, failed = false;
+    };
+    void rebuild();
+    std::map<int, Entry> solves_;
+    int device_, next_id_ = 0, last_launches_ = 0;
+    size_t bytes_ = 0;
+    cudaStream_t st_;
+    bool dirty_ = true;
+    struct Class {
+        int N = 0, nR = 0, precision = 0, grouped_rk = 0;
+        bool vg = false;
+        std::vector<int> ids;
+        const WanDev **d_descs = nullptr;
+        WanTileRef *d_tiles = nullptr;
+        int ntiles = 0;
+    };
+    std::vector<Class> classes_;
+    std::vector<int> polled_;   // ids whose controllers the last step copied, in slot order
+    WanCtl *h_ctls_ = nullptr;
+    int cap_ = 0;
+    cudaEvent_t copied_ = nullptr;
+    bool pending_ = false;
 };
 
 // The reference's output arrays of a table model from its per-step sums

@@ -219,8 +219,11 @@ void sbe_batch_destroy(sbe_batch *b);
 
 /* Continuous-batching server: a worker thread admits submitted solves while
  * device memory allows, advances all resident solves together, and retires
- * them as they finish.  Thread-safe.  Requests return the output arrays of
- * sbe_outputs; density snapshots are taken by sbe_solver_* and sbe_batch_*. */
+ * them as they finish.  Two-band Haldane requests share the engine's ticks;
+ * N-band requests (table and continuum models) advance a few attempted steps
+ * per tick in batched launches, each with its own step-size controller.
+ * Thread-safe.  Requests return the output arrays of sbe_outputs; density
+ * snapshots are taken by sbe_solver_* and sbe_batch_*. */
 typedef struct sbe_server_opts {
     int device;
     int precision;

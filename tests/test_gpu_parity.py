@@ -108,6 +108,32 @@ def test_batch_equals_single_solves_bitwise():
         b.close()
 
 
+@pytest.mark.parametrize("gauge", ["Velocity", "Wannier"])
+def test_packed_mixed_kernels_are_launch_split_neutral(gauge):
+    """The packed mixed kernels carry FP32 increments between folds into the
+    FP64 state (every 8 absolute steps) and keep an unfolded sum in the state
+    at a launch's end, so where launches split the time loop changes no bit."""
+    case = variant(top__gauge=gauge, calc__Npoints=[16, 16])
+    shape = dict(precision="mixed", k_per_thread=2, tile_k=64)
+    a = ab.solve(case, steps_per_launch=1024, **shape)
+    for opts in (dict(steps_per_launch=37), dict(steps_per_launch=100, use_graph=True)):
+        b = ab.solve(case, **shape, **opts)
+        assert np.array_equal(b.inter, a.inter) and np.array_equal(b.intra, a.intra), opts
+        assert np.array_equal(b.occ, a.occ), opts
+
+
+@pytest.mark.parametrize("gauge", ["Velocity", "Wannier"])
+def test_packed_and_scalar_mixed_kernels_agree(gauge):
+    """Two k-points per thread (packed f32x2) and one (scalar FP32) do the same
+    arithmetic up to FP32 operation order."""
+    case = variant(top__gauge=gauge, calc__Npoints=[20, 18])
+    a = ab.solve(case, precision="mixed", k_per_thread=1, tile_k=64)
+    b = ab.solve(case, precision="mixed", k_per_thread=2, tile_k=128)
+    scale = max(np.abs(a.inter).max(), np.abs(a.intra).max())
+    for key in ("inter", "intra"):
+        assert np.abs(getattr(a, key) - getattr(b, key)).max() < 1e-5 * scale, key
+
+
 MIXED_TOL = 1e-3   # relative error per harmonic band, bands >= 1e-8 of the strongest
 
 

@@ -183,3 +183,31 @@ def test_batch_nband_mixed_precision_and_snapshots():
     for key in ("occ1d", "nc", "pi"):
         assert np.array_equal(got[key], shots[key]), key
     b.close()
+
+
+def test_server_serves_nband_requests_beside_haldane():
+    """N-band requests (a SyntheticWannier model with dipoles and Cash-Karp
+    steps, an analytic material, the continuum MultiWSM model) go through the
+    continuous-batching server beside two-band Haldane requests: each result
+    equals the same request served alone bit for bit, and the N-band ones
+    equal their plain solves (same kernels, own controller)."""
+    from cases import MATERIAL_CASES, MULTIWSM_CASES, variant
+
+    cases = [small_case("cashkarp45", tol=1e-9), MATERIAL_CASES["kanemele_w"], variant(calc__Npoints=[9, 7]),
+             small_case("rk5", n=(5, 5), seed=6), MULTIWSM_CASES["multiwsm_v"],
+             variant(top__gauge="Wannier", calc__Npoints=[8, 6])]
+    probs = [ab.Problem.from_dict(c) for c in cases]
+    srv = ab.Server(precision="fp64", steps_per_launch=128)
+    alone = []
+    for p in probs:
+        alone.append(srv.wait(srv.submit(p), timeout=300)[0])
+    ids = [srv.submit(p) for p in probs]
+    for i, (rid, a) in enumerate(zip(ids, alone)):
+        o, lat = srv.wait(rid, timeout=300)
+        assert lat > 0
+        assert _same(o, a), i
+    for i in (0, 1, 3, 4):   # the N-band requests
+        assert _same(alone[i], ab.solve(probs[i], precision="fp64")), i
+    st = srv.stats()
+    assert st["failed"] == 0 and st["completed"] == 2 * len(probs) and st["resident"] == 0
+    srv.close()
