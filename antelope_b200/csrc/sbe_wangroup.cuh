@@ -115,7 +115,8 @@ __host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
     L.U = o;  o += al16(NN * 16);
     L.Tm = o; o += al16(NN * 16);
     L.pk = o; o += al16((size_t)nR * tf);
-    L.ph = o; o += al16(std::max((size_t)nR * tf, NU * 16));   // also S_x (packed) at current steps
+    // also S_x (packed) at current steps and a full scratch matrix of the tracker
+    L.ph = o; o += al16(std::max((size_t)nR * tf, NN * 16));
     L.jc = o; o += al16((size_t)N * 8);
     L.js = o; o += al16((size_t)N * 8);
     L.je = o; o += al16((size_t)N * 16);
@@ -331,6 +332,171 @@ __device__ __forceinline__ void g_track(const GView<RF> &w, const GHead &gh, int
     }
 }
 
+// B = U^dag H0 U (packed) for the groups with `act` (all lanes call it)
+template <class RF, int N>
+__device__ __forceinline__ void g_formB(const GView<RF> &w, const GHead &gh, int gl, bool act)
+{
+    using D = GDim<N>;
+#pragma unroll
+    for (int x = 0; x < D::NF; ++x) {
+        const int e = gl + WG * x;
+        if (!act || e >= D::NN) continue;
+        const int m = e / N, n = e % N;
+        double2 a = make_double2(0, 0);
+#pragma unroll
+        for (int l = 0; l < N; ++l) cfma(a, herm<N>(w.H0, m, l), w.U[l * N + n]);
+        w.Tm[e] = a;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < D::NO; ++j) {
+        const int u = gl + WG * j;
+        if (!act || u >= D::NU) continue;
+        const int m = gh.ut[u][0], n = gh.ut[u][1];
+        double2 a = make_double2(0, 0);
+#pragma unroll
+        for (int l = 0; l < N; ++l) cfmac(a, w.U[l * N + m], w.Tm[l * N + n]);
+        if (m == n) a.y = 0.0;
+        w.B[u] = a;
+    }
+    __syncwarp();
+}
+
+// |offdiag(B)|^2 <= tol2 |diag(B)|^2 of the group's k-point (group-uniform);
+// full-mask shuffles: every lane of the warp must call it
+template <int N>
+__device__ __forceinline__ bool g_diagonal(const double2 *B, const GHead &gh, int gl, double tol2)
+{
+    using D = GDim<N>;
+    double off = 0.0, dia = 0.0;
+    for (int u = gl; u < D::NU; u += WG) {
+        const double v = B[u].x * B[u].x + B[u].y * B[u].y;
+        if (gh.ut[u][0] == gh.ut[u][1]) dia += v;
+        else off += 2.0 * v;
+    }
+    return grp_sum(off) <= tol2 * grp_sum(dia);
+}
+
+// One perturbative step of the eigenbasis for the groups with `act`: with
+// X_mn = B_mn / (B_nn - B_mm) (m != n; anti-Hermitian, the first-order
+// rotation that diagonalises B = U^dag H0 U) and x = max |X_mn|:
+//   x <= xfin:  U <- U exp(X) to second order, which finishes the tracking
+//               (an O(x^2) error, as g_track's first-order finish) -> 1;
+//   x <= 1e-2:  U <- U exp(X) to fourth order (unitary to O(x^5)) -> 2, and
+//               B must be formed again;
+//   otherwise (or a zero gap): nothing changes -> 3 (Jacobi sweeps needed).
+// exp(X) is applied as U + UX + (UX)X/2 + ..., products with X only; the
+// scratch matrix holds the running product.  B is left stale.  Returns 0 for
+// groups without `act`.  Group-uniform result; all lanes call it.
+template <class RF, int N>
+__device__ __forceinline__ int g_pstep(const GView<RF> &w, const GHead &gh, int gl, double xfin, bool act)
+{
+    using D = GDim<N>;
+    double xm = 0.0, zero_gap = 0.0;
+    if (act) {
+        for (int u = gl; u < D::NU; u += WG) {
+            const int m = gh.ut[u][0], n = gh.ut[u][1];
+            if (m == n) {
+                w.Tm[m * N + m] = make_double2(0.0, 0.0);
+                continue;
+            }
+            const double d = w.B[pidx(n, n, N)].x - w.B[pidx(m, m, N)].x;
+            const double2 b = w.B[u];
+            double2 x = make_double2(0.0, 0.0);
+            if (b.x != 0.0 || b.y != 0.0) {
+                if (d == 0.0) {
+                    zero_gap = 1.0;
+                } else {
+                    const double id = 1.0 / d;
+                    x = make_double2(b.x * id, b.y * id);
+                    xm = fmax(xm, sqrt(x.x * x.x + x.y * x.y));
+                }
+            }
+            w.Tm[m * N + n] = x;
+            w.Tm[n * N + m] = make_double2(-x.x, x.y);
+        }
+    }
+    xm = grp_max(xm);
+    zero_gap = grp_max(zero_gap);
+    const int st = !act ? 0 : (zero_gap != 0.0 || !(xm <= 1e-2)) ? 3 : (xm <= xfin ? 1 : 2);
+    const bool go = st == 1 || st == 2;
+    const int nt = st == 2 ? 4 : 2;   // Taylor order of this group
+    __syncwarp();
+    double2 *Pb = reinterpret_cast<double2 *>(w.ph);   // running product
+    double2 acc[D::NF], q[D::NF];
+#pragma unroll
+    for (int x = 0; x < D::NF; ++x) {   // P1 = U X
+        const int e = gl + WG * x;
+        acc[x] = q[x] = make_double2(0, 0);
+        if (!go || e >= D::NN) continue;
+        const int m = e / N, n = e % N;
+        double2 a = make_double2(0, 0);
+#pragma unroll
+        for (int l = 0; l < N; ++l) cfma(a, w.U[m * N + l], w.Tm[l * N + n]);
+        q[x] = a;
+        acc[x] = make_double2(w.U[e].x + a.x, w.U[e].y + a.y);
+    }
+    const int tmax = __any_sync(WG_FULL, st == 2) ? 4 : 2;   // warp-uniform trip count
+#pragma unroll 1
+    for (int t = 2; t <= tmax; ++t) {   // P_t = P_{t-1} X / t
+        const bool on = go && t <= nt;
+#pragma unroll
+        for (int x = 0; x < D::NF; ++x) {
+            const int e = gl + WG * x;
+            if (on && e < D::NN) Pb[e] = q[x];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int x = 0; x < D::NF; ++x) {
+            const int e = gl + WG * x;
+            if (!on || e >= D::NN) continue;
+            const int m = e / N, n = e % N;
+            double2 a = make_double2(0, 0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) cfma(a, Pb[m * N + l], w.Tm[l * N + n]);
+            const double c = t == 2 ? 0.5 : (t == 3 ? 1.0 / 3.0 : 0.25);
+            q[x] = make_double2(a.x * c, a.y * c);
+            acc[x].x += q[x].x;
+            acc[x].y += q[x].y;
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int x = 0; x < D::NF; ++x) {
+        const int e = gl + WG * x;
+        if (go && e < D::NN) w.U[e] = acc[x];
+    }
+    __syncwarp();
+    return st;
+}
+
+// Eigenbasis tracking by perturbative steps (g_pstep) while B = U^dag H0 U is
+// not diagonal to tol2: a fourth-order step forms B again and repeats, a
+// second-order step finishes; groups whose rotation is not small (near-
+// degenerate bands) or that are not done after three rounds fall back on
+// Jacobi sweeps (g_track), which end in the same tolerances.
+template <class RF, int N>
+__device__ __forceinline__ void g_track_pert(const GView<RF> &w, const GHead &gh, int gl, double tol2, double xmax,
+                                             bool live)
+{
+    bool need = live, rest = false;
+#pragma unroll 1
+    for (int round = 0; round < 3; ++round) {
+        // every lane takes part in the group reduction (full-mask shuffles),
+        // whatever its group's state
+        const bool diag = g_diagonal<N>(w.B, gh, gl, tol2);
+        need = need && !diag;
+        if (!__any_sync(WG_FULL, need)) break;
+        const int st = g_pstep<RF, N>(w, gh, gl, xmax, need);
+        rest = rest || st == 3;
+        need = st == 2;
+        if (!__any_sync(WG_FULL, need)) break;
+        g_formB<RF, N>(w, gh, gl, need);
+    }
+    rest = rest || need;
+    if (__any_sync(WG_FULL, rest)) g_track<RF, N>(w, gh, gl, 6, tol2, xmax, rest);
+}
+
 template <class RF, int N, int RK>
 __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
     wan_attempt_g(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs,
@@ -498,13 +664,6 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 s1[j] = make_double2(sy.x, sy.y);
             }
             __syncwarp();
-            if (with_cur) {   // packed S_x into the phase buffer, which is no longer read
-#pragma unroll
-                for (int j = 0; j < D::NO; ++j) {
-                    const int u = gl + WG * j;
-                    if (u < D::NU) reinterpret_cast<T *>(w.ph)[u] = s0[j];
-                }
-            }
             // B = U^dag H0 U
 #pragma unroll
             for (int x = 0; x < D::NF; ++x) {
@@ -530,7 +689,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
             }
             __syncwarp();
             // eigenbasis tracking (tolerances as wan_attempt)
-            g_track<RF, N>(w, gh, gl, 6, F32 ? 1e-20 : 1e-30, F32 ? 1e-5 : 1e-7, live);
+            g_track_pert<RF, N>(w, gh, gl, F32 ? 1e-20 : 1e-30, F32 ? 1e-5 : 1e-7, live);
             if (gh.tab.c[s] == 1.0 && live) {
                 T *Uo = P.U[1 - buf] + (size_t)kc * D::NN;
                 for (int e = gl; e < D::NN; e += WG) Uo[e] = w.U[e];
@@ -555,11 +714,16 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
             }
             __syncwarp();
             if (with_cur) {
-                // S_y packed into B (free after the tracking)
+                // S_x packed into the phase buffer and S_y into B (both free
+                // after the Fourier sums and the tracking, which uses the
+                // phase buffer as scratch)
 #pragma unroll
                 for (int j = 0; j < D::NO; ++j) {
                     const int u = gl + WG * j;
-                    if (u < D::NU) w.B[u] = s1[j];
+                    if (u < D::NU) {
+                        reinterpret_cast<T *>(w.ph)[u] = s0[j];
+                        w.B[u] = s1[j];
+                    }
                 }
                 __syncwarp();
                 const T *Sx = reinterpret_cast<const T *>(w.ph), *Sy = w.B;
