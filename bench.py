@@ -242,6 +242,7 @@ def run_ours(args):
     ach_m = FLOPS_PER_KSTEP[4] * kst * len(kt_mixed) / (propm * 1e-3) / 1e12
     shapes = read_tune_cache()
     kpt_mixed = args.kpt or next((v["k_per_thread"] for k, v in shapes.items() if k.startswith("vg-mixed")), 2)
+    kpt_fp64 = args.kpt or next((v["k_per_thread"] for k, v in shapes.items() if k.startswith("vg-fp64")), 1)
     mixed_kernel = "propagate_vg_x2<4> (2 k-points per thread, packed f32x2)" if kpt_mixed == 2 \
         else "propagate_vg<float,4,1>"
 
@@ -261,7 +262,8 @@ def run_ours(args):
                      "frac": achieved / fp64_tf, "traffic": read_traffic("fp64"),
                      "peak_source": "measured FMA-chain microbenchmark on this GPU in this run "
                                     "(MEASURED_PEAKS.json has no FP64/FP32 figure)",
-                     "flops_per_kstep": FLOPS_PER_KSTEP[4], "kernel": "propagate_vg<double,4,1>",
+                     "flops_per_kstep": FLOPS_PER_KSTEP[4],
+                     "kernel": f"propagate_vg<double,4,{kpt_fp64}>",
                      "kernel_share": prop64 / (prop64 + red64)},
         "mixed": {"value": mixed_value, "unit": UNIT, "dtype": "f32 stages / f64 state and sums",
                   "ms_per_solve": statistics.mean(ms_mixed), "solves_per_hour": mixed_value / kst * 3600.0,
@@ -441,19 +443,50 @@ def run_wannier(args, stream, fp64_tf):
            "spectral_error": {"max_floor_1e-6": max(errs6), "max_floor_1e-8": max(errs8),
                               "vs": f"fp64 solves of the first {len(fp64_out)} seeds"}}
     if not args.no_cpu_baseline:
-        out["cpu_baseline"] = wannier_cpu_baseline(args.wannier_cycles, budget_s=args.cpu_seconds / 2)
+        out["cpu_baseline"] = wannier_cpu_baseline(args.wannier_cycles, budget_s=args.cpu_seconds / 2,
+                                                   grid=args.wannier_grid)
     return out
 
 
-def wannier_cpu_baseline(ncycles: float, budget_s: float):
-    """The C restatement of the reference's length-gauge propagation with the
-    Wannier model form, on all host cores, on a k-subgrid of the same model and
-    pulse sized to ~budget_s (the reference itself has no compiled Wannier
-    model)."""
-    from antelope_b200 import wannier
+def wannier_cpu_baseline(ncycles: float, budget_s: float, grid: int = 300):
+    """The reference's own propagation of the N = 6 model on all host cores:
+    the harness build (the reference's SBEs/laser code with the
+    SyntheticWannier material, oracle/make_harness.py) on ParaRange k-slices
+    of the same grid, model and pulse, one emulated rank per core, sized to
+    ~budget_s.  The reference has no adaptive integrator; its fixed-step
+    Fehlberg-5 takes the same six stages per step as a Cash-Karp attempt, and
+    at tol 1e-8 the Cash-Karp runs take one attempt per output step, so the
+    work per k-point step is the same.  Without the harness build: the C
+    oracle on a k-subgrid (kind "port")."""
+    from antelope_b200 import cfgtext, wannier
     from oracle import pyoracle
 
     cores = os.cpu_count() or 1
+    if os.path.exists(pyoracle.HARNESS_EXE):
+        c = wannier.wannier_case(seed=1, n=grid, ncycles=ncycles, rk=None)
+        c["calc"]["RKorder"] = 5
+        del c["calc"]["precision"]
+        per_kstep = 2.7e-4                      # single-core seconds per k-point step, N = 6, length gauge
+        Nt_est = int(44129 * ncycles / 10.0) + 1
+        ntot = grid * grid
+        size = max(cores, int(ntot / max(1.0, budget_s / (Nt_est * per_kstep))))
+        with tempfile.TemporaryDirectory() as d:
+            with open(os.path.join(d, "inputParam.cfg"), "w") as f:
+                f.write(cfgtext.dumps(c))
+            t0 = time.perf_counter()
+            procs = [subprocess.Popen([pyoracle.HARNESS_EXE], cwd=d, stdout=subprocess.DEVNULL,
+                                      env=dict(os.environ, REF_RANK=str(r), REF_SIZE=str(size)))
+                     for r in range(cores)]
+            rc = [p.wait() for p in procs]
+            wall = time.perf_counter() - t0
+            with open(os.path.join(d, "outlaserdata.dat")) as f:
+                Nt = sum(1 for line in f if line.strip())
+        if any(rc):
+            raise RuntimeError(f"reference harness run failed: {rc}")
+        kdone = sum(ntot // size + (1 if ntot % size > r else 0) for r in range(cores))
+        return {"value": kdone * Nt / wall, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"reference harness build (Fehlberg-5), {cores} processes x 1 emulated rank of {size} "
+                          f"(ParaRange slices of the {grid}x{grid} grid, {kdone} k-points) x {Nt} steps"}
 
     def timed(g, cyc):
         c = wannier.wannier_case(seed=1, n=g, ncycles=cyc, rk="cashkarp45", tol=1e-8)
