@@ -90,6 +90,7 @@ struct GHead {
     double part[WG_WARPS][WAN_WARPS][WAN_NSLOT];
     double errw[WG_WARPS];
     WTab tab;
+    int gp[WAN_MAXR];   // lattice-vector index of each pair (R, -R)
     unsigned char ut[WAN_MAXU_][2];
     signed char mate[WAN_MAXN - 1][WAN_MAXN];
 };
@@ -103,9 +104,9 @@ __host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
     GSmem L;
     const size_t NU = (size_t)N * (N + 1) / 2, NN = (size_t)N * N, tf = 2 * (size_t)rf_bytes;
     L.cA = al16(sizeof(GHead));
-    L.Rc = L.cA + al16(6 * (size_t)nR * tf);
+    L.Rc = L.cA + al16(6 * (size_t)nR * tf);   // R of each lattice-vector pair
     L.tabs = L.Rc + al16((size_t)nR * 2 * rf_bytes);
-    const size_t row = (size_t)((N * (N + 1) / 2 + WG - 1) / WG) * 3 * WG;   // table entries per vector
+    const size_t row = (size_t)((N * (N + 1) / 2 + WG - 1) / WG) * 3 * 2 * WG;   // table entries per pair
     L.k0 = L.tabs + (SBE_WG_SMEM_TABLES ? al16((size_t)nR * row * tf) : 0);
     size_t o = 0;
     L.Y = o;  o += al16(NU * 16);
@@ -121,7 +122,9 @@ __host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
     L.js = o; o += al16((size_t)N * 8);
     L.je = o; o += al16((size_t)N * 16);
     L.dv = o; o += al16((size_t)N * 16);
-    L.kbytes = o;
+    // k-point regions 32 bytes past a multiple of 128: the four groups of a
+    // warp reading the same element of their matrices hit distinct banks
+    L.kbytes = (o + 127) / 128 * 128 + 32;
     L.total = L.k0 + (size_t)WG_WARPS * WAN_WARPS * L.kbytes;
     return L;
 }
@@ -332,32 +335,42 @@ __device__ __forceinline__ void g_track(const GView<RF> &w, const GHead &gh, int
     }
 }
 
-// B = U^dag H0 U (packed) for the groups with `act` (all lanes call it)
+// B = U^dag H0 U (packed) for the groups with `act` (all lanes call it).
+// Row m of each product is lane m's (m < N): lane m holds row m of H0 (then
+// column m of U) in registers and reads the other factor's element (l, n),
+// the same address for every lane of the group, so one shared-memory
+// wavefront serves the group's lanes instead of one load per lane and term.
 template <class RF, int N>
 __device__ __forceinline__ void g_formB(const GView<RF> &w, const GHead &gh, int gl, bool act)
 {
-    using D = GDim<N>;
+    const bool on = act && gl < N;
+    if (on) {
+        double2 hr[N];
 #pragma unroll
-    for (int x = 0; x < D::NF; ++x) {
-        const int e = gl + WG * x;
-        if (!act || e >= D::NN) continue;
-        const int m = e / N, n = e % N;
-        double2 a = make_double2(0, 0);
+        for (int l = 0; l < N; ++l) hr[l] = herm<N>(w.H0, gl, l);
 #pragma unroll
-        for (int l = 0; l < N; ++l) cfma(a, herm<N>(w.H0, m, l), w.U[l * N + n]);
-        w.Tm[e] = a;
+        for (int n = 0; n < N; ++n) {
+            double2 a = make_double2(0, 0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) cfma(a, hr[l], w.U[l * N + n]);
+            w.Tm[gl * N + n] = a;
+        }
     }
     __syncwarp();
+    if (on) {
+        double2 uc[N];
 #pragma unroll
-    for (int j = 0; j < D::NO; ++j) {
-        const int u = gl + WG * j;
-        if (!act || u >= D::NU) continue;
-        const int m = gh.ut[u][0], n = gh.ut[u][1];
-        double2 a = make_double2(0, 0);
+        for (int l = 0; l < N; ++l) uc[l] = w.U[l * N + gl];
+        const int row = pidx(gl, gl, N) - gl;
 #pragma unroll
-        for (int l = 0; l < N; ++l) cfmac(a, w.U[l * N + m], w.Tm[l * N + n]);
-        if (m == n) a.y = 0.0;
-        w.B[u] = a;
+        for (int n = 0; n < N; ++n) {
+            if (n < gl) continue;
+            double2 a = make_double2(0, 0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) cfmac(a, uc[l], w.Tm[l * N + n]);
+            if (n == gl) a.y = 0.0;
+            w.B[row + n] = a;
+        }
     }
     __syncwarp();
 }
@@ -385,86 +398,77 @@ __device__ __forceinline__ bool g_diagonal(const double2 *B, const GHead &gh, in
 //   x <= 1e-2:  U <- U exp(X) to fourth order (unitary to O(x^5)) -> 2, and
 //               B must be formed again;
 //   otherwise (or a zero gap): nothing changes -> 3 (Jacobi sweeps needed).
-// exp(X) is applied as U + UX + (UX)X/2 + ..., products with X only; the
-// scratch matrix holds the running product.  B is left stale.  Returns 0 for
-// groups without `act`.  Group-uniform result; all lanes call it.
+// Lane m (m < N) forms row m of X (scratch matrix) and row m of
+// U + UX + (UX)X/2 + ..., reading X by element (the same address for the
+// group's lanes).  B is left stale.  Returns 0 for groups
+// without `act`.  Group-uniform result; all lanes call it.
 template <class RF, int N>
 __device__ __forceinline__ int g_pstep(const GView<RF> &w, const GHead &gh, int gl, double xfin, bool act)
 {
-    using D = GDim<N>;
+    const bool on = act && gl < N;
     double xm = 0.0, zero_gap = 0.0;
-    if (act) {
-        for (int u = gl; u < D::NU; u += WG) {
-            const int m = gh.ut[u][0], n = gh.ut[u][1];
-            if (m == n) {
-                w.Tm[m * N + m] = make_double2(0.0, 0.0);
-                continue;
-            }
-            const double d = w.B[pidx(n, n, N)].x - w.B[pidx(m, m, N)].x;
-            const double2 b = w.B[u];
+    if (on) {
+        const double dm = w.B[pidx(gl, gl, N)].x;
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
             double2 x = make_double2(0.0, 0.0);
-            if (b.x != 0.0 || b.y != 0.0) {
-                if (d == 0.0) {
-                    zero_gap = 1.0;
-                } else {
-                    const double id = 1.0 / d;
-                    x = make_double2(b.x * id, b.y * id);
-                    xm = fmax(xm, sqrt(x.x * x.x + x.y * x.y));
+            if (n != gl) {
+                const double2 b = herm<N>(w.B, gl, n);
+                if (b.x != 0.0 || b.y != 0.0) {
+                    const double d = w.B[pidx(n, n, N)].x - dm;
+                    if (d == 0.0) {
+                        zero_gap = 1.0;
+                    } else {
+                        const double id = 1.0 / d;
+                        x = make_double2(b.x * id, b.y * id);
+                        xm = fmax(xm, sqrt(x.x * x.x + x.y * x.y));
+                    }
                 }
             }
-            w.Tm[m * N + n] = x;
-            w.Tm[n * N + m] = make_double2(-x.x, x.y);
+            w.Tm[gl * N + n] = x;
         }
     }
     xm = grp_max(xm);
     zero_gap = grp_max(zero_gap);
     const int st = !act ? 0 : (zero_gap != 0.0 || !(xm <= 1e-2)) ? 3 : (xm <= xfin ? 1 : 2);
-    const bool go = st == 1 || st == 2;
+    const bool go = (st == 1 || st == 2) && gl < N;
     const int nt = st == 2 ? 4 : 2;   // Taylor order of this group
     __syncwarp();
-    double2 *Pb = reinterpret_cast<double2 *>(w.ph);   // running product
-    double2 acc[D::NF], q[D::NF];
+    if (go) {
+        // row m of U X, then of (U X) X / 2, ...: each term's row is kept in
+        // the lane's own row of the scratch matrix and added to row m of U
+        double2 *Pb = reinterpret_cast<double2 *>(w.ph) + gl * N;
+        double2 *Um = w.U + gl * N;
+        {
+            double2 ur[N];
 #pragma unroll
-    for (int x = 0; x < D::NF; ++x) {   // P1 = U X
-        const int e = gl + WG * x;
-        acc[x] = q[x] = make_double2(0, 0);
-        if (!go || e >= D::NN) continue;
-        const int m = e / N, n = e % N;
-        double2 a = make_double2(0, 0);
+            for (int n = 0; n < N; ++n) ur[n] = Um[n];
 #pragma unroll
-        for (int l = 0; l < N; ++l) cfma(a, w.U[m * N + l], w.Tm[l * N + n]);
-        q[x] = a;
-        acc[x] = make_double2(w.U[e].x + a.x, w.U[e].y + a.y);
-    }
-    const int tmax = __any_sync(WG_FULL, st == 2) ? 4 : 2;   // warp-uniform trip count
+            for (int n = 0; n < N; ++n) {
+                double2 a = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) cfma(a, ur[l], w.Tm[l * N + n]);
+                Pb[n] = a;
+                Um[n] = make_double2(ur[n].x + a.x, ur[n].y + a.y);
+            }
+        }
 #pragma unroll 1
-    for (int t = 2; t <= tmax; ++t) {   // P_t = P_{t-1} X / t
-        const bool on = go && t <= nt;
-#pragma unroll
-        for (int x = 0; x < D::NF; ++x) {
-            const int e = gl + WG * x;
-            if (on && e < D::NN) Pb[e] = q[x];
-        }
-        __syncwarp();
-#pragma unroll
-        for (int x = 0; x < D::NF; ++x) {
-            const int e = gl + WG * x;
-            if (!on || e >= D::NN) continue;
-            const int m = e / N, n = e % N;
-            double2 a = make_double2(0, 0);
-#pragma unroll
-            for (int l = 0; l < N; ++l) cfma(a, Pb[m * N + l], w.Tm[l * N + n]);
+        for (int t = 2; t <= nt; ++t) {
             const double c = t == 2 ? 0.5 : (t == 3 ? 1.0 / 3.0 : 0.25);
-            q[x] = make_double2(a.x * c, a.y * c);
-            acc[x].x += q[x].x;
-            acc[x].y += q[x].y;
-        }
-        __syncwarp();
-    }
+            double2 qr[N];
 #pragma unroll
-    for (int x = 0; x < D::NF; ++x) {
-        const int e = gl + WG * x;
-        if (go && e < D::NN) w.U[e] = acc[x];
+            for (int l = 0; l < N; ++l) qr[l] = Pb[l];
+#pragma unroll
+            for (int n = 0; n < N; ++n) {
+                double2 a = make_double2(0, 0);
+#pragma unroll
+                for (int l = 0; l < N; ++l) cfma(a, qr[l], w.Tm[l * N + n]);
+                a = make_double2(a.x * c, a.y * c);
+                Pb[n] = a;
+                const double2 un = Um[n];
+                Um[n] = make_double2(un.x + a.x, un.y + a.y);
+            }
+        }
     }
     __syncwarp();
     return st;
@@ -495,6 +499,47 @@ __device__ __forceinline__ void g_track_pert(const GView<RF> &w, const GHead &gh
     }
     rest = rest || need;
     if (__any_sync(WG_FULL, rest)) g_track<RF, N>(w, gh, gl, 6, tol2, xmax, rest);
+}
+
+// Fourier sums of the lane's owned upper elements over the lattice-vector
+// pairs: quantity q (h, d_x, d_y; Q of them) accumulates c sig + s tau per
+// pair, e^{iKR} = c + i s; with CUR also S_a = sum R_a h_R e^{iKR}, whose pair
+// term is R_a (h_R e^{iKR} - h_-R e^{-iKR}) = R_a (c (-i tau) + s (i sig)).
+// All accumulator chains of a pair are independent, so the loads of one pair
+// and the multiply-adds of the previous one overlap.
+template <class RF, int N, int Q, bool CUR>
+__device__ __forceinline__ void g_fourier(const typename Cx<RF>::T *tb, int gstride, const typename Cx<RF>::T *ph,
+                                          const RF *Rp, int np, typename Cx<RF>::T (&a)[3][GDim<N>::NO],
+                                          typename Cx<RF>::T (&sx)[GDim<N>::NO], typename Cx<RF>::T (&sy)[GDim<N>::NO])
+{
+    using TF = typename Cx<RF>::T;
+    constexpr int NO = GDim<N>::NO;
+#pragma unroll 1
+    for (int p = 0; p < np; ++p) {
+        const TF e = ph[p];
+        const TF *tr = tb + (size_t)p * gstride;
+        RF rx = RF(0), ry = RF(0);
+        if (CUR) {
+            rx = Rp[2 * p];
+            ry = Rp[2 * p + 1];
+        }
+#pragma unroll
+        for (int j = 0; j < NO; ++j) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const TF sg = tr[(j * 3 + q) * 2 * WG], ta = tr[((j * 3 + q) * 2 + 1) * WG];
+                a[q][j].x = fma(e.x, sg.x, fma(e.y, ta.x, a[q][j].x));
+                a[q][j].y = fma(e.x, sg.y, fma(e.y, ta.y, a[q][j].y));
+                if (CUR && q == 0) {
+                    const RF ox = fma(e.x, ta.y, -e.y * sg.y), oy = fma(e.y, sg.x, -e.x * ta.x);
+                    sx[j].x = fma(rx, ox, sx[j].x);
+                    sx[j].y = fma(rx, oy, sx[j].y);
+                    sy[j].x = fma(ry, ox, sy[j].x);
+                    sy[j].y = fma(ry, oy, sy[j].y);
+                }
+            }
+        }
+    }
 }
 
 template <class RF, int N, int RK>
@@ -533,7 +578,13 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
         for (int r = 0; r < D::P - 1; ++r)
             for (int i = 0; i < N; ++i) gh.mate[r][i] = (signed char)rr_mate(i, r, D::P);
     }
-    load_lattice<RF>(P, Rc);
+    const int np = P.npair;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        const int r = P.gpair[i];
+        gh.gp[i] = r;
+        Rc[2 * i] = RF(P.V[2 * r]);
+        Rc[2 * i + 1] = RF(P.V[2 * r + 1]);
+    }
     const TF *cAg = static_cast<const TF *>(P.stage_cA);
     for (int i = threadIdx.x; i < S * nR; i += blockDim.x) cA[i] = cAg[i];
     for (int i = threadIdx.x; i < 36; i += blockDim.x) gh.AE[i / 6][i % 6] = P.stage_AE[i];
@@ -541,7 +592,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
     {
         TF *ts = reinterpret_cast<TF *>(smem_raw + L.tabs);
         const TF *tg = static_cast<const TF *>(P.gtab);
-        const int n = nR * D::NO * 3 * WG;
+        const int n = np * D::NO * 3 * 2 * WG;
         for (int i = threadIdx.x; i < n; i += blockDim.x) ts[i] = tg[i];
     }
 #endif
@@ -558,10 +609,11 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
         const GView<RF> w(smem_raw + L.k0 + (size_t)(wi * WAN_WARPS + grp) * L.kbytes, L);
         double kv[3], wk;
         kpoint(P, kc, kv, wk);
-        for (int r = gl; r < nR; r += WG) {
+        for (int q = gl; q < np; q += WG) {
+            const int r = gh.gp[q];
             double sn, cs;
             sincos(kv[0] * P.V[2 * r] + kv[1] * P.V[2 * r + 1], &sn, &cs);
-            w.pk[r] = cx<TF>(cs, sn);
+            w.pk[q] = cx<TF>(cs, sn);
         }
         const T *Ug = P.U[buf] + (size_t)kc * D::NN;
         for (int e = gl; e < D::NN; e += WG) w.U[e] = Ug[e];
@@ -585,7 +637,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
 #else
         const TF *gt = static_cast<const TF *>(P.gtab);
 #endif
-        const int gstride = D::NO * 3 * WG;   // table entries per lattice vector
+        const int gstride = D::NO * 3 * 2 * WG;   // table entries per lattice-vector pair
         const bool dip = P.has_dip;
         double emax = 0.0;
 #pragma unroll
@@ -607,109 +659,92 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 if (om[j] == on[j]) y.y = 0;
                 w.Y[u] = y;
             }
-            for (int r = gl; r < nR; r += WG) w.ph[r] = cmul(w.pk[r], cA[s * nR + r]);
+            for (int q = gl; q < np; q += WG) w.ph[q] = cmul(w.pk[q], cA[s * nR + gh.gp[q]]);
             __syncwarp();
             const bool with_cur = cur && s == 0;
             // Fourier sums of the owned elements: H0, D_x, D_y (and S_x, S_y)
             const double Ex = gh.AE[s][3], Ey = gh.AE[s][4];
             T d0[D::NO], d1[D::NO], s0[D::NO], s1[D::NO];
+            {
+                TF a[3][D::NO], sx[D::NO], sy[D::NO];
 #pragma unroll
-            for (int j = 0; j < D::NO; ++j) {
-                const int u = gl + WG * j;
-                d0[j] = d1[j] = s0[j] = s1[j] = make_double2(0, 0);
-                if (u >= D::NU) continue;
-                const TF *tb = gt + (size_t)(j * 3) * WG + gl;
-                TF a0 = cx<TF>(0, 0), a1 = cx<TF>(0, 0), a2 = cx<TF>(0, 0);
-                TF sx = cx<TF>(0, 0), sy = cx<TF>(0, 0);
-                if (with_cur) {
-                    for (int r = 0; r < nR; ++r) {
-                        const TF p = w.ph[r];
-                        const TF ph = cmul(tb[(size_t)r * gstride], p);
-                        a0.x += ph.x;
-                        a0.y += ph.y;
-                        sx.x = fma(Rc[2 * r], ph.x, sx.x);
-                        sx.y = fma(Rc[2 * r], ph.y, sx.y);
-                        sy.x = fma(Rc[2 * r + 1], ph.x, sy.x);
-                        sy.y = fma(Rc[2 * r + 1], ph.y, sy.y);
-                        if (dip) {
-                            cfma(a1, tb[(size_t)r * gstride + WG], p);
-                            cfma(a2, tb[(size_t)r * gstride + 2 * WG], p);
+                for (int j = 0; j < D::NO; ++j) a[0][j] = a[1][j] = a[2][j] = sx[j] = sy[j] = cx<TF>(0, 0);
+                const TF *tb = gt + gl;
+                if (with_cur) g_fourier<RF, N, 3, true>(tb, gstride, w.ph, Rc, np, a, sx, sy);
+                else if (dip) g_fourier<RF, N, 3, false>(tb, gstride, w.ph, Rc, np, a, sx, sy);
+                else g_fourier<RF, N, 1, false>(tb, gstride, w.ph, Rc, np, a, sx, sy);
+#pragma unroll
+                for (int j = 0; j < D::NO; ++j) {
+                    const int u = gl + WG * j;
+                    const T v0 = make_double2(a[0][j].x, a[0][j].y), v1 = make_double2(a[1][j].x, a[1][j].y),
+                            v2 = make_double2(a[2][j].x, a[2][j].y);
+                    d0[j] = v1;
+                    d1[j] = v2;
+                    s0[j] = make_double2(sx[j].x, sx[j].y);
+                    s1[j] = make_double2(sy[j].x, sy[j].y);
+                    if (u >= D::NU) continue;
+                    w.H0[u] = v0;
+                    w.HT[u] = make_double2(fma(Ex, v1.x, fma(Ey, v2.x, v0.x)), fma(Ex, v1.y, fma(Ey, v2.y, v0.y)));
+                }
+            }
+            __syncwarp();
+            // total current at the output step: computed before the tracking,
+            // which needs no D_a, so D_a leaves the registers early
+            double tot[2] = {0.0, 0.0};
+            if (with_cur) {
+                // total: Re Tr(Y J_a), J_a = -i S_a + i [D_a, H0], over the owned
+                // upper elements: diagonal Y_mm Im(S_mm) - Im(C_mm) Re(D_mm),
+                // off-diagonal -2 Im(Y_mn conj(S_mn)) - 2 Im(C_mn conj(D_mn)),
+                // C = [H0, Y]
+#pragma unroll
+                for (int j = 0; j < D::NO; ++j) {
+                    const int u = gl + WG * j;
+                    if (u >= D::NU) continue;
+                    const int m = om[j], n = on[j];
+                    T c = make_double2(0, 0);
+#pragma unroll
+                    for (int l = 0; l < N; ++l) {
+                        cfma(c, herm<N>(w.H0, m, l), herm<N>(w.Y, l, n));
+                        const T t2 = cmul(herm<N>(w.Y, m, l), herm<N>(w.H0, l, n));
+                        c.x -= t2.x;
+                        c.y -= t2.y;
+                    }
+                    const T y = w.Y[u];
+#pragma unroll
+                    for (int a = 0; a < 2; ++a) {
+                        const T sv = a == 0 ? s0[j] : s1[j];
+                        const T dd = a == 0 ? d0[j] : d1[j];
+                        if (m == n) {
+                            tot[a] += y.x * sv.y - c.y * dd.x;
+                        } else {
+                            // Im(z conj(w)) = z.y w.x - z.x w.y
+                            tot[a] -= 2.0 * (y.y * sv.x - y.x * sv.y) + 2.0 * (c.y * dd.x - c.x * dd.y);
                         }
                     }
-                } else if (dip) {
-                    for (int r = 0; r < nR; ++r) {
-                        const TF p = w.ph[r];
-                        const TF *tr = tb + (size_t)r * gstride;
-                        cfma(a0, tr[0], p);
-                        cfma(a1, tr[WG], p);
-                        cfma(a2, tr[2 * WG], p);
-                    }
-                } else {
-                    TF b0 = cx<TF>(0, 0);
-                    int r = 0;
-                    for (; r + 2 <= nR; r += 2) {
-                        cfma(a0, tb[(size_t)r * gstride], w.ph[r]);
-                        cfma(b0, tb[(size_t)(r + 1) * gstride], w.ph[r + 1]);
-                    }
-                    if (r < nR) cfma(a0, tb[(size_t)r * gstride], w.ph[r]);
-                    a0.x += b0.x;
-                    a0.y += b0.y;
                 }
-                const T v0 = make_double2(a0.x, a0.y), v1 = make_double2(a1.x, a1.y), v2 = make_double2(a2.x, a2.y);
-                w.H0[u] = v0;
-                w.HT[u] = make_double2(fma(Ex, v1.x, fma(Ey, v2.x, v0.x)), fma(Ex, v1.y, fma(Ey, v2.y, v0.y)));
-                d0[j] = v1;
-                d1[j] = v2;
-                s0[j] = make_double2(sx.x, sx.y);
-                s1[j] = make_double2(sy.x, sy.y);
             }
-            __syncwarp();
             // B = U^dag H0 U
-#pragma unroll
-            for (int x = 0; x < D::NF; ++x) {
-                const int e = gl + WG * x;
-                if (e >= D::NN) continue;
-                const int m = e / N, n = e % N;
-                T a = make_double2(0, 0);
-#pragma unroll
-                for (int l = 0; l < N; ++l) cfma(a, herm<N>(w.H0, m, l), w.U[l * N + n]);
-                w.Tm[e] = a;
-            }
-            __syncwarp();
-#pragma unroll
-            for (int j = 0; j < D::NO; ++j) {
-                const int u = gl + WG * j;
-                if (u >= D::NU) continue;
-                const int m = om[j], n = on[j];
-                T a = make_double2(0, 0);
-#pragma unroll
-                for (int l = 0; l < N; ++l) cfmac(a, w.U[l * N + m], w.Tm[l * N + n]);
-                if (m == n) a.y = 0.0;
-                w.B[u] = a;
-            }
-            __syncwarp();
+            g_formB<RF, N>(w, gh, gl, true);
             // eigenbasis tracking (tolerances as wan_attempt)
             g_track_pert<RF, N>(w, gh, gl, F32 ? 1e-20 : 1e-30, F32 ? 1e-5 : 1e-7, live);
             if (gh.tab.c[s] == 1.0 && live) {
                 T *Uo = P.U[1 - buf] + (size_t)kc * D::NN;
                 for (int e = gl; e < D::NN; e += WG) Uo[e] = w.U[e];
             }
-            // dv = diag(U^dag Y U)
-#pragma unroll
-            for (int x = 0; x < D::NF; ++x) {
-                const int e = gl + WG * x;
-                if (e >= D::NN) continue;
-                const int m = e / N, n = e % N;
-                T a = make_double2(0, 0);
-#pragma unroll
-                for (int l = 0; l < N; ++l) cfma(a, herm<N>(w.Y, m, l), w.U[l * N + n]);
-                w.Tm[e] = a;
-            }
-            __syncwarp();
+            // dv = diag(U^dag Y U): lane n forms (Y U)_ln from column n of U
+            // and reads Y by element (the same address for the group's lanes)
             if (gl < N) {
+                T uc[N];
+#pragma unroll
+                for (int l = 0; l < N; ++l) uc[l] = w.U[l * N + gl];
                 T a = make_double2(0, 0);
 #pragma unroll
-                for (int l = 0; l < N; ++l) cfmac(a, w.U[l * N + gl], w.Tm[l * N + gl]);
+                for (int l = 0; l < N; ++l) {
+                    T t = make_double2(0, 0);
+#pragma unroll
+                    for (int p = 0; p < N; ++p) cfma(t, herm<N>(w.Y, l, p), uc[p]);
+                    cfmac(a, uc[l], t);
+                }
                 w.dv[gl] = a;
             }
             __syncwarp();
@@ -727,37 +762,6 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 }
                 __syncwarp();
                 const T *Sx = reinterpret_cast<const T *>(w.ph), *Sy = w.B;
-                // total: Re Tr(Y J_a), J_a = -i S_a + i [D_a, H0], over the owned
-                // upper elements: diagonal Y_mm Im(S_mm) - Im(C_mm) Re(D_mm),
-                // off-diagonal -2 Im(Y_mn conj(S_mn)) - 2 Im(C_mn conj(D_mn)),
-                // C = [H0, Y]
-                double tot[2] = {0.0, 0.0};
-#pragma unroll
-                for (int j = 0; j < D::NO; ++j) {
-                    const int u = gl + WG * j;
-                    if (u >= D::NU) continue;
-                    const int m = om[j], n = on[j];
-                    T c = make_double2(0, 0);
-#pragma unroll
-                    for (int l = 0; l < N; ++l) {
-                        cfma(c, herm<N>(w.H0, m, l), herm<N>(w.Y, l, n));
-                        const T t2 = cmul(herm<N>(w.Y, m, l), herm<N>(w.H0, l, n));
-                        c.x -= t2.x;
-                        c.y -= t2.y;
-                    }
-                    const T y = w.Y[u];
-#pragma unroll
-                    for (int a = 0; a < 2; ++a) {
-                        const T sv = (a == 0 ? Sx : Sy)[u];
-                        const T dd = a == 0 ? d0[j] : d1[j];
-                        if (m == n) {
-                            tot[a] += y.x * sv.y - c.y * dd.x;
-                        } else {
-                            // Im(z conj(w)) = z.y w.x - z.x w.y
-                            tot[a] -= 2.0 * (y.y * sv.x - y.x * sv.y) + 2.0 * (c.y * dd.x - c.x * dd.y);
-                        }
-                    }
-                }
                 // intraband: sum_n Re[dv_n (U^dag (-i S_a) U)_nn]; tasks (a, n)
                 double intra[2] = {0.0, 0.0};
                 for (int t = gl; t < 2 * N; t += WG) {
@@ -794,30 +798,46 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 __syncwarp();
             }
             // right-hand side of the owned elements: -i((HY) - (HY)^dag)
-            // - (g2 Y + (g1 - g2) U diag(dv) U^dag)   (SBEs.h:808-861)
+            // - (g2 Y + (g1 - g2) U diag(dv) U^dag)   (SBEs.h:808-861).  Lane m
+            // forms row m of HY (scratch matrix) and of U diag(dv) U^dag (phase
+            // buffer, free after the currents) with the second factor read by
+            // element; then each lane combines its owned elements.
             const double g1 = P.g1, g2 = P.g2;
+            const bool deph = g1 != 0.0 || g2 != 0.0;
+            T *Pr = reinterpret_cast<T *>(w.ph);
+            if (gl < N) {
+                T hr[N];
+#pragma unroll
+                for (int l = 0; l < N; ++l) hr[l] = herm<N>(w.HT, gl, l);
+#pragma unroll
+                for (int n = 0; n < N; ++n) {
+                    T a = make_double2(0, 0);
+#pragma unroll
+                    for (int l = 0; l < N; ++l) cfma(a, hr[l], herm<N>(w.Y, l, n));
+                    w.Tm[gl * N + n] = a;
+                }
+                if (deph) {
+#pragma unroll
+                    for (int p = 0; p < N; ++p) hr[p] = cmul(w.U[gl * N + p], w.dv[p]);
+#pragma unroll
+                    for (int n = 0; n < N; ++n) {
+                        T a = make_double2(0, 0);
+#pragma unroll
+                        for (int p = 0; p < N; ++p) cfma(a, hr[p], cconj(w.U[n * N + p]));
+                        Pr[gl * N + n] = a;
+                    }
+                }
+            }
+            __syncwarp();
 #pragma unroll
             for (int j = 0; j < D::NO; ++j) {
                 const int u = gl + WG * j;
                 if (u >= D::NU) continue;
                 const int m = om[j], n = on[j];
-                T c = make_double2(0, 0), c2 = make_double2(0, 0);
-#pragma unroll
-                for (int l = 0; l < N; ++l) {
-                    cfma(c, herm<N>(w.HT, m, l), herm<N>(w.Y, l, n));
-                    cfma(c2, herm<N>(w.HT, n, l), herm<N>(w.Y, l, m));
-                }
-                c.x -= c2.x;
-                c.y += c2.y;
-                T kv2 = make_double2(c.y, -c.x);
-                if (g1 != 0.0 || g2 != 0.0) {
-                    T pr = make_double2(0, 0);
-#pragma unroll
-                    for (int p = 0; p < N; ++p) {
-                        const T t2 = cmul(w.U[m * N + p], w.dv[p]);
-                        cfma(pr, t2, cconj(w.U[n * N + p]));
-                    }
-                    const T y = w.Y[u];
+                const T c = w.Tm[m * N + n], c2 = w.Tm[n * N + m];
+                T kv2 = make_double2(c.y + c2.y, -(c.x - c2.x));
+                if (deph) {
+                    const T pr = Pr[m * N + n], y = w.Y[u];
                     kv2.x -= g2 * y.x + (g1 - g2) * pr.x;
                     kv2.y -= g2 * y.y + (g1 - g2) * pr.y;
                 }

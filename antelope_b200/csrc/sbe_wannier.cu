@@ -1621,7 +1621,7 @@ bool wan_grouped_applies(const WanDev &w)
     return (w.rk == 4 || w.rk == 5 || w.rk == 45) && g_smem(w.N, w.nR, 8).total <= 227 * 1024;
 }
 bool wan_grouped(const WanDev &w) { return w.gtab != nullptr && wan_grouped_applies(w); }
-int wan_gtab_row(int N) { return ((N * (N + 1) / 2 + WG - 1) / WG) * 3 * WG; }
+int wan_gtab_row(int N) { return ((N * (N + 1) / 2 + WG - 1) / WG) * 3 * 2 * WG; }
 
 template <class RF, int N> static WanKernel wan_attempt_g_rk(int rk)
 {

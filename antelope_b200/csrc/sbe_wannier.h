@@ -64,8 +64,13 @@ struct WanDev {
     const void *d;          // [nR][2][N*N] complex, same precision (or null)
     const void *jt;         // [nR][2][N*N] current-operator tables, same precision (or null:
                             // J_a = -dH/dk_a + i[D_a, H])
-    const void *gtab;       // h and d re-laid for the grouped attempt kernel, [nR][NO][3][8]
-                            // complex (NO = ceil(N(N+1)/2 / 8)), same precision; null: not used
+    // h and d re-laid for the grouped attempt kernel by lattice-vector pairs
+    // (R, -R): [npair][NO][3][2][8] complex (NO = ceil(N(N+1)/2 / 8)), the pair
+    // sum h_R + h_-R and i (h_R - h_-R) of quantity q (h, d_x, d_y) of upper
+    // element l + 8 j; same precision; null: not used
+    const void *gtab;
+    const int *gpair;       // [npair] index of each pair's vector R (the other is -R)
+    int npair;
     double2 *rho[2];        // [nk][N*N] committed / trial state (Wannier basis, full matrix), FP64
     double2 *U[2];          // [nk][N*N] tracked eigenbasis of H0(k+A), FP64
     double *weight;         // [nk]
@@ -118,7 +123,7 @@ size_t wan_smem_bytes(int N, int nR, int precision);
 constexpr int WAN_GROUP_TILES = 4;
 bool wan_grouped_applies(const WanDev &w);
 bool wan_grouped(const WanDev &w);
-// entries of the re-laid table per lattice vector (complex numbers)
+// entries of the re-laid table per lattice-vector pair (complex numbers)
 int wan_gtab_row(int N);
 cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st);
 cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st);

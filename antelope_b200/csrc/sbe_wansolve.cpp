@@ -100,32 +100,64 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     w_.h = h;
     w_.d = d;
     w_.jt = j;
-    // the tables re-laid for the grouped attempt kernel: entry (r, j, q, l) is
-    // quantity q (h, d_x, d_y) of upper element u = l + 8 j, zero past the
-    // triangle or without dipoles
+    // the tables re-laid for the grouped attempt kernel.  The lattice vectors
+    // are taken in pairs (R, -R) (a vector without its negative, R = 0
+    // included, stands alone): h_R e^{iKR} + h_-R e^{-iKR} = c sig + s tau
+    // with e^{iKR} = c + i s, sig = h_R + h_-R and tau = i (h_R - h_-R), half
+    // the multiplications of the two terms.  Entry (p, j, q, 0|1, l) holds sig
+    // or tau of quantity q (h, d_x, d_y) of upper element u = l + 8 j, zero
+    // past the triangle or without dipoles.
     std::vector<double> gt;
+    std::vector<int> gpair;
     if (wan_grouped_applies(w_)) {
         const int NU = N * (N + 1) / 2, NO = (NU + 7) / 8, row = wan_gtab_row(N), nR = w_.nR;
-        gt.assign((size_t)nR * row * 2, 0.0);
+        std::vector<int> mate(nR, -1);
+        std::vector<char> used(nR, 0);
+        for (int r = 0; r < nR; ++r) {
+            if (used[r]) continue;
+            used[r] = 1;
+            for (int r2 = r + 1; r2 < nR; ++r2)
+                if (!used[r2] && p.w_vec[2 * r2] == -p.w_vec[2 * r] && p.w_vec[2 * r2 + 1] == -p.w_vec[2 * r + 1]) {
+                    mate[r] = r2;
+                    used[r2] = 1;
+                    break;
+                }
+            gpair.push_back(r);
+        }
+        const int np = (int)gpair.size();
+        gt.assign((size_t)np * row * 2, 0.0);
         std::vector<int> um(NU), un(NU);
         for (int m = 0, u = 0; m < N; ++m)
             for (int n = m; n < N; ++n, ++u) { um[u] = m; un[u] = n; }
-        for (int r = 0; r < nR; ++r)
+        auto entry = [&](int q, int r, int u, double &re, double &im) {
+            const size_t src = q == 0 ? ((size_t)(r * N + um[u]) * N + un[u]) * 2
+                                      : ((size_t)((r * 2 + q - 1) * N + um[u]) * N + un[u]) * 2;
+            const std::vector<double> &tab = q == 0 ? p.w_h : p.w_d;
+            re = tab[src];
+            im = tab[src + 1];
+        };
+        for (int pi = 0; pi < np; ++pi)
             for (int jj = 0; jj < NO; ++jj)
                 for (int q = 0; q < 3; ++q)
                     for (int l = 0; l < 8; ++l) {
                         const int u = l + 8 * jj;
                         if (u >= NU || (q > 0 && !w_.has_dip)) continue;
-                        const size_t src = q == 0 ? ((size_t)(r * N + um[u]) * N + un[u]) * 2
-                                                  : ((size_t)((r * 2 + q - 1) * N + um[u]) * N + un[u]) * 2;
-                        const std::vector<double> &tab = q == 0 ? p.w_h : p.w_d;
-                        const size_t dst = ((((size_t)r * NO + jj) * 3 + q) * 8 + l) * 2;
-                        gt[dst] = tab[src];
-                        gt[dst + 1] = tab[src + 1];
+                        double a, b, a2 = 0.0, b2 = 0.0;
+                        entry(q, gpair[pi], u, a, b);
+                        if (mate[gpair[pi]] >= 0) entry(q, mate[gpair[pi]], u, a2, b2);
+                        const size_t dst = (((((size_t)pi * NO + jj) * 3 + q) * 2) * 8 + l) * 2;
+                        gt[dst] = a + a2;                 // sig
+                        gt[dst + 1] = b + b2;
+                        gt[dst + 16] = -(b - b2);         // tau = i (h_R - h_-R)
+                        gt[dst + 17] = a - a2;
                     }
         void *g = nullptr;
+        int *gp = nullptr;
         dalloc(&g, cplx * gt.size() / 2, st, "alloc grouped tables");
+        dalloc(&gp, sizeof(int) * np, st, "alloc lattice-vector pairs");
         w_.gtab = g;
+        w_.gpair = gp;
+        w_.npair = np;
     }
     UploadRing &ring = UploadRing::shared();
     if (!p.w_vec.empty()) ring.upload(V, p.w_vec.data(), sizeof(double) * p.w_vec.size(), st);
@@ -141,6 +173,7 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     if (w_.has_dip) up_real(d, p.w_d);
     if (w_.has_jtab && !w_.cont) up_real(j, p.w_j);
     if (w_.gtab) up_real(const_cast<void *>(w_.gtab), gt);
+    if (w_.gpair) ring.upload(const_cast<int *>(w_.gpair), gpair.data(), sizeof(int) * gpair.size(), st);
     cuda_check(cudaMemsetAsync(w_.jout, 0, sizeof(double) * (size_t)w_.Nt * WAN_NSLOT, st), "clear outputs");
     // initial controller state: t = t_min, h = dt, currents first
     WanCtl c{};
@@ -172,6 +205,7 @@ WannierSolve::~WannierSolve()
     if (w_.d) cudaFreeAsync((void *)w_.d, stream_);
     if (w_.jt) cudaFreeAsync((void *)w_.jt, stream_);
     if (w_.gtab) cudaFreeAsync((void *)w_.gtab, stream_);
+    if (w_.gpair) cudaFreeAsync((void *)w_.gpair, stream_);
     for (int b = 0; b < 2; ++b) {
         cudaFreeAsync(w_.rho[b], stream_);
         cudaFreeAsync(w_.U[b], stream_);
