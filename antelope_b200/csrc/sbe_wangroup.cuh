@@ -97,8 +97,11 @@ struct GHead {
 struct GSmem {
     size_t cA, Rc, tabs, k0, kbytes, total;
     // offsets inside a k-point region
-    size_t Y, H0, HT, B, U, Tm, pk, ph, jc, js, je, dv;
+    size_t Y, H0, HT, B, U, Tm, pk, ph, dv;
 };
+// lattice-vector pairs the per-k phase arrays hold: a grouped solve's vectors
+// come in pairs (R, -R) but for at most one (R = 0)
+__host__ __device__ constexpr int g_npair_cap(int nR) { return nR / 2 + 1; }
 __host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
 {
     GSmem L;
@@ -115,12 +118,11 @@ __host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
     L.B = o;  o += al16(NU * 16);
     L.U = o;  o += al16(NN * 16);
     L.Tm = o; o += al16(NN * 16);
-    L.pk = o; o += al16((size_t)nR * tf);
-    // also S_x (packed) at current steps and a full scratch matrix of the tracker
-    L.ph = o; o += al16(std::max((size_t)nR * tf, NN * 16));
-    L.jc = o; o += al16((size_t)N * 8);
-    L.js = o; o += al16((size_t)N * 8);
-    L.je = o; o += al16((size_t)N * 16);
+    const size_t np = (size_t)g_npair_cap(nR);
+    L.pk = o; o += al16(np * tf);
+    // the stage phases; also S_x (packed) at current steps, the tracker's
+    // full scratch matrix and the rotations of a Jacobi round (c, s, phase)
+    L.ph = o; o += al16(std::max(np * tf, std::max(NN * 16, (size_t)WAN_MAXN * 32)));
     L.dv = o; o += al16((size_t)N * 16);
     // k-point regions 32 bytes past a multiple of 128: the four groups of a
     // warp reading the same element of their matrices hit distinct banks
@@ -144,9 +146,9 @@ template <class RF> struct GView {
         Tm = reinterpret_cast<double2 *>(b + L.Tm);
         pk = reinterpret_cast<TF *>(b + L.pk);
         ph = reinterpret_cast<TF *>(b + L.ph);
-        jc = reinterpret_cast<double *>(b + L.jc);
-        js = reinterpret_cast<double *>(b + L.js);
-        je = reinterpret_cast<double2 *>(b + L.je);
+        jc = reinterpret_cast<double *>(b + L.ph);
+        js = jc + WAN_MAXN;
+        je = reinterpret_cast<double2 *>(js + WAN_MAXN);
         dv = reinterpret_cast<double2 *>(b + L.dv);
     }
 };
@@ -395,8 +397,8 @@ __device__ __forceinline__ bool g_diagonal(const double2 *B, const GHead &gh, in
 // rotation that diagonalises B = U^dag H0 U) and x = max |X_mn|:
 //   x <= xfin:  U <- U exp(X) to second order, which finishes the tracking
 //               (an O(x^2) error, as g_track's first-order finish) -> 1;
-//   x <= 1e-2:  U <- U exp(X) to fourth order (unitary to O(x^5)) -> 2, and
-//               B must be formed again;
+//   x <= 1e-2:  U <- U exp(X) to third order for x <= 5e-4, else to fourth
+//               (unitary to 3e-15 or O(x^5)) -> 2, and B must be formed again;
 //   otherwise (or a zero gap): nothing changes -> 3 (Jacobi sweeps needed).
 // Lane m (m < N) forms row m of X (scratch matrix) and row m of
 // U + UX + (UX)X/2 + ..., reading X by element (the same address for the
@@ -432,7 +434,9 @@ __device__ __forceinline__ int g_pstep(const GView<RF> &w, const GHead &gh, int 
     zero_gap = grp_max(zero_gap);
     const int st = !act ? 0 : (zero_gap != 0.0 || !(xm <= 1e-2)) ? 3 : (xm <= xfin ? 1 : 2);
     const bool go = (st == 1 || st == 2) && gl < N;
-    const int nt = st == 2 ? 4 : 2;   // Taylor order of this group
+    // Taylor order of this group: a finishing step 2; a larger step 3 while
+    // its truncation, |X|^4 / 24, stays below 3e-15, else 4
+    const int nt = st == 2 ? (xm <= 5e-4 ? 3 : 4) : 2;
     __syncwarp();
     if (go) {
         // row m of U X, then of (U X) X / 2, ...: each term's row is kept in
@@ -619,17 +623,15 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
         for (int e = gl; e < D::NN; e += WG) w.U[e] = Ug[e];
         const double2 *rho = P.rho[buf] + (size_t)kc * D::NN;
         T r64[D::NO];
-        int om[D::NO], on[D::NO];
+        // row and column of the owned upper element j (read from the block's
+        // table when needed rather than held in registers)
+        auto om = [&](int j) { return (int)gh.ut[min(gl + WG * j, D::NU - 1)][0]; };
+        auto on = [&](int j) { return (int)gh.ut[min(gl + WG * j, D::NU - 1)][1]; };
 #pragma unroll
         for (int j = 0; j < D::NO; ++j) {
             const int u = gl + WG * j;
-            om[j] = on[j] = 0;
             r64[j] = make_double2(0, 0);
-            if (u < D::NU) {
-                om[j] = gh.ut[u][0];
-                on[j] = gh.ut[u][1];
-                r64[j] = rho[om[j] * N + on[j]];
-            }
+            if (u < D::NU) r64[j] = rho[om(j) * N + on(j)];
         }
         T ks[S][D::NO];
 #if SBE_WG_SMEM_TABLES
@@ -656,7 +658,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                         y.y = fma(a, ks[i][j].y, y.y);
                     }
                 }
-                if (om[j] == on[j]) y.y = 0;
+                if (om(j) == on(j)) y.y = 0;
                 w.Y[u] = y;
             }
             for (int q = gl; q < np; q += WG) w.ph[q] = cmul(w.pk[q], cA[s * nR + gh.gp[q]]);
@@ -695,20 +697,27 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 // total: Re Tr(Y J_a), J_a = -i S_a + i [D_a, H0], over the owned
                 // upper elements: diagonal Y_mm Im(S_mm) - Im(C_mm) Re(D_mm),
                 // off-diagonal -2 Im(Y_mn conj(S_mn)) - 2 Im(C_mn conj(D_mn)),
-                // C = [H0, Y]
+                // C = [H0, Y] = H0 Y - (H0 Y)^dag; lane m forms row m of H0 Y
+                if (gl < N) {
+                    T hr[N];
+#pragma unroll
+                    for (int l = 0; l < N; ++l) hr[l] = herm<N>(w.H0, gl, l);
+#pragma unroll
+                    for (int n = 0; n < N; ++n) {
+                        T a = make_double2(0, 0);
+#pragma unroll
+                        for (int l = 0; l < N; ++l) cfma(a, hr[l], herm<N>(w.Y, l, n));
+                        w.Tm[gl * N + n] = a;
+                    }
+                }
+                __syncwarp();
 #pragma unroll
                 for (int j = 0; j < D::NO; ++j) {
                     const int u = gl + WG * j;
                     if (u >= D::NU) continue;
-                    const int m = om[j], n = on[j];
-                    T c = make_double2(0, 0);
-#pragma unroll
-                    for (int l = 0; l < N; ++l) {
-                        cfma(c, herm<N>(w.H0, m, l), herm<N>(w.Y, l, n));
-                        const T t2 = cmul(herm<N>(w.Y, m, l), herm<N>(w.H0, l, n));
-                        c.x -= t2.x;
-                        c.y -= t2.y;
-                    }
+                    const int m = om(j), n = on(j);
+                    const T c1 = w.Tm[m * N + n], c2 = w.Tm[n * N + m];
+                    const T c = make_double2(c1.x - c2.x, c1.y + c2.y);
                     const T y = w.Y[u];
 #pragma unroll
                     for (int a = 0; a < 2; ++a) {
@@ -722,6 +731,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                         }
                     }
                 }
+                __syncwarp();
             }
             // B = U^dag H0 U
             g_formB<RF, N>(w, gh, gl, true);
@@ -731,27 +741,12 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 T *Uo = P.U[1 - buf] + (size_t)kc * D::NN;
                 for (int e = gl; e < D::NN; e += WG) Uo[e] = w.U[e];
             }
-            // dv = diag(U^dag Y U): lane n forms (Y U)_ln from column n of U
-            // and reads Y by element (the same address for the group's lanes)
-            if (gl < N) {
-                T uc[N];
-#pragma unroll
-                for (int l = 0; l < N; ++l) uc[l] = w.U[l * N + gl];
-                T a = make_double2(0, 0);
-#pragma unroll
-                for (int l = 0; l < N; ++l) {
-                    T t = make_double2(0, 0);
-#pragma unroll
-                    for (int p = 0; p < N; ++p) cfma(t, herm<N>(w.Y, l, p), uc[p]);
-                    cfmac(a, uc[l], t);
-                }
-                w.dv[gl] = a;
-            }
-            __syncwarp();
+            // dv = diag(U^dag Y U) and, at an output step, the intraband
+            // current sum_n Re[dv_n (U^dag (-i S_a) U)_nn]: lane n holds column n
+            // of U and reads Y (S_a) by element, the same address for the
+            // group's lanes.  S_x goes packed into the phase buffer and S_y into
+            // B, both free after the tracking.
             if (with_cur) {
-                // S_x packed into the phase buffer and S_y into B (both free
-                // after the Fourier sums and the tracking, which uses the
-                // phase buffer as scratch)
 #pragma unroll
                 for (int j = 0; j < D::NO; ++j) {
                     const int u = gl + WG * j;
@@ -761,24 +756,40 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                     }
                 }
                 __syncwarp();
-                const T *Sx = reinterpret_cast<const T *>(w.ph), *Sy = w.B;
-                // intraband: sum_n Re[dv_n (U^dag (-i S_a) U)_nn]; tasks (a, n)
-                double intra[2] = {0.0, 0.0};
-                for (int t = gl; t < 2 * N; t += WG) {
-                    const int a = t / N, n = t % N;
-                    const T *Sa = a == 0 ? Sx : Sy;
-                    T pn = make_double2(0, 0);
+            }
+            double intra[2] = {0.0, 0.0};
+            if (gl < N) {
+                T uc[N];
 #pragma unroll
-                    for (int l = 0; l < N; ++l) {
-                        T q = make_double2(0, 0);   // (S U)_ln
+                for (int l = 0; l < N; ++l) uc[l] = w.U[l * N + gl];
+                T dvn = make_double2(0, 0);
 #pragma unroll
-                        for (int p = 0; p < N; ++p) cfma(q, aherm<N>(Sa, l, p), w.U[p * N + n]);
-                        cfmac(pn, w.U[l * N + n], q);
-                    }
-                    // -i pn
-                    const T mj = make_double2(pn.y, -pn.x);
-                    intra[a] += w.dv[n].x * mj.x - w.dv[n].y * mj.y;
+                for (int l = 0; l < N; ++l) {
+                    T t = make_double2(0, 0);
+#pragma unroll
+                    for (int p = 0; p < N; ++p) cfma(t, herm<N>(w.Y, l, p), uc[p]);
+                    cfmac(dvn, uc[l], t);
                 }
+                w.dv[gl] = dvn;
+                if (with_cur) {
+#pragma unroll
+                    for (int a = 0; a < 2; ++a) {
+                        const T *Sa = a == 0 ? reinterpret_cast<const T *>(w.ph) : w.B;
+                        T pn = make_double2(0, 0);
+#pragma unroll
+                        for (int l = 0; l < N; ++l) {
+                            T q = make_double2(0, 0);   // (S U)_ln
+#pragma unroll
+                            for (int p = 0; p < N; ++p) cfma(q, aherm<N>(Sa, l, p), uc[p]);
+                            cfmac(pn, uc[l], q);
+                        }
+                        // Re[dv_n (-i pn)]
+                        intra[a] = dvn.x * pn.y + dvn.y * pn.x;
+                    }
+                }
+            }
+            __syncwarp();
+            if (with_cur) {
                 double *val = gh.part[wi][grp];
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
@@ -833,7 +844,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
             for (int j = 0; j < D::NO; ++j) {
                 const int u = gl + WG * j;
                 if (u >= D::NU) continue;
-                const int m = om[j], n = on[j];
+                const int m = om(j), n = on(j);
                 const T c = w.Tm[m * N + n], c2 = w.Tm[n * N + m];
                 T kv2 = make_double2(c.y + c2.y, -(c.x - c2.x));
                 if (deph) {
@@ -866,7 +877,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 }
             }
             double2 v = make_double2(r64[j].x + inc.x, r64[j].y + inc.y);
-            const int m = om[j], n = on[j];
+            const int m = om(j), n = on(j);
             if (m == n) v.y = 0.0;
             if (live) {
                 rout[m * N + n] = v;

@@ -1622,6 +1622,7 @@ bool wan_grouped_applies(const WanDev &w)
 }
 bool wan_grouped(const WanDev &w) { return w.gtab != nullptr && wan_grouped_applies(w); }
 int wan_gtab_row(int N) { return ((N * (N + 1) / 2 + WG - 1) / WG) * 3 * 2 * WG; }
+int wan_npair_cap(int nR) { return g_npair_cap(nR); }
 
 template <class RF, int N> static WanKernel wan_attempt_g_rk(int rk)
 {

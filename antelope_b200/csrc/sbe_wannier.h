@@ -125,6 +125,9 @@ bool wan_grouped_applies(const WanDev &w);
 bool wan_grouped(const WanDev &w);
 // entries of the re-laid table per lattice-vector pair (complex numbers)
 int wan_gtab_row(int N);
+// lattice-vector pairs (R, -R) a grouped solve may have (its vectors pair up
+// but for R = 0)
+int wan_npair_cap(int nR);
 cudaError_t launch_wan_init(const WanDev &w, int precision, cudaStream_t st);
 cudaError_t launch_wan_prepare(const WanDev *dw, int precision, cudaStream_t st);
 cudaError_t launch_wan_attempt(const WanDev &w, const WanDev *dw, int precision, cudaStream_t st);

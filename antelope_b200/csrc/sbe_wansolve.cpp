@@ -108,10 +108,9 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
     // or tau of quantity q (h, d_x, d_y) of upper element u = l + 8 j, zero
     // past the triangle or without dipoles.
     std::vector<double> gt;
-    std::vector<int> gpair;
+    std::vector<int> gpair, mate(w_.nR, -1);
     if (wan_grouped_applies(w_)) {
-        const int NU = N * (N + 1) / 2, NO = (NU + 7) / 8, row = wan_gtab_row(N), nR = w_.nR;
-        std::vector<int> mate(nR, -1);
+        const int nR = w_.nR;
         std::vector<char> used(nR, 0);
         for (int r = 0; r < nR; ++r) {
             if (used[r]) continue;
@@ -124,6 +123,12 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
                 }
             gpair.push_back(r);
         }
+        // more vectors without their negatives than R = 0: the grouped
+        // kernel's per-k phase arrays are sized for pairs, wan_attempt runs it
+        if ((int)gpair.size() > wan_npair_cap(nR)) gpair.clear();
+    }
+    if (!gpair.empty()) {
+        const int NU = N * (N + 1) / 2, NO = (NU + 7) / 8, row = wan_gtab_row(N);
         const int np = (int)gpair.size();
         gt.assign((size_t)np * row * 2, 0.0);
         std::vector<int> um(NU), un(NU);
