@@ -29,14 +29,16 @@
 // -dH/dk + i[D, H], BaseMaterial.h:62-68) at N = 4 and 6; other models and
 // band counts run on wan_attempt.
 
-// Tuning: resident blocks per SM the registers are sized for, and whether
-// the re-laid tables are staged in shared memory (one copy per block) or
-// read through L1 (measured equal on the N = 6 configuration).
+// Tuning: resident blocks per SM the registers are sized for.  (Tables
+// staged in shared memory, one copy per block, measured no faster than
+// reading them through L1 and leave room for fewer blocks.)
 #ifndef SBE_WG_MINB
 #define SBE_WG_MINB 3
 #endif
-#ifndef SBE_WG_SMEM_TABLES
-#define SBE_WG_SMEM_TABLES 0
+// |X|^2 up to which the plain method's larger tracking steps are second
+// order (then U is restored to unitary once per attempt); 0: fourth order
+#ifndef SBE_WG_X2_LOW
+#define SBE_WG_X2_LOW 1e-6
 #endif
 constexpr int WG = 8;          // lanes per k-point
 constexpr int WG_WARPS = 4;    // warps per block (tiles per block)
@@ -95,7 +97,7 @@ struct GHead {
     signed char mate[WAN_MAXN - 1][WAN_MAXN];
 };
 struct GSmem {
-    size_t cA, Rc, tabs, k0, kbytes, total;
+    size_t cA, Rc, k0, kbytes, total;
     // offsets inside a k-point region
     size_t Y, H0, HT, B, U, Tm, pk, ph, dv;
 };
@@ -108,9 +110,7 @@ __host__ __device__ inline GSmem g_smem(int N, int nR, int rf_bytes)
     const size_t NU = (size_t)N * (N + 1) / 2, NN = (size_t)N * N, tf = 2 * (size_t)rf_bytes;
     L.cA = al16(sizeof(GHead));
     L.Rc = L.cA + al16(6 * (size_t)nR * tf);   // R of each lattice-vector pair
-    L.tabs = L.Rc + al16((size_t)nR * 2 * rf_bytes);
-    const size_t row = (size_t)((N * (N + 1) / 2 + WG - 1) / WG) * 3 * 2 * WG;   // table entries per pair
-    L.k0 = L.tabs + (SBE_WG_SMEM_TABLES ? al16((size_t)nR * row * tf) : 0);
+    L.k0 = L.Rc + al16((size_t)nR * 2 * rf_bytes);
     size_t o = 0;
     L.Y = o;  o += al16(NU * 16);
     L.H0 = o; o += al16(NU * 16);
@@ -350,29 +350,76 @@ __device__ __forceinline__ void g_formB(const GView<RF> &w, const GHead &gh, int
         double2 hr[N];
 #pragma unroll
         for (int l = 0; l < N; ++l) hr[l] = herm<N>(w.H0, gl, l);
+        // the whole row first, then its stores: a store between the loads
+        // would keep the compiler from overlapping the rows' chains
+        double2 a[N];
 #pragma unroll
         for (int n = 0; n < N; ++n) {
-            double2 a = make_double2(0, 0);
+            a[n] = make_double2(0, 0);
 #pragma unroll
-            for (int l = 0; l < N; ++l) cfma(a, hr[l], w.U[l * N + n]);
-            w.Tm[gl * N + n] = a;
+            for (int l = 0; l < N; ++l) cfma(a[n], hr[l], w.U[l * N + n]);
         }
+#pragma unroll
+        for (int n = 0; n < N; ++n) w.Tm[gl * N + n] = a[n];
     }
     __syncwarp();
     if (on) {
-        double2 uc[N];
+        double2 uc[N], a[N];
 #pragma unroll
         for (int l = 0; l < N; ++l) uc[l] = w.U[l * N + gl];
         const int row = pidx(gl, gl, N) - gl;
 #pragma unroll
         for (int n = 0; n < N; ++n) {
+            a[n] = make_double2(0, 0);
             if (n < gl) continue;
-            double2 a = make_double2(0, 0);
 #pragma unroll
-            for (int l = 0; l < N; ++l) cfmac(a, uc[l], w.Tm[l * N + n]);
-            if (n == gl) a.y = 0.0;
-            w.B[row + n] = a;
+            for (int l = 0; l < N; ++l) cfmac(a[n], uc[l], w.Tm[l * N + n]);
         }
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            if (n < gl) continue;
+            if (n == gl) a[n].y = 0.0;
+            w.B[row + n] = a[n];
+        }
+    }
+    __syncwarp();
+}
+
+// U <- U (3I - U^dag U) / 2 (one Newton-Schulz step): with U^dag U = I + F
+// the result has U^dag U = I + O(F^2), which removes the unitarity defect
+// that second-order rotation steps leave (|X|^4 / 4 each).  Rows as in
+// g_formB; all lanes call it.
+template <class RF, int N>
+__device__ __forceinline__ void g_orthonormalize(const GView<RF> &w, int gl)
+{
+    __syncwarp();
+    if (gl < N) {
+        double2 uc[N], a[N];
+#pragma unroll
+        for (int l = 0; l < N; ++l) uc[l] = w.U[l * N + gl];
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            a[n] = make_double2(0, 0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) cfmac(a[n], uc[l], w.U[l * N + n]);
+        }
+#pragma unroll
+        for (int n = 0; n < N; ++n)   // (3I - U^dag U) / 2, row gl
+            w.Tm[gl * N + n] = make_double2((n == gl ? 1.5 : 0.0) - 0.5 * a[n].x, -0.5 * a[n].y);
+    }
+    __syncwarp();
+    if (gl < N) {
+        double2 ur[N], a[N];
+#pragma unroll
+        for (int l = 0; l < N; ++l) ur[l] = w.U[gl * N + l];
+#pragma unroll
+        for (int n = 0; n < N; ++n) {
+            a[n] = make_double2(0, 0);
+#pragma unroll
+            for (int l = 0; l < N; ++l) cfma(a[n], ur[l], w.Tm[l * N + n]);
+        }
+#pragma unroll
+        for (int n = 0; n < N; ++n) w.U[gl * N + n] = a[n];
     }
     __syncwarp();
 }
@@ -397,18 +444,20 @@ __device__ __forceinline__ bool g_diagonal(const double2 *B, const GHead &gh, in
 // rotation that diagonalises B = U^dag H0 U) and x = max |X_mn|:
 //   x <= xfin:  U <- U exp(X) to second order, which finishes the tracking
 //               (an O(x^2) error, as g_track's first-order finish) -> 1;
-//   x <= 1e-2:  U <- U exp(X) to third order for x <= 5e-4, else to fourth
-//               (unitary to 3e-15 or O(x^5)) -> 2, and B must be formed again;
+//   x <= 1e-2:  U <- U exp(X) to second order if x^2 <= x2_low, else to
+//               fourth (unitary to x^4 / 4 or O(x^6)) -> 2, and B must be
+//               formed again;
 //   otherwise (or a zero gap): nothing changes -> 3 (Jacobi sweeps needed).
 // Lane m (m < N) forms row m of X (scratch matrix) and row m of
 // U + UX + (UX)X/2 + ..., reading X by element (the same address for the
 // group's lanes).  B is left stale.  Returns 0 for groups
 // without `act`.  Group-uniform result; all lanes call it.
 template <class RF, int N>
-__device__ __forceinline__ int g_pstep(const GView<RF> &w, const GHead &gh, int gl, double xfin, bool act)
+__device__ __forceinline__ int g_pstep(const GView<RF> &w, const GHead &gh, int gl, double xfin, double x2_low,
+                                       bool act)
 {
     const bool on = act && gl < N;
-    double xm = 0.0, zero_gap = 0.0;
+    double xm2 = 0.0, zero_gap = 0.0;   // max |X_mn|^2
     if (on) {
         const double dm = w.B[pidx(gl, gl, N)].x;
 #pragma unroll
@@ -416,61 +465,53 @@ __device__ __forceinline__ int g_pstep(const GView<RF> &w, const GHead &gh, int 
             double2 x = make_double2(0.0, 0.0);
             if (n != gl) {
                 const double2 b = herm<N>(w.B, gl, n);
-                if (b.x != 0.0 || b.y != 0.0) {
-                    const double d = w.B[pidx(n, n, N)].x - dm;
-                    if (d == 0.0) {
-                        zero_gap = 1.0;
-                    } else {
-                        const double id = 1.0 / d;
-                        x = make_double2(b.x * id, b.y * id);
-                        xm = fmax(xm, sqrt(x.x * x.x + x.y * x.y));
-                    }
+                const double d = w.B[pidx(n, n, N)].x - dm;
+                if (d != 0.0) {
+                    const double id = 1.0 / d;
+                    x = make_double2(b.x * id, b.y * id);
+                    xm2 = fmax(xm2, x.x * x.x + x.y * x.y);
+                } else if (b.x != 0.0 || b.y != 0.0) {
+                    zero_gap = 1.0;
                 }
             }
             w.Tm[gl * N + n] = x;
         }
     }
-    xm = grp_max(xm);
+    xm2 = grp_max(xm2);
     zero_gap = grp_max(zero_gap);
-    const int st = !act ? 0 : (zero_gap != 0.0 || !(xm <= 1e-2)) ? 3 : (xm <= xfin ? 1 : 2);
+    const int st = !act ? 0 : (zero_gap != 0.0 || !(xm2 <= 1e-4)) ? 3 : (xm2 <= xfin * xfin ? 1 : 2);
     const bool go = (st == 1 || st == 2) && gl < N;
-    // Taylor order of this group: a finishing step 2; a larger step 3 while
-    // its truncation, |X|^4 / 24, stays below 3e-15, else 4
-    const int nt = st == 2 ? (xm <= 5e-4 ? 3 : 4) : 2;
+    // Taylor order of this group: a finishing step 2, a larger step 2 or 4.
+    // With X anti-Hermitian the truncated series E of order 2 has
+    // E^dag E = I + X^4 / 4 and of order 4 I + O(X^6): U stays unitary to that,
+    // a defect no later rotation removes (orders are even for that reason)
+    const int nt = st == 2 && !(xm2 <= x2_low) ? 4 : 2;
     __syncwarp();
     if (go) {
         // row m of U X, then of (U X) X / 2, ...: each term's row is kept in
-        // the lane's own row of the scratch matrix and added to row m of U
+        // the lane's own row of the scratch matrix and added to row m of U; a
+        // row is formed whole before its stores
         double2 *Pb = reinterpret_cast<double2 *>(w.ph) + gl * N;
         double2 *Um = w.U + gl * N;
-        {
-            double2 ur[N];
-#pragma unroll
-            for (int n = 0; n < N; ++n) ur[n] = Um[n];
-#pragma unroll
-            for (int n = 0; n < N; ++n) {
-                double2 a = make_double2(0, 0);
-#pragma unroll
-                for (int l = 0; l < N; ++l) cfma(a, ur[l], w.Tm[l * N + n]);
-                Pb[n] = a;
-                Um[n] = make_double2(ur[n].x + a.x, ur[n].y + a.y);
-            }
-        }
 #pragma unroll 1
-        for (int t = 2; t <= nt; ++t) {
-            const double c = t == 2 ? 0.5 : (t == 3 ? 1.0 / 3.0 : 0.25);
-            double2 qr[N];
+        for (int t = 1; t <= nt; ++t) {
+            const double c = t == 1 ? 1.0 : t == 2 ? 0.5 : (t == 3 ? 1.0 / 3.0 : 0.25);
+            const double2 *src = t == 1 ? Um : Pb;
+            double2 qr[N], a[N];
 #pragma unroll
-            for (int l = 0; l < N; ++l) qr[l] = Pb[l];
+            for (int l = 0; l < N; ++l) qr[l] = src[l];
 #pragma unroll
             for (int n = 0; n < N; ++n) {
-                double2 a = make_double2(0, 0);
+                a[n] = make_double2(0, 0);
 #pragma unroll
-                for (int l = 0; l < N; ++l) cfma(a, qr[l], w.Tm[l * N + n]);
-                a = make_double2(a.x * c, a.y * c);
-                Pb[n] = a;
-                const double2 un = Um[n];
-                Um[n] = make_double2(un.x + a.x, un.y + a.y);
+                for (int l = 0; l < N; ++l) cfma(a[n], qr[l], w.Tm[l * N + n]);
+            }
+#pragma unroll
+            for (int n = 0; n < N; ++n) {
+                const double2 q = make_double2(a[n].x * c, a[n].y * c);
+                const double2 un = t == 1 ? qr[n] : Um[n];
+                Pb[n] = q;
+                Um[n] = make_double2(un.x + q.x, un.y + q.y);
             }
         }
     }
@@ -495,7 +536,10 @@ __device__ __forceinline__ void g_track_pert(const GView<RF> &w, const GHead &gh
         const bool diag = g_diagonal<N>(w.B, gh, gl, tol2);
         need = need && !diag;
         if (!__any_sync(WG_FULL, need)) break;
-        const int st = g_pstep<RF, N>(w, gh, gl, xmax, need);
+        // second-order steps up to |X| = 1e-3 (unitary to 2.5e-13; the plain
+        // method restores unitarity once per attempt) or, in the mixed
+        // method, whose tolerance is looser, up to 1e-2; fourth order above
+        const int st = g_pstep<RF, N>(w, gh, gl, xmax, std::is_same<RF, float>::value ? 1e-4 : SBE_WG_X2_LOW, need);
         rest = rest || st == 3;
         need = st == 2;
         if (!__any_sync(WG_FULL, need)) break;
@@ -503,6 +547,24 @@ __device__ __forceinline__ void g_track_pert(const GView<RF> &w, const GHead &gh
     }
     rest = rest || need;
     if (__any_sync(WG_FULL, rest)) g_track<RF, N>(w, gh, gl, 6, tol2, xmax, rest);
+}
+
+// Table loads through the read-only path with the L1 eviction priority
+// evict_last: the re-laid tables (about 44 KB in FP64 at N = 6, 37 vectors)
+// are read by every stage of every k-point and should stay in the L1 that
+// the blocks' shared memory leaves, while the per-k state streams past it
+// (loaded and stored at the L2 only).
+__device__ __forceinline__ double2 g_ldtab(const double2 *p)
+{
+    double2 v;
+    asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float2 g_ldtab(const float2 *p)
+{
+    float2 v;
+    asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
 }
 
 // Fourier sums of the lane's owned upper elements over the lattice-vector
@@ -531,7 +593,7 @@ __device__ __forceinline__ void g_fourier(const typename Cx<RF>::T *tb, int gstr
         for (int j = 0; j < NO; ++j) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
-                const TF sg = tr[(j * 3 + q) * 2 * WG], ta = tr[((j * 3 + q) * 2 + 1) * WG];
+                const TF sg = g_ldtab(tr + (j * 3 + q) * 2 * WG), ta = g_ldtab(tr + ((j * 3 + q) * 2 + 1) * WG);
                 a[q][j].x = fma(e.x, sg.x, fma(e.y, ta.x, a[q][j].x));
                 a[q][j].y = fma(e.x, sg.y, fma(e.y, ta.y, a[q][j].y));
                 if (CUR && q == 0) {
@@ -592,14 +654,6 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
     const TF *cAg = static_cast<const TF *>(P.stage_cA);
     for (int i = threadIdx.x; i < S * nR; i += blockDim.x) cA[i] = cAg[i];
     for (int i = threadIdx.x; i < 36; i += blockDim.x) gh.AE[i / 6][i % 6] = P.stage_AE[i];
-#if SBE_WG_SMEM_TABLES
-    {
-        TF *ts = reinterpret_cast<TF *>(smem_raw + L.tabs);
-        const TF *tg = static_cast<const TF *>(P.gtab);
-        const int n = np * D::NO * 3 * 2 * WG;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) ts[i] = tg[i];
-    }
-#endif
     for (int q = threadIdx.x; q < WG_WARPS * WAN_WARPS * WAN_NSLOT; q += blockDim.x)
         (&gh.part[0][0][0])[q] = 0.0;
     if (threadIdx.x < WG_WARPS) gh.errw[threadIdx.x] = 0.0;
@@ -620,7 +674,8 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
             w.pk[q] = cx<TF>(cs, sn);
         }
         const T *Ug = P.U[buf] + (size_t)kc * D::NN;
-        for (int e = gl; e < D::NN; e += WG) w.U[e] = Ug[e];
+        for (int e = gl; e < D::NN; e += WG) w.U[e] = __ldcg(Ug + e);
+        if (!F32 && SBE_WG_X2_LOW > 0.0) g_orthonormalize<RF, N>(w, gl);
         const double2 *rho = P.rho[buf] + (size_t)kc * D::NN;
         T r64[D::NO];
         // row and column of the owned upper element j (read from the block's
@@ -631,14 +686,10 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
         for (int j = 0; j < D::NO; ++j) {
             const int u = gl + WG * j;
             r64[j] = make_double2(0, 0);
-            if (u < D::NU) r64[j] = rho[om(j) * N + on(j)];
+            if (u < D::NU) r64[j] = __ldcg(rho + om(j) * N + on(j));
         }
         T ks[S][D::NO];
-#if SBE_WG_SMEM_TABLES
-        const TF *gt = reinterpret_cast<const TF *>(smem_raw + L.tabs);
-#else
         const TF *gt = static_cast<const TF *>(P.gtab);
-#endif
         const int gstride = D::NO * 3 * 2 * WG;   // table entries per lattice-vector pair
         const bool dip = P.has_dip;
         double emax = 0.0;
@@ -702,13 +753,15 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                     T hr[N];
 #pragma unroll
                     for (int l = 0; l < N; ++l) hr[l] = herm<N>(w.H0, gl, l);
+                    T a[N];
 #pragma unroll
                     for (int n = 0; n < N; ++n) {
-                        T a = make_double2(0, 0);
+                        a[n] = make_double2(0, 0);
 #pragma unroll
-                        for (int l = 0; l < N; ++l) cfma(a, hr[l], herm<N>(w.Y, l, n));
-                        w.Tm[gl * N + n] = a;
+                        for (int l = 0; l < N; ++l) cfma(a[n], hr[l], herm<N>(w.Y, l, n));
                     }
+#pragma unroll
+                    for (int n = 0; n < N; ++n) w.Tm[gl * N + n] = a[n];
                 }
                 __syncwarp();
 #pragma unroll
@@ -739,7 +792,7 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
             g_track_pert<RF, N>(w, gh, gl, F32 ? 1e-20 : 1e-30, F32 ? 1e-5 : 1e-7, live);
             if (gh.tab.c[s] == 1.0 && live) {
                 T *Uo = P.U[1 - buf] + (size_t)kc * D::NN;
-                for (int e = gl; e < D::NN; e += WG) Uo[e] = w.U[e];
+                for (int e = gl; e < D::NN; e += WG) __stcg(Uo + e, w.U[e]);
             }
             // dv = diag(U^dag Y U) and, at an output step, the intraband
             // current sum_n Re[dv_n (U^dag (-i S_a) U)_nn]: lane n holds column n
@@ -820,23 +873,26 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                 T hr[N];
 #pragma unroll
                 for (int l = 0; l < N; ++l) hr[l] = herm<N>(w.HT, gl, l);
+                T a[N];
 #pragma unroll
                 for (int n = 0; n < N; ++n) {
-                    T a = make_double2(0, 0);
+                    a[n] = make_double2(0, 0);
 #pragma unroll
-                    for (int l = 0; l < N; ++l) cfma(a, hr[l], herm<N>(w.Y, l, n));
-                    w.Tm[gl * N + n] = a;
+                    for (int l = 0; l < N; ++l) cfma(a[n], hr[l], herm<N>(w.Y, l, n));
                 }
+#pragma unroll
+                for (int n = 0; n < N; ++n) w.Tm[gl * N + n] = a[n];
                 if (deph) {
 #pragma unroll
                     for (int p = 0; p < N; ++p) hr[p] = cmul(w.U[gl * N + p], w.dv[p]);
 #pragma unroll
                     for (int n = 0; n < N; ++n) {
-                        T a = make_double2(0, 0);
+                        a[n] = make_double2(0, 0);
 #pragma unroll
-                        for (int p = 0; p < N; ++p) cfma(a, hr[p], cconj(w.U[n * N + p]));
-                        Pr[gl * N + n] = a;
+                        for (int p = 0; p < N; ++p) cfma(a[n], hr[p], cconj(w.U[n * N + p]));
                     }
+#pragma unroll
+                    for (int n = 0; n < N; ++n) Pr[gl * N + n] = a[n];
                 }
             }
             __syncwarp();
@@ -880,8 +936,8 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
             const int m = om(j), n = on(j);
             if (m == n) v.y = 0.0;
             if (live) {
-                rout[m * N + n] = v;
-                rout[n * N + m] = make_double2(v.x, -v.y);
+                __stcg(rout + m * N + n, v);
+                __stcg(rout + n * N + m, make_double2(v.x, -v.y));
                 emax = fmax(emax, sqrt(er.x * er.x + er.y * er.y));
             }
         }
