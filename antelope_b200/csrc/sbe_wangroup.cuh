@@ -608,6 +608,34 @@ __device__ __forceinline__ void g_fourier(const typename Cx<RF>::T *tb, int gstr
     }
 }
 
+// The same sums for H0 and E.D at a stage without currents: the second from
+// the stage's table of E_x d_x + E_y d_y (tT, [pair][j][half][lane]), so D_x
+// and D_y need no sums of their own.  (A table of h + E.D would give H0 + E.D
+// directly, but in the mixed method its single-precision rounding of h, not
+// of E.D, would then drive the field term: 3x the spectral error.)
+template <class RF, int N>
+__device__ __forceinline__ void g_fourier_ht(const typename Cx<RF>::T *tb, int gstride, const typename Cx<RF>::T *tT,
+                                             const typename Cx<RF>::T *ph, int np,
+                                             typename Cx<RF>::T (&a)[3][GDim<N>::NO])
+{
+    using TF = typename Cx<RF>::T;
+    constexpr int NO = GDim<N>::NO;
+#pragma unroll 1
+    for (int p = 0; p < np; ++p) {
+        const TF e = ph[p];
+        const TF *tr = tb + (size_t)p * gstride, *ts = tT + (size_t)p * NO * 2 * WG;
+#pragma unroll
+        for (int j = 0; j < NO; ++j) {
+            const TF sg = g_ldtab(tr + j * 3 * 2 * WG), ta = g_ldtab(tr + (j * 3 * 2 + 1) * WG);
+            const TF sT = g_ldtab(ts + j * 2 * WG), tT2 = g_ldtab(ts + (j * 2 + 1) * WG);
+            a[0][j].x = fma(e.x, sg.x, fma(e.y, ta.x, a[0][j].x));
+            a[0][j].y = fma(e.x, sg.y, fma(e.y, ta.y, a[0][j].y));
+            a[1][j].x = fma(e.x, sT.x, fma(e.y, tT2.x, a[1][j].x));
+            a[1][j].y = fma(e.x, sT.y, fma(e.y, tT2.y, a[1][j].y));
+        }
+    }
+}
+
 template <class RF, int N, int RK>
 __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
     wan_attempt_g(const WanDev *__restrict__ Pp, const WanDev *const *__restrict__ descs,
@@ -723,8 +751,14 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
 #pragma unroll
                 for (int j = 0; j < D::NO; ++j) a[0][j] = a[1][j] = a[2][j] = sx[j] = sy[j] = cx<TF>(0, 0);
                 const TF *tb = gt + gl;
+                // E.D from the stage's combined table where the currents need
+                // no D_a (dipole models)
+                const bool ht = !with_cur && dip && P.stage_gt != nullptr;
                 if (with_cur) g_fourier<RF, N, 3, true>(tb, gstride, w.ph, Rc, np, a, sx, sy);
-                else if (dip) g_fourier<RF, N, 3, false>(tb, gstride, w.ph, Rc, np, a, sx, sy);
+                else if (ht) {
+                    const TF *tT = static_cast<const TF *>(P.stage_gt) + (size_t)s * np * D::NO * 2 * WG + gl;
+                    g_fourier_ht<RF, N>(tb, gstride, tT, w.ph, np, a);
+                } else if (dip) g_fourier<RF, N, 3, false>(tb, gstride, w.ph, Rc, np, a, sx, sy);
                 else g_fourier<RF, N, 1, false>(tb, gstride, w.ph, Rc, np, a, sx, sy);
 #pragma unroll
                 for (int j = 0; j < D::NO; ++j) {
@@ -737,7 +771,8 @@ __global__ void __launch_bounds__(32 * WG_WARPS, SBE_WG_MINB)
                     s1[j] = make_double2(sy[j].x, sy[j].y);
                     if (u >= D::NU) continue;
                     w.H0[u] = v0;
-                    w.HT[u] = make_double2(fma(Ex, v1.x, fma(Ey, v2.x, v0.x)), fma(Ex, v1.y, fma(Ey, v2.y, v0.y)));
+                    w.HT[u] = ht ? make_double2(v0.x + v1.x, v0.y + v1.y)
+                                 : make_double2(fma(Ex, v1.x, fma(Ey, v2.x, v0.x)), fma(Ex, v1.y, fma(Ey, v2.y, v0.y)));
                 }
             }
             __syncwarp();

@@ -1298,6 +1298,22 @@ template <class RF> __device__ void prepare_stages(const WanDev &P, const WanCtl
         sincos(AE[s][0] * P.V[2 * r] + AE[s][1] * P.V[2 * r + 1], &sn, &cs);
         cA[s * P.nR + r] = cx<TF>(cs, sn);
     }
+    if (P.stage_gt) {
+        // the grouped kernel's per-stage table of E_x d_x + E_y d_y: entry
+        // (s, pair, j, half, l) from entries (pair, j, q, half, l) of the
+        // re-laid table (layout of WanDev::gtab)
+        const TF *g = static_cast<const TF *>(P.gtab);
+        TF *o = static_cast<TF *>(P.stage_gt);
+        const int NO = (P.N * (P.N + 1) / 2 + 7) / 8, per = P.npair * NO * 16;
+        for (int task = threadIdx.x; task < S * per; task += blockDim.x) {
+            const int s = task / per, e = task % per;
+            const int pj = e / 16, hl = e % 16;   // (pair, j), (half, lane)
+            const TF *src = g + (size_t)pj * 48 + hl;
+            const TF dx = src[16], dy = src[32];
+            const RF ex = RF(AE[s][3]), ey = RF(AE[s][4]);
+            o[(size_t)s * per + e] = cx<TF>(fma(ey, dy.x, ex * dx.x), fma(ey, dy.y, ex * dx.y));
+        }
+    }
 }
 
 template <class RF> __global__ void __launch_bounds__(256) wan_prepare(const WanDev *__restrict__ Pp)

@@ -71,6 +71,10 @@ struct WanDev {
     const void *gtab;
     const int *gpair;       // [npair] index of each pair's vector R (the other is -R)
     int npair;
+    // with dipoles, per stage of the next attempt the pair table of
+    // E_x(t_s) d_x + E_y(t_s) d_y ([6][npair][NO][2][8] complex, Fourier
+    // precision), whose sum is E.D in one sum; written by the controller
+    void *stage_gt;
     double2 *rho[2];        // [nk][N*N] committed / trial state (Wannier basis, full matrix), FP64
     double2 *U[2];          // [nk][N*N] tracked eigenbasis of H0(k+A), FP64
     double *weight;         // [nk]

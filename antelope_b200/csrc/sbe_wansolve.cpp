@@ -163,6 +163,11 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
         w_.gtab = g;
         w_.gpair = gp;
         w_.npair = np;
+        if (w_.has_dip) {
+            void *sg = nullptr;
+            dalloc(&sg, cplx * (size_t)6 * np * NO * 2 * 8, st, "alloc stage tables");
+            w_.stage_gt = sg;
+        }
     }
     UploadRing &ring = UploadRing::shared();
     if (!p.w_vec.empty()) ring.upload(V, p.w_vec.data(), sizeof(double) * p.w_vec.size(), st);
@@ -211,6 +216,7 @@ WannierSolve::~WannierSolve()
     if (w_.jt) cudaFreeAsync((void *)w_.jt, stream_);
     if (w_.gtab) cudaFreeAsync((void *)w_.gtab, stream_);
     if (w_.gpair) cudaFreeAsync((void *)w_.gpair, stream_);
+    if (w_.stage_gt) cudaFreeAsync(w_.stage_gt, stream_);
     for (int b = 0; b < 2; ++b) {
         cudaFreeAsync(w_.rho[b], stream_);
         cudaFreeAsync(w_.U[b], stream_);
@@ -417,7 +423,7 @@ size_t WannierPool::bytes_needed(const Problem &p, int precision)
     const size_t real = precision == 0 ? 8 : 4, cplx = 2 * real;
     const size_t ntiles = (nk + WAN_WARPS - 1) / WAN_WARPS;
     size_t b = 4 * nk * NN * 16 + nk * 8;                              // rho, U (two each), weights
-    b += nR * NN * cplx * 5 + nR * 16 + nR * 72 * cplx;                // h, d, current and re-laid tables, vectors
+    b += nR * NN * cplx * 5 + nR * 16 + nR * 216 * cplx;               // h, d, current, re-laid and stage tables, vectors
     b += ntiles * 8 * (1 + WAN_NSLOT) + (size_t)p.laser.Nt * WAN_NSLOT * 8;   // tile results, per-step sums
     if (p.gauge == GAUGE_VELOCITY) b += nk * N * 16 + nk * 3 * NN * 16;  // bands, momentum matrices
     return b + 4096;
