@@ -1310,8 +1310,8 @@ template <class RF> __device__ void prepare_stages(const WanDev &P, const WanCtl
             const int pj = e / 16, hl = e % 16;   // (pair, j), (half, lane)
             const TF *src = g + (size_t)pj * 48 + hl;
             const TF dx = src[16], dy = src[32];
-            const RF ex = RF(AE[s][3]), ey = RF(AE[s][4]);
-            o[(size_t)s * per + e] = cx<TF>(fma(ey, dy.x, ex * dx.x), fma(ey, dy.y, ex * dx.y));
+            const double ex = AE[s][3], ey = AE[s][4];   // in FP64, rounded once
+            o[(size_t)s * per + e] = cx<TF>(fma(ey, (double)dy.x, ex * (double)dx.x), fma(ey, (double)dy.y, ex * (double)dx.y));
         }
     }
 }
