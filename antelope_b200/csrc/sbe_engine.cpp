@@ -266,8 +266,10 @@ Shape Engine::shape_for(const Problem &p, const EngineOptions &o) const
         s.tile_k = threads * s.kpt;
     }
     s.threads = s.tile_k / s.kpt;
-    if (s.threads < 32 || s.threads > 256 || s.threads % 32 || s.tile_k % s.kpt)
-        throw CfgError("tile_k / kpt must be a multiple of 32 between 32 and 256");
+    const int tmax = propagate_max_threads(vg ? VAR_HALDANE_VG : VAR_HALDANE_LW, prec, p.rk, s.kpt);
+    if (s.threads < 32 || s.threads > tmax || s.threads % 32 || s.tile_k % s.kpt)
+        throw CfgError(tmax > 256 ? "tile_k / kpt must be a multiple of 32 between 32 and 512"
+                                  : "tile_k / kpt must be a multiple of 32 between 32 and 256");
     return s;
 }
 

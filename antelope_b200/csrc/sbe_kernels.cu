@@ -273,8 +273,10 @@ __device__ __forceinline__ void vg_rhs(const VgField<Real> &h, Real hc0, const R
 
 // RK4 fits in 128 registers without spilling (4 CTAs of 128 threads per SM
 // instead of 3 at the compiler's unbounded choice); Fehlberg-5 would spill.
+// RK4 CTAs may have up to 512 threads at the same 128 registers, so that the
+// autotuner can choose a tile count that fills the last wave of CTAs.
 template <class Real, int RK, int KPT, bool G1>
-__global__ void __launch_bounds__(256, RK == 4 ? 2 : 1) propagate_vg(const TileDev *__restrict__ tiles,
+__global__ void __launch_bounds__(RK == 4 ? 512 : 256, 1) propagate_vg(const TileDev *__restrict__ tiles,
                                                     const SolveDev *__restrict__ solves, int tick, int S)
 {
     using T2 = typename V2<Real>::T;
@@ -1487,10 +1489,20 @@ static cudaError_t launch_lw_x2_t(const LaunchArgs &la)
     SBE_CHECK_LAUNCH();
 }
 
+int propagate_max_threads(int variant, int precision, int rk, int kpt)
+{
+    // propagate_vg with RK4 (FP64, or one k-point per thread in FP32); the
+    // packed mixed kernels and the length gauge stage 8 warps at most
+    const bool vg_scalar = variant == VAR_HALDANE_VG && rk == 4 && (precision == PREC_FP64 || kpt == 1);
+    return vg_scalar ? 512 : 256;
+}
+
 cudaError_t launch_propagate(const LaunchArgs &la)
 {
     if (la.ntiles <= 0) return cudaSuccess;
-    if (la.threads <= 0 || la.threads > 256 || (la.threads & 31)) return cudaErrorInvalidValue;
+    if (la.threads <= 0 || la.threads > propagate_max_threads(la.variant, la.precision, la.rk, la.kpt) ||
+        (la.threads & 31))
+        return cudaErrorInvalidValue;
     const bool g1 = la.has_g1;
     if (la.variant == VAR_HALDANE_VG) {
 #define SBE_VG(R, RK)                                                       \

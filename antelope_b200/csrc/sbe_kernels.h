@@ -27,6 +27,8 @@ struct InitArgs {
     double Ef, dt;
 };
 
+// largest CTA (threads) the propagate kernel of a class of solves accepts
+int propagate_max_threads(int variant, int precision, int rk, int kpt);
 cudaError_t launch_propagate(const LaunchArgs &la);
 cudaError_t launch_reduce(const SolveDev *solves, const int *solve_ids, int nsolves, int tick, int S,
                           cudaStream_t stream);

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "sbe_engine.h"
+#include "sbe_kernels.h"
 
 namespace sbe {
 
@@ -105,13 +106,15 @@ Shape autotune_shape(int device, const Problem &p, int precision)
         if ((long long)threads * kpt > 2LL * nk && threads > 32) return;  // tiles far larger than the grid
         cand.push_back(Shape{threads * kpt, kpt, threads});
     };
-    // every CTA size in warps: the best one balances occupancy against the
-    // quantisation of the tile count into waves of resident CTAs
-    for (int t = 32; t <= 256; t += 32) addc(t, 1);
+    // every CTA size in warps the kernel accepts: the best one balances
+    // occupancy against the quantisation of the tile count into waves of
+    // resident CTAs
+    const int variant = vg ? VAR_HALDANE_VG : VAR_HALDANE_LW;
+    for (int t = 32; t <= propagate_max_threads(variant, precision, p.rk, 1); t += 32) addc(t, 1);
     // two k-points per thread: the FP64 velocity gauge and the packed mixed
     // kernels of both gauges
     if (vg || precision != PREC_FP64)
-        for (int t = 32; t <= 256; t += 32) addc(t, 2);
+        for (int t = 32; t <= propagate_max_threads(variant, precision, p.rk, 2); t += 32) addc(t, 2);
     Problem q = p;
     const int S = 128;
     q.laser.Nt = std::min(p.laser.Nt, 3 * S);

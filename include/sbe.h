@@ -56,7 +56,9 @@ typedef struct sbe_dims {
 
 /* Run options.  precision: -1 = calc.precision of the cfg (default fp64),
  * 0 = plain FP64, 1 = mixed FP32 stages / FP64 sums.  tile_k, k_per_thread,
- * steps_per_launch: 0 = tuned defaults.  use_graph: capture the launches of
+ * steps_per_launch: 0 = tuned defaults; tile_k / k_per_thread (threads per
+ * CTA) is a multiple of 32 up to 256, or up to 512 for the two-band velocity
+ * gauge with RK4 in FP64 or with one k-point per thread.  use_graph: capture the launches of
  * a run into one CUDA graph.  profile: see sbe_solver_kernel_times. */
 typedef struct sbe_opts {
     int device;
