@@ -211,3 +211,28 @@ def test_server_serves_nband_requests_beside_haldane():
     st = srv.stats()
     assert st["failed"] == 0 and st["completed"] == 2 * len(probs) and st["resident"] == 0
     srv.close()
+
+
+def with_zero_vectors(c, extra):
+    """The same model with lattice vectors `extra` added whose tables are zero."""
+    g = c["SyntheticWannier"]
+    N = int(g["Nband"])
+    g["R"] = list(g["R"]) + [int(x) for r in extra for x in r]
+    g["h_re"] = list(g["h_re"]) + [0.0] * (len(extra) * N * N)
+    g["h_im"] = list(g["h_im"]) + [0.0] * (len(extra) * N * N)
+    g["d_re"] = list(g["d_re"]) + [0.0] * (len(extra) * 2 * N * N)
+    g["d_im"] = list(g["d_im"]) + [0.0] * (len(extra) * 2 * N * N)
+    return c
+
+
+@pytest.mark.parametrize("extra", [[(5, 1), (-5, -1)], [(5, 1), (6, -2)]])
+def test_lattice_vector_pairing_and_fallback(extra):
+    """The grouped kernel sums the Fourier series over pairs (R, -R) that
+    the host finds in the model's vectors; a model whose vectors do not pair
+    up (more than R = 0 alone) runs on the general attempt kernel instead.
+    Zero-table vectors leave the model unchanged: with an added pair the
+    grouped kernel runs, with two unpaired vectors the fallback, and both
+    match the oracle on the same model to the FP64 bar."""
+    c = with_zero_vectors(small_case("cashkarp45", tol=1e-8), extra)
+    out = ab.solve(c, precision="fp64")
+    check(out, pyoracle.run(c), FP64_TOL)
