@@ -123,8 +123,9 @@ WannierSolve::WannierSolve(const Problem &p, int precision, int device, cudaStre
                 }
             gpair.push_back(r);
         }
-        // more vectors without their negatives than R = 0: the grouped
-        // kernel's per-k phase arrays are sized for pairs, wan_attempt runs it
+        // more vectors without their negatives than R = 0 (the SyntheticWannier
+        // reader already refuses such a model): the grouped kernel's per-k
+        // phase arrays are sized for pairs, so wan_attempt would run it
         if ((int)gpair.size() > wan_npair_cap(nR)) gpair.clear();
     }
     if (!gpair.empty()) {

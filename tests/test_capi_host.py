@@ -212,3 +212,20 @@ def test_snapshot_writer_formats(tmp_path):
     assert np.array_equal(np.fromfile(tmp_path / "fisrt_conduction.dat"), ref["nc"])
     assert np.array_equal(np.fromfile(tmp_path / "fisrt_coherence.dat", dtype=np.complex128), ref["pi"])
     assert (tmp_path / "snapshot_log.dat").read_bytes() == b""
+
+
+def test_synthetic_wannier_vectors_must_pair():
+    """A SyntheticWannier model must list -R for every R (H(k) is Hermitian
+    only then); the reader refuses one that does not, so the grouped N-band
+    kernel's sums over pairs (R, -R) always find their pairs."""
+    from antelope_b200 import wannier
+
+    c = wannier.wannier_case(seed=4, n=6, ncycles=1.0)
+    g = c["SyntheticWannier"]
+    N = int(g["Nband"])
+    g["R"] = list(g["R"]) + [5, 1]
+    for key, m in (("h_re", 1), ("h_im", 1), ("d_re", 2), ("d_im", 2)):
+        g[key] = list(g[key]) + [0.0] * (m * N * N)
+    with pytest.raises(SbeError) as e:
+        Problem.from_dict(c)
+    assert e.value.name == "SBE_BAD_CONFIG" and "-R for every R" in str(e.value)
