@@ -3,22 +3,25 @@
 //
 // The same step as wan_attempt -- SBEs::GenDifferentialDM (SBEs.h:762-872)
 // with the Wannier model form (Materials/Wannier90.h:297-387), the currents
-// of SBEs::GenInterIntraCurrent (SBEs.h:694-760), Jacobi tracking of the
-// eigenbasis and the eigenbasis dephasing -- laid out for throughput:
+// of SBEs::GenInterIntraCurrent (SBEs.h:694-760), tracking of the eigenbasis
+// and the eigenbasis dephasing -- laid out for throughput:
 //
 //  - eight lanes per k-point, four k-points per warp (one warp is one tile of
 //    WAN_WARPS k-points, so the controller's tile reduction is unchanged);
 //    the four groups of a warp run in lockstep, so every Fourier-table load is
 //    one 128-byte row shared by the four k-points;
-//  - the tables are re-laid per lane ([R][j][q][lane], built on the host,
-//    WanDev::gtab): lane l of a group owns the upper elements u = l + 8j and
-//    computes H0, D_x, D_y (and, for the currents, S_a = sum R_a h_R e^{iKR})
-//    for exactly those, so the right-hand side and the current traces of an
-//    owned element need no other lane's Fourier sums;
+//  - the tables are re-laid per lane and per lattice-vector pair (R, -R)
+//    ([pair][j][q][sigma|tau][lane], built on the host, WanDev::gtab): lane l
+//    of a group owns the upper elements u = l + 8j and computes H0, E.D (or
+//    D_x, D_y at output steps, and S_a = sum R_a h_R e^{iKR}) for exactly
+//    those, with one phase and half the multiply-adds per pair;
+//  - the matrix products (B = U^dag H0 U, the tracking steps, dv, the
+//    commutators, the dephasing) are formed one row per lane, the second
+//    factor read by element at an address shared by the group's lanes;
 //  - Hermitian matrices (Y, H0, H0 + E.D, B = U^dag H0 U) are stored as packed
-//    upper triangles, the unitary U and one scratch matrix in full: ~4 KB of
-//    shared memory per k-point instead of ~9 KB, so more k-points stay
-//    resident and the tables stay in L1;
+//    upper triangles, the unitary U and one scratch matrix in full: ~3.6 KB
+//    of shared memory per k-point, so 3 blocks fit with 60 KB of L1 left for
+//    the tables;
 //  - the stage slopes live in registers and the stage loop is unrolled for the
 //    compile-time tableau, so only the slopes still needed are live.
 //
@@ -85,8 +88,8 @@ __device__ __forceinline__ double grp_max(double v)
     return v;
 }
 
-// Shared memory: block head, stage phase factors e^{iA(t_s)R} and lattice
-// vectors, then one region per k-point.
+// Shared memory: block head, stage phase factors e^{iA(t_s)R} and the
+// pairs' lattice vectors, then one region per k-point.
 struct GHead {
     double AE[6][6];
     double part[WG_WARPS][WAN_WARPS][WAN_NSLOT];
@@ -520,8 +523,8 @@ __device__ __forceinline__ int g_pstep(const GView<RF> &w, const GHead &gh, int 
 }
 
 // Eigenbasis tracking by perturbative steps (g_pstep) while B = U^dag H0 U is
-// not diagonal to tol2: a fourth-order step forms B again and repeats, a
-// second-order step finishes; groups whose rotation is not small (near-
+// not diagonal to tol2: a larger step forms B again and repeats, a finishing
+// step ends it; groups whose rotation is not small (near-
 // degenerate bands) or that are not done after three rounds fall back on
 // Jacobi sweeps (g_track), which end in the same tolerances.
 template <class RF, int N>
